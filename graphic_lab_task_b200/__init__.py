@@ -1,0 +1,6 @@
+"""B200-native LiteRT ray query (BVHRT::RayQuery_NearestHit) behind the CrossRT
+ISceneObject API.  The compute path is liblrt_b200.so (sm_100a CUDA); this
+package only binds it (lrt.py), mirrors its C structs (_abi.py), builds it
+(build.py) and generates benchmark workloads (workloads.py)."""
+from ._abi import HIT_DTYPE, Camera, Preset, default_preset, parity_preset  # noqa: F401
+from .lrt import LrtError, SceneRT, lib  # noqa: F401

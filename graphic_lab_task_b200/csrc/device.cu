@@ -1,0 +1,315 @@
+// device.cu — device half of the scene object: upload of the reference arrays
+// plus the derived layouts, and the ray-query entry points of the C-ABI.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "layout.h"
+#include "scene.h"
+#include "trace_api.h"
+
+namespace lrt {
+
+// Per-stream launch state: the persistent grid's ray counter, the error word
+// and the work counters.  One slot per stream keeps concurrent traces of one
+// scene on different streams independent.
+struct StreamSlot {
+  unsigned long long work;
+  unsigned long long counters[LRT_COUNTER_COUNT];
+  uint32_t err;
+  uint32_t _pad[5];
+};
+constexpr int kMaxStreams = 64;
+
+struct DeviceScene {
+  std::vector<void*> allocs;
+  DevScene S{};
+  uint32_t stackCap = 0;
+  int grid = 0;
+  StreamSlot* slots = nullptr; // device, kMaxStreams
+  std::map<cudaStream_t, int> slotOf;
+  // staging buffers for host-pointer calls
+  float4* rays = nullptr;
+  lrt_hit* hits = nullptr;
+  uint64_t cap = 0;
+  ~DeviceScene()
+  {
+    for (void* p : allocs) cudaFree(p);
+    if (rays) cudaFree(rays);
+    if (hits) cudaFree(hits);
+  }
+};
+
+namespace {
+
+lrt_status cuda_fail(lrt_scene* s, cudaError_t e, const char* what)
+{
+  return fail(s, e == cudaErrorMemoryAllocation ? LRT_ERR_OUT_OF_MEMORY : LRT_ERR_CUDA, "%s: %s", what,
+              cudaGetErrorString(e));
+}
+
+template <class T>
+lrt_status upload_vec(lrt_scene* s, DeviceScene* d, const T* src, size_t count, const T** out, const char* name)
+{
+  *out = nullptr;
+  if (count == 0) return LRT_OK;
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+  if (e != cudaSuccess) return cuda_fail(s, e, name);
+  d->allocs.push_back(p);
+  e = cudaMemcpy(p, src, count * sizeof(T), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(s, e, name);
+  *out = static_cast<const T*>(p);
+  return LRT_OK;
+}
+
+uint32_t preset_flags(const lrt_preset& p)
+{
+  const uint32_t m = p.render_mode; // need_normal(), BVH2Common.cpp:19-32
+  const bool nn = m == 1 || m == 8 || m == 12 || m == 17 || m == 20 || m == 7 || m == 18 || m == 23 || m == 21 ||
+                  m == 11 || m == 27;
+  uint32_t f = 0;
+  if (nn) f |= kFlagNeedNormal;
+  if (m == LRT_RENDER_MODE_ST_ITERATIONS) f |= kFlagStIterations;
+  if (p.representation_mode == 0) f |= kFlagSurfaceMode;
+  if (p.sdf_node_intersect == 3) f |= kFlagBBoxMode;
+  return f;
+}
+
+lrt_status slot_for(lrt_scene* s, cudaStream_t stream, StreamSlot** out)
+{
+  DeviceScene* d = s->dev;
+  auto it = d->slotOf.find(stream);
+  int idx;
+  if (it == d->slotOf.end()) {
+    if (int(d->slotOf.size()) >= kMaxStreams)
+      return fail(s, LRT_ERR_INVALID_ARGUMENT, "more than %d streams used with one scene", kMaxStreams);
+    idx = int(d->slotOf.size());
+    d->slotOf[stream] = idx;
+  } else {
+    idx = it->second;
+  }
+  *out = d->slots + idx;
+  return LRT_OK;
+}
+
+lrt_status launch(lrt_scene* s, const float4* rays, lrt_hit* hits, uint64_t n, cudaStream_t stream, uint32_t flags,
+                  StreamSlot* slot)
+{
+  DeviceScene* d = s->dev;
+  DevScene S = d->S;
+  S.flags = preset_flags(s->preset);
+  const bool count = (flags & LRT_TRACE_COUNT_WORK) != 0;
+  cudaError_t e = cudaMemsetAsync(&slot->work, 0, count ? offsetof(StreamSlot, err) : sizeof(unsigned long long),
+                                  stream);
+  if (e != cudaSuccess) return cuda_fail(s, e, "cudaMemsetAsync");
+  const uint64_t warps = (n + 31) / 32;
+  const int grid = int(std::min<uint64_t>(uint64_t(d->grid), (warps * 32 + kTraceThreads - 1) / kTraceThreads));
+  if (flags & LRT_TRACE_FAST_MATH)
+    e = lrt_fast::launch_trace(S, rays, hits, n, &slot->work, slot->counters, &slot->err, d->stackCap, grid, stream,
+                               count);
+  else
+    e = lrt_exact::launch_trace(S, rays, hits, n, &slot->work, slot->counters, &slot->err, d->stackCap, grid,
+                                stream, count);
+  if (e != cudaSuccess) return cuda_fail(s, e, "trace launch");
+  return LRT_OK;
+}
+
+// Reads back (and clears) the error word and, if asked, the counters of a slot.
+lrt_status finish(lrt_scene* s, cudaStream_t stream, StreamSlot* slot, bool count)
+{
+  StreamSlot hs;
+  cudaError_t e = cudaMemcpyAsync(&hs, slot, sizeof(hs), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return cuda_fail(s, e, "trace");
+  if (count)
+    for (int k = 0; k < LRT_COUNTER_COUNT; k++) s->counters[k] = hs.counters[k];
+  if (hs.err) {
+    cudaMemsetAsync(&slot->err, 0, sizeof(uint32_t), stream);
+    cudaStreamSynchronize(stream);
+    return fail(s, LRT_ERR_DEVICE_LIMIT, "trace hit a bounded-loop limit (error bits 0x%x: 1 = stack, 2 = voxel march)",
+                hs.err);
+  }
+  return LRT_OK;
+}
+
+} // namespace
+
+lrt_status device_upload(lrt_scene* s)
+{
+  device_release(s);
+  cudaError_t e = cudaGetDevice(&s->device);
+  if (e != cudaSuccess) return cuda_fail(s, e, "cudaGetDevice (no CUDA device?)");
+  DeviceScene* d = new DeviceScene();
+  s->dev = d;
+  const HostArrays& h = s->h;
+  DevScene& S = d->S;
+  std::vector<DevGeom> geoms;
+  std::vector<float> soup, dense;
+  std::vector<DevSbs> sbs;
+  build_geoms(h, geoms);
+  build_tri_soup(h, soup);
+  build_sbs_dense(h, sbs, dense);
+  lrt_status st = LRT_OK;
+#define UP(dst, vec, T, name)                                                                        \
+  if (st == LRT_OK) {                                                                                 \
+    const T* p = nullptr;                                                                             \
+    st = upload_vec(s, d, reinterpret_cast<const T*>(vec.data()), vec.size() * sizeof(vec[0]) / sizeof(T), &p, name); \
+    S.dst = p;                                                                                        \
+  }
+  UP(tlas, h.nodesTLAS, lrt_bvh_node, "TLAS nodes")
+  UP(pairs, h.allNodePairs, lrt_bvh_node_pair, "BLAS node pairs")
+  UP(instances, h.instanceData, DevInstance, "instances")
+  UP(geoms, geoms, DevGeom, "geometry table")
+  UP(primIdCount, h.primIdCount, uint32_t, "leaf table")
+  UP(triSoup, soup, float4, "triangles")
+  UP(primIndices, h.primIndices, uint32_t, "primIndices")
+  UP(origNodes, h.origNodes, lrt_bvh_node, "origNodes")
+  UP(frameOctreeNodes, h.sdfFrameOctreeNodes, lrt_sdf_frame_octree_node, "frame-octree nodes")
+  UP(svsNodes, h.sdfSVSNodes, lrt_sdf_svs_node, "SVS nodes")
+  UP(sbsNodes, h.sdfSBSNodes, lrt_sdf_sbs_node, "SBS nodes")
+  UP(sbsData, h.sdfSBSData, uint32_t, "SBS data")
+  UP(sbsDataF, h.sdfSBSDataF, float, "SBS float data")
+  UP(sbsDense, dense, float, "SBS dense bricks")
+  UP(sbs, sbs, DevSbs, "SBS table")
+#undef UP
+  if (st != LRT_OK) {
+    device_release(s);
+    return st;
+  }
+  d->stackCap = std::max<uint32_t>(s->info.maxBlasDepth + 1, 8u);
+  // The dynamic shared-memory limit is a per-kernel attribute shared by all
+  // scenes: raise it once to the largest stack any scene may use.
+  e = lrt_exact::set_trace_smem(kMaxStack + 1);
+  if (e == cudaSuccess) e = lrt_fast::set_trace_smem(kMaxStack + 1);
+  int perSm = 0, sms = 0;
+  if (e == cudaSuccess) e = lrt_exact::trace_occupancy(d->stackCap, &perSm);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+  if (e == cudaSuccess) e = cudaMalloc(&d->slots, sizeof(StreamSlot) * kMaxStreams);
+  if (e == cudaSuccess) {
+    d->allocs.push_back(d->slots);
+    e = cudaMemset(d->slots, 0, sizeof(StreamSlot) * kMaxStreams);
+  }
+  if (e != cudaSuccess) {
+    st = cuda_fail(s, e, "trace setup");
+    device_release(s);
+    return st;
+  }
+  d->grid = std::max(1, perSm) * sms;
+  return LRT_OK;
+}
+
+void device_release(lrt_scene* s)
+{
+  if (s->dev) {
+    delete s->dev;
+    s->dev = nullptr;
+  }
+}
+
+} // namespace lrt
+
+using namespace lrt;
+
+extern "C" {
+
+lrt_status lrt_trace_nearest(lrt_scene* s, const float* rays, lrt_hit* hits, uint64_t n, void* stream_p,
+                             uint32_t flags)
+{
+  if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  if (!s->committed || !s->dev) return fail(s, LRT_ERR_NOT_COMMITTED, "trace before CommitScene/upload");
+  if (n == 0) return LRT_OK;
+  if (!rays || !hits) return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_trace_nearest: NULL rays or hits");
+  lrt_status st = check_preset(s);
+  if (st != LRT_OK) return st;
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_p);
+  StreamSlot* slot = nullptr;
+  st = slot_for(s, stream, &slot);
+  if (st != LRT_OK) return st;
+  DeviceScene* d = s->dev;
+  if (flags & LRT_TRACE_DEVICE_POINTERS) {
+    if ((reinterpret_cast<uintptr_t>(rays) | reinterpret_cast<uintptr_t>(hits)) & 15)
+      return fail(s, LRT_ERR_INVALID_ARGUMENT, "device rays/hits must be 16-byte aligned");
+    return launch(s, reinterpret_cast<const float4*>(rays), hits, n, stream, flags, slot);
+  }
+  if (n > d->cap) {
+    if (d->rays) cudaFree(d->rays);
+    if (d->hits) cudaFree(d->hits);
+    d->rays = nullptr;
+    d->hits = nullptr;
+    d->cap = 0;
+    cudaError_t e = cudaMalloc(&d->rays, n * 32);
+    if (e == cudaSuccess) e = cudaMalloc(&d->hits, n * sizeof(lrt_hit));
+    if (e != cudaSuccess) return cuda_fail(s, e, "staging buffers");
+    d->cap = n;
+  }
+  cudaError_t e = cudaMemcpyAsync(d->rays, rays, n * 32, cudaMemcpyHostToDevice, stream);
+  if (e != cudaSuccess) return cuda_fail(s, e, "rays host->device");
+  st = launch(s, d->rays, d->hits, n, stream, flags, slot);
+  if (st != LRT_OK) return st;
+  e = cudaMemcpyAsync(hits, d->hits, n * sizeof(lrt_hit), cudaMemcpyDeviceToHost, stream);
+  if (e != cudaSuccess) return cuda_fail(s, e, "hits device->host");
+  return finish(s, stream, slot, (flags & LRT_TRACE_COUNT_WORK) != 0);
+}
+
+// Waits for the stream's traces and reports a bounded-loop limit hit by any of
+// them (device-pointer traces are asynchronous).
+lrt_status lrt_trace_sync(lrt_scene* s, void* stream_p, int32_t read_counters)
+{
+  if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  if (!s->dev) return fail(s, LRT_ERR_NOT_COMMITTED, "no device scene");
+  StreamSlot* slot = nullptr;
+  lrt_status st = slot_for(s, static_cast<cudaStream_t>(stream_p), &slot);
+  if (st != LRT_OK) return st;
+  return finish(s, static_cast<cudaStream_t>(stream_p), slot, read_counters != 0);
+}
+
+lrt_status lrt_ray_query_nearest_hit(lrt_scene* s, const float pn[4], const float df[4], lrt_hit* out)
+{
+  if (!s || !pn || !df || !out) return fail(s, LRT_ERR_INVALID_ARGUMENT, "RayQuery_NearestHit: NULL argument");
+  float ray[8];
+  std::memcpy(ray, pn, 16);
+  std::memcpy(ray + 4, df, 16);
+  return lrt_trace_nearest(s, ray, out, 1, nullptr, 0);
+}
+
+lrt_status lrt_ray_query_any_hit(lrt_scene* s, const float pn[4], const float df[4], int32_t* out)
+{
+  if (!s || !pn || !df || !out) return fail(s, LRT_ERR_INVALID_ARGUMENT, "RayQuery_AnyHit: NULL argument");
+  // BVH2Common.cpp:3394-3399: negate tfar to request stop-on-first-hit
+  float d2[4] = {df[0], df[1], df[2], -df[3]};
+  lrt_hit h;
+  lrt_status st = lrt_ray_query_nearest_hit(s, pn, d2, &h);
+  if (st != LRT_OK) return st;
+  *out = h.geomId != 0xFFFFFFFFu;
+  return LRT_OK;
+}
+
+lrt_status lrt_get_work_counters(lrt_scene* s, uint64_t counters[LRT_COUNTER_COUNT])
+{
+  if (!s || !counters) return LRT_ERR_INVALID_ARGUMENT;
+  std::memcpy(counters, s->counters, sizeof(s->counters));
+  return LRT_OK;
+}
+
+lrt_status lrt_generate_eye_rays(lrt_scene* s, const lrt_camera* cam, float* rays_dev, void* stream)
+{
+  if (!cam || !rays_dev) return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_generate_eye_rays: NULL argument");
+  if (reinterpret_cast<uintptr_t>(rays_dev) & 15)
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "rays must be 16-byte aligned");
+  DevCamera c;
+  std::memcpy(c.proj_inv, cam->proj_inv, sizeof(c.proj_inv));
+  std::memcpy(c.world_view_inv, cam->world_view_inv, sizeof(c.world_view_inv));
+  c.width = cam->width;
+  c.height = cam->height;
+  c.tnear = cam->tnear;
+  c.tfar = cam->tfar;
+  cudaError_t e = lrt_exact::launch_eye_rays(c, reinterpret_cast<float4*>(rays_dev), static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return s ? cuda_fail(s, e, "eye rays") : LRT_ERR_CUDA;
+  return LRT_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,106 @@
+// device_layout.h — what the trace kernels read from HBM.
+//
+// The reference arrays are uploaded as-is where the kernels read them
+// directly (TLAS nodes, BLAS node pairs, instances, leaf table, primIndices,
+// SDF nodes, SBS data for hit colours).  Three derived layouts are built at
+// upload for the B200 memory system:
+//   * triSoup   — per reordered triangle {A, B-A, C-A} as 3 float4 (48 B, one
+//                 128-B line per 2.7 triangles) instead of 3 index loads and 3
+//                 dependent vertex gathers (BVH2Common.cpp:1580-1589);
+//   * sbsDense  — every SBS brick resolved to a dense (brick_size+1)^3 fp32
+//                 corner grid (2.9 KB for 8^3 bricks), so a voxel visit is 8
+//                 loads from 4 adjacent 8-byte pairs instead of 8 index loads
+//                 followed by 8 dependent value loads (BVH2Common.cpp:846-882);
+//   * geoms     — 32 B per geometry with the tag, BLAS offset, leaf-table base
+//                 and SDF ids the traversal needs (one load per BLAS entry).
+// Values are copied bit for bit, so results do not depend on the layout.
+#pragma once
+#include <stdint.h>
+#include <vector_types.h>
+
+#include "../../include/lrt_b200.h"
+
+namespace lrt {
+
+constexpr int kTraceThreads = 128;
+constexpr uint32_t kLeafBit = 0x80000000u;
+constexpr uint32_t kMaxVoxelSteps = 4096u; // voxel-march cap per brick (the reference loop is unbounded)
+
+// preset-derived flags
+constexpr uint32_t kFlagNeedNormal = 1u;
+constexpr uint32_t kFlagStIterations = 2u;
+constexpr uint32_t kFlagSurfaceMode = 4u; // REPRESENTATION_MODE_SURFACE
+constexpr uint32_t kFlagBBoxMode = 8u;    // SDF_OCTREE_NODE_INTERSECT_BBOX
+
+// error bits of the per-launch error word
+constexpr uint32_t kErrStackOverflow = 1u;
+constexpr uint32_t kErrVoxelCap = 2u;
+
+// work counters (same order as LRT_COUNTER_COUNT in lrt_b200.h)
+enum : int {
+  kCntTlasNodes = 0,
+  kCntInstances,
+  kCntBlasPairs,
+  kCntLeafCalls,
+  kCntTriTests,
+  kCntBricks,
+  kCntVoxels,
+  kCntStSteps,
+  kCntOctreeLeaves,
+  kCntSvsLeaves,
+  kCntHits,
+  kCntNormals
+};
+
+struct DevGeom {
+  uint32_t tag;       // TAG_* (m_geomTags)
+  uint32_t type;      // TYPE_* (GeomData.type)
+  uint32_t bvhOffset; // first node pair of the BLAS
+  uint32_t aabbBase;  // startEnd.x: base of this geometry's leaf table
+  uint32_t triBase;   // triangles: GeomData.offset.x / 3
+  uint32_t sdfId;     // SDF: GeomData.offset.x (index into roots/headers)
+  uint32_t sdfRoot;   // SDF: root node index of this model
+  uint32_t _pad;
+};
+static_assert(sizeof(DevGeom) == 32, "DevGeom is 32 bytes");
+
+struct DevSbs {
+  uint64_t denseBase;   // first float of node `root` in sbsDense
+  uint32_t denseStride; // (brick_size+1)^3
+  uint32_t brick_size;
+  uint32_t v3;          // (brick_size + 2*pad + 1)^3
+  uint32_t colorLayout; // 1 for the indexed ID32F layouts (hit colour from sbsDataF)
+  uint32_t nodeCount;   // nodes of this model (leaves naming a node past it are skipped)
+  uint32_t _pad;
+};
+
+typedef lrt_instance_data DevInstance;
+
+struct DevScene {
+  const lrt_bvh_node* tlas;
+  const lrt_bvh_node_pair* pairs;
+  const DevInstance* instances;
+  const DevGeom* geoms;
+  const uint32_t* primIdCount;
+  const float4* triSoup;
+  const uint32_t* primIndices;
+  const lrt_bvh_node* origNodes;
+  const lrt_sdf_frame_octree_node* frameOctreeNodes;
+  const lrt_sdf_svs_node* svsNodes;
+  const lrt_sdf_sbs_node* sbsNodes;
+  const uint32_t* sbsData;
+  const float* sbsDataF;
+  const float* sbsDense;
+  const DevSbs* sbs;
+  uint32_t flags;
+  uint32_t numRays; // unused by the trace kernel; kept for diagnostics
+};
+
+struct DevCamera {
+  float proj_inv[16];
+  float world_view_inv[16];
+  uint32_t width, height;
+  float tnear, tfar;
+};
+
+} // namespace lrt

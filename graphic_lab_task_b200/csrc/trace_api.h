@@ -1,0 +1,18 @@
+// trace_api.h — host launchers exported by trace_exact.cu and trace_fast.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "device_layout.h"
+
+#define LRT_DECLARE_TRACE_API(NS)                                                                               \
+  namespace NS {                                                                                                \
+  cudaError_t launch_trace(const lrt::DevScene& S, const float4* rays, lrt_hit* hits, uint64_t n,               \
+                           unsigned long long* work_counter, unsigned long long* counters, uint32_t* err_word,  \
+                           uint32_t stack_cap, int grid, cudaStream_t stream, bool count);                      \
+  cudaError_t set_trace_smem(uint32_t stack_cap);                                                               \
+  cudaError_t trace_occupancy(uint32_t stack_cap, int* blocks_per_sm);                                          \
+  cudaError_t launch_eye_rays(const lrt::DevCamera& cam, float4* rays, cudaStream_t stream);                    \
+  }
+
+LRT_DECLARE_TRACE_API(lrt_exact)
+LRT_DECLARE_TRACE_API(lrt_fast)

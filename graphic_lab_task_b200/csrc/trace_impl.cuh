@@ -1,0 +1,497 @@
+// trace_impl.cuh — sm_100a nearest-hit traversal (BVHRT::RayQuery_NearestHit).
+//
+// Included by trace_exact.cu (-fmad=false: bit-identical to the reference CPU
+// build with -ffp-contract=off) and trace_fast.cu (FMA contraction on).  Each
+// includer defines LRT_NS to put its copy of the kernels in its own namespace.
+//
+// Structure follows the reference path function by function:
+//   trace_one        RayQuery_NearestHit        MultiRenderer/BVH2Common.cpp:3322-3392
+//   blas             BVH2TraverseF32            :3239-3320
+//   leaf             IntersectAllPrimitivesInLeaf :47-124
+//   triangles        IntersectAllTrianglesInLeaf  :1571-1635
+//   octree_node      OctreeNodeIntersect + RayNodeIntersection :727-749, 141-218
+//   octree_brick     OctreeBrickIntersect + load_distance_values :884-1112, 846-882
+//   local_surface    LocalSurfaceIntersection (ST/BBOX) :345-391, 618-690
+// The device reads B200-specific layouts built at upload (device_layout.h):
+// pre-gathered triangles (vertex A + two edges, 48 B), bricks resolved to
+// dense (brick_size+1)^3 fp32 corner grids, and a 32-B per-geometry table.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device_layout.h"
+#include "lrt_math.h"
+
+namespace LRT_NS {
+using namespace lrt;
+
+struct Counters {
+  uint32_t c[LRT_COUNTER_COUNT];
+};
+
+template <bool COUNT>
+struct Ctx {
+  const DevScene& S;
+  Counters cnt;
+  uint32_t err;
+  __device__ explicit Ctx(const DevScene& s) : S(s), err(0)
+  {
+#pragma unroll
+    for (int i = 0; i < LRT_COUNTER_COUNT; i++) cnt.c[i] = 0;
+  }
+  __device__ __forceinline__ void inc(int k, uint32_t v = 1)
+  {
+    if (COUNT) cnt.c[k] += v;
+  }
+};
+
+__device__ __forceinline__ f3 ld3(const float4 v) { return mk3(v.x, v.y, v.z); }
+
+template <bool COUNT>
+__device__ void local_surface(Ctx<COUNT>& c, uint32_t type, f3 ray_dir, uint32_t instId, uint32_t geomId,
+                              const float* values, uint32_t primId, float d, float qNear, float qFar, f2 fNearFar,
+                              f3 start_q, lrt_hit& hit)
+{
+  const DevScene& S = c.S;
+  const float EPS = 1e-6f;
+  const float d_inv = 1.0f / d;
+  float t = qNear;
+  bool early_hit = false, hitf = false;
+  unsigned iter = 0;
+  float start_sign = 1;
+  float start_dist = trilinear(values, start_q + t * ray_dir);
+  c.inc(kCntStSteps);
+  if (S.flags & kFlagSurfaceMode) start_sign = ssign(start_dist);
+  start_dist *= start_sign;
+  if (start_dist <= EPS || (S.flags & kFlagBBoxMode)) {
+    early_hit = true;
+    hitf = true;
+  } else {
+    float dist = start_dist;
+    while (t < qFar && dist > EPS && iter < 256) {
+      t += dist * d_inv;
+      dist = start_sign * trilinear(values, start_q + t * ray_dir);
+      iter++;
+    }
+    c.inc(kCntStSteps, iter);
+    hitf = (dist <= EPS);
+  }
+  const float tReal = fNearFar.x + d * t;
+  if (t <= qFar && hitf && tReal < hit.t) {
+    f3 norm = mk3(0, 0, 1);
+    if (S.flags & kFlagNeedNormal) {
+      if (early_hit && (S.flags & kFlagBBoxMode)) {
+        const float q[3] = {start_q.x, start_q.y, start_q.z};
+        const f3 v = mk3(smax(start_q.x, 1 - start_q.x), smax(start_q.y, 1 - start_q.y), smax(start_q.z, 1 - start_q.z));
+        int dim = 0;
+        if (v.y > v.x && v.y > v.z) dim = 1;
+        else if (v.z > v.x && v.z > v.y) dim = 2;
+        float nn[3] = {0, 0, 0};
+        nn[dim] = q[dim] < 0.5f ? -1.0f : 1.0f;
+        norm = mk3(nn[0], nn[1], nn[2]);
+      } else {
+        const f3 p0 = start_q + t * ray_dir;
+        const float h = 0.001f;
+        const float ddx =
+            (trilinear(values, p0 + mk3(h, 0, 0)) - trilinear(values, p0 + mk3(-h, 0, 0))) / (2 * h);
+        const float ddy =
+            (trilinear(values, p0 + mk3(0, h, 0)) - trilinear(values, p0 + mk3(0, -h, 0))) / (2 * h);
+        const float ddz =
+            (trilinear(values, p0 + mk3(0, 0, h)) - trilinear(values, p0 + mk3(0, 0, -h))) / (2 * h);
+        norm = start_sign * mk3(ddx, ddy, ddz);
+      }
+      norm = normalize(matmul4(S.instances[instId].transformInvTransposed, norm, 1.0f));
+      c.inc(kCntNormals);
+    }
+    const f2 en = encode_normal(norm);
+    hit.t = tReal;
+    hit.primId = (S.flags & kFlagStIterations) ? iter : primId;
+    hit.instId = instId;
+    hit.geomId = geomId | (type << 24);
+    hit.coords[0] = 0;
+    hit.coords[1] = 0;
+    hit.coords[2] = en.x;
+    hit.coords[3] = en.y;
+  }
+}
+
+template <bool COUNT>
+__device__ void octree_node(Ctx<COUNT>& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, float tNear, uint32_t instId,
+                            uint32_t geomId, uint32_t bvhNodeId, lrt_hit& hit)
+{
+  const DevScene& S = c.S;
+  float values[8];
+  uint32_t primId;
+  f3 min_pos, max_pos;
+  if (g.type == LRT_TYPE_SDF_FRAME_OCTREE) {
+    c.inc(kCntOctreeLeaves);
+    // origNodes box (32 B) + the node's 8 corner values
+    const float4* on = reinterpret_cast<const float4*>(S.origNodes + bvhNodeId);
+    const float4 a = __ldg(on), b = __ldg(on + 1);
+    primId = __float_as_uint(a.w);
+    const uint64_t nodeId = uint64_t(primId) + g.sdfRoot;
+    min_pos = ld3(a);
+    max_pos = ld3(b);
+    const float* vals = S.frameOctreeNodes[nodeId].values;
+#pragma unroll
+    for (int i = 0; i < 8; i++) values[i] = __ldg(vals + i);
+  } else {
+    c.inc(kCntSvsLeaves);
+    primId = bvhNodeId;
+    const uint4 n = __ldg(reinterpret_cast<const uint4*>(S.svsNodes) + (uint64_t(primId) + g.sdfRoot));
+    const float px = float(n.x >> 16), py = float(n.x & 0x0000FFFF);
+    const float pz = float(n.y >> 16), sz = float(n.y & 0x0000FFFF);
+    const float d_max = 2 * 1.73205081f / sz;
+    min_pos = mk3(-1, -1, -1) + (2.0f * mk3(px, py, pz)) / sz;
+    max_pos = min_pos + (2.0f * mk3(1, 1, 1)) / sz;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const uint32_t w = (i < 4) ? n.z : n.w;
+      values[i] = -d_max + 2.0f * d_max * (1.0f / 255.0f) * ((w >> (8 * (i % 4))) & 0xFF);
+    }
+  }
+  const f3 size = max_pos - min_pos;
+  const f2 fNearFar = ray_box(ray_pos, safe_inverse(ray_dir), min_pos, max_pos);
+  const f3 start_pos = ray_pos + fNearFar.x * ray_dir;
+  const float d = smax(size.x, smax(size.y, size.z));
+  const f3 start_q = (start_pos - min_pos) / d;
+  const float qFar = (fNearFar.y - fNearFar.x) / d;
+  const float qNear = tNear > fNearFar.x ? (tNear - fNearFar.x) / d : 0.0f;
+  if (qNear > 0.0f) return; // ray starts inside this node (BVH2Common.cpp:744-745)
+  local_surface(c, g.type, ray_dir, instId, geomId, values, primId, d, qNear, qFar, fNearFar, start_q, hit);
+}
+
+template <bool COUNT>
+__device__ void octree_brick(Ctx<COUNT>& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, float tNear, uint32_t instId,
+                             uint32_t geomId, uint32_t bvhNodeId, lrt_hit& hit)
+{
+  const DevScene& S = c.S;
+  const DevSbs& sb = S.sbs[g.sdfId];
+  const uint32_t primId = bvhNodeId;
+  const uint32_t nodeId = primId + g.sdfRoot;
+  c.inc(kCntBricks);
+  if (primId >= sb.nodeCount) return; // padding box of a one-brick model
+  const uint4 node = __ldg(reinterpret_cast<const uint4*>(S.sbsNodes) + nodeId);
+  const float px = float(node.x >> 16), py = float(node.x & 0x0000FFFF);
+  const float pz = float(node.y >> 16), sz = float(node.y & 0x0000FFFF);
+  const uint32_t bs = sb.brick_size;
+  const float sz_inv = 2.0f / sz;
+  const float d = 2.0f / (sz * bs);
+  const f3 brick_min_pos = mk3(-1, -1, -1) + sz_inv * mk3(px, py, pz);
+  const f3 brick_max_pos = brick_min_pos + sz_inv * mk3(1, 1, 1);
+  const f3 inv_dir = safe_inverse(ray_dir);
+  f2 bnf = ray_box(ray_pos, inv_dir, brick_min_pos, brick_max_pos);
+  const float old_t = hit.t;
+  const float scale = 0.5f * sz * bs;
+  const float hiClamp = bs - 1e-6f;
+  const uint32_t V1 = bs + 1;
+  const float* dense = S.sbsDense + sb.denseBase + uint64_t(primId) * sb.denseStride;
+  float values[8];
+  uint32_t steps = 0;
+  while (bnf.x < bnf.y && hit.t == old_t) {
+    if (steps++ >= kMaxVoxelSteps) {
+      c.err |= kErrVoxelCap;
+      break;
+    }
+    c.inc(kCntVoxels);
+    const f3 hit_pos = ray_pos + bnf.x * ray_dir;
+    const f3 local_pos = (hit_pos - brick_min_pos) * scale;
+    const f3 voxelPos = mk3(floorf(sclamp(local_pos.x, 1e-6f, hiClamp)), floorf(sclamp(local_pos.y, 1e-6f, hiClamp)),
+                            floorf(sclamp(local_pos.z, 1e-6f, hiClamp)));
+    const f3 min_pos = brick_min_pos + d * voxelPos;
+    const f3 max_pos = min_pos + d * mk3(1, 1, 1);
+    // 8 corners of the voxel from the dense (bs+1)^3 grid, x-major
+    const uint32_t vx = uint32_t(voxelPos.x), vy = uint32_t(voxelPos.y), vz = uint32_t(voxelPos.z);
+    const float* base = dense + (vx * V1 + vy) * V1 + vz;
+    values[0] = __ldg(base);
+    values[1] = __ldg(base + 1);
+    values[2] = __ldg(base + V1);
+    values[3] = __ldg(base + V1 + 1);
+    values[4] = __ldg(base + V1 * V1);
+    values[5] = __ldg(base + V1 * V1 + 1);
+    values[6] = __ldg(base + V1 * V1 + V1);
+    values[7] = __ldg(base + V1 * V1 + V1 + 1);
+    float vmin = 1e6f;
+#pragma unroll
+    for (int i = 0; i < 8; i++) vmin = smin(vmin, values[i]);
+    const f2 fNearFar = ray_box(ray_pos, inv_dir, min_pos, max_pos);
+    if (tNear < fNearFar.x && vmin <= 0.0f) {
+      const f3 start_pos = ray_pos + fNearFar.x * ray_dir;
+      const f3 start_q = (start_pos - min_pos) * scale;
+      const float qFar = (fNearFar.y - fNearFar.x) * scale;
+      local_surface(c, g.type, ray_dir, instId, geomId, values, primId, d, 0.0f, qFar, fNearFar, start_q, hit);
+    }
+    bnf.x += smax(0.0f, fNearFar.y - bnf.x) + 1e-6f;
+  }
+  if (hit.t < old_t && sb.colorLayout) {
+    // colour of the hit for the indexed layouts (BVH2Common.cpp:1081-1110)
+    const f3 pos = ray_pos + hit.t * ray_dir;
+    const f3 dp = (pos - brick_min_pos) * (0.5f * sz);
+    const uint32_t* tofs = S.sbsData + node.z + sb.v3;
+    f3 col = mk3(0, 0, 0);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const uint32_t b = __ldg(tofs + k);
+      const float wx = (k & 4) ? dp.x : (1 - dp.x);
+      const float wy = (k & 2) ? dp.y : (1 - dp.y);
+      const float wz = (k & 1) ? dp.z : (1 - dp.z);
+      const float w = wx * wy * wz;
+      const f3 cc = w * mk3(__ldg(S.sbsDataF + b), __ldg(S.sbsDataF + b + 1), __ldg(S.sbsDataF + b + 2));
+      col = (k == 0) ? cc : col + cc;
+    }
+    col = mk3(sclamp(floorf(255.0f * col.x + 0.5f), 0.0f, 255.0f), sclamp(floorf(255.0f * col.y + 0.5f), 0.0f, 255.0f),
+              sclamp(floorf(255.0f * col.z + 0.5f), 0.0f, 255.0f));
+    hit.coords[0] = col.x + col.y / 256.0f;
+    hit.coords[1] = col.z;
+  }
+}
+
+template <bool COUNT>
+__device__ void triangles(Ctx<COUNT>& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, float tNear, uint32_t instId,
+                          uint32_t geomId, uint32_t a_start, uint32_t a_count, lrt_hit& hit)
+{
+  const DevScene& S = c.S;
+  const float4* tri = S.triSoup + 3 * (uint64_t(g.triBase) + a_start);
+  for (uint32_t i = 0; i < a_count; i++, tri += 3) {
+    c.inc(kCntTriTests);
+    const float4 A = __ldg(tri), E1 = __ldg(tri + 1), E2 = __ldg(tri + 2);
+    const f3 Ap = ld3(A), edge1 = ld3(E1), edge2 = ld3(E2);
+    const f3 pvec = cross(ray_dir, edge2);
+    const f3 tvec = ray_pos - Ap;
+    const f3 qvec = cross(tvec, edge1);
+    const float invDet = 1.0f / dot(edge1, pvec);
+    const float v = dot(tvec, pvec) * invDet;
+    const float u = dot(qvec, ray_dir) * invDet;
+    const float t = dot(edge2, qvec) * invDet;
+    if (v >= -1e-6f && u >= -1e-6f && (u + v <= 1.0f + 1e-6f) && t > tNear && t < hit.t) {
+      hit.t = t;
+      hit.primId = a_start + i;
+      hit.instId = instId;
+      hit.geomId = geomId | (LRT_TYPE_MESH_TRIANGLE << 24);
+      hit.coords[0] = u;
+      hit.coords[1] = v;
+      if (S.flags & kFlagNeedNormal) {
+        f3 n = cross(edge1, edge2);
+        n = normalize(matmul4(S.instances[instId].transformInvTransposed, n, 1.0f));
+        const f2 en = encode_normal(n);
+        hit.coords[2] = en.x;
+        hit.coords[3] = en.y;
+      } else {
+        hit.coords[2] = 0;
+        hit.coords[3] = 0;
+      }
+    }
+  }
+}
+
+// IntersectAllPrimitivesInLeaf: returns the tag if the hit moved closer.
+template <bool COUNT>
+__device__ __forceinline__ uint32_t leaf(Ctx<COUNT>& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, float tNear,
+                                         uint32_t aabbId, uint32_t instId, uint32_t geomId, lrt_hit& hit)
+{
+  const float tPrev = hit.t;
+  c.inc(kCntLeafCalls);
+  const uint32_t packed = __ldg(c.S.primIdCount + g.aabbBase + aabbId);
+  const uint32_t a_start = packed & 0x0FFFFFFFu;
+  const uint32_t a_count = (packed & 0x70000000u) >> 28;
+  switch (g.tag) {
+    case LRT_TAG_TRIANGLE: triangles(c, g, ray_pos, ray_dir, tNear, instId, geomId, a_start, a_count, hit); break;
+    case LRT_TAG_SDF_NODE: octree_node(c, g, ray_pos, ray_dir, tNear, instId, geomId, a_start, hit); break;
+    case LRT_TAG_SDF_BRICK: octree_brick(c, g, ray_pos, ray_dir, tNear, instId, geomId, a_start, hit); break;
+    default: break;
+  }
+  return (hit.t >= tPrev) ? LRT_TAG_NONE : g.tag;
+}
+
+// BVH2TraverseF32 with the stack in shared memory (thread-strided).
+template <bool COUNT>
+__device__ void blas(Ctx<COUNT>& c, uint32_t* stack, uint32_t stride, uint32_t cap, f3 ray_pos, f3 ray_dir,
+                     float tNear, uint32_t instId, uint32_t geomId, bool stopOnFirstHit, lrt_hit& hit)
+{
+  const DevScene& S = c.S;
+  const DevGeom g = S.geoms[geomId];
+  const float4* pairs = reinterpret_cast<const float4*>(S.pairs + g.bvhOffset);
+  int top = 0;
+  uint32_t leftNodeOffset = 0;
+  bool hitFound = false;
+  stack[0] = 0;
+  const f3 inv = safe_inverse(ray_dir);
+  while (top >= 0 && !hitFound) {
+    while (top >= 0 && ((leftNodeOffset & kLeafBit) == 0)) {
+      c.inc(kCntBlasPairs);
+      const float4* p = pairs + 4 * uint64_t(leftNodeOffset);
+      const float4 l0 = __ldg(p), l1 = __ldg(p + 1), r0 = __ldg(p + 2), r1 = __ldg(p + 3);
+      const uint32_t n0 = __float_as_uint(l0.w), n1 = __float_as_uint(r0.w);
+      const f2 tm0 = ray_box(ray_pos, inv, ld3(l0), ld3(l1));
+      const f2 tm1 = ray_box(ray_pos, inv, ld3(r0), ld3(r1));
+      const bool h0 = (tm0.x <= tm0.y) && (tm0.y >= tNear) && (tm0.x <= hit.t);
+      const bool h1 = (tm1.x <= tm1.y) && (tm1.y >= tNear) && (tm1.x <= hit.t);
+      leftNodeOffset = h0 ? n0 : n1;
+      if (h0 && h1) {
+        if (uint32_t(top) >= cap) {
+          c.err |= kErrStackOverflow;
+          return;
+        }
+        const bool nearFirst = tm0.x <= tm1.x;
+        leftNodeOffset = nearFirst ? n0 : n1;
+        stack[top * stride] = nearFirst ? n1 : n0;
+        top++;
+      }
+      if (!h0 && !h1) {
+        top--;
+        leftNodeOffset = stack[(top > 0 ? top : 0) * stride];
+      }
+    }
+    if (top >= 0 && leftNodeOffset != 0xFFFFFFFFu) {
+      const float tNearSdf = smax(tNear, 0.01f); // SDF_BIAS (BVH2Common.cpp:3306-3307)
+      const uint32_t tag = leaf(c, g, ray_pos, ray_dir, tNearSdf, leftNodeOffset & 0x0FFFFFFFu, instId, geomId, hit);
+      hitFound = (tag != 0) && (tag != LRT_TAG_TRIANGLE || stopOnFirstHit);
+    }
+    top--;
+    leftNodeOffset = stack[(top > 0 ? top : 0) * stride];
+  }
+}
+
+// RayQuery_NearestHit for one ray.
+template <bool COUNT>
+__device__ void trace_one(Ctx<COUNT>& c, uint32_t* stack, uint32_t stride, uint32_t cap, float4 pn, float4 df,
+                          lrt_hit& hit)
+{
+  const DevScene& S = c.S;
+  float dirW = df.w;
+  const bool stopOnFirstHit = (dirW <= 0.0f);
+  if (stopOnFirstHit) dirW *= -1.0f;
+  const f3 pos = mk3(pn.x, pn.y, pn.z), dir = mk3(df.x, df.y, df.z);
+  const float tmin = pn.w;
+  const f3 inv = safe_inverse(dir);
+  hit.t = dirW;
+  hit.primId = 0xFFFFFFFFu;
+  hit.instId = 0xFFFFFFFFu;
+  hit.geomId = 0xFFFFFFFFu;
+  hit.coords[0] = 1.0f;
+  hit.coords[1] = 0.0f;
+  hit.coords[2] = 0.0f;
+  hit.coords[3] = 0.0f;
+  uint32_t nodeIdx = 0;
+  do {
+    uint32_t travFlags = 0, leftOffset = 0;
+    do {
+      c.inc(kCntTlasNodes);
+      const float4* np = reinterpret_cast<const float4*>(S.tlas + nodeIdx);
+      const float4 a = __ldg(np), b = __ldg(np + 1);
+      const f2 bh = ray_box(pos, inv, ld3(a), ld3(b));
+      const uint32_t intersects = (bh.x <= bh.y) && (bh.y > tmin) && (bh.x < hit.t);
+      const uint32_t lo = __float_as_uint(a.w);
+      travFlags = (lo & kLeafBit) | intersects;
+      leftOffset = lo;
+      const bool leafOrNot = (travFlags & kLeafBit) != 0 || (travFlags & 1) == 0;
+      nodeIdx = leafOrNot ? __float_as_uint(b.w) : leftOffset;
+    } while (travFlags != (kLeafBit | 1u) && nodeIdx != 0 && nodeIdx < 0xFFFFFFFEu);
+    if (travFlags == (kLeafBit | 1u)) {
+      const uint32_t instId = leftOffset & 0x0FFFFFFFu;
+      const DevInstance& I = S.instances[instId];
+      c.inc(kCntInstances);
+      const f3 rp = matmul4(I.transformInv, pos, 1.0f);
+      const f3 rd = matmul4(I.transformInv, dir, 0.0f);
+      blas(c, stack, stride, cap, rp, rd, tmin, instId, I.geomId, stopOnFirstHit, hit);
+      if (c.err & kErrStackOverflow) break;
+    }
+  } while (nodeIdx < 0xFFFFFFFEu && !(stopOnFirstHit && hit.primId != 0xFFFFFFFFu));
+  if (hit.geomId < 0xFFFFFFFFu && ((hit.geomId >> 24) == LRT_TYPE_MESH_TRIANGLE)) {
+    const DevGeom& g = S.geoms[hit.geomId & 0x00FFFFFFu];
+    hit.primId = __ldg(S.primIndices + g.triBase + hit.primId);
+  }
+  if (hit.primId != 0xFFFFFFFFu) c.inc(kCntHits);
+}
+
+// One thread per ray; warps fetch 32-ray batches from a global counter
+// (persistent grid of ~one wave).  Stacks live in shared memory,
+// stack[i * blockDim + tid].
+template <bool COUNT>
+__global__ void __launch_bounds__(kTraceThreads) k_trace(DevScene S, const float4* __restrict__ rays,
+                                                         lrt_hit* __restrict__ hits, uint64_t n,
+                                                         unsigned long long* __restrict__ work_counter,
+                                                         unsigned long long* __restrict__ counters,
+                                                         uint32_t* __restrict__ err_word, uint32_t stack_cap)
+{
+  extern __shared__ uint32_t smem_stack[];
+  uint32_t* stack = smem_stack + threadIdx.x;
+  const uint32_t lane = threadIdx.x & 31;
+  Ctx<COUNT> c(S);
+  for (;;) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(work_counter, 32ull);
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    if (base >= n) break;
+    const uint64_t i = base + lane;
+    if (i < n) {
+      const float4 pn = __ldg(rays + 2 * i), df = __ldg(rays + 2 * i + 1);
+      lrt_hit h;
+      trace_one(c, stack, blockDim.x, stack_cap, pn, df, h);
+      float4* out = reinterpret_cast<float4*>(hits + i);
+      out[0] = make_float4(h.t, __uint_as_float(h.primId), __uint_as_float(h.instId), __uint_as_float(h.geomId));
+      out[1] = make_float4(h.coords[0], h.coords[1], h.coords[2], h.coords[3]);
+    }
+  }
+  if (c.err) atomicOr(err_word, c.err);
+  if (COUNT) {
+#pragma unroll
+    for (int k = 0; k < LRT_COUNTER_COUNT; k++) {
+      uint32_t v = c.cnt.c[k];
+      // warp-reduce before the atomic
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+      if (lane == 0 && v) atomicAdd(counters + k, (unsigned long long)v);
+    }
+  }
+}
+
+// Eye rays of one camera (MultiRenderer::initEyeRay), row-major pixels.
+__global__ void k_eye_rays(DevCamera cam, float4* __restrict__ rays)
+{
+  const uint64_t n = uint64_t(cam.width) * cam.height;
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+    float r[8];
+    eye_ray(cam.proj_inv, cam.world_view_inv, uint32_t(i % cam.width), uint32_t(i / cam.width), cam.width,
+            cam.height, cam.tnear, cam.tfar, r);
+    rays[2 * i] = make_float4(r[0], r[1], r[2], r[3]);
+    rays[2 * i + 1] = make_float4(r[4], r[5], r[6], r[7]);
+  }
+}
+
+// Host-side launchers (one copy per namespace; declared in trace_api.h).
+cudaError_t launch_trace(const DevScene& S, const float4* rays, lrt_hit* hits, uint64_t n,
+                                unsigned long long* work_counter, unsigned long long* counters, uint32_t* err_word,
+                                uint32_t stack_cap, int grid, cudaStream_t stream, bool count)
+{
+  const size_t smem = size_t(stack_cap) * kTraceThreads * sizeof(uint32_t);
+  if (count)
+    k_trace<true><<<grid, kTraceThreads, smem, stream>>>(S, rays, hits, n, work_counter, counters, err_word, stack_cap);
+  else
+    k_trace<false><<<grid, kTraceThreads, smem, stream>>>(S, rays, hits, n, work_counter, counters, err_word,
+                                                          stack_cap);
+  return cudaGetLastError();
+}
+
+cudaError_t set_trace_smem(uint32_t stack_cap)
+{
+  const int smem = int(stack_cap * kTraceThreads * sizeof(uint32_t));
+  cudaError_t e = cudaFuncSetAttribute(k_trace<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_trace<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+
+cudaError_t trace_occupancy(uint32_t stack_cap, int* blocks_per_sm)
+{
+  const size_t smem = size_t(stack_cap) * kTraceThreads * sizeof(uint32_t);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_trace<false>, kTraceThreads, smem);
+}
+
+cudaError_t launch_eye_rays(const DevCamera& cam, float4* rays, cudaStream_t stream)
+{
+  const uint64_t n = uint64_t(cam.width) * cam.height;
+  const int grid = int(std::min<uint64_t>((n + 255) / 256, 148ull * 16));
+  k_eye_rays<<<grid, 256, 0, stream>>>(cam, rays);
+  return cudaGetLastError();
+}
+
+} // namespace LRT_NS

@@ -1,0 +1,245 @@
+"""Python host binding of liblrt_b200.so, mirroring the reference's scene API.
+
+``SceneRT`` follows CrossRT's ISceneObject (CrossRT/CrossRT.h:43-175) and the
+BVHRT SDF adders (MultiRenderer/BVH2Common.h:95-104): same method names,
+argument meaning and call order (AddGeom_* -> AddInstance -> CommitScene ->
+RayQuery_NearestHit).  Errors are raised as ``LrtError`` carrying the
+library's status and message; nothing falls back to a CPU path — if the CUDA
+library is missing or no GPU is present the calls fail loudly.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from ._abi import (HIT_DTYPE, LRT_COUNTER_COUNT, LRT_TRACE_COUNT_WORK, LRT_TRACE_DEVICE_POINTERS,
+                   LRT_TRACE_FAST_MATH, STATUS_NAMES, Preset, SceneArrays, arrays_to_struct, parity_preset,
+                   struct_to_arrays)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblrt_b200.so")
+
+# Every extern "C" symbol declared in include/lrt_b200.h and include/lrt_workloads.h.
+EXPORTED = (
+    "lrt_scene_create", "lrt_scene_destroy", "lrt_last_error", "lrt_set_preset", "lrt_default_preset",
+    "lrt_clear_geom", "lrt_add_geom_triangles3f", "lrt_add_geom_aabb", "lrt_add_geom_sdf_frame_octree",
+    "lrt_add_geom_sdf_svs", "lrt_add_geom_sdf_sbs", "lrt_clear_scene", "lrt_add_instance", "lrt_commit_scene",
+    "lrt_scene_upload", "lrt_scene_export", "lrt_trace_nearest", "lrt_trace_sync", "lrt_ray_query_nearest_hit",
+    "lrt_ray_query_any_hit", "lrt_get_work_counters", "lrt_generate_eye_rays",
+    "lrt_wl_noisy_sphere", "lrt_wl_spheres", "lrt_wl_sphere_sdf", "lrt_wl_sbs_from_spheres",
+    "lrt_wl_frame_octree_from_spheres", "lrt_wl_svs_from_spheres",
+)
+
+
+class LrtError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("%s: %s" % (STATUS_NAMES.get(status, status), message))
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    """Load liblrt_b200.so (building it first if it is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from .build import build
+        build()
+    L = C.CDLL(LIB_PATH)
+    vp, u32, u64, sz = C.c_void_p, C.c_uint32, C.c_uint64, C.c_size_t
+    P = C.POINTER
+    sig = {
+        "lrt_scene_create": [C.c_char_p, C.c_char_p, P(vp)],
+        "lrt_scene_destroy": [vp],
+        "lrt_set_preset": [vp, P(Preset)],
+        "lrt_default_preset": [P(Preset)],
+        "lrt_clear_geom": [vp],
+        "lrt_add_geom_triangles3f": [vp, vp, sz, vp, sz, u32, sz, P(u32)],
+        "lrt_add_geom_aabb": [vp, u32, vp, sz, u32, P(u32)],
+        "lrt_add_geom_sdf_frame_octree": [vp, vp, sz, P(u32)],
+        "lrt_add_geom_sdf_svs": [vp, vp, sz, P(u32)],
+        "lrt_add_geom_sdf_sbs": [vp, vp, vp, sz, vp, sz, vp, sz, P(u32)],
+        "lrt_clear_scene": [vp],
+        "lrt_add_instance": [vp, u32, vp, P(u32)],
+        "lrt_commit_scene": [vp, u32],
+        "lrt_scene_upload": [vp, P(SceneArrays)],
+        "lrt_scene_export": [vp, P(SceneArrays)],
+        "lrt_trace_nearest": [vp, vp, vp, u64, vp, u32],
+        "lrt_trace_sync": [vp, vp, C.c_int32],
+        "lrt_ray_query_nearest_hit": [vp, vp, vp, vp],
+        "lrt_ray_query_any_hit": [vp, vp, vp, P(C.c_int32)],
+        "lrt_get_work_counters": [vp, vp],
+        "lrt_generate_eye_rays": [vp, vp, vp, vp],
+        "lrt_wl_noisy_sphere": [u32, C.c_float, C.c_float, u64, vp, vp, P(u64), P(u64)],
+        "lrt_wl_spheres": [u32, C.c_float, C.c_float, C.c_float, u64, vp],
+        "lrt_wl_sbs_from_spheres": [vp, u32, u32, u32, u32, vp, vp, vp, vp, P(u64), P(u64), P(u64)],
+        "lrt_wl_frame_octree_from_spheres": [vp, u32, u32, vp, P(u64)],
+        "lrt_wl_svs_from_spheres": [vp, u32, u32, vp, P(u64)],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = C.c_int32
+    L.lrt_last_error.argtypes = [vp]
+    L.lrt_last_error.restype = C.c_char_p
+    L.lrt_wl_sphere_sdf.argtypes = [vp, u32, C.c_double, C.c_double, C.c_double]
+    L.lrt_wl_sphere_sdf.restype = C.c_double
+    _lib = L
+    return L
+
+
+def check(status, scene_handle=None):
+    if status != 0:
+        msg = lib().lrt_last_error(scene_handle)
+        raise LrtError(status, msg.decode() if msg else "")
+
+
+def _ptr(a):
+    return a.ctypes.data if a is not None and len(a) else None
+
+
+class SceneRT:
+    """CreateSceneRT("BVH2Common_B200", build_name, layout_name)."""
+
+    def __init__(self, build_name="cbvh_embree2", layout_name="SuperTreeletAlignedMerged4", preset=None):
+        L = lib()
+        h = C.c_void_p()
+        check(L.lrt_scene_create(build_name.encode() if build_name else None,
+                                 layout_name.encode() if layout_name else None, C.byref(h)))
+        self.h = h
+        self.SetPreset(preset if preset is not None else parity_preset())
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            lib().lrt_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st):
+        check(st, self.h)
+
+    # -- ISceneObject ------------------------------------------------------
+    def SetPreset(self, preset):
+        self.preset = preset
+        self._check(lib().lrt_set_preset(self.h, C.byref(preset)))
+
+    def GetPreset(self):
+        return self.preset
+
+    def ClearGeom(self):
+        self._check(lib().lrt_clear_geom(self.h))
+
+    def AddGeom_Triangles3f(self, vpos3f, tri_indices, flags=4, vByteStride=12):
+        v = np.ascontiguousarray(vpos3f, dtype=np.float32).reshape(-1)
+        t = np.ascontiguousarray(tri_indices, dtype=np.uint32).reshape(-1)
+        nvert = len(v) * 4 // vByteStride
+        gid = C.c_uint32()
+        self._check(lib().lrt_add_geom_triangles3f(self.h, _ptr(v), nvert, _ptr(t), len(t), flags, vByteStride,
+                                                   C.byref(gid)))
+        return gid.value
+
+    def AddGeom_AABB(self, typeId, boxMinMaxF8, flags=4):
+        b = np.ascontiguousarray(boxMinMaxF8, dtype=np.float32).reshape(-1, 8)
+        gid = C.c_uint32()
+        self._check(lib().lrt_add_geom_aabb(self.h, typeId, _ptr(b), len(b), flags, C.byref(gid)))
+        return gid.value
+
+    def AddGeom_SdfFrameOctree(self, nodes):
+        gid = C.c_uint32()
+        self._check(lib().lrt_add_geom_sdf_frame_octree(self.h, _ptr(nodes), len(nodes), C.byref(gid)))
+        return gid.value
+
+    def AddGeom_SdfSVS(self, nodes):
+        gid = C.c_uint32()
+        self._check(lib().lrt_add_geom_sdf_svs(self.h, _ptr(nodes), len(nodes), C.byref(gid)))
+        return gid.value
+
+    def AddGeom_SdfSBS(self, header, nodes, values, values_f=None):
+        hdr = np.ascontiguousarray(header)
+        vals = np.ascontiguousarray(values, dtype=np.uint32)
+        vf = None if values_f is None else np.ascontiguousarray(values_f, dtype=np.float32)
+        gid = C.c_uint32()
+        self._check(lib().lrt_add_geom_sdf_sbs(self.h, hdr.ctypes.data, _ptr(nodes), len(nodes), _ptr(vals),
+                                               len(vals), _ptr(vf), 0 if vf is None else len(vf), C.byref(gid)))
+        return gid.value
+
+    def ClearScene(self):
+        self._check(lib().lrt_clear_scene(self.h))
+
+    def AddInstance(self, geomId, matrix_col_major):
+        m = np.ascontiguousarray(matrix_col_major, dtype=np.float32).reshape(16)
+        iid = C.c_uint32()
+        self._check(lib().lrt_add_instance(self.h, geomId, m.ctypes.data, C.byref(iid)))
+        return iid.value
+
+    def CommitScene(self, options=4, host_only=False):
+        """Builds the TLAS and uploads to the current CUDA device; with
+        host_only the arrays are built and validated but not uploaded."""
+        self._check(lib().lrt_commit_scene(self.h, options | (0x100 if host_only else 0)))
+
+    def RayQuery_NearestHit(self, posAndNear, dirAndFar):
+        pn = np.ascontiguousarray(posAndNear, dtype=np.float32)
+        df = np.ascontiguousarray(dirAndFar, dtype=np.float32)
+        hit = np.zeros(1, dtype=HIT_DTYPE)
+        self._check(lib().lrt_ray_query_nearest_hit(self.h, pn.ctypes.data, df.ctypes.data, hit.ctypes.data))
+        return hit[0]
+
+    def RayQuery_AnyHit(self, posAndNear, dirAndFar):
+        pn = np.ascontiguousarray(posAndNear, dtype=np.float32)
+        df = np.ascontiguousarray(dirAndFar, dtype=np.float32)
+        out = C.c_int32()
+        self._check(lib().lrt_ray_query_any_hit(self.h, pn.ctypes.data, df.ctypes.data, C.byref(out)))
+        return bool(out.value)
+
+    # -- batched form and the drop-in array boundary -----------------------
+    def RayQuery_NearestHitBatch(self, rays, fast_math=False, count_work=False):
+        """rays: (n, 8) float32 host array {posAndNear, dirAndFar} -> hits (n,) HIT_DTYPE."""
+        r = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        hits = np.zeros(len(r), dtype=HIT_DTYPE)
+        flags = (LRT_TRACE_FAST_MATH if fast_math else 0) | (LRT_TRACE_COUNT_WORK if count_work else 0)
+        self._check(lib().lrt_trace_nearest(self.h, r.ctypes.data, hits.ctypes.data, len(r), None, flags))
+        return hits
+
+    def trace_device(self, rays_ptr, hits_ptr, n, stream=0, fast_math=False, count_work=False):
+        """Asynchronous trace of device buffers (16-byte aligned) on `stream`."""
+        flags = LRT_TRACE_DEVICE_POINTERS | (LRT_TRACE_FAST_MATH if fast_math else 0) | \
+            (LRT_TRACE_COUNT_WORK if count_work else 0)
+        self._check(lib().lrt_trace_nearest(self.h, C.c_void_p(rays_ptr), C.c_void_p(hits_ptr), n,
+                                            C.c_void_p(stream) if stream else None, flags))
+
+    def sync(self, stream=0, read_counters=False):
+        self._check(lib().lrt_trace_sync(self.h, C.c_void_p(stream) if stream else None, int(read_counters)))
+
+    def work_counters(self):
+        c = np.zeros(LRT_COUNTER_COUNT, dtype=np.uint64)
+        self._check(lib().lrt_get_work_counters(self.h, c.ctypes.data))
+        return c
+
+    def upload_arrays(self, arrays):
+        s, keep = arrays_to_struct(arrays)
+        self._check(lib().lrt_scene_upload(self.h, C.byref(s)))
+        del keep
+
+    def export_arrays(self):
+        s = SceneArrays()
+        self._check(lib().lrt_scene_export(self.h, C.byref(s)))
+        return struct_to_arrays(s)
+
+    def generate_eye_rays(self, camera, rays_ptr, stream=0):
+        self._check(lib().lrt_generate_eye_rays(self.h, C.byref(camera), C.c_void_p(rays_ptr),
+                                                C.c_void_p(stream) if stream else None))

@@ -1,0 +1,331 @@
+/*
+ * lrt_b200.h — C-ABI of the B200 ray-query library (liblrt_b200.so).
+ *
+ * The library replaces LiteRT's CPU/Vulkan implementation of
+ * BVHRT::RayQuery_NearestHit (MultiRenderer/BVH2Common.cpp:3322-3392) with
+ * hand-written sm_100a CUDA kernels.  Every entry point takes plain pointers
+ * and sizes; no C++ or torch type crosses this boundary.
+ *
+ * Data layouts below are byte-for-byte the reference's device-visible structs
+ * (the arrays that kernel1D_FillGbuffer.slang:6-50 binds), so a BVHRT that was
+ * filled by the reference's own host code can be uploaded unchanged.
+ *
+ * Conventions
+ *  - Every function returns an lrt_status; nothing aborts.  On failure the
+ *    scene keeps a message readable with lrt_last_error().
+ *  - A scene is confined to one host thread at a time.  Concurrent traces of
+ *    one scene go through different CUDA streams.
+ *  - Host pointers passed to lrt_add_* / lrt_scene_upload are copied before
+ *    the call returns (reference ownership rule, BVH2Common_host.cpp:317-327).
+ */
+#ifndef LRT_B200_H
+#define LRT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                             */
+/* ------------------------------------------------------------------------ */
+typedef int32_t lrt_status;
+enum {
+  LRT_OK = 0,
+  LRT_ERR_INVALID_ARGUMENT = 1,  /* null pointer, bad id, bad size          */
+  LRT_ERR_BAD_SCENE = 2,         /* uploaded arrays fail validation          */
+  LRT_ERR_NOT_COMMITTED = 3,     /* trace before CommitScene / upload        */
+  LRT_ERR_CUDA = 4,              /* a CUDA runtime call failed               */
+  LRT_ERR_DEVICE_LIMIT = 5,      /* kernel reported a bounded-loop limit     */
+  LRT_ERR_UNSUPPORTED = 6,       /* preset or layout outside the hot path    */
+  LRT_ERR_OUT_OF_MEMORY = 7
+};
+
+/* ------------------------------------------------------------------------ */
+/* Reference PODs (same sizes, field order and meaning)                     */
+/* ------------------------------------------------------------------------ */
+
+/* CRT_Hit, CrossRT/CrossRT.h:26-33 (32 bytes). */
+typedef struct lrt_hit {
+  float t;
+  uint32_t primId;
+  uint32_t instId;
+  uint32_t geomId; /* type << 24 | geometry id */
+  float coords[4];
+} lrt_hit;
+
+/* BVHNode, utils/raytracing/cbvh.h:21-27 (32 bytes). */
+typedef struct lrt_bvh_node {
+  float boxMin[3];
+  uint32_t leftOffset; /* LEAF_BIT 0x80000000 marks a leaf */
+  float boxMax[3];
+  uint32_t escapeIndex;
+} lrt_bvh_node;
+
+/* BVHNodePair, utils/raytracing/cbvh.h:29-33 (64 bytes). */
+typedef struct lrt_bvh_node_pair {
+  lrt_bvh_node left;
+  lrt_bvh_node right;
+} lrt_bvh_node_pair;
+
+/* GeomData, utils/raytracing/intersection_common.h:33-44 (64 bytes). */
+typedef struct lrt_geom_data {
+  float boxMin[4];
+  float boxMax[4];
+  uint32_t bvhOffset;
+  uint32_t type;      /* TYPE_* of core/render_settings.h */
+  uint32_t offset[2]; /* triangles: (index offset, vertex offset); SDF: (sdf id, 0) */
+  uint32_t hasChannels;
+  uint32_t _pad[3];
+} lrt_geom_data;
+
+/* InstanceData, utils/raytracing/intersection_common.h:47-56 (256 bytes).
+ * Matrices are LiteMath float4x4: column-major, element (row r, col c) at
+ * [c*4 + r]. */
+typedef struct lrt_instance_data {
+  float boxMin[4];
+  float boxMax[4];
+  uint32_t geomId;
+  uint32_t _pad[7];
+  float transform[16];
+  float transformInv[16];
+  float transformInvTransposed[16];
+} lrt_instance_data;
+
+/* SdfFrameOctreeNode, sdf/simple/sdf_simple_shared.h:23-27 (36 bytes). */
+typedef struct lrt_sdf_frame_octree_node {
+  float values[8];
+  uint32_t offset; /* children start (8 consecutive nodes); 0 = leaf */
+} lrt_sdf_frame_octree_node;
+
+/* SdfSVSNode, sdf/simple/sdf_simple_shared.h:30-35 (16 bytes). */
+typedef struct lrt_sdf_svs_node {
+  uint32_t pos_xy;
+  uint32_t pos_z_lod_size;
+  uint32_t values[2]; /* 8 x u8 quantised distances */
+} lrt_sdf_svs_node;
+
+/* SdfSBSNode, sdf/simple/sdf_simple_shared.h:39-45 (16 bytes). */
+typedef struct lrt_sdf_sbs_node {
+  uint32_t pos_xy;
+  uint32_t pos_z_lod_size;
+  uint32_t data_offset; /* in uint32 words of the SBS data array */
+  uint32_t _pad;
+} lrt_sdf_sbs_node;
+
+/* SdfSBSHeader, sdf/simple/sdf_simple_shared.h:49-55 (16 bytes). */
+typedef struct lrt_sdf_sbs_header {
+  uint32_t brick_size;
+  uint32_t brick_pad;
+  uint32_t bytes_per_value;
+  uint32_t aux_data; /* SDF_SBS_NODE_LAYOUT_* */
+} lrt_sdf_sbs_header;
+
+/* MultiRenderPreset, core/render_settings.h:116-137 (60 bytes). */
+typedef struct lrt_preset {
+  uint32_t render_mode;
+  uint32_t sdf_node_intersect;
+  uint32_t normal_mode;
+  uint32_t ray_gen_mode;
+  uint32_t interpolation_mode;
+  uint32_t representation_mode;
+  uint32_t spp;
+  uint32_t fixed_lod;
+  float level_of_detail;
+  float compact_sdf_eps;
+  float LOD_distance;
+  uint32_t channel_render_mode;
+  uint32_t channel_id;
+  uint32_t component_id;
+  uint32_t CTF_id;
+} lrt_preset;
+
+/* Constants of the reference the C-ABI exposes. */
+#define LRT_TYPE_MESH_TRIANGLE 0u  /* core/render_settings.h:4 */
+#define LRT_TYPE_SDF_FRAME_OCTREE 3u
+#define LRT_TYPE_SDF_SVS 5u
+#define LRT_TYPE_SDF_SBS 6u
+#define LRT_TYPE_SDF_SBS_TEX 10u
+#define LRT_TYPE_SDF_SBS_COL 11u
+#define LRT_TAG_NONE 0u            /* MultiRenderer/BVH2Common.h:30-43 */
+#define LRT_TAG_TRIANGLE 1u
+#define LRT_TAG_SDF_BRICK 4u
+#define LRT_TAG_SDF_NODE 8u
+#define LRT_SBS_LAYOUT_UNDEFINED (0u << 24)  /* sdf_simple_shared.h:12-20 */
+#define LRT_SBS_LAYOUT_DX (1u << 24)
+#define LRT_SBS_LAYOUT_DX_UV16 (2u << 24)
+#define LRT_SBS_LAYOUT_DX_RGB8 (3u << 24)
+#define LRT_SBS_LAYOUT_ID32F_IRGB32F (4u << 24)
+#define LRT_SBS_LAYOUT_ID32F_IRGB32F_IN (5u << 24)
+#define LRT_SBS_LAYOUT_MASK 0xFF000000u
+#define LRT_RENDER_MODE_LAMBERT_NO_TEX 1u
+#define LRT_RENDER_MODE_ST_ITERATIONS 10u
+#define LRT_SDF_INTERSECT_ST 0u
+#define LRT_NORMAL_MODE_GEOMETRY 0u
+#define LRT_INTERPOLATION_TRILINEAR 0u
+#define LRT_REPRESENTATION_VOLUME 1u
+
+/* ------------------------------------------------------------------------ */
+/* Scene object (ISceneObject, CrossRT/CrossRT.h:43-175)                    */
+/* ------------------------------------------------------------------------ */
+typedef struct lrt_scene lrt_scene;
+
+/* CreateSceneRT("BVH2Common_B200", build, layout)
+ * (BVH2Common_host.cpp:1594-1600).  build_name follows the reference's
+ * BuilderPresetsFromString: a trailing digit sets primitives per triangle
+ * leaf ("cbvh_embree2" -> 2).  Either name may be NULL. */
+lrt_status lrt_scene_create(const char* build_name, const char* layout_name, lrt_scene** out);
+lrt_status lrt_scene_destroy(lrt_scene* scene);
+
+/* Message of the last failed call on this scene (or of the last failed
+ * lrt_scene_create when scene is NULL).  Never NULL. */
+const char* lrt_last_error(const lrt_scene* scene);
+
+/* BVHRT::SetPreset (BVH2Common_host.cpp:1437-1454).  Takes effect for the
+ * next trace; no recommit needed. */
+lrt_status lrt_set_preset(lrt_scene* scene, const lrt_preset* preset);
+/* getDefaultPreset() (core/render_settings.h:139-160). */
+lrt_status lrt_default_preset(lrt_preset* out);
+
+/* ISceneObject::ClearGeom (CrossRT.h:60; BVH2Common_host.cpp:128-156). */
+lrt_status lrt_clear_geom(lrt_scene* scene);
+
+/* ISceneObject::AddGeom_Triangles3f (CrossRT.h:71-72;
+ * BVH2Common_host.cpp:307-359).  vertex_byte_stride 0 means 12. */
+lrt_status lrt_add_geom_triangles3f(lrt_scene* scene, const float* vpos3f, size_t vert_count,
+                                    const uint32_t* tri_indices, size_t index_count, uint32_t build_flags,
+                                    size_t vertex_byte_stride, uint32_t* geom_id_out);
+
+/* ISceneObject::AddGeom_AABB (CrossRT.h:95; BVH2Common_host.cpp:441-459).
+ * boxes: n x {float4 boxMin, float4 boxMax}.  Like the reference, this adds
+ * the BLAS and its leaf table only; the SDF adders below call it. */
+lrt_status lrt_add_geom_aabb(lrt_scene* scene, uint32_t type_tag, const float* boxes_min_max_f8,
+                             size_t box_count, uint32_t build_flags, uint32_t* geom_id_out);
+
+/* BVHRT::AddGeom_SdfFrameOctree (BVH2Common_host.cpp:501-534). */
+lrt_status lrt_add_geom_sdf_frame_octree(lrt_scene* scene, const lrt_sdf_frame_octree_node* nodes,
+                                         size_t node_count, uint32_t* geom_id_out);
+/* BVHRT::AddGeom_SdfSVS (BVH2Common_host.cpp:536-599). */
+lrt_status lrt_add_geom_sdf_svs(lrt_scene* scene, const lrt_sdf_svs_node* nodes, size_t node_count,
+                                uint32_t* geom_id_out);
+/* BVHRT::AddGeom_SdfSBS (BVH2Common_host.cpp:601-695).  values_f may be NULL
+ * for the DX layouts. */
+lrt_status lrt_add_geom_sdf_sbs(lrt_scene* scene, const lrt_sdf_sbs_header* header,
+                                const lrt_sdf_sbs_node* nodes, size_t node_count, const uint32_t* values,
+                                size_t values_count, const float* values_f, size_t values_f_count,
+                                uint32_t* geom_id_out);
+
+/* ISceneObject::ClearScene / AddInstance / CommitScene (CrossRT.h:101-115;
+ * BVH2Common_host.cpp:1230-1301).  matrix: 16 floats, column-major.
+ * CommitScene builds the TLAS and uploads everything to the current device. */
+lrt_status lrt_clear_scene(lrt_scene* scene);
+lrt_status lrt_add_instance(lrt_scene* scene, uint32_t geom_id, const float* matrix_col_major16,
+                            uint32_t* inst_id_out);
+/* build_flags may include LRT_COMMIT_HOST_ONLY: build the TLAS and validate,
+ * but leave the device untouched (for a host that hands the arrays to another
+ * implementation through lrt_scene_export). */
+#define LRT_COMMIT_HOST_ONLY 0x100u
+lrt_status lrt_commit_scene(lrt_scene* scene, uint32_t build_flags);
+
+/* ------------------------------------------------------------------------ */
+/* Drop-in upload of arrays flattened by the reference's BVHRT host code.     */
+/* ------------------------------------------------------------------------ */
+/* One {pointer, element count} per BVHRT member the traversal reads
+ * (MultiRenderer/BVH2Common.h:262-365).  startEnd holds uint2 pairs and
+ * vertPos float4s: their counts are in pairs / float4s. */
+typedef struct lrt_scene_arrays {
+  const lrt_bvh_node* nodesTLAS;                        uint64_t nodesTLAS_count;
+  const lrt_bvh_node_pair* allNodePairs;                uint64_t allNodePairs_count;
+  const lrt_instance_data* instanceData;                uint64_t instanceData_count;
+  const lrt_geom_data* geomData;                        uint64_t geomData_count;
+  const uint32_t* geomTags;                             uint64_t geomTags_count;
+  const uint32_t* startEnd;                             uint64_t startEnd_count;
+  const uint32_t* primIdCount;                          uint64_t primIdCount_count;
+  const uint32_t* indices;                              uint64_t indices_count;
+  const float* vertPos;                                 uint64_t vertPos_count;
+  const uint32_t* primIndices;                          uint64_t primIndices_count;
+  const lrt_bvh_node* origNodes;                        uint64_t origNodes_count;
+  const lrt_sdf_frame_octree_node* sdfFrameOctreeNodes; uint64_t sdfFrameOctreeNodes_count;
+  const uint32_t* sdfFrameOctreeRoots;                  uint64_t sdfFrameOctreeRoots_count;
+  const lrt_sdf_svs_node* sdfSVSNodes;                  uint64_t sdfSVSNodes_count;
+  const uint32_t* sdfSVSRoots;                          uint64_t sdfSVSRoots_count;
+  const lrt_sdf_sbs_node* sdfSBSNodes;                  uint64_t sdfSBSNodes_count;
+  const uint32_t* sdfSBSData;                           uint64_t sdfSBSData_count;
+  const float* sdfSBSDataF;                             uint64_t sdfSBSDataF_count;
+  const uint32_t* sdfSBSRoots;                          uint64_t sdfSBSRoots_count;
+  const lrt_sdf_sbs_header* sdfSBSHeaders;              uint64_t sdfSBSHeaders_count;
+} lrt_scene_arrays;
+
+/* Replace the scene's host arrays with copies of `arrays`, validate them and
+ * upload to the current device.  Equivalent of the reference GPU class's
+ * CommitDeviceData (MultiRenderer_slang_comp.cpp:264). */
+lrt_status lrt_scene_upload(lrt_scene* scene, const lrt_scene_arrays* arrays);
+
+/* Read-only view of the scene's host arrays (valid until the next mutating
+ * call).  Lets a host that built the scene with lrt_add_* hand the same
+ * arrays to another implementation. */
+lrt_status lrt_scene_export(const lrt_scene* scene, lrt_scene_arrays* out);
+
+/* ------------------------------------------------------------------------ */
+/* Ray queries                                                              */
+/* ------------------------------------------------------------------------ */
+/* Flags for the trace calls. */
+#define LRT_TRACE_DEVICE_POINTERS 0x1u /* rays/hits are device pointers     */
+#define LRT_TRACE_FAST_MATH 0x2u       /* FMA-contracted kernels (tolerance
+                                          parity); default is the exact build */
+#define LRT_TRACE_COUNT_WORK 0x4u      /* also accumulate work counters     */
+
+/* Batched BVHRT::RayQuery_NearestHit.  rays: n x {float4 posAndNear,
+ * float4 dirAndFar} (32 bytes per ray), hits: n x lrt_hit.  A ray whose
+ * dirAndFar.w <= 0 is traced stop-on-first-hit with tfar = -w, exactly like
+ * the reference (BVH2Common.cpp:3324-3326).  stream is a cudaStream_t (NULL =
+ * legacy default stream).  With host pointers the call is synchronous. */
+lrt_status lrt_trace_nearest(lrt_scene* scene, const float* rays, lrt_hit* hits, uint64_t n, void* stream,
+                             uint32_t flags);
+
+/* Waits for the traces queued on `stream` (device-pointer traces are
+ * asynchronous) and returns LRT_ERR_DEVICE_LIMIT if one of them hit a
+ * bounded-loop limit.  With read_counters != 0 the work counters of the last
+ * LRT_TRACE_COUNT_WORK trace on the stream become readable. */
+lrt_status lrt_trace_sync(lrt_scene* scene, void* stream, int32_t read_counters);
+
+/* ISceneObject::RayQuery_NearestHit / RayQuery_AnyHit for one ray
+ * (CrossRT.h:145,163).  Synchronous; forwards to a 1-ray batch. */
+lrt_status lrt_ray_query_nearest_hit(lrt_scene* scene, const float pos_and_near[4], const float dir_and_far[4],
+                                     lrt_hit* hit_out);
+lrt_status lrt_ray_query_any_hit(lrt_scene* scene, const float pos_and_near[4], const float dir_and_far[4],
+                                 int32_t* hit_out);
+
+/* Work counters of the last LRT_TRACE_COUNT_WORK trace (summed over rays):
+ * TLAS node visits, instances entered, BLAS node-pair visits, leaf calls,
+ * triangle tests, SBS brick entries, SBS voxel visits, ST steps,
+ * frame-octree leaf tests, SVS leaf tests, hits, normals computed. */
+#define LRT_COUNTER_COUNT 12
+lrt_status lrt_get_work_counters(lrt_scene* scene, uint64_t counters[LRT_COUNTER_COUNT]);
+
+/* ------------------------------------------------------------------------ */
+/* Eye rays (MultiRenderer::initEyeRay, MultiRenderer.cpp:142-183)           */
+/* ------------------------------------------------------------------------ */
+/* One pinhole camera: the inverses of the projection and world-view matrices
+ * (column-major), the image size and the ray interval.  Rays are generated
+ * for pixel centres (spp = 1, frame 0); the cutting plane is off, so the
+ * reference would use tnear = 1e-9 and tfar = 1e9. */
+typedef struct lrt_camera {
+  float proj_inv[16];
+  float world_view_inv[16];
+  uint32_t width;
+  uint32_t height;
+  float tnear;
+  float tfar;
+} lrt_camera;
+
+/* Write width*height rays of `camera` (row-major pixel order) to device
+ * memory `rays_dev`. */
+lrt_status lrt_generate_eye_rays(lrt_scene* scene, const lrt_camera* camera, float* rays_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LRT_B200_H */

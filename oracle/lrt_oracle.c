@@ -1,0 +1,579 @@
+/*
+ * lrt_oracle.c — CPU restatement of LiteRT's nearest-hit ray query.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA path: only
+ * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it.
+ * The product library never links or calls it.
+ *
+ * It restates, in plain C with IEEE single-precision arithmetic evaluated in
+ * the reference's operation order (build with -ffp-contract=off), the path
+ *   BVHRT::RayQuery_NearestHit   MultiRenderer/BVH2Common.cpp:3322-3392
+ *   BVHRT::BVH2TraverseF32       MultiRenderer/BVH2Common.cpp:3239-3320
+ *   IntersectAllPrimitivesInLeaf MultiRenderer/BVH2Common.cpp:47-124
+ *   IntersectAllTrianglesInLeaf  MultiRenderer/BVH2Common.cpp:1571-1635
+ *   OctreeNodeIntersect / RayNodeIntersection  :727-749, :141-218
+ *   OctreeBrickIntersect / load_distance_values :884-1112, :846-882
+ *   LocalSurfaceIntersection (ST branch)        :345-391, :618-690
+ * over the flattened BVHRT arrays (lrt_scene_arrays).  Its results are
+ * pinned against the reference compiled from its own sources (oracle/ref)
+ * and against committed golden vectors (tests/golden).
+ *
+ * Differences from the reference, all on inputs where the reference is
+ * undefined: the BLAS stack is checked against its 80-entry capacity
+ * (raytrace_common.h:36 has no check), the SBS voxel march is capped at
+ * LRTO_MAX_VOXEL_STEPS iterations (the reference loop can stall when
+ * t + 1e-6 rounds back to t), and out-of-range node ids end the leaf test.
+ * Each such event increments the `limits` counter instead.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "../include/lrt_b200.h"
+
+#define LEAF_BIT 0x80000000u
+#define START_MASK 0x0FFFFFFFu
+#define SIZE_MASK 0x70000000u
+#define STACK_SIZE 80
+#define LRTO_MAX_VOXEL_STEPS 4096u
+
+enum {
+  C_TLAS_NODES = 0, C_INSTANCES, C_BLAS_PAIRS, C_LEAF_CALLS, C_TRI_TESTS, C_BRICKS, C_VOXELS, C_ST_STEPS,
+  C_OCTREE_LEAVES, C_SVS_LEAVES, C_HITS, C_NORMALS
+};
+
+typedef struct { float x, y, z; } f3;
+typedef struct { float x, y; } f2;
+
+/* std::min / std::max / LiteMath::clamp / LiteMath::sign, in their exact
+ * comparison forms (NaN propagation matters for bit parity). */
+static inline float smin(float a, float b) { return (b < a) ? b : a; }
+static inline float smax(float a, float b) { return (a < b) ? b : a; }
+static inline float sclamp(float u, float a, float b) { return smin(smax(a, u), b); }
+static inline float ssign(float x) { return x == 0.0f ? 0.0f : (x < 0.0f ? -1.0f : 1.0f); }
+
+static inline f3 mk3(float x, float y, float z) { f3 r = {x, y, z}; return r; }
+static inline f3 add3(f3 a, f3 b) { return mk3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline f3 sub3(f3 a, f3 b) { return mk3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline f3 mul3(f3 a, f3 b) { return mk3(a.x * b.x, a.y * b.y, a.z * b.z); }
+static inline f3 scl3(float s, f3 a) { return mk3(s * a.x, s * a.y, s * a.z); }
+static inline f3 div3s(f3 a, float s) { return mk3(a.x / s, a.y / s, a.z / s); }
+static inline float dot3(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+/* LiteMath cross (LiteMath.h:987-992) */
+static inline f3 cross3(f3 a, f3 b) { return mk3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+/* LiteMath normalize: v * (1/sqrt(dot(v,v))) (LiteMath.h:966) */
+static inline f3 normalize3(f3 v) { float inv = 1.0f / sqrtf(dot3(v, v)); return mk3(v.x * inv, v.y * inv, v.z * inv); }
+static inline f3 ld3(const float* p) { return mk3(p[0], p[1], p[2]); }
+
+/* float4x4 (column-major) times float4, mat4_colmajor_mul_vec4
+ * (LiteMath.h:1813-1819); matmul4x3 uses w=1, matmul3x3 w=0
+ * (raytrace_common.h:85-93). */
+static inline f3 matmul4(const float* m, f3 v, float w)
+{
+  f3 r;
+  r.x = v.x * m[0] + v.y * m[4] + v.z * m[8] + w * m[12];
+  r.y = v.x * m[1] + v.y * m[5] + v.z * m[9] + w * m[13];
+  r.z = v.x * m[2] + v.y * m[6] + v.z * m[10] + w * m[14];
+  return r;
+}
+
+/* SafeInverse, raytrace_common.h:59-67 */
+static inline f3 safe_inverse(f3 d)
+{
+  const float ooeps = 1.0e-36f;
+  f3 r;
+  r.x = 1.0f / (fabsf(d.x) > ooeps ? d.x : fabsf(ooeps) * ssign(d.x));
+  r.y = 1.0f / (fabsf(d.y) > ooeps ? d.y : fabsf(ooeps) * ssign(d.y));
+  r.z = 1.0f / (fabsf(d.z) > ooeps ? d.z : fabsf(ooeps) * ssign(d.z));
+  return r;
+}
+
+/* RayBoxIntersection2, raytrace_common.h:69-82 */
+static inline f2 ray_box(f3 o, f3 inv, f3 bmin, f3 bmax)
+{
+  const float lo = inv.x * (bmin.x - o.x);
+  const float hi = inv.x * (bmax.x - o.x);
+  const float lo1 = inv.y * (bmin.y - o.y);
+  const float hi1 = inv.y * (bmax.y - o.y);
+  const float lo2 = inv.z * (bmin.z - o.z);
+  const float hi2 = inv.z * (bmax.z - o.z);
+  const float tmin = smax(smin(lo, hi), smin(lo1, hi1));
+  const float tmax = smin(smax(lo, hi), smax(lo1, hi1));
+  f2 r = {smax(tmin, smin(lo2, hi2)), smin(tmax, smax(lo2, hi2))};
+  return r;
+}
+
+/* encode_normal, intersection_common.h:96-101 */
+static inline f2 encode_normal(f3 v)
+{
+  const float inv = 1.0f / (fabsf(v.x) + fabsf(v.y) + fabsf(v.z));
+  f2 p = {v.x * inv, v.y * inv};
+  const float sx = (p.x >= 0.0f) ? 1.0f : -1.0f;
+  const float sy = (p.y >= 0.0f) ? 1.0f : -1.0f;
+  if (v.z <= 0.0f) {
+    f2 r = {(1.0f - fabsf(p.y)) * sx, (1.0f - fabsf(p.x)) * sy};
+    return r;
+  }
+  return p;
+}
+
+/* eval_dist_trilinear, BVH2Common.cpp:126-136 */
+static inline float trilinear(const float v[8], f3 dp)
+{
+  return (1 - dp.x) * (1 - dp.y) * (1 - dp.z) * v[0] + (1 - dp.x) * (1 - dp.y) * (dp.z) * v[1] +
+         (1 - dp.x) * (dp.y) * (1 - dp.z) * v[2] + (1 - dp.x) * (dp.y) * (dp.z) * v[3] +
+         (dp.x) * (1 - dp.y) * (1 - dp.z) * v[4] + (dp.x) * (1 - dp.y) * (dp.z) * v[5] +
+         (dp.x) * (dp.y) * (1 - dp.z) * v[6] + (dp.x) * (dp.y) * (dp.z) * v[7];
+}
+
+typedef struct {
+  const lrt_scene_arrays* a;
+  const lrt_preset* p;
+  uint64_t* cnt;   /* LRT_COUNTER_COUNT entries (thread-local) */
+  uint64_t limits; /* bounded-loop / bounds events */
+} ctx_t;
+
+/* BVHRT::need_normal, BVH2Common.cpp:19-32 */
+static int need_normal(const lrt_preset* p)
+{
+  const uint32_t m = p->render_mode;
+  return m == 1 || m == 8 || m == 12 || m == 17 || m == 20 || m == 7 || m == 18 || m == 23 || m == 21 ||
+         m == 11 || m == 27;
+}
+
+/* LocalSurfaceIntersection, ST + BBOX branches, trilinear (BVH2Common.cpp:345-391, 618-690).
+ * is_surface_node is always false on this path (OctreeNodeIntersect and
+ * OctreeBrickIntersect pass false), so EPS is the base 1e-6. */
+static void local_surface(ctx_t* c, uint32_t type, f3 ray_dir, uint32_t instId, uint32_t geomId,
+                          const float values[8], uint32_t primId, float d, float qNear, float qFar, f2 fNearFar,
+                          f3 start_q, lrt_hit* hit)
+{
+  const lrt_preset* P = c->p;
+  const float EPS = 1e-6f;
+  const float d_inv = 1.0f / d;
+  float t = qNear;
+  int early_hit = 0, hitf = 0;
+  unsigned iter = 0;
+  float start_sign = 1;
+  float start_dist = trilinear(values, add3(start_q, scl3(t, ray_dir)));
+  c->cnt[C_ST_STEPS]++;
+  if (P->representation_mode == 0 /* SURFACE */) start_sign = ssign(start_dist);
+  start_dist *= start_sign;
+  if (start_dist <= EPS || P->sdf_node_intersect == 3 /* BBOX */) {
+    early_hit = 1;
+    hitf = 1;
+  } else {
+    float dist = start_dist;
+    while (t < qFar && dist > EPS && iter < 256) {
+      t += dist * d_inv;
+      dist = start_sign * trilinear(values, add3(start_q, scl3(t, ray_dir)));
+      iter++;
+    }
+    c->cnt[C_ST_STEPS] += iter;
+    hitf = (dist <= EPS);
+  }
+  const float tReal = fNearFar.x + d * t;
+  if (t <= qFar && hitf && tReal < hit->t) {
+    f3 norm = mk3(0, 0, 1);
+    if (need_normal(P)) {
+      const lrt_instance_data* inst = &c->a->instanceData[instId];
+      if (early_hit && P->sdf_node_intersect == 3) {
+        /* BVH2Common.cpp:644-656 */
+        float q[3] = {start_q.x, start_q.y, start_q.z};
+        f3 v = mk3(smax(start_q.x, 1 - start_q.x), smax(start_q.y, 1 - start_q.y), smax(start_q.z, 1 - start_q.z));
+        int dim = 0;
+        if (v.y > v.x && v.y > v.z) dim = 1;
+        else if (v.z > v.x && v.z > v.y) dim = 2;
+        float n[3] = {0, 0, 0};
+        n[dim] = q[dim] < 0.5f ? -1.0f : 1.0f;
+        norm = mk3(n[0], n[1], n[2]);
+      } else {
+        /* qNear is 0 on this path, so the cutting-plane branch (:640-643) is unreachable */
+        const f3 p0 = add3(start_q, scl3(t, ray_dir));
+        const float h = 0.001f;
+        float ddx = (trilinear(values, add3(p0, mk3(h, 0, 0))) - trilinear(values, add3(p0, mk3(-h, 0, 0)))) / (2 * h);
+        float ddy = (trilinear(values, add3(p0, mk3(0, h, 0))) - trilinear(values, add3(p0, mk3(0, -h, 0)))) / (2 * h);
+        float ddz = (trilinear(values, add3(p0, mk3(0, 0, h))) - trilinear(values, add3(p0, mk3(0, 0, -h)))) / (2 * h);
+        norm = scl3(start_sign, mk3(ddx, ddy, ddz));
+      }
+      norm = normalize3(matmul4(inst->transformInvTransposed, norm, 1.0f));
+      c->cnt[C_NORMALS]++;
+    }
+    const f2 en = encode_normal(norm);
+    hit->t = tReal;
+    hit->primId = primId;
+    hit->instId = instId;
+    hit->geomId = geomId | (type << 24);
+    hit->coords[0] = 0;
+    hit->coords[1] = 0;
+    hit->coords[2] = en.x;
+    hit->coords[3] = en.y;
+    if (P->render_mode == LRT_RENDER_MODE_ST_ITERATIONS) hit->primId = iter;
+  }
+}
+
+/* OctreeNodeIntersect + RayNodeIntersection (BVH2Common.cpp:727-749, 141-218). */
+static void octree_node(ctx_t* c, uint32_t type, f3 ray_pos, f3 ray_dir, float tNear, uint32_t instId,
+                        uint32_t geomId, uint32_t bvhNodeId, lrt_hit* hit)
+{
+  const lrt_scene_arrays* A = c->a;
+  float values[8];
+  uint32_t primId;
+  f3 min_pos, max_pos;
+  const uint32_t sdfId = A->geomData[geomId].offset[0];
+  if (type == LRT_TYPE_SDF_FRAME_OCTREE) {
+    c->cnt[C_OCTREE_LEAVES]++;
+    if (bvhNodeId >= A->origNodes_count) { c->limits++; return; }
+    const lrt_bvh_node* on = &A->origNodes[bvhNodeId];
+    primId = on->leftOffset;
+    const uint64_t nodeId = (uint64_t)primId + A->sdfFrameOctreeRoots[sdfId];
+    if (nodeId >= A->sdfFrameOctreeNodes_count) { c->limits++; return; }
+    min_pos = ld3(on->boxMin);
+    max_pos = ld3(on->boxMax);
+    for (int i = 0; i < 8; i++) values[i] = A->sdfFrameOctreeNodes[nodeId].values[i];
+  } else if (type == LRT_TYPE_SDF_SVS) {
+    c->cnt[C_SVS_LEAVES]++;
+    primId = bvhNodeId;
+    const uint64_t nodeId = (uint64_t)primId + A->sdfSVSRoots[sdfId];
+    if (nodeId >= A->sdfSVSNodes_count) { c->limits++; return; }
+    const lrt_sdf_svs_node* n = &A->sdfSVSNodes[nodeId];
+    const float px = (float)(n->pos_xy >> 16);
+    const float py = (float)(n->pos_xy & 0x0000FFFF);
+    const float pz = (float)(n->pos_z_lod_size >> 16);
+    const float sz = (float)(n->pos_z_lod_size & 0x0000FFFF);
+    const float d_max = 2 * 1.73205081f / sz;
+    min_pos = add3(mk3(-1, -1, -1), div3s(scl3(2.0f, mk3(px, py, pz)), sz));
+    max_pos = add3(min_pos, div3s(scl3(2.0f, mk3(1, 1, 1)), sz));
+    for (int i = 0; i < 8; i++)
+      values[i] = -d_max + 2.0f * d_max * (1.0f / 255.0f) * ((n->values[i / 4] >> (8 * (i % 4))) & 0xFF);
+  } else {
+    return;
+  }
+  const f3 size = sub3(max_pos, min_pos);
+  const f2 fNearFar = ray_box(ray_pos, safe_inverse(ray_dir), min_pos, max_pos);
+  const f3 start_pos = add3(ray_pos, scl3(fNearFar.x, ray_dir));
+  const float d = smax(size.x, smax(size.y, size.z));
+  const f3 start_q = div3s(sub3(start_pos, min_pos), d);
+  const float qFar = (fNearFar.y - fNearFar.x) / d;
+  const float qNear = tNear > fNearFar.x ? (tNear - fNearFar.x) / d : 0.0f;
+  if (qNear > 0.0f) return; /* ray starts inside this node (:744-745) */
+  local_surface(c, type, ray_dir, instId, geomId, values, primId, d, qNear, qFar, fNearFar, start_q, hit);
+}
+
+/* load_distance_values, BVH2Common.cpp:846-882 (trilinear corners 000..111, x major). */
+static float load_distance_values(ctx_t* c, uint32_t nodeId, f3 voxelPos, uint32_t v_size, float sz_inv,
+                                  const lrt_sdf_sbs_header* h, float values[8])
+{
+  const lrt_scene_arrays* A = c->a;
+  float vmin = 1e6f;
+  const uint32_t v_off = A->sdfSBSNodes[nodeId].data_offset;
+  const uint32_t layout = h->aux_data & LRT_SBS_LAYOUT_MASK;
+  const uint32_t vx = (uint32_t)voxelPos.x, vy = (uint32_t)voxelPos.y, vz = (uint32_t)voxelPos.z;
+  if (layout == LRT_SBS_LAYOUT_ID32F_IRGB32F || layout == LRT_SBS_LAYOUT_ID32F_IRGB32F_IN) {
+    for (int i = 0; i < 8; i++) {
+      const uint32_t x = vx + ((i & 4) >> 2), y = vy + ((i & 2) >> 1), z = vz + (i & 1);
+      const uint32_t vId = (x + h->brick_pad) * v_size * v_size + (y + h->brick_pad) * v_size + (z + h->brick_pad);
+      values[i] = A->sdfSBSDataF[A->sdfSBSData[v_off + vId]];
+      vmin = smin(vmin, values[i]);
+    }
+  } else {
+    const uint32_t vals_per_int = 4 / h->bytes_per_value;
+    const uint32_t bits = 8 * h->bytes_per_value;
+    const uint32_t max_val = h->bytes_per_value == 4 ? 0xFFFFFFFFu : ((1u << bits) - 1);
+    const float d_max = 1.73205081f * sz_inv;
+    const float mult = 2 * d_max / max_val;
+    for (int i = 0; i < 8; i++) {
+      const uint32_t x = vx + ((i & 4) >> 2), y = vy + ((i & 2) >> 1), z = vz + (i & 1);
+      const uint32_t vId = (x + h->brick_pad) * v_size * v_size + (y + h->brick_pad) * v_size + (z + h->brick_pad);
+      const uint32_t word = A->sdfSBSData[v_off + vId / vals_per_int];
+      const uint32_t sh = bits * (vId % vals_per_int);
+      const uint32_t field = (sh >= 32 ? 0u : (word >> sh)) & max_val;
+      values[i] = -d_max + mult * field;
+      vmin = smin(vmin, values[i]);
+    }
+  }
+  return vmin;
+}
+
+/* OctreeBrickIntersect, trilinear, BVH2Common.cpp:884-1112 (SMOOTHED normals
+ * and tricubic filtering are outside the path). */
+static void octree_brick(ctx_t* c, uint32_t type, f3 ray_pos, f3 ray_dir, float tNear, uint32_t instId,
+                         uint32_t geomId, uint32_t bvhNodeId, lrt_hit* hit)
+{
+  const lrt_scene_arrays* A = c->a;
+  const uint32_t sdfId = A->geomData[geomId].offset[0];
+  const uint32_t primId = bvhNodeId;
+  const uint64_t nodeId64 = (uint64_t)primId + A->sdfSBSRoots[sdfId];
+  c->cnt[C_BRICKS]++;
+  if (nodeId64 >= A->sdfSBSNodes_count) { c->limits++; return; }
+  const uint32_t nodeId = (uint32_t)nodeId64;
+  const lrt_sdf_sbs_header h = A->sdfSBSHeaders[sdfId];
+  const uint32_t v_size = h.brick_size + 2 * h.brick_pad + 1;
+  const lrt_sdf_sbs_node* n = &A->sdfSBSNodes[nodeId];
+  const float px = (float)(n->pos_xy >> 16);
+  const float py = (float)(n->pos_xy & 0x0000FFFF);
+  const float pz = (float)(n->pos_z_lod_size >> 16);
+  const float sz = (float)(n->pos_z_lod_size & 0x0000FFFF);
+  const float sz_inv = 2.0f / sz;
+  const float d = 2.0f / (sz * h.brick_size);
+  const f3 brick_min_pos = add3(mk3(-1, -1, -1), scl3(sz_inv, mk3(px, py, pz)));
+  const f3 brick_max_pos = add3(brick_min_pos, scl3(sz_inv, mk3(1, 1, 1)));
+  const f3 inv_dir = safe_inverse(ray_dir);
+  f2 bnf = ray_box(ray_pos, inv_dir, brick_min_pos, brick_max_pos);
+  const float old_t = hit->t;
+  const float scale = 0.5f * sz * h.brick_size;
+  float values[8];
+  uint32_t steps = 0;
+  while (bnf.x < bnf.y && hit->t == old_t) {
+    if (steps++ >= LRTO_MAX_VOXEL_STEPS) { c->limits++; break; }
+    c->cnt[C_VOXELS]++;
+    const f3 hit_pos = add3(ray_pos, scl3(bnf.x, ray_dir));
+    const f3 local_pos = scl3(scale, sub3(hit_pos, brick_min_pos));
+    const float hi = h.brick_size - 1e-6f;
+    const f3 voxelPos = mk3(floorf(sclamp(local_pos.x, 1e-6f, hi)), floorf(sclamp(local_pos.y, 1e-6f, hi)),
+                            floorf(sclamp(local_pos.z, 1e-6f, hi)));
+    const f3 min_pos = add3(brick_min_pos, scl3(d, voxelPos));
+    const f3 max_pos = add3(min_pos, scl3(d, mk3(1, 1, 1)));
+    const float vmin = load_distance_values(c, nodeId, voxelPos, v_size, sz_inv, &h, values);
+    const f2 fNearFar = ray_box(ray_pos, inv_dir, min_pos, max_pos);
+    if (tNear < fNearFar.x && vmin <= 0.0f) {
+      const f3 start_pos = add3(ray_pos, scl3(fNearFar.x, ray_dir));
+      const f3 start_q = scl3(scale, sub3(start_pos, min_pos));
+      const float qFar = (fNearFar.y - fNearFar.x) * scale;
+      local_surface(c, type, ray_dir, instId, geomId, values, primId, d, 0.0f, qFar, fNearFar, start_q, hit);
+    }
+    bnf.x += smax(0.0f, fNearFar.y - bnf.x) + 1e-6f;
+  }
+  if (hit->t < old_t) {
+    const uint32_t layout = h.aux_data & LRT_SBS_LAYOUT_MASK;
+    if (layout == LRT_SBS_LAYOUT_ID32F_IRGB32F || layout == LRT_SBS_LAYOUT_ID32F_IRGB32F_IN) {
+      /* colour of the hit (BVH2Common.cpp:1081-1110) */
+      const f3 pos = add3(ray_pos, scl3(hit->t, ray_dir));
+      const f3 dp = scl3(0.5f * sz, sub3(pos, brick_min_pos));
+      const uint32_t t_off = n->data_offset + v_size * v_size * v_size;
+      f3 col = mk3(0, 0, 0);
+      for (int k = 0; k < 8; k++) {
+        const uint32_t b = A->sdfSBSData[t_off + k];
+        const float wx = (k & 4) ? dp.x : (1 - dp.x);
+        const float wy = (k & 2) ? dp.y : (1 - dp.y);
+        const float wz = (k & 1) ? dp.z : (1 - dp.z);
+        const float w = wx * wy * wz;
+        const f3 cc = scl3(w, mk3(A->sdfSBSDataF[b + 0], A->sdfSBSDataF[b + 1], A->sdfSBSDataF[b + 2]));
+        col = (k == 0) ? cc : add3(col, cc);
+      }
+      col = mk3(sclamp(floorf(255.0f * col.x + 0.5f), 0.0f, 255.0f), sclamp(floorf(255.0f * col.y + 0.5f), 0.0f, 255.0f),
+                sclamp(floorf(255.0f * col.z + 0.5f), 0.0f, 255.0f));
+      hit->coords[0] = col.x + col.y / 256.0f;
+      hit->coords[1] = col.z;
+    }
+  }
+}
+
+/* IntersectAllTrianglesInLeaf, BVH2Common.cpp:1571-1635 (NORMAL_MODE_GEOMETRY). */
+static void triangles(ctx_t* c, f3 ray_pos, f3 ray_dir, float tNear, uint32_t instId, uint32_t geomId,
+                      uint32_t a_start, uint32_t a_count, lrt_hit* hit)
+{
+  const lrt_scene_arrays* A = c->a;
+  const uint32_t* go = A->geomData[geomId].offset;
+  for (uint32_t triId = a_start; triId < a_start + a_count; triId++) {
+    c->cnt[C_TRI_TESTS]++;
+    const uint32_t ia = A->indices[go[0] + triId * 3 + 0];
+    const uint32_t ib = A->indices[go[0] + triId * 3 + 1];
+    const uint32_t ic = A->indices[go[0] + triId * 3 + 2];
+    const f3 Ap = ld3(A->vertPos + 4 * (uint64_t)(go[1] + ia));
+    const f3 Bp = ld3(A->vertPos + 4 * (uint64_t)(go[1] + ib));
+    const f3 Cp = ld3(A->vertPos + 4 * (uint64_t)(go[1] + ic));
+    const f3 edge1 = sub3(Bp, Ap);
+    const f3 edge2 = sub3(Cp, Ap);
+    const f3 pvec = cross3(ray_dir, edge2);
+    const f3 tvec = sub3(ray_pos, Ap);
+    const f3 qvec = cross3(tvec, edge1);
+    const float invDet = 1.0f / dot3(edge1, pvec);
+    const float v = dot3(tvec, pvec) * invDet;
+    const float u = dot3(qvec, ray_dir) * invDet;
+    const float t = dot3(edge2, qvec) * invDet;
+    if (v >= -1e-6f && u >= -1e-6f && (u + v <= 1.0f + 1e-6f) && t > tNear && t < hit->t) {
+      hit->t = t;
+      hit->primId = triId;
+      hit->instId = instId;
+      hit->geomId = geomId | (LRT_TYPE_MESH_TRIANGLE << 24);
+      hit->coords[0] = u;
+      hit->coords[1] = v;
+      if (need_normal(c->p)) {
+        f3 nn = cross3(edge1, edge2);
+        nn = normalize3(matmul4(A->instanceData[instId].transformInvTransposed, nn, 1.0f));
+        const f2 en = encode_normal(nn);
+        hit->coords[2] = en.x;
+        hit->coords[3] = en.y;
+      } else {
+        hit->coords[2] = 0;
+        hit->coords[3] = 0;
+      }
+    }
+  }
+}
+
+/* IntersectAllPrimitivesInLeaf, BVH2Common.cpp:47-124 */
+static uint32_t leaf(ctx_t* c, f3 ray_pos, f3 ray_dir, float tNear, uint32_t aabbId, uint32_t instId,
+                     uint32_t geomId, lrt_hit* hit)
+{
+  const lrt_scene_arrays* A = c->a;
+  const float tPrev = hit->t;
+  c->cnt[C_LEAF_CALLS]++;
+  const uint32_t globalAABBId = A->startEnd[2 * geomId] + aabbId;
+  const uint32_t packed = A->primIdCount[globalAABBId];
+  const uint32_t a_start = packed & START_MASK;
+  const uint32_t a_count = (packed & SIZE_MASK) >> 28;
+  const uint32_t tag = A->geomTags[geomId];
+  switch (tag) {
+    case LRT_TAG_TRIANGLE: triangles(c, ray_pos, ray_dir, tNear, instId, geomId, a_start, a_count, hit); break;
+    case LRT_TAG_SDF_NODE:
+      octree_node(c, A->geomData[geomId].type, ray_pos, ray_dir, tNear, instId, geomId, a_start, hit);
+      break;
+    case LRT_TAG_SDF_BRICK:
+      octree_brick(c, A->geomData[geomId].type, ray_pos, ray_dir, tNear, instId, geomId, a_start, hit);
+      break;
+    default: break;
+  }
+  return (hit->t >= tPrev) ? LRT_TAG_NONE : tag;
+}
+
+/* BVHRT::BVH2TraverseF32, BVH2Common.cpp:3239-3320 */
+static void blas(ctx_t* c, f3 ray_pos, f3 ray_dir, float tNear, uint32_t instId, uint32_t geomId, int stopOnFirstHit,
+                 lrt_hit* hit)
+{
+  const lrt_scene_arrays* A = c->a;
+  const uint32_t bvhOffset = A->geomData[geomId].bvhOffset;
+  uint32_t stack[STACK_SIZE];
+  int top = 0;
+  uint32_t leftNodeOffset = 0;
+  int hitFound = 0;
+  stack[0] = 0;
+  const f3 inv = safe_inverse(ray_dir);
+  while (top >= 0 && !hitFound) {
+    while (top >= 0 && ((leftNodeOffset & LEAF_BIT) == 0)) {
+      c->cnt[C_BLAS_PAIRS]++;
+      const lrt_bvh_node_pair* fat = &A->allNodePairs[bvhOffset + leftNodeOffset];
+      const uint32_t n0 = fat->left.leftOffset, n1 = fat->right.leftOffset;
+      const f2 tm0 = ray_box(ray_pos, inv, ld3(fat->left.boxMin), ld3(fat->left.boxMax));
+      const f2 tm1 = ray_box(ray_pos, inv, ld3(fat->right.boxMin), ld3(fat->right.boxMax));
+      const int h0 = (tm0.x <= tm0.y) && (tm0.y >= tNear) && (tm0.x <= hit->t);
+      const int h1 = (tm1.x <= tm1.y) && (tm1.y >= tNear) && (tm1.x <= hit->t);
+      leftNodeOffset = h0 ? n0 : n1;
+      if (h0 && h1) {
+        if (top >= STACK_SIZE) { c->limits++; return; }
+        leftNodeOffset = (tm0.x <= tm1.x) ? n0 : n1;
+        stack[top] = (tm0.x <= tm1.x) ? n1 : n0;
+        top++;
+      }
+      if (!h0 && !h1) {
+        top--;
+        leftNodeOffset = stack[top > 0 ? top : 0];
+      }
+    }
+    if (top >= 0 && leftNodeOffset != 0xFFFFFFFFu) {
+      const float tNearSdf = smax(tNear, 0.01f); /* SDF_BIAS, :3306-3307 */
+      const uint32_t tag = leaf(c, ray_pos, ray_dir, tNearSdf, leftNodeOffset & START_MASK, instId, geomId, hit);
+      hitFound = (tag != 0) && (tag != LRT_TAG_TRIANGLE || stopOnFirstHit);
+    }
+    top--;
+    leftNodeOffset = stack[top > 0 ? top : 0];
+  }
+}
+
+/* BVHRT::RayQuery_NearestHit, BVH2Common.cpp:3322-3392 */
+static lrt_hit nearest_hit(ctx_t* c, const float pn[4], const float dfar[4])
+{
+  const lrt_scene_arrays* A = c->a;
+  float dirW = dfar[3];
+  const int stopOnFirstHit = (dirW <= 0.0f);
+  if (stopOnFirstHit) dirW *= -1.0f;
+  const f3 pos = ld3(pn), dir = ld3(dfar);
+  const float tmin = pn[3];
+  const f3 inv = safe_inverse(dir);
+  lrt_hit hit;
+  hit.t = dirW;
+  hit.primId = 0xFFFFFFFFu;
+  hit.instId = 0xFFFFFFFFu;
+  hit.geomId = 0xFFFFFFFFu;
+  hit.coords[0] = 1.0f;
+  hit.coords[1] = 0.0f;
+  hit.coords[2] = 0.0f;
+  hit.coords[3] = 0.0f;
+  uint32_t nodeIdx = 0;
+  uint64_t guard = 0;
+  const uint64_t guard_max = 2 * A->nodesTLAS_count + 4;
+  do {
+    uint32_t travFlags = 0, leftOffset = 0;
+    do {
+      if (nodeIdx >= A->nodesTLAS_count || ++guard > guard_max) { c->limits++; goto done; }
+      c->cnt[C_TLAS_NODES]++;
+      const lrt_bvh_node* nd = &A->nodesTLAS[nodeIdx];
+      const f2 bh = ray_box(pos, inv, ld3(nd->boxMin), ld3(nd->boxMax));
+      const uint32_t intersects = (bh.x <= bh.y) && (bh.y > tmin) && (bh.x < hit.t);
+      travFlags = (nd->leftOffset & LEAF_BIT) | intersects;
+      leftOffset = nd->leftOffset;
+      const int leafOrNot = (travFlags & LEAF_BIT) != 0 || (travFlags & 1) == 0;
+      nodeIdx = leafOrNot ? nd->escapeIndex : leftOffset;
+    } while (travFlags != (LEAF_BIT | 1u) && nodeIdx != 0 && nodeIdx < 0xFFFFFFFEu);
+    if (travFlags == (LEAF_BIT | 1u)) {
+      const uint32_t instId = leftOffset & START_MASK;
+      const lrt_instance_data* inst = &A->instanceData[instId];
+      const uint32_t geomId = inst->geomId;
+      c->cnt[C_INSTANCES]++;
+      const f3 rp = matmul4(inst->transformInv, pos, 1.0f);
+      const f3 rd = matmul4(inst->transformInv, dir, 0.0f);
+      blas(c, rp, rd, tmin, instId, geomId, stopOnFirstHit, &hit);
+    }
+  } while (nodeIdx < 0xFFFFFFFEu && !(stopOnFirstHit && hit.primId != 0xFFFFFFFFu));
+done:
+  if (hit.geomId < 0xFFFFFFFFu && ((hit.geomId >> 24) == LRT_TYPE_MESH_TRIANGLE)) {
+    const uint32_t g = hit.geomId & 0x00FFFFFFu;
+    hit.primId = A->primIndices[A->geomData[g].offset[0] / 3 + hit.primId];
+  }
+  if (hit.primId != 0xFFFFFFFFu) c->cnt[C_HITS]++;
+  return hit;
+}
+
+/* Trace n rays (n x {posAndNear, dirAndFar}).  counters may be NULL; it
+ * receives LRT_COUNTER_COUNT sums.  Returns the number of bounded-loop /
+ * bounds events (0 on well-formed scenes). */
+uint64_t lrto_trace(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* rays, lrt_hit* hits,
+                    uint64_t n, uint64_t* counters, int threads)
+{
+  uint64_t total[LRT_COUNTER_COUNT];
+  memset(total, 0, sizeof(total));
+  uint64_t limits = 0;
+  (void)threads;
+#ifdef _OPENMP
+#pragma omp parallel num_threads(threads > 0 ? threads : 1) reduction(+ : limits)
+#endif
+  {
+    uint64_t local[LRT_COUNTER_COUNT];
+    memset(local, 0, sizeof(local));
+    ctx_t c = {arrays, preset, local, 0};
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 256)
+#endif
+    for (int64_t i = 0; i < (int64_t)n; i++) hits[i] = nearest_hit(&c, rays + 8 * i, rays + 8 * i + 4);
+    limits += c.limits;
+#ifdef _OPENMP
+#pragma omp critical
+#endif
+    for (int k = 0; k < LRT_COUNTER_COUNT; k++) total[k] += local[k];
+  }
+  if (counters)
+    for (int k = 0; k < LRT_COUNTER_COUNT; k++) counters[k] = total[k];
+  return limits;
+}
+
+/* Per-ray work counters (n x LRT_COUNTER_COUNT), single-threaded. */
+void lrto_trace_counted(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* rays, lrt_hit* hits,
+                        uint64_t n, uint64_t* per_ray_counters)
+{
+  for (uint64_t i = 0; i < n; i++) {
+    ctx_t c = {arrays, preset, per_ray_counters + i * LRT_COUNTER_COUNT, 0};
+    memset(c.cnt, 0, sizeof(uint64_t) * LRT_COUNTER_COUNT);
+    hits[i] = nearest_hit(&c, rays + 8 * i, rays + 8 * i + 4);
+  }
+}

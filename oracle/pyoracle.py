@@ -1,0 +1,192 @@
+"""Python bindings of the checkers (TEST INFRASTRUCTURE ONLY).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module.  Two checkers:
+
+* ``Port`` — oracle/lrt_oracle.c, the C restatement of the reference ray query,
+  built into oracle/_build/liblrt_oracle.so.
+* ``RefScene`` — the reference's own BVHRT compiled from its sources
+  (oracle/_ref/liblrt_ref.so, bit-parity build; liblrt_ref_fast.so, the
+  reference's Release flags), driven through oracle/ref/ref_harness.cpp.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from graphic_lab_task_b200._abi import (HIT_DTYPE, LRT_COUNTER_COUNT, Preset, SceneArrays, arrays_to_struct,
+                                        parity_preset, struct_to_arrays)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SO = os.path.join(HERE, "_build", "liblrt_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "liblrt_ref.so")
+REF_FAST_SO = os.path.join(HERE, "_ref", "liblrt_ref_fast.so")
+REFERENCE_SRC = "/root/reference"
+
+
+def build(with_reference=True):
+    """Compile the C restatement and, where the reference sources exist, the
+    reference build (oracle/Makefile)."""
+    targets = ["port"]
+    if with_reference and os.path.isdir(REFERENCE_SRC):
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", HERE, "-j8"] + targets, check=True)
+
+
+_port = None
+_refs = {}
+
+
+def port_lib():
+    global _port
+    if _port is None:
+        if not os.path.exists(PORT_SO):
+            build(with_reference=False)
+        lib = C.CDLL(PORT_SO)
+        lib.lrto_trace.restype = C.c_uint64
+        lib.lrto_trace.argtypes = [C.POINTER(SceneArrays), C.POINTER(Preset), C.c_void_p, C.c_void_p, C.c_uint64,
+                                   C.c_void_p, C.c_int]
+        lib.lrto_trace_counted.restype = None
+        lib.lrto_trace_counted.argtypes = [C.POINTER(SceneArrays), C.POINTER(Preset), C.c_void_p, C.c_void_p,
+                                           C.c_uint64, C.c_void_p]
+        _port = lib
+    return _port
+
+
+def ref_available(fast=False):
+    return os.path.exists(REF_FAST_SO if fast else REF_SO)
+
+
+def ref_lib(fast=False):
+    key = bool(fast)
+    if key not in _refs:
+        path = REF_FAST_SO if fast else REF_SO
+        if not os.path.exists(path):
+            raise RuntimeError("reference build %s is missing (make -C oracle ref)" % path)
+        lib = C.CDLL(path)
+        lib.lrtr_create.restype = C.c_void_p
+        lib.lrtr_create.argtypes = [C.c_char_p, C.c_char_p]
+        lib.lrtr_destroy.argtypes = [C.c_void_p]
+        lib.lrtr_set_preset.argtypes = [C.c_void_p, C.POINTER(Preset)]
+        for fn in ("lrtr_add_triangles", "lrtr_add_frame_octree", "lrtr_add_svs", "lrtr_add_sbs",
+                   "lrtr_add_instance"):
+            getattr(lib, fn).restype = C.c_uint32
+        lib.lrtr_add_triangles.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64]
+        lib.lrtr_add_frame_octree.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64]
+        lib.lrtr_add_svs.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64]
+        lib.lrtr_add_sbs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64,
+                                     C.c_void_p, C.c_uint64]
+        lib.lrtr_add_instance.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+        lib.lrtr_commit.argtypes = [C.c_void_p]
+        lib.lrtr_export.argtypes = [C.c_void_p, C.POINTER(SceneArrays)]
+        lib.lrtr_import.argtypes = [C.c_void_p, C.POINTER(SceneArrays)]
+        lib.lrtr_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_int]
+        _refs[key] = lib
+    return _refs[key]
+
+
+def port_trace(arrays, rays, preset=None, threads=os.cpu_count(), counters=False):
+    """Trace with the C restatement.  Returns hits (and summed counters)."""
+    lib = port_lib()
+    s, keep = arrays_to_struct(arrays)
+    p = preset if preset is not None else parity_preset()
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    hits = np.zeros(len(rays), dtype=HIT_DTYPE)
+    cnt = np.zeros(LRT_COUNTER_COUNT, dtype=np.uint64)
+    limits = lib.lrto_trace(C.byref(s), C.byref(p), rays.ctypes.data, hits.ctypes.data, len(rays),
+                            cnt.ctypes.data, int(threads))
+    del keep
+    if counters:
+        return hits, cnt, int(limits)
+    return hits
+
+
+def port_trace_per_ray_counters(arrays, rays, preset=None):
+    lib = port_lib()
+    s, keep = arrays_to_struct(arrays)
+    p = preset if preset is not None else parity_preset()
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    hits = np.zeros(len(rays), dtype=HIT_DTYPE)
+    cnt = np.zeros((len(rays), LRT_COUNTER_COUNT), dtype=np.uint64)
+    lib.lrto_trace_counted(C.byref(s), C.byref(p), rays.ctypes.data, hits.ctypes.data, len(rays), cnt.ctypes.data)
+    del keep
+    return hits, cnt
+
+
+class RefScene:
+    """A reference BVHRT (CreateSceneRT("BVH2Common", ...)) in oracle/_ref."""
+
+    def __init__(self, build_name="cbvh_embree2", layout_name="SuperTreeletAlignedMerged4", fast=False,
+                 preset=None):
+        self.lib = ref_lib(fast)
+        self.h = self.lib.lrtr_create(build_name.encode(), layout_name.encode())
+        if not self.h:
+            raise RuntimeError("CreateSceneRT failed")
+        self.set_preset(preset if preset is not None else parity_preset())
+
+    def close(self):
+        if self.h:
+            self.lib.lrtr_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_preset(self, preset):
+        self.preset = preset
+        self.lib.lrtr_set_preset(self.h, C.byref(preset))
+
+    def add_triangles(self, verts, tris):
+        v = np.ascontiguousarray(verts, dtype=np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(tris, dtype=np.uint32).reshape(-1)
+        return self.lib.lrtr_add_triangles(self.h, v.ctypes.data, len(v), t.ctypes.data, len(t))
+
+    def add_frame_octree(self, nodes):
+        return self.lib.lrtr_add_frame_octree(self.h, nodes.ctypes.data, len(nodes))
+
+    def add_svs(self, nodes):
+        return self.lib.lrtr_add_svs(self.h, nodes.ctypes.data, len(nodes))
+
+    def add_sbs(self, header, nodes, values, values_f=None):
+        hdr = np.ascontiguousarray(header)
+        vf = np.zeros(0, np.float32) if values_f is None else np.ascontiguousarray(values_f, np.float32)
+        vals = np.ascontiguousarray(values, np.uint32)
+        return self.lib.lrtr_add_sbs(self.h, hdr.ctypes.data, nodes.ctypes.data, len(nodes), vals.ctypes.data,
+                                     len(vals), vf.ctypes.data if len(vf) else None, len(vf))
+
+    def add_instance(self, geom_id, matrix_col_major):
+        m = np.ascontiguousarray(matrix_col_major, dtype=np.float32).reshape(16)
+        return self.lib.lrtr_add_instance(self.h, geom_id, m.ctypes.data)
+
+    def commit(self):
+        self.lib.lrtr_commit(self.h)
+
+    def export(self):
+        s = SceneArrays()
+        self.lib.lrtr_export(self.h, C.byref(s))
+        return struct_to_arrays(s)
+
+    def import_arrays(self, arrays):
+        s, keep = arrays_to_struct(arrays)
+        self.lib.lrtr_import(self.h, C.byref(s))
+        del keep
+
+    def trace(self, rays, threads=1):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        hits = np.zeros(len(rays), dtype=HIT_DTYPE)
+        self.lib.lrtr_trace(self.h, rays.ctypes.data, hits.ctypes.data, len(rays), int(threads))
+        return hits
+
+
+def ref_trace(arrays, rays, preset=None, threads=1, fast=False):
+    """Trace already-flattened arrays with the reference BVHRT."""
+    sc = RefScene(fast=fast, preset=preset)
+    try:
+        sc.import_arrays(arrays)
+        return sc.trace(rays, threads=threads)
+    finally:
+        sc.close()
