@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 nearest-hit ray query (BVHRT::RayQuery_NearestHit).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step"): one plain nearest-hit pass over 1920x1080 primary rays
+of a sparse-brick-set SDF — the union of 64 seeded spheres sampled on a
+virtual 512^3 grid, 8^3-voxel bricks with a 1-voxel border, fp32 distances in
+the indexed layout, camera at (0,0,3) looking at the origin, 60 degree fovy,
+tmin 1e-4.  Rays and the scene are resident in HBM when timing starts; the
+L2 is flushed (a 256 MiB write) before every timed step and each step is
+timed with CUDA events on the launching stream.
+
+Multi-GPU: rays are independent, so N ranks each trace the full workload on
+their own GPU (replicas, weak scaling); the time is the max over ranks.
+
+Printed JSON (rank 0): value = Mrays/s over all ranks; roofline of the trace
+kernel against the measured HBM copy bandwidth; e2e = the same metric through
+lrt_trace_nearest with pinned host buffers (host->device rays, device->host
+hits inside the timed region); cpu_baseline = the reference's own CPU code
+(compiled from its sources, OpenMP over rays) on a bounded sample of the
+same rays and scene arrays.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+WIDTH, HEIGHT = 1920, 1080
+GRID, BRICK, PAD = 512, 8, 1
+N_SPHERES, SPHERE_SEED = 64, 1
+TMIN, TMAX = 1e-4, 1e9
+WORKLOAD = "sbs_sphere_union_512cube_1920x1080"
+METRIC = "Mrays/s (plain nearest-hit, SBS 1920x1080)"
+FLUSH_BYTES = 256 << 20
+
+
+def workload_scene():
+    from graphic_lab_task_b200 import workloads as wl
+    sph = wl.spheres(N_SPHERES, seed=SPHERE_SEED)
+    model = wl.sbs_from_spheres(sph, grid_res=GRID, brick_size=BRICK, brick_pad=PAD)
+    cam = wl.camera((0, 0, 3), width=WIDTH, height=HEIGHT, tnear=TMIN, tfar=TMAX)
+    return model, cam
+
+
+def config_dict(extra=None):
+    d = {"workload": WORKLOAD, "rays_per_step": WIDTH * HEIGHT, "image": [WIDTH, HEIGHT], "virtual_grid": GRID,
+         "brick_size": BRICK, "brick_pad": PAD, "spheres": N_SPHERES, "sbs_layout": "ID32F_IRGB32F (fp32)",
+         "preset": "LAMBERT_NO_TEX, ST, GEOMETRY normals, TRILINEAR, VOLUME", "l2": "flushed before every step (256 MiB)"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, power, reasons = [], None, [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+                power.append(float(p[3]))
+            except ValueError:
+                continue
+            for name, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+# ---------------------------------------------------------------------------
+# reference CPU path
+# ---------------------------------------------------------------------------
+def cpu_reference_rate(ref_scene, rays, seconds=12.0, threads=None):
+    """Mrays/s of BVHRT::RayQuery_NearestHit on a bounded sample of about
+    `seconds` of CPU work: a strided subset of the rays when one pass over all
+    of them takes longer, else whole passes repeated.  Returns
+    (Mrays/s, rays traced, threads, wall s, description)."""
+    threads = threads or os.cpu_count()
+    n = len(rays)
+    probe = rays[:: max(1, n // 65536)]
+    t0 = time.perf_counter()
+    ref_scene.trace(probe, threads=threads)
+    rate = len(probe) / max(time.perf_counter() - t0, 1e-6)
+    want = rate * seconds
+    if want < n:
+        sample = rays[np.linspace(0, n - 1, int(max(len(probe), want))).astype(np.int64)]
+        passes, desc = 1, "%d of %d rays (strided over the image)" % (len(sample), n)
+    else:
+        sample = rays
+        passes = int(max(1, round(want / n)))
+        desc = "%d passes over all %d rays" % (passes, n)
+    t0 = time.perf_counter()
+    for _ in range(passes):
+        ref_scene.trace(sample, threads=threads)
+    dt = time.perf_counter() - t0
+    return passes * len(sample) / dt / 1e6, passes * len(sample), threads, dt, desc
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's own host build (AddGeom_SdfSBS,
+    CommitScene) and CPU ray query on all host cores, rank 0 only."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import pyoracle as po
+    from graphic_lab_task_b200 import workloads as wl
+    if not po.ref_available(fast=True):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/liblrt_ref_fast.so not built (make -C oracle ref)"}))
+        return
+    (hdr, nodes, vals, vf), cam = workload_scene()
+    rays = wl.eye_rays_host(cam)
+    ref = po.RefScene(fast=True)
+    g = ref.add_sbs(hdr, nodes, vals, vf)
+    ref.add_instance(g, wl.IDENTITY)
+    ref.commit()
+    threads = os.cpu_count()
+    n = len(rays)
+    probe = rays[:: max(1, n // 32768)]
+    t0 = time.perf_counter()
+    ref.trace(probe, threads=threads)
+    rate = len(probe) / max(time.perf_counter() - t0, 1e-6)
+    # each step is a strided sample sized so that all steps take ~60 s
+    per_step = max(len(probe), min(n, int(rate * 60.0 / max(1, args.steps + args.warmup))))
+    sample = rays[np.linspace(0, n - 1, per_step).astype(np.int64)]
+    for _ in range(args.warmup):
+        ref.trace(sample[: max(1, per_step // 8)], threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ref.trace(sample, threads=threads)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * sum(times) / len(times)
+    value = per_step / (ms * 1e-3) / 1e6
+    desc = "%d of %d rays (strided) per step, OpenMP over rays" % (per_step, n)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "config": config_dict(),
+        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": "reference", "sample": desc},
+        "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def read_traffic():
+    """dram bytes per trace launch from the committed ncu summary, if any."""
+    p = os.path.join(HERE, "profiles", "k_trace_sbs_1920x1080.txt")
+    if not os.path.exists(p):
+        return None
+    for ln in open(p):
+        if ln.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(ln.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from graphic_lab_task_b200 import SceneRT, workloads as wl
+    from graphic_lab_task_b200._abi import COUNTER_NAMES
+    from graphic_lab_task_b200.workbytes import algorithmic_bytes
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    (hdr, nodes, vals, vf), cam = workload_scene()
+    sc = SceneRT()
+    g = sc.AddGeom_SdfSBS(hdr, nodes, vals, vf)
+    sc.AddInstance(g, wl.IDENTITY)
+    sc.CommitScene()
+    n = WIDTH * HEIGHT
+    rays = torch.empty(n * 8, dtype=torch.float32, device=dev)
+    hits = torch.empty(n * 8, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    sc.generate_eye_rays(cam, rays.data_ptr(), sp)
+    # counting pass (untimed): algorithmic bytes of one launch
+    sc.trace_device(rays.data_ptr(), hits.data_ptr(), n, stream=sp, count_work=True)
+    sc.sync(stream=sp, read_counters=True)
+    counters = sc.work_counters()
+    hit_count = int(counters[list(COUNTER_NAMES).index("hits")])
+    bytes_per_launch = algorithmic_bytes(counters, n, sbs_colour_hits=hit_count)
+    for _ in range(args.warmup):
+        sc.trace_device(rays.data_ptr(), hits.data_ptr(), n, stream=sp)
+    sc.sync(stream=sp)
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local_rank)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    time.sleep(0.3)
+    for i in range(args.steps):
+        flush.zero_()
+        starts[i].record(stream)
+        sc.trace_device(rays.data_ptr(), hits.data_ptr(), n, stream=sp)
+        ends[i].record(stream)
+    torch.cuda.synchronize(dev)
+    sc.sync(stream=sp)
+    kernel_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    # end to end through the public API with pinned host buffers
+    host_rays = torch.empty(n * 8, dtype=torch.float32, pin_memory=True)
+    host_rays.copy_(rays.cpu())
+    host_hits = torch.empty(n * 8, dtype=torch.float32, pin_memory=True)
+    sc.trace_host(host_rays.data_ptr(), host_hits.data_ptr(), n)
+    e_s = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    e_e = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    for i in range(args.steps):
+        flush.zero_()
+        e_s[i].record(stream)
+        sc.trace_host(host_rays.data_ptr(), host_hits.data_ptr(), n)
+        e_e[i].record(stream)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    e2e_ms = [s.elapsed_time(e) for s, e in zip(e_s, e_e)]
+    t = torch.tensor([sum(kernel_ms), sum(e2e_ms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_kernel_ms, total_e2e_ms = float(t[0]), float(t[1])
+    ms = total_kernel_ms / args.steps
+    value = world * n * args.steps / (total_kernel_ms * 1e-3) / 1e6
+    e2e_value = world * n * args.steps / (total_e2e_ms * 1e-3) / 1e6
+    if rank != 0:
+        return
+    peaks = {}
+    pp = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(pp):
+        peaks = json.load(open(pp))
+    peak = peaks.get("hbm_gbs")
+    peak_src = "measured" if peak else "fallback"
+    peak = peak or 6650.0
+    achieved = bytes_per_launch / (ms * 1e-3) / 1e9
+    traffic = read_traffic()
+    out = {
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded 64-sphere SDF union, no dataset)",
+        "config": config_dict({"parallelism": "replicas" if world > 1 else "single"}),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": peak_src,
+                     "algorithmic_bytes_per_launch": bytes_per_launch,
+                     "bytes_per_ray": bytes_per_launch / n, "kernel": "k_trace (exact build)"},
+        "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * 32,
+                "ms_per_step": total_e2e_ms / args.steps},
+        "clocks": clk,
+        "gpu_launches": 2 * args.steps,
+        "work_counters": {k: int(v) for k, v in zip(COUNTER_NAMES, counters)},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(sc, rays, n)
+    print(json.dumps(out))
+
+
+def cpu_baseline(sc, rays_dev, n):
+    """The reference CPU ray query (oracle/_ref, Release flags) on the same
+    scene arrays and rays, all host cores, bounded sample."""
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    try:
+        import pyoracle as po
+    except ImportError as e:
+        return {"value": None, "unit": "Mrays/s", "cores": 0, "kind": "reference", "sample": "unavailable: %s" % e}
+    if not po.ref_available(fast=True):
+        return {"value": None, "unit": "Mrays/s", "cores": 0, "kind": "reference",
+                "sample": "unavailable: oracle/_ref not built"}
+    rays = rays_dev.cpu().numpy().reshape(-1, 8)
+    ref = po.RefScene(fast=True)
+    ref.import_arrays(sc.export_arrays())
+    rate, m, threads, dt, desc = cpu_reference_rate(ref, rays)
+    ref.close()
+    return {"value": rate, "unit": "Mrays/s", "cores": threads, "kind": "reference",
+            "sample": "%s, %.1f s wall, OpenMP over rays, same scene arrays as the GPU" % (desc, dt)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -137,5 +137,5 @@ def struct_to_arrays(s):
             out[name] = np.zeros(0, dtype=dt)
             continue
         buf = (C.c_char * (n * dt.itemsize)).from_address(p)
-        out[name] = np.frombuffer(bytes(buf), dtype=dt).copy()
+        out[name] = np.frombuffer(buf, dtype=dt).copy()
     return out

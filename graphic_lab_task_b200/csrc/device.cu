@@ -102,6 +102,7 @@ lrt_status launch(lrt_scene* s, const float4* rays, lrt_hit* hits, uint64_t n, c
   DeviceScene* d = s->dev;
   DevScene S = d->S;
   S.flags = preset_flags(s->preset);
+  S.voxelStepCap = s->voxelStepCap ? s->voxelStepCap : kMaxVoxelSteps;
   const bool count = (flags & LRT_TRACE_COUNT_WORK) != 0;
   cudaError_t e = cudaMemsetAsync(&slot->work, 0, count ? offsetof(StreamSlot, err) : sizeof(unsigned long long),
                                   stream);
@@ -285,6 +286,13 @@ lrt_status lrt_ray_query_any_hit(lrt_scene* s, const float pn[4], const float df
   lrt_status st = lrt_ray_query_nearest_hit(s, pn, d2, &h);
   if (st != LRT_OK) return st;
   *out = h.geomId != 0xFFFFFFFFu;
+  return LRT_OK;
+}
+
+lrt_status lrt_set_voxel_step_limit(lrt_scene* s, uint32_t steps)
+{
+  if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  s->voxelStepCap = steps;
   return LRT_OK;
 }
 

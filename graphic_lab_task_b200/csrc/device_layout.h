@@ -93,7 +93,7 @@ struct DevScene {
   const float* sbsDense;
   const DevSbs* sbs;
   uint32_t flags;
-  uint32_t numRays; // unused by the trace kernel; kept for diagnostics
+  uint32_t voxelStepCap; // bounded SBS voxel march (kMaxVoxelSteps unless set)
 };
 
 struct DevCamera {

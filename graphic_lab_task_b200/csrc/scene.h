@@ -65,6 +65,7 @@ struct lrt_scene {
   lrt::HostArrays h;
   lrt_preset preset;
   uint32_t primsInLeaf = 2;
+  uint32_t voxelStepCap = 0; // 0 = kMaxVoxelSteps
   bool committed = false;
   lrt::SceneInfo info;
   lrt::DeviceScene* dev = nullptr;

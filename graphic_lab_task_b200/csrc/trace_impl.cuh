@@ -189,7 +189,7 @@ __device__ void octree_brick(Ctx<COUNT>& c, const DevGeom& g, f3 ray_pos, f3 ray
   float values[8];
   uint32_t steps = 0;
   while (bnf.x < bnf.y && hit.t == old_t) {
-    if (steps++ >= kMaxVoxelSteps) {
+    if (steps++ >= S.voxelStepCap) {
       c.err |= kErrVoxelCap;
       break;
     }

@@ -25,7 +25,7 @@ EXPORTED = (
     "lrt_clear_geom", "lrt_add_geom_triangles3f", "lrt_add_geom_aabb", "lrt_add_geom_sdf_frame_octree",
     "lrt_add_geom_sdf_svs", "lrt_add_geom_sdf_sbs", "lrt_clear_scene", "lrt_add_instance", "lrt_commit_scene",
     "lrt_scene_upload", "lrt_scene_export", "lrt_trace_nearest", "lrt_trace_sync", "lrt_ray_query_nearest_hit",
-    "lrt_ray_query_any_hit", "lrt_get_work_counters", "lrt_generate_eye_rays",
+    "lrt_ray_query_any_hit", "lrt_get_work_counters", "lrt_generate_eye_rays", "lrt_set_voxel_step_limit",
     "lrt_wl_noisy_sphere", "lrt_wl_spheres", "lrt_wl_sphere_sdf", "lrt_wl_sbs_from_spheres",
     "lrt_wl_frame_octree_from_spheres", "lrt_wl_svs_from_spheres",
 )
@@ -72,6 +72,7 @@ def lib():
         "lrt_ray_query_nearest_hit": [vp, vp, vp, vp],
         "lrt_ray_query_any_hit": [vp, vp, vp, P(C.c_int32)],
         "lrt_get_work_counters": [vp, vp],
+        "lrt_set_voxel_step_limit": [vp, u32],
         "lrt_generate_eye_rays": [vp, vp, vp, vp],
         "lrt_wl_noisy_sphere": [u32, C.c_float, C.c_float, u64, vp, vp, P(u64), P(u64)],
         "lrt_wl_spheres": [u32, C.c_float, C.c_float, C.c_float, u64, vp],
@@ -215,6 +216,12 @@ class SceneRT:
         self._check(lib().lrt_trace_nearest(self.h, r.ctypes.data, hits.ctypes.data, len(r), None, flags))
         return hits
 
+    def trace_host(self, rays_ptr, hits_ptr, n, fast_math=False):
+        """Synchronous trace of host buffers (pinned host memory copies fastest):
+        host->device copy, kernel and device->host copy in one call."""
+        flags = LRT_TRACE_FAST_MATH if fast_math else 0
+        self._check(lib().lrt_trace_nearest(self.h, C.c_void_p(rays_ptr), C.c_void_p(hits_ptr), n, None, flags))
+
     def trace_device(self, rays_ptr, hits_ptr, n, stream=0, fast_math=False, count_work=False):
         """Asynchronous trace of device buffers (16-byte aligned) on `stream`."""
         flags = LRT_TRACE_DEVICE_POINTERS | (LRT_TRACE_FAST_MATH if fast_math else 0) | \
@@ -224,6 +231,9 @@ class SceneRT:
 
     def sync(self, stream=0, read_counters=False):
         self._check(lib().lrt_trace_sync(self.h, C.c_void_p(stream) if stream else None, int(read_counters)))
+
+    def set_voxel_step_limit(self, steps):
+        self._check(lib().lrt_set_voxel_step_limit(self.h, steps))
 
     def work_counters(self):
         c = np.zeros(LRT_COUNTER_COUNT, dtype=np.uint64)

@@ -109,6 +109,14 @@ def col_major(m):
 IDENTITY = col_major(np.eye(4))
 
 
+def similarity(scale, translation):
+    """Column-major matrix of a uniform scale followed by a translation."""
+    m = np.eye(4)
+    m[:3, :3] *= scale
+    m[:3, 3] = translation
+    return col_major(m)
+
+
 def look_at(eye, center, up):
     """LiteMath lookAt (LiteMath.h:3315-3340): the world-to-view matrix."""
     eye, center, up = (np.asarray(v, np.float64) for v in (eye, center, up))

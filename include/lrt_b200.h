@@ -298,6 +298,12 @@ lrt_status lrt_ray_query_nearest_hit(lrt_scene* scene, const float pos_and_near[
 lrt_status lrt_ray_query_any_hit(lrt_scene* scene, const float pos_and_near[4], const float dir_and_far[4],
                                  int32_t* hit_out);
 
+/* Iteration cap of the SBS voxel march per brick (default 4096).  The
+ * reference loop (BVH2Common.cpp:919-1032) has no cap; a ray that reaches
+ * the cap stops marching that brick and the trace returns
+ * LRT_ERR_DEVICE_LIMIT instead of hanging.  0 restores the default. */
+lrt_status lrt_set_voxel_step_limit(lrt_scene* scene, uint32_t steps);
+
 /* Work counters of the last LRT_TRACE_COUNT_WORK trace (summed over rays):
  * TLAS node visits, instances entered, BLAS node-pair visits, leaf calls,
  * triangle tests, SBS brick entries, SBS voxel visits, ST steps,

@@ -1,0 +1,71 @@
+"""Shared helpers of the tests: golden fixtures and hit comparison."""
+import glob
+import os
+
+import numpy as np
+
+from graphic_lab_task_b200._abi import ARRAY_FIELDS, HIT_DTYPE, parity_preset
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+MISS = 0xFFFFFFFF
+
+
+def golden_names():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def load_golden(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    arrays = {}
+    for field, dt in ARRAY_FIELDS:
+        raw = z["arr_" + field]
+        if dt.subdtype is not None:  # uint2 / float4 fields
+            base, shape = dt.subdtype
+            arrays[field] = raw.view(base).reshape((-1,) + shape)
+        else:
+            arrays[field] = raw.view(dt) if raw.size else np.zeros(0, dt)
+    preset = parity_preset()
+    p = z["preset"]
+    (preset.render_mode, preset.sdf_node_intersect, preset.normal_mode, preset.ray_gen_mode,
+     preset.interpolation_mode, preset.representation_mode, preset.spp, preset.fixed_lod) = [int(x) for x in p]
+    hits = z["hits"].reshape(-1).view(HIT_DTYPE)
+    return arrays, z["rays"], hits, preset
+
+
+def bit_equal(a, b):
+    """Per-ray bitwise equality of two hit arrays."""
+    return (a.view(np.uint8).reshape(len(a), 32) == b.view(np.uint8).reshape(len(b), 32)).all(axis=1)
+
+
+def hit_summary(got, want):
+    same = bit_equal(got, want)
+    bad = np.nonzero(~same)[0]
+    return "%d/%d bit-identical; first mismatches %s" % (same.sum(), len(same), [
+        (int(i), tuple(got[i].tolist()), tuple(want[i].tolist())) for i in bad[:3]])
+
+
+def decode_normal(e):
+    """decode_normal (utils/raytracing/render_common.h:257-266), vectorised."""
+    e = np.asarray(e, np.float64)
+    v = np.stack([e[:, 0], e[:, 1], 1.0 - np.abs(e[:, 0]) - np.abs(e[:, 1])], axis=1)
+    neg = v[:, 2] < 0
+    vx = v[neg, 0].copy()
+    v[neg, 0] = (1.0 - np.abs(v[neg, 1])) * np.where(vx >= 0, 1.0, -1.0)
+    v[neg, 1] = (1.0 - np.abs(vx)) * np.where(v[neg, 1] >= 0, 1.0, -1.0)
+    return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+
+def tolerance_report(got, want, rays=None):
+    """Compares with the hot-path tolerances: ids exact, t within 1e-5
+    relative, decoded normals within 1e-4.  Rays whose hit status or ids
+    differ are returned separately (near ties / silhouettes)."""
+    hg, hw = got["primId"] != MISS, want["primId"] != MISS
+    ids = (got["primId"] == want["primId"]) & (got["instId"] == want["instId"]) & (got["geomId"] == want["geomId"])
+    both = hg & hw & ids
+    rel_t = np.abs(got["t"][both].astype(np.float64) - want["t"][both]) / np.maximum(np.abs(want["t"][both]), 1e-30)
+    ng = decode_normal(got["coords"][both][:, 2:4])
+    nw = decode_normal(want["coords"][both][:, 2:4])
+    dn = np.abs(ng - nw).max(axis=1) if len(ng) else np.zeros(0)
+    return {"id_mismatch": int((~ids).sum()), "max_rel_t": float(rel_t.max()) if len(rel_t) else 0.0,
+            "max_normal_err": float(dn.max()) if len(dn) else 0.0, "t_fail": int((rel_t > 1e-5).sum()),
+            "n_fail": int((dn > 1e-4).sum()), "mismatch_idx": np.nonzero(~ids)[0]}

@@ -1,0 +1,157 @@
+"""The product's scene assembly (csrc/scene.cpp): flattened arrays with the
+reference's layouts, traced identically by the reference and the oracle, and
+upload validation of malformed arrays (no GPU needed)."""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from graphic_lab_task_b200 import LrtError, SceneRT, workloads as wl
+from helpers import MISS, bit_equal, hit_summary
+
+LEAF = 0x80000000
+
+
+def build_mixed(seed=0, n_inst=8):
+    sph = wl.spheres(12, seed=200 + seed)
+    sc = SceneRT()
+    v, t = wl.noisy_sphere(20, seed=seed)
+    gm = sc.AddGeom_Triangles3f(v, t)
+    hdr, nodes, vals, vf = wl.sbs_from_spheres(sph, grid_res=32, brick_size=4, brick_pad=1)
+    gb = sc.AddGeom_SdfSBS(hdr, nodes, vals, vf)
+    go = sc.AddGeom_SdfFrameOctree(wl.frame_octree_from_spheres(sph, 4))
+    gs = sc.AddGeom_SdfSVS(wl.svs_from_spheres(sph, 4))
+    for i, m in enumerate(wl.random_instances(n_inst, seed=seed, scale=(0.3, 0.8), trans=1.2)):
+        sc.AddInstance([gm, gb, go, gs][i % 4], m)
+    sc.CommitScene(host_only=True)
+    return sc, (v, t)
+
+
+def test_blas_layout_matches_reference_conventions():
+    sc, (v, t) = build_mixed()
+    a = sc.export_arrays()
+    pairs, gd, se = a["allNodePairs"], a["geomData"], a["startEnd"]
+    for g in range(len(gd)):
+        base = int(gd["bvhOffset"][g])
+        a0, a1 = int(se[g][0]), int(se[g][1])
+        seen = set()
+        stack = [0]
+        leaves = 0
+        while stack:
+            k = stack.pop()
+            assert k not in seen
+            seen.add(k)
+            for side in ("left", "right"):
+                lo = int(pairs[base + k][side]["leftOffset"])
+                if lo & LEAF:
+                    if lo != 0xFFFFFFFF and lo != LEAF:
+                        leaves += 1
+                        assert (lo & 0x0FFFFFFF) < a1 - a0
+                        assert (lo >> 28) & 7 == 1      # Pack(id, 1)
+                else:
+                    assert lo > k                       # depth-first pre-order
+                    stack.append(lo)
+        assert leaves == a1 - a0
+    # triangle leaves: primIdCount packs (start, count <= primsInLeaf), m_indices is the reordered index buffer
+    g = 0
+    pc = a["primIdCount"][se[g][0]:se[g][1]]
+    counts = (pc >> 28) & 7
+    assert counts.min() >= 1 and counts.max() <= 2 and counts.sum() == len(t)
+    assert np.array_equal(a["indices"].reshape(-1, 3)[:len(t)], t[a["primIndices"][:len(t)]])
+
+
+def test_tlas_escape_layout():
+    sc, _ = build_mixed(n_inst=13)
+    nodes = sc.export_arrays()["nodesTLAS"]
+    assert nodes[0]["escapeIndex"] == 1 and nodes[1]["escapeIndex"] == 0xFFFFFFFE
+    leaves = set()
+    stack = [(0, 0xFFFFFFFE)]
+    while stack:
+        a, esc = stack.pop()
+        assert nodes[a]["escapeIndex"] == a + 1 and nodes[a + 1]["escapeIndex"] == esc
+        for j in (0, 1):
+            lo = int(nodes[a + j]["leftOffset"])
+            if lo & LEAF:
+                leaves.add(lo & 0x0FFFFFFF)
+            else:
+                stack.append((lo, int(nodes[a + j]["escapeIndex"])))
+    assert leaves == set(range(13))
+
+
+def test_single_instance_tlas_is_one_leaf():
+    sc = SceneRT()
+    v, t = wl.noisy_sphere(8)
+    sc.AddInstance(sc.AddGeom_Triangles3f(v, t), wl.IDENTITY)
+    sc.CommitScene(host_only=True)
+    n = sc.export_arrays()["nodesTLAS"]
+    assert len(n) == 1 and n[0]["leftOffset"] == LEAF and n[0]["escapeIndex"] == 0xFFFFFFFF
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_product_arrays_trace_like_reference(seed):
+    sc, _ = build_mixed(seed)
+    arrays = sc.export_arrays()
+    rays = wl.eye_rays_host(wl.camera((0.3, 0.9, 3.2), width=48, height=36))
+    rays = np.concatenate([rays, rays[::5] * np.array([1, 1, 1, 1, 1, 1, 1, -1], np.float32)])
+    got, cnt, lim = po.port_trace(arrays, rays, counters=True)
+    assert lim == 0 and (got["primId"] != MISS).sum() > 100
+    if po.ref_available():
+        want = po.ref_trace(arrays, rays)
+        assert bit_equal(got, want).all(), hit_summary(got, want)
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference build absent (make -C oracle ref)")
+def test_triangle_hits_independent_of_builder():
+    """Nearest triangle hits do not depend on the tree: the product builder
+    and the reference builder give the same answers on a mesh."""
+    v, t = wl.noisy_sphere(40, seed=3)
+    rays = wl.eye_rays_host(wl.camera((0, 0, 3), width=64, height=64))
+    ref = po.RefScene()
+    ref.add_instance(ref.add_triangles(v, t), wl.IDENTITY)
+    ref.commit()
+    want = ref.trace(rays)
+    sc = SceneRT()
+    sc.AddInstance(sc.AddGeom_Triangles3f(v, t), wl.IDENTITY)
+    sc.CommitScene(host_only=True)
+    got = po.port_trace(sc.export_arrays(), rays)
+    assert bit_equal(got, want).all(), hit_summary(got, want)
+
+
+def _upload_error(arrays):
+    sc = SceneRT()
+    with pytest.raises(LrtError) as e:
+        sc.upload_arrays(arrays)
+    return e.value
+
+
+def test_upload_validation_rejects_malformed_arrays():
+    sc, _ = build_mixed()
+    good = sc.export_arrays()
+
+    bad = {k: v.copy() for k, v in good.items()}
+    bad["nodesTLAS"]["leftOffset"][0] = LEAF | (1 << 28) | 999
+    assert _upload_error(bad).status == 2
+
+    bad = {k: v.copy() for k, v in good.items()}
+    bad["nodesTLAS"]["escapeIndex"][1] = 0
+    assert _upload_error(bad).status == 2
+
+    bad = {k: v.copy() for k, v in good.items()}
+    pairs = bad["allNodePairs"]
+    inner = np.nonzero((pairs["left"]["leftOffset"] & LEAF) == 0)[0]
+    pairs["left"]["leftOffset"][inner[1]] = 0        # points back at the root pair: a cycle
+    assert _upload_error(bad).status == 2
+
+    bad = {k: v.copy() for k, v in good.items()}
+    bad["sdfSBSData"] = bad["sdfSBSData"][:-100]
+    assert _upload_error(bad).status == 2
+
+    bad = {k: v.copy() for k, v in good.items()}
+    bad["instanceData"]["geomId"][0] = 77
+    err = _upload_error(bad)
+    assert err.status == 2 and "geometry 77" in str(err)
+
+
+def test_unsupported_presets_are_reported():
+    from graphic_lab_task_b200 import default_preset
+    sc = SceneRT(preset=default_preset())  # ANALYTIC node intersection, VERTEX normals
+    assert sc.GetPreset().sdf_node_intersect == 1

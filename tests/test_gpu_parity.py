@@ -1,0 +1,150 @@
+"""Parity of the sm_100a kernels, called through the C-ABI, with the
+reference (golden vectors) and with the oracle on the benchmark workloads.
+
+Bar: the exact build (the default) is bit-identical to the reference CPU path
+on every ray.  The FMA build (LRT_TRACE_FAST_MATH) must give the same
+geometry/instance/primitive ids except on near ties and silhouette rays,
+t within 1e-4 relative on rays with equal ids.  Its SDF normals are only
+bounded loosely (0.1 on the decoded vector): the reference's SDF normals are
+central differences with h = 0.001 voxel (BVH2Common.cpp:659-673), which
+magnify a one-ulp change of the contracted trilinear sums about 500-fold, and
+on 8-bit quantised SVS voxels that reaches a few 1e-2.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from graphic_lab_task_b200 import SceneRT, workloads as wl
+from helpers import MISS, bit_equal, golden_names, hit_summary, load_golden, tolerance_report
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_uploaded_reference_arrays_match_reference_hits(cuda, name):
+    """Drop-in path: arrays flattened by the reference's host code go through
+    lrt_scene_upload; hits equal the reference's bit for bit."""
+    arrays, rays, want, preset = load_golden(name)
+    sc = SceneRT(preset=preset)
+    sc.upload_arrays(arrays)
+    got = sc.RayQuery_NearestHitBatch(rays)
+    assert bit_equal(got, want).all(), hit_summary(got, want)
+    fast = sc.RayQuery_NearestHitBatch(rays, fast_math=True)
+    rep = tolerance_report(fast, want)
+    assert rep["id_mismatch"] <= max(1, len(rays) // 1000), rep
+    assert rep["max_rel_t"] <= 1e-4 and rep["max_normal_err"] <= 0.1, rep
+
+
+def test_single_ray_api_matches_batch(cuda):
+    arrays, rays, want, preset = load_golden("hand_triangle")
+    sc = SceneRT(preset=preset)
+    sc.upload_arrays(arrays)
+    for i in range(len(rays)):
+        h = sc.RayQuery_NearestHit(rays[i, :4], rays[i, 4:])
+        assert h.tobytes() == want[i].tobytes()
+        # a hit exists in the interval whether or not the query stops at the first one
+        assert sc.RayQuery_AnyHit(rays[i, :4], rays[i, 4:]) == (want[i]["geomId"] != MISS)
+
+
+def _oracle_check(sc, rays, sample=None):
+    arrays = sc.export_arrays()
+    got = sc.RayQuery_NearestHitBatch(rays)
+    idx = np.arange(len(rays)) if sample is None else np.unique(
+        np.linspace(0, len(rays) - 1, sample).astype(np.int64))
+    want = po.port_trace(arrays, rays[idx])
+    assert bit_equal(got[idx], want).all(), hit_summary(got[idx], want)
+    return got
+
+
+def test_mesh_200k_triangles_256x256(cuda):
+    v, t = wl.noisy_sphere(317, seed=0)
+    sc = SceneRT()
+    sc.AddInstance(sc.AddGeom_Triangles3f(v, t), wl.IDENTITY)
+    sc.CommitScene()
+    rays = wl.eye_rays_host(wl.camera((0, 0, 3), width=256, height=256))
+    got = _oracle_check(sc, rays)
+    assert (got["primId"] != MISS).sum() > 15000
+    assert np.all((got["geomId"][got["primId"] != MISS] >> 24) == 0)
+
+
+def test_sbs_reduced_grid(cuda):
+    sph = wl.spheres(64, seed=1)
+    hdr, nodes, vals, vf = wl.sbs_from_spheres(sph, grid_res=128)
+    sc = SceneRT()
+    sc.AddInstance(sc.AddGeom_SdfSBS(hdr, nodes, vals, vf), wl.IDENTITY)
+    sc.CommitScene()
+    rays = wl.eye_rays_host(wl.camera((0, 0, 3), width=320, height=180))
+    got = _oracle_check(sc, rays)
+    hit = got["primId"] != MISS
+    assert hit.sum() > 5000 and np.all((got["geomId"][hit] >> 24) == 11)  # TYPE_SDF_SBS_COL
+
+
+def test_sbs_full_size_sample_and_properties(cuda):
+    """The benchmark workload itself: 512^3 virtual grid, 1920x1080 rays;
+    exact parity on a 16k-ray strided sample, properties on every ray."""
+    sph = wl.spheres(64, seed=1)
+    hdr, nodes, vals, vf = wl.sbs_from_spheres(sph, grid_res=512)
+    sc = SceneRT()
+    sc.AddInstance(sc.AddGeom_SdfSBS(hdr, nodes, vals, vf), wl.IDENTITY)
+    sc.CommitScene()
+    rays = wl.eye_rays_host(wl.camera((0, 0, 3), width=1920, height=1080))
+    got = _oracle_check(sc, rays, sample=16384)
+    hit = got["primId"] != MISS
+    assert hit.mean() > 0.1
+    t = got["t"][hit]
+    assert np.all((t > 0.01) & (t < 6.0))
+    # hit points lie on the sphere union: 99% within a quarter voxel; sphere
+    # tracing the trilinear field overshoots by up to ~2 voxels at the creases
+    # where spheres meet (the reference oracle shows the same distribution)
+    p = rays[hit, :3] + t[:, None] * rays[hit, 4:7]
+    d = np.abs(np.min(np.linalg.norm(p[:, None, :] - sph[None, :, :3], axis=2) - sph[None, :, 3], axis=1))
+    vox = 2.0 / 512
+    assert np.quantile(d, 0.99) < 0.25 * vox and d.max() < 3 * vox
+    # the FMA build agrees within tolerance
+    fast = sc.RayQuery_NearestHitBatch(rays, fast_math=True)
+    rep = tolerance_report(fast, got)
+    assert rep["id_mismatch"] <= len(rays) // 10000, rep
+    assert rep["max_rel_t"] <= 1e-4, rep
+
+
+def test_instanced_mixed_scene(cuda):
+    sph = wl.spheres(32, seed=4)
+    sc = SceneRT()
+    v, t = wl.noisy_sphere(60, seed=2)
+    gm = sc.AddGeom_Triangles3f(v, t)
+    go = sc.AddGeom_SdfFrameOctree(wl.frame_octree_from_spheres(sph, 6))
+    gs = sc.AddGeom_SdfSVS(wl.svs_from_spheres(sph, 6))
+    hdr, nodes, vals, vf = wl.sbs_from_spheres(sph, grid_res=64)
+    gb = sc.AddGeom_SdfSBS(hdr, nodes, vals, vf)
+    for i, m in enumerate(wl.random_instances(64, seed=7, scale=(0.1, 0.4), trans=1.5)):
+        sc.AddInstance([gm, go, gs, gb][i % 4], m)
+    sc.CommitScene()
+    rays = wl.eye_rays_host(wl.camera((0.5, 0.7, 3.5), width=200, height=150))
+    rays = np.concatenate([rays, rays[::4] * np.array([1, 1, 1, 1, 1, 1, 1, -1], np.float32)])
+    got = _oracle_check(sc, rays)
+    types = set((got["geomId"][got["primId"] != MISS] >> 24).tolist())
+    assert {0, 3, 5, 11} <= types
+
+
+def test_device_eye_rays_equal_host(cuda):
+    torch = cuda
+    v, t = wl.noisy_sphere(10)
+    sc = SceneRT()
+    sc.AddInstance(sc.AddGeom_Triangles3f(v, t), wl.IDENTITY)
+    sc.CommitScene()
+    for eye, (w, h) in (((0, 0, 3), (256, 256)), ((1.3, -2.0, 2.1), (331, 127))):
+        cam = wl.camera(eye, width=w, height=h)
+        buf = torch.empty(w * h * 8, dtype=torch.float32, device="cuda")
+        sc.generate_eye_rays(cam, buf.data_ptr())
+        torch.cuda.synchronize()
+        assert np.array_equal(buf.cpu().numpy().view(np.uint32), wl.eye_rays_host(cam).reshape(-1).view(np.uint32))
+
+
+def test_work_counters_equal_oracle(cuda):
+    arrays, rays, want, preset = load_golden("instanced_mix")
+    sc = SceneRT(preset=preset)
+    sc.upload_arrays(arrays)
+    got = sc.RayQuery_NearestHitBatch(rays, count_work=True)
+    assert bit_equal(got, want).all()
+    _, cnt, _ = po.port_trace(arrays, rays, preset=preset, counters=True)
+    assert np.array_equal(sc.work_counters(), cnt)

@@ -1,0 +1,74 @@
+"""The C restatement (oracle/lrt_oracle.c) against the reference's own golden
+vectors, and — where the reference build exists — against the reference on
+fresh scenes."""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from graphic_lab_task_b200 import workloads as wl
+from graphic_lab_task_b200._abi import COUNTER_NAMES
+from helpers import MISS, bit_equal, golden_names, hit_summary, load_golden
+
+GOLDEN = golden_names()
+
+
+def test_golden_set_is_complete():
+    for name in ("hand_triangle", "hand_brick", "mesh_small", "sbs_small", "instanced_mix", "ref_frame_octree",
+                 "ref_svs_crop", "ref_sbs_crop"):
+        assert name in GOLDEN
+
+
+@pytest.mark.parametrize("name", GOLDEN)
+def test_port_matches_reference_golden(name):
+    arrays, rays, want, preset = load_golden(name)
+    got, cnt, limits = po.port_trace(arrays, rays, preset=preset, threads=4, counters=True)
+    assert limits == 0
+    assert bit_equal(got, want).all(), hit_summary(got, want)
+    assert int(cnt[list(COUNTER_NAMES).index("hits")]) == int((want["primId"] != MISS).sum())
+
+
+def test_hand_triangle_semantics():
+    arrays, rays, want, _ = load_golden("hand_triangle")
+    t = want["t"]
+    assert t[0] == pytest.approx(1.0) and want["primId"][0] == 0
+    assert want["primId"][2] == MISS           # t = 0.005 is inside the 0.01 leaf bias
+    assert t[3] == pytest.approx(0.02)
+    assert want["primId"][4] == MISS           # tfar = 0.5 before the triangle
+    assert want["primId"][5] == 0              # any-hit ray still reports the hit
+    assert want["primId"][9] == MISS
+
+
+def test_planted_mistake_is_detected():
+    """Moving one vertex of the golden mesh changes the oracle's answer."""
+    arrays, rays, want, preset = load_golden("mesh_small")
+    bad = {k: v.copy() for k, v in arrays.items()}
+    first_hit = int(np.nonzero(want["primId"] != MISS)[0][0])
+    g_off = int(bad["geomData"]["offset"][0][1])
+    tri = int(want["primId"][first_hit])
+    # the reordered triangle slot of that primitive
+    slot = int(np.nonzero(bad["primIndices"] == tri)[0][0])
+    vid = int(bad["indices"][3 * slot])
+    bad["vertPos"][g_off + vid, :3] += np.float32(0.05)
+    got = po.port_trace(bad, rays, preset=preset)
+    assert not bit_equal(got, want).all()
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference build absent (make -C oracle ref)")
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_port_matches_reference_on_fresh_scenes(seed):
+    rng = np.random.default_rng(seed)
+    sph = wl.spheres(12, seed=100 + seed)
+    v, t = wl.noisy_sphere(int(rng.integers(8, 30)), seed=seed)
+    ref = po.RefScene()
+    gm = ref.add_triangles(v, t)
+    hdr, nodes, vals, vf = wl.sbs_from_spheres(sph, grid_res=32, brick_size=4, brick_pad=1)
+    gb = ref.add_sbs(hdr, nodes, vals, vf)
+    gs = ref.add_svs(wl.svs_from_spheres(sph, 4))
+    for i, m in enumerate(wl.random_instances(7, seed=seed, scale=(0.3, 0.8), trans=1.2)):
+        ref.add_instance([gm, gb, gs][i % 3], m)
+    ref.commit()
+    rays = wl.eye_rays_host(wl.camera((0.5, 1.0, 3.5), width=40, height=30))
+    rays = np.concatenate([rays, rays[::3] * np.array([1, 1, 1, 1, 1, 1, 1, -1], np.float32)])
+    want = ref.trace(rays)
+    got = po.port_trace(ref.export(), rays)
+    assert bit_equal(got, want).all(), hit_summary(got, want)
