@@ -321,3 +321,117 @@ lrt_status lrt_generate_eye_rays(lrt_scene* s, const lrt_camera* cam, float* ray
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free trace (lrt_trace_nearest_noalloc)
+//
+// For callers that cannot call cudaMalloc once their scene is uploaded: a host
+// application that hands the whole GPU memory budget to its own pool, or that
+// forbids device allocation inside its frame loop.  The trace kernel's
+// scratch — the persistent grid's ray counter, the work counters and the
+// bounded-loop error word — and, for host buffers, the staging copies of the
+// rays and hits live in one file-scope __device__ array instead of memory
+// from cudaMalloc.  Its size is fixed: 256 bytes of launch state plus room for
+// kNoAllocMaxRays rays and hits (1 MiB + 256 B in all), held by every GPU that
+// loads this library until the process exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr uint64_t kNoAllocMaxRays = 16384; // host-buffer calls: rays per call
+constexpr size_t kNoAllocStateBytes = 256;  // one StreamSlot, padded
+constexpr size_t kNoAllocBytes = kNoAllocStateBytes + kNoAllocMaxRays * (32 + sizeof(lrt_hit));
+static_assert(sizeof(lrt::StreamSlot) <= kNoAllocStateBytes, "launch state fits its 256 bytes");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Device address of g_noalloc_scratch on each device, looked up once per
+// device with that device current (the symbol name is only a host-side
+// stand-in and must never be handed to a kernel).
+constexpr int kNoAllocMaxDevices = 64;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+lrt_status noalloc_scratch(lrt_scene* s, unsigned char** out)
+{
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return lrt::fail(s, LRT_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+  if (dev != s->device)
+    return lrt::fail(s, LRT_ERR_INVALID_ARGUMENT,
+                     "lrt_trace_nearest_noalloc: make the scene's device (%d) current, not %d", s->device, dev);
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    return lrt::fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_trace_nearest_noalloc: device %d out of range", dev);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      return lrt::fail(s, LRT_ERR_CUDA, "cudaGetSymbolAddress(static scratch): %s", cudaGetErrorString(e));
+    g_noalloc_addr[dev] = p;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_addr[dev]);
+  return LRT_OK;
+}
+
+} // namespace
+
+extern "C" lrt_status lrt_trace_nearest_noalloc(lrt_scene* s, const float* rays, lrt_hit* hits, uint64_t n,
+                                                void* stream_p, uint32_t flags)
+{
+  using namespace lrt;
+  if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  if (!s->committed || !s->dev) return fail(s, LRT_ERR_NOT_COMMITTED, "trace before CommitScene/upload");
+  if (n == 0) return LRT_OK;
+  if (!rays || !hits) return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_trace_nearest_noalloc: NULL rays or hits");
+  if (flags & LRT_TRACE_COUNT_WORK)
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_trace_nearest_noalloc: LRT_TRACE_COUNT_WORK is not supported");
+  const bool onDevice = (flags & LRT_TRACE_DEVICE_POINTERS) != 0;
+  if (!onDevice && n > kNoAllocMaxRays)
+    return fail(s, LRT_ERR_INVALID_ARGUMENT,
+                "lrt_trace_nearest_noalloc: %llu rays exceed the static scratch capacity of %llu rays per call",
+                (unsigned long long)n, (unsigned long long)kNoAllocMaxRays);
+  if (onDevice && ((reinterpret_cast<uintptr_t>(rays) | reinterpret_cast<uintptr_t>(hits)) & 15))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "device rays/hits must be 16-byte aligned");
+  lrt_status st = check_preset(s);
+  if (st != LRT_OK) return st;
+  unsigned char* base = nullptr;
+  st = noalloc_scratch(s, &base);
+  if (st != LRT_OK) return st;
+  StreamSlot* slot = reinterpret_cast<StreamSlot*>(base);
+  float4* srays = reinterpret_cast<float4*>(base + kNoAllocStateBytes);
+  lrt_hit* shits = reinterpret_cast<lrt_hit*>(base + kNoAllocStateBytes + kNoAllocMaxRays * 32);
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_p);
+  DeviceScene* d = s->dev;
+  DevScene S = d->S;
+  S.flags = preset_flags(s->preset);
+  S.voxelStepCap = s->voxelStepCap ? s->voxelStepCap : kMaxVoxelSteps;
+  // the array keeps the previous call's contents: the ray counter and the
+  // error word must start at zero
+  cudaError_t e = cudaMemsetAsync(slot, 0, sizeof(StreamSlot), stream);
+  if (e != cudaSuccess) return cuda_fail(s, e, "cudaMemsetAsync(static scratch)");
+  const float4* krays = onDevice ? reinterpret_cast<const float4*>(rays) : srays;
+  lrt_hit* khits = onDevice ? hits : shits;
+  if (!onDevice) {
+    e = cudaMemcpyAsync(srays, rays, n * 32, cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return cuda_fail(s, e, "rays host->static scratch");
+  }
+  const uint64_t warps = (n + 31) / 32;
+  const int grid = int(std::min<uint64_t>(uint64_t(d->grid), (warps * 32 + kTraceThreads - 1) / kTraceThreads));
+  if (flags & LRT_TRACE_FAST_MATH)
+    e = lrt_fast::launch_trace(S, krays, khits, n, &slot->work, slot->counters, &slot->err, d->stackCap, grid,
+                               stream, false);
+  else
+    e = lrt_exact::launch_trace(S, krays, khits, n, &slot->work, slot->counters, &slot->err, d->stackCap, grid,
+                                stream, false);
+  if (e != cudaSuccess) return cuda_fail(s, e, "trace launch");
+  if (!onDevice) {
+    e = cudaMemcpyAsync(hits, shits, n * sizeof(lrt_hit), cudaMemcpyDeviceToHost, stream);
+    if (e != cudaSuccess) return cuda_fail(s, e, "hits static scratch->host");
+  }
+  uint32_t err = 0;
+  e = cudaMemcpyAsync(&err, &slot->err, sizeof(err), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return cuda_fail(s, e, "trace");
+  if (err)
+    return fail(s, LRT_ERR_DEVICE_LIMIT,
+                "trace hit a bounded-loop limit (error bits 0x%x: 1 = stack, 2 = voxel march)", err);
+  return LRT_OK;
+}

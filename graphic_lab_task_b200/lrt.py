@@ -26,6 +26,7 @@ EXPORTED = (
     "lrt_add_geom_sdf_svs", "lrt_add_geom_sdf_sbs", "lrt_clear_scene", "lrt_add_instance", "lrt_commit_scene",
     "lrt_scene_upload", "lrt_scene_export", "lrt_trace_nearest", "lrt_trace_sync", "lrt_ray_query_nearest_hit",
     "lrt_ray_query_any_hit", "lrt_get_work_counters", "lrt_generate_eye_rays", "lrt_set_voxel_step_limit",
+    "lrt_trace_nearest_noalloc",
     "lrt_wl_noisy_sphere", "lrt_wl_spheres", "lrt_wl_sphere_sdf", "lrt_wl_sbs_from_spheres",
     "lrt_wl_frame_octree_from_spheres", "lrt_wl_svs_from_spheres",
 )
@@ -68,6 +69,7 @@ def lib():
         "lrt_scene_upload": [vp, P(SceneArrays)],
         "lrt_scene_export": [vp, P(SceneArrays)],
         "lrt_trace_nearest": [vp, vp, vp, u64, vp, u32],
+        "lrt_trace_nearest_noalloc": [vp, vp, vp, u64, vp, u32],
         "lrt_trace_sync": [vp, vp, C.c_int32],
         "lrt_ray_query_nearest_hit": [vp, vp, vp, vp],
         "lrt_ray_query_any_hit": [vp, vp, vp, P(C.c_int32)],

@@ -285,6 +285,25 @@ lrt_status lrt_scene_export(const lrt_scene* scene, lrt_scene_arrays* out);
 lrt_status lrt_trace_nearest(lrt_scene* scene, const float* rays, lrt_hit* hits, uint64_t n, void* stream,
                              uint32_t flags);
 
+/* Allocation-free variant of lrt_trace_nearest.  No counterpart in the
+ * reference: it exists for hosts that cannot call cudaMalloc once their scene
+ * is uploaded (an application that gives its whole GPU memory budget to its
+ * own pool, or forbids device allocation inside its frame loop).  The trace
+ * kernel's scratch (ray counter, error word) and, for host buffers, the
+ * staging copies of rays and hits live in a fixed file-scope device array of
+ * 1 MiB + 256 B that every GPU loading the library keeps until exit.  With
+ * host pointers at most 16384 rays per call are accepted (larger n returns
+ * LRT_ERR_INVALID_ARGUMENT); with LRT_TRACE_DEVICE_POINTERS any n.  The call
+ * calls no cudaMalloc/cudaFree and returns after `stream` has drained, with
+ * LRT_ERR_DEVICE_LIMIT if the kernel hit a bounded-loop limit.  The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress) with
+ * the scene's device current; make that first call before any stream capture.
+ * All calls share the one array: calls that overlap on the GPU (different
+ * streams, threads or scenes on one device) race and must be serialised by
+ * the caller.  LRT_TRACE_COUNT_WORK is not supported. */
+lrt_status lrt_trace_nearest_noalloc(lrt_scene* scene, const float* rays, lrt_hit* hits, uint64_t n, void* stream,
+                                     uint32_t flags);
+
 /* Waits for the traces queued on `stream` (device-pointer traces are
  * asynchronous) and returns LRT_ERR_DEVICE_LIMIT if one of them hit a
  * bounded-loop limit.  With read_counters != 0 the work counters of the last
