@@ -34,9 +34,9 @@ assert GEOM_DATA_DTYPE.itemsize == 64 and INSTANCE_DTYPE.itemsize == 256
 assert FRAME_OCTREE_NODE_DTYPE.itemsize == 36 and SVS_NODE_DTYPE.itemsize == 16
 assert SBS_NODE_DTYPE.itemsize == 16 and SBS_HEADER_DTYPE.itemsize == 16
 
-LRT_COUNTER_COUNT = 12
+LRT_COUNTER_COUNT = 13
 COUNTER_NAMES = ("tlas_nodes", "instances", "blas_pairs", "leaf_calls", "tri_tests", "bricks", "voxels",
-                 "st_steps", "octree_leaves", "svs_leaves", "hits", "normals")
+                 "st_steps", "octree_leaves", "svs_leaves", "hits", "normals", "voxel_loads")
 
 # Constants (core/render_settings.h, MultiRenderer/BVH2Common.h:30-43, sdf_simple_shared.h:12-20)
 TYPE_MESH_TRIANGLE = 0

@@ -151,9 +151,13 @@ lrt_status device_upload(lrt_scene* s)
   std::vector<DevGeom> geoms;
   std::vector<float> soup, dense;
   std::vector<DevSbs> sbs;
+  std::vector<uint32_t> mask;
   build_geoms(h, geoms);
   build_tri_soup(h, soup);
   build_sbs_dense(h, sbs, dense);
+  build_sbs_masks(h, sbs, dense, mask);
+  std::vector<lrt_bvh_node_pair> pairs;
+  prune_sbs_pairs(h, geoms, sbs, mask, pairs);
   lrt_status st = LRT_OK;
 #define UP(dst, vec, T, name)                                                                        \
   if (st == LRT_OK) {                                                                                 \
@@ -162,7 +166,7 @@ lrt_status device_upload(lrt_scene* s)
     S.dst = p;                                                                                        \
   }
   UP(tlas, h.nodesTLAS, lrt_bvh_node, "TLAS nodes")
-  UP(pairs, h.allNodePairs, lrt_bvh_node_pair, "BLAS node pairs")
+  UP(pairs, pairs, lrt_bvh_node_pair, "BLAS node pairs")
   UP(instances, h.instanceData, DevInstance, "instances")
   UP(geoms, geoms, DevGeom, "geometry table")
   UP(primIdCount, h.primIdCount, uint32_t, "leaf table")
@@ -175,6 +179,7 @@ lrt_status device_upload(lrt_scene* s)
   UP(sbsData, h.sdfSBSData, uint32_t, "SBS data")
   UP(sbsDataF, h.sdfSBSDataF, float, "SBS float data")
   UP(sbsDense, dense, float, "SBS dense bricks")
+  UP(sbsMask, mask, uint32_t, "SBS surface-voxel masks")
   UP(sbs, sbs, DevSbs, "SBS table")
 #undef UP
   if (st != LRT_OK) {

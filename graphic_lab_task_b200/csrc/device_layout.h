@@ -49,7 +49,8 @@ enum : int {
   kCntOctreeLeaves,
   kCntSvsLeaves,
   kCntHits,
-  kCntNormals
+  kCntNormals,
+  kCntVoxelLoads
 };
 
 struct DevGeom {
@@ -71,8 +72,16 @@ struct DevSbs {
   uint32_t v3;          // (brick_size + 2*pad + 1)^3
   uint32_t colorLayout; // 1 for the indexed ID32F layouts (hit colour from sbsDataF)
   uint32_t nodeCount;   // nodes of this model (leaves naming a node past it are skipped)
-  uint32_t _pad;
+  uint32_t maskStride;  // words per brick in sbsMask: 1 + ceil(brick_size^3 / 32)
+  uint64_t maskBase;    // first word of node `root` in sbsMask
 };
+
+// sbsMask, per brick: word 0 is nonzero iff some voxel can start a sphere
+// trace; words 1.. hold one bit per voxel (index (x*bs + y)*bs + z) that is
+// set iff min of its 8 corner values <= 0 — the test OctreeBrickIntersect
+// applies before LocalSurfaceIntersection (BVH2Common.cpp:941), evaluated on
+// the same floats.  A clear bit means the reference does nothing in that
+// voxel but advance the march.
 
 typedef lrt_instance_data DevInstance;
 
@@ -91,6 +100,7 @@ struct DevScene {
   const uint32_t* sbsData;
   const float* sbsDataF;
   const float* sbsDense;
+  const uint32_t* sbsMask;
   const DevSbs* sbs;
   uint32_t flags;
   uint32_t voxelStepCap; // bounded SBS voxel march (kMaxVoxelSteps unless set)

@@ -3,6 +3,8 @@
 // as the reference computes it on the fly).
 #include <algorithm>
 #include <cstring>
+#include <functional>
+#include <limits>
 
 #include "layout.h"
 
@@ -57,6 +59,88 @@ void build_tri_soup(const HostArrays& h, std::vector<float>& soup)
       }
     }
   }
+}
+
+// Surface-voxel masks of every brick from its dense corner grid (see
+// device_layout.h): vmin is reduced exactly as load_distance_values does
+// (BVH2Common.cpp:861-866), so the bit equals the reference's `vmin <= 0`.
+void build_sbs_masks(const HostArrays& h, std::vector<DevSbs>& sbs, const std::vector<float>& dense,
+                     std::vector<uint32_t>& mask)
+{
+  uint64_t total = 0;
+  for (size_t i = 0; i < sbs.size(); i++) {
+    const uint32_t bs = sbs[i].brick_size;
+    sbs[i].maskStride = 1 + (bs * bs * bs + 31) / 32;
+    sbs[i].maskBase = total;
+    total += uint64_t(sbs[i].nodeCount) * sbs[i].maskStride;
+  }
+  mask.assign(total, 0u);
+  for (size_t i = 0; i < sbs.size(); i++) {
+    const DevSbs& d = sbs[i];
+    const uint32_t bs = d.brick_size, V1 = bs + 1;
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < int64_t(d.nodeCount); k++) {
+      const float* g = dense.data() + d.denseBase + uint64_t(k) * d.denseStride;
+      uint32_t* m = mask.data() + d.maskBase + uint64_t(k) * d.maskStride;
+      for (uint32_t x = 0; x < bs; x++)
+        for (uint32_t y = 0; y < bs; y++)
+          for (uint32_t z = 0; z < bs; z++) {
+            float vmin = 1e6f;
+            for (int c = 0; c < 8; c++) {
+              const float v = g[((x + ((c & 4) >> 2)) * V1 + (y + ((c & 2) >> 1))) * V1 + (z + (c & 1))];
+              vmin = (v < vmin) ? v : vmin;
+            }
+            if (vmin <= 0.0f) {
+              const uint32_t vid = (x * bs + y) * bs + z;
+              m[1 + vid / 32] |= 1u << (vid % 32);
+              m[0] = 1;
+            }
+          }
+    }
+  }
+  (void)h;
+}
+
+// Device copy of the BLAS node pairs in which every child subtree of an SBS
+// BLAS that holds no brick able to start a sphere trace gets a NaN box.  A
+// NaN box fails the child test of BVH2TraverseF32 (tmin <= tmax is false) for
+// every ray, so such a subtree is never entered.  This cannot change a
+// result: the pruned leaves never touch the hit, and the depth-first
+// near-first order of the remaining leaves is unchanged — at a node whose
+// other child is pruned the reference would visit that child (before or
+// after) without effect.  Returns the number of pruned children.
+uint64_t prune_sbs_pairs(const HostArrays& h, const std::vector<DevGeom>& geoms, const std::vector<DevSbs>& sbs,
+                         const std::vector<uint32_t>& mask, std::vector<lrt_bvh_node_pair>& pairs)
+{
+  pairs = h.allNodePairs;
+  const float qnan = std::numeric_limits<float>::quiet_NaN();
+  uint64_t pruned = 0;
+  for (size_t g = 0; g < geoms.size(); g++) {
+    if (geoms[g].tag != LRT_TAG_SDF_BRICK) continue;
+    const DevSbs& sb = sbs[geoms[g].sdfId];
+    const uint32_t base = geoms[g].bvhOffset, a0 = geoms[g].aabbBase;
+    // returns true if the subtree under `lo` (a child word) can produce a hit
+    std::function<bool(uint32_t)> live = [&](uint32_t lo) -> bool {
+      if (lo & kLeafBit) {
+        if (lo == kLeafNormal) return false;
+        const uint32_t primId = h.primIdCount[a0 + (lo & kStartMask)] & kStartMask;
+        if (primId >= sb.nodeCount) return false;
+        return mask[sb.maskBase + uint64_t(primId) * sb.maskStride] != 0;
+      }
+      lrt_bvh_node_pair& p = pairs[base + lo];
+      const bool l = live(p.left.leftOffset), r = live(p.right.leftOffset);
+      for (int j = 0; j < 2; j++) {
+        lrt_bvh_node& n = j ? p.right : p.left;
+        if (!(j ? r : l)) {
+          for (int k = 0; k < 3; k++) n.boxMin[k] = n.boxMax[k] = qnan;
+          pruned++;
+        }
+      }
+      return l || r;
+    };
+    live(0); // the root pair
+  }
+  return pruned;
 }
 
 // Dense (brick_size+1)^3 corner grids per SBS node; values as

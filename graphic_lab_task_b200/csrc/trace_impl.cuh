@@ -171,6 +171,10 @@ __device__ void octree_brick(Ctx<COUNT>& c, const DevGeom& g, f3 ray_pos, f3 ray
   const uint32_t nodeId = primId + g.sdfRoot;
   c.inc(kCntBricks);
   if (primId >= sb.nodeCount) return; // padding box of a one-brick model
+  // No voxel of this brick passes the reference's `vmin <= 0` test: its
+  // march could only advance t and cannot change the hit.
+  const uint32_t* mask = S.sbsMask + sb.maskBase + uint64_t(primId) * sb.maskStride;
+  if (__ldg(mask) == 0) return;
   const uint4 node = __ldg(reinterpret_cast<const uint4*>(S.sbsNodes) + nodeId);
   const float px = float(node.x >> 16), py = float(node.x & 0x0000FFFF);
   const float pz = float(node.y >> 16), sz = float(node.y & 0x0000FFFF);
@@ -200,22 +204,23 @@ __device__ void octree_brick(Ctx<COUNT>& c, const DevGeom& g, f3 ray_pos, f3 ray
                             floorf(sclamp(local_pos.z, 1e-6f, hiClamp)));
     const f3 min_pos = brick_min_pos + d * voxelPos;
     const f3 max_pos = min_pos + d * mk3(1, 1, 1);
-    // 8 corners of the voxel from the dense (bs+1)^3 grid, x-major
     const uint32_t vx = uint32_t(voxelPos.x), vy = uint32_t(voxelPos.y), vz = uint32_t(voxelPos.z);
-    const float* base = dense + (vx * V1 + vy) * V1 + vz;
-    values[0] = __ldg(base);
-    values[1] = __ldg(base + 1);
-    values[2] = __ldg(base + V1);
-    values[3] = __ldg(base + V1 + 1);
-    values[4] = __ldg(base + V1 * V1);
-    values[5] = __ldg(base + V1 * V1 + 1);
-    values[6] = __ldg(base + V1 * V1 + V1);
-    values[7] = __ldg(base + V1 * V1 + V1 + 1);
-    float vmin = 1e6f;
-#pragma unroll
-    for (int i = 0; i < 8; i++) vmin = smin(vmin, values[i]);
+    const uint32_t vid = (vx * bs + vy) * bs + vz;
+    // surface bit == (min of the 8 corner values <= 0), precomputed
+    const bool surface = (__ldg(mask + 1 + (vid >> 5)) >> (vid & 31)) & 1u;
     const f2 fNearFar = ray_box(ray_pos, inv_dir, min_pos, max_pos);
-    if (tNear < fNearFar.x && vmin <= 0.0f) {
+    if (tNear < fNearFar.x && surface) {
+      c.inc(kCntVoxelLoads);
+      // 8 corners of the voxel from the dense (bs+1)^3 grid, x-major
+      const float* base = dense + (vx * V1 + vy) * V1 + vz;
+      values[0] = __ldg(base);
+      values[1] = __ldg(base + 1);
+      values[2] = __ldg(base + V1);
+      values[3] = __ldg(base + V1 + 1);
+      values[4] = __ldg(base + V1 * V1);
+      values[5] = __ldg(base + V1 * V1 + 1);
+      values[6] = __ldg(base + V1 * V1 + V1);
+      values[7] = __ldg(base + V1 * V1 + V1 + 1);
       const f3 start_pos = ray_pos + fNearFar.x * ray_dir;
       const f3 start_q = (start_pos - min_pos) * scale;
       const float qFar = (fNearFar.y - fNearFar.x) * scale;

@@ -18,8 +18,9 @@ BYTES_PER_UNIT = {
     "blas_pairs": 64,      # BVHNodePair, 4 x 16-byte loads
     "leaf_calls": 4,       # packed {start,count} of m_primIdCount
     "tri_tests": 48,       # {A, B-A, C-A} as 3 float4
-    "bricks": 48,          # SdfSBSNode 16 + per-model SBS table 32
-    "voxels": 32,          # 8 fp32 corners of a dense brick
+    "bricks": 52,          # SdfSBSNode 16 + per-model SBS table 32 + brick occupancy word 4
+    "voxels": 4,           # surface-voxel mask word of one march iteration
+    "voxel_loads": 32,     # 8 fp32 corners of a dense brick (surface voxels only)
     "st_steps": 0,         # register-only
     "octree_leaves": 64,   # origNodes box 32 + 8 corner values 32
     "svs_leaves": 16,      # SdfSVSNode

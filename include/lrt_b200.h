@@ -325,9 +325,13 @@ lrt_status lrt_set_voxel_step_limit(lrt_scene* scene, uint32_t steps);
 
 /* Work counters of the last LRT_TRACE_COUNT_WORK trace (summed over rays):
  * TLAS node visits, instances entered, BLAS node-pair visits, leaf calls,
- * triangle tests, SBS brick entries, SBS voxel visits, ST steps,
- * frame-octree leaf tests, SVS leaf tests, hits, normals computed. */
-#define LRT_COUNTER_COUNT 12
+ * triangle tests, SBS brick entries, SBS voxel-march iterations, ST steps,
+ * frame-octree leaf tests, SVS leaf tests, hits, normals computed, and SBS
+ * voxels whose 8 corner values were loaded to start a sphere trace.  The
+ * kernels never enter SBS subtrees or bricks that hold no voxel able to start
+ * a sphere trace, so their node-pair, leaf-call, brick and voxel-march counts
+ * are at most the reference algorithm's; every other counter equals it. */
+#define LRT_COUNTER_COUNT 13
 lrt_status lrt_get_work_counters(lrt_scene* scene, uint64_t counters[LRT_COUNTER_COUNT]);
 
 /* ------------------------------------------------------------------------ */

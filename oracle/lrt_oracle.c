@@ -39,7 +39,7 @@
 
 enum {
   C_TLAS_NODES = 0, C_INSTANCES, C_BLAS_PAIRS, C_LEAF_CALLS, C_TRI_TESTS, C_BRICKS, C_VOXELS, C_ST_STEPS,
-  C_OCTREE_LEAVES, C_SVS_LEAVES, C_HITS, C_NORMALS
+  C_OCTREE_LEAVES, C_SVS_LEAVES, C_HITS, C_NORMALS, C_VOXEL_LOADS
 };
 
 typedef struct { float x, y, z; } f3;
@@ -337,6 +337,7 @@ static void octree_brick(ctx_t* c, uint32_t type, f3 ray_pos, f3 ray_dir, float 
     const float vmin = load_distance_values(c, nodeId, voxelPos, v_size, sz_inv, &h, values);
     const f2 fNearFar = ray_box(ray_pos, inv_dir, min_pos, max_pos);
     if (tNear < fNearFar.x && vmin <= 0.0f) {
+      c->cnt[C_VOXEL_LOADS]++;
       const f3 start_pos = add3(ray_pos, scl3(fNearFar.x, ray_dir));
       const f3 start_q = scl3(scale, sub3(start_pos, min_pos));
       const float qFar = (fNearFar.y - fNearFar.x) * scale;
