@@ -74,6 +74,22 @@ class Camera(C.Structure):
                 ("height", C.c_uint32), ("tnear", C.c_float), ("tfar", C.c_float)]
 
 
+class BatchShape(C.Structure):
+    """lrt_batch_shape: launch shape of the batched multi-camera trace."""
+    _fields_ = [("tile_w", C.c_uint32), ("tile_h", C.c_uint32), ("rays_per_lane", C.c_uint32),
+                ("stack_cap", C.c_uint32)]
+
+    def as_tuple(self):
+        return (self.tile_w, self.tile_h, self.rays_per_lane, self.stack_cap)
+
+
+class TuneEntry(C.Structure):
+    _fields_ = [("shape", BatchShape), ("ms", C.c_float)]
+
+
+LRT_BATCH_NO_GRAPH = 0x1
+
+
 def default_preset():
     """getDefaultPreset() (core/render_settings.h:139-160)."""
     return Preset(render_mode=1, sdf_node_intersect=1, normal_mode=1, ray_gen_mode=0, interpolation_mode=0,

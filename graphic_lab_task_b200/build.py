@@ -34,11 +34,12 @@ SOURCES = {
     "trace_exact.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
     "trace_fast.cu": ["-fmad=true", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
     "device.cu": [],
+    "batch.cu": [],
     "scene.cpp": None,
     "layout.cpp": None,
     "workloads.cpp": None,
 }
-HEADERS = ["trace_impl.cuh", "device_layout.h", "lrt_math.h", "scene.h", "layout.h", "trace_api.h"]
+HEADERS = ["trace_impl.cuh", "device_layout.h", "lrt_math.h", "scene.h", "layout.h", "trace_api.h", "device_scene.h"]
 
 
 def _stale(obj, src):

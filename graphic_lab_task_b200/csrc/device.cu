@@ -7,49 +7,33 @@
 #include <map>
 #include <vector>
 
+#include "device_scene.h"
 #include "layout.h"
 #include "scene.h"
 #include "trace_api.h"
 
 namespace lrt {
 
-// Per-stream launch state: the persistent grid's ray counter, the error word
-// and the work counters.  One slot per stream keeps concurrent traces of one
-// scene on different streams independent.
-struct StreamSlot {
-  unsigned long long work;
-  unsigned long long counters[LRT_COUNTER_COUNT];
-  uint32_t err;
-  uint32_t _pad[5];
-};
-constexpr int kMaxStreams = 64;
-
-struct DeviceScene {
-  std::vector<void*> allocs;
-  DevScene S{};
-  uint32_t stackCap = 0;
-  int grid = 0;
-  StreamSlot* slots = nullptr; // device, kMaxStreams
-  std::map<cudaStream_t, int> slotOf;
-  // staging buffers for host-pointer calls
-  float4* rays = nullptr;
-  lrt_hit* hits = nullptr;
-  uint64_t cap = 0;
-  ~DeviceScene()
-  {
-    for (void* p : allocs) cudaFree(p);
-    if (rays) cudaFree(rays);
-    if (hits) cudaFree(hits);
-  }
-};
-
-namespace {
-
 lrt_status cuda_fail(lrt_scene* s, cudaError_t e, const char* what)
 {
   return fail(s, e == cudaErrorMemoryAllocation ? LRT_ERR_OUT_OF_MEMORY : LRT_ERR_CUDA, "%s: %s", what,
               cudaGetErrorString(e));
 }
+
+uint32_t preset_flags(const lrt_preset& p)
+{
+  const uint32_t m = p.render_mode; // need_normal(), BVH2Common.cpp:19-32
+  const bool nn = m == 1 || m == 8 || m == 12 || m == 17 || m == 20 || m == 7 || m == 18 || m == 23 || m == 21 ||
+                  m == 11 || m == 27;
+  uint32_t f = 0;
+  if (nn) f |= kFlagNeedNormal;
+  if (m == LRT_RENDER_MODE_ST_ITERATIONS) f |= kFlagStIterations;
+  if (p.representation_mode == 0) f |= kFlagSurfaceMode;
+  if (p.sdf_node_intersect == 3) f |= kFlagBBoxMode;
+  return f;
+}
+
+namespace {
 
 template <class T>
 lrt_status upload_vec(lrt_scene* s, DeviceScene* d, const T* src, size_t count, const T** out, const char* name)
@@ -64,19 +48,6 @@ lrt_status upload_vec(lrt_scene* s, DeviceScene* d, const T* src, size_t count, 
   if (e != cudaSuccess) return cuda_fail(s, e, name);
   *out = static_cast<const T*>(p);
   return LRT_OK;
-}
-
-uint32_t preset_flags(const lrt_preset& p)
-{
-  const uint32_t m = p.render_mode; // need_normal(), BVH2Common.cpp:19-32
-  const bool nn = m == 1 || m == 8 || m == 12 || m == 17 || m == 20 || m == 7 || m == 18 || m == 23 || m == 21 ||
-                  m == 11 || m == 27;
-  uint32_t f = 0;
-  if (nn) f |= kFlagNeedNormal;
-  if (m == LRT_RENDER_MODE_ST_ITERATIONS) f |= kFlagStIterations;
-  if (p.representation_mode == 0) f |= kFlagSurfaceMode;
-  if (p.sdf_node_intersect == 3) f |= kFlagBBoxMode;
-  return f;
 }
 
 lrt_status slot_for(lrt_scene* s, cudaStream_t stream, StreamSlot** out)

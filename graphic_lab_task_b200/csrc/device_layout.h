@@ -23,6 +23,7 @@
 namespace lrt {
 
 constexpr int kTraceThreads = 128;
+constexpr uint32_t kMaxStackDev = 80; // STACK_SIZE of raytrace_common.h:36
 constexpr uint32_t kLeafBit = 0x80000000u;
 constexpr uint32_t kMaxVoxelSteps = 4096u; // voxel-march cap per brick (the reference loop is unbounded)
 
@@ -111,6 +112,22 @@ struct DevCamera {
   float world_view_inv[16];
   uint32_t width, height;
   float tnear, tfar;
+};
+
+// One camera of a batched multi-camera trace: its rays are generated in the
+// kernel, tile by tile; hits go to out[rayOffset + y*width + x].
+struct DevBatchCamera {
+  DevCamera cam;
+  uint64_t rayOffset;
+  uint32_t tileBase; // first global tile index of this camera
+  uint32_t tilesX;   // tiles per image row
+};
+
+// Launch shape of the batched trace, chosen by the autotuner: tiles of
+// tileW x tileH pixels (tileW*tileH = 32*raysPerLane) fetched by one warp at
+// a time; each lane traces raysPerLane pixels of its tile one after another.
+struct DevBatchShape {
+  uint32_t tileW, tileH, raysPerLane, stackCap;
 };
 
 } // namespace lrt

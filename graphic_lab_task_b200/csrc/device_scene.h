@@ -1,0 +1,47 @@
+// device_scene.h — the device half of an lrt_scene (internal to liblrt_b200.so).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <vector>
+
+#include "device_layout.h"
+#include "scene.h"
+
+namespace lrt {
+
+// Per-stream launch state: the persistent grid's ray counter, the error word
+// and the work counters.  One slot per stream keeps concurrent traces of one
+// scene on different streams independent.
+struct StreamSlot {
+  unsigned long long work;
+  unsigned long long counters[LRT_COUNTER_COUNT];
+  uint32_t err;
+  uint32_t _pad[5];
+};
+constexpr int kMaxStreams = 64;
+
+struct DeviceScene {
+  std::vector<void*> allocs;
+  DevScene S{};
+  uint32_t stackCap = 0;
+  int grid = 0;
+  StreamSlot* slots = nullptr; // device, kMaxStreams
+  std::map<cudaStream_t, int> slotOf;
+  // staging buffers for host-pointer calls
+  float4* rays = nullptr;
+  lrt_hit* hits = nullptr;
+  uint64_t cap = 0;
+  ~DeviceScene()
+  {
+    for (void* p : allocs) cudaFree(p);
+    if (rays) cudaFree(rays);
+    if (hits) cudaFree(hits);
+  }
+};
+
+// device.cu
+uint32_t preset_flags(const lrt_preset& p);
+lrt_status cuda_fail(lrt_scene* s, cudaError_t e, const char* what);
+
+} // namespace lrt

@@ -12,6 +12,11 @@
   cudaError_t set_trace_smem(uint32_t stack_cap);                                                               \
   cudaError_t trace_occupancy(uint32_t stack_cap, int* blocks_per_sm);                                          \
   cudaError_t launch_eye_rays(const lrt::DevCamera& cam, float4* rays, cudaStream_t stream);                    \
+  cudaError_t launch_trace_cameras(const lrt::DevScene& S, const lrt::DevBatchCamera* cams, uint32_t ncams,     \
+                                   uint32_t ntiles, const lrt::DevBatchShape& shape, lrt_hit* hits,             \
+                                   unsigned long long* work_counter, uint32_t* err_word, int grid,              \
+                                   cudaStream_t stream);                                                        \
+  cudaError_t cameras_occupancy(uint32_t stack_cap, int* blocks_per_sm);                                        \
   }
 
 LRT_DECLARE_TRACE_API(lrt_exact)

@@ -450,6 +450,72 @@ __global__ void __launch_bounds__(kTraceThreads) k_trace(DevScene S, const float
   }
 }
 
+// Batched multi-camera form: one persistent launch over the pixel tiles of
+// all cameras.  A warp takes one tile at a time from the global counter,
+// finds its camera by binary search over the tile bases, and each lane
+// generates (lrt::eye_ray, the function k_eye_rays uses) and traces its
+// raysPerLane pixels, so every hit equals the plain per-camera path's.
+__global__ void __launch_bounds__(kTraceThreads) k_trace_cameras(DevScene S, const DevBatchCamera* __restrict__ cams,
+                                                                 uint32_t ncams, uint32_t ntiles, DevBatchShape shape,
+                                                                 lrt_hit* __restrict__ hits,
+                                                                 unsigned long long* __restrict__ work_counter,
+                                                                 uint32_t* __restrict__ err_word)
+{
+  extern __shared__ uint32_t smem_stack[];
+  uint32_t* stack = smem_stack + threadIdx.x;
+  const uint32_t lane = threadIdx.x & 31;
+  Ctx<false> c(S);
+  for (;;) {
+    unsigned long long tile = 0;
+    if (lane == 0) tile = atomicAdd(work_counter, 1ull);
+    tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
+    if (tile >= ntiles) break;
+    // camera of this tile: the last camera whose tileBase <= tile (uniform in the warp)
+    uint32_t lo = 0, hi = ncams - 1;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (__ldg(&cams[mid].tileBase) <= tile) lo = mid;
+      else hi = mid - 1;
+    }
+    const DevBatchCamera& bc = cams[lo];
+    const uint32_t local = uint32_t(tile) - bc.tileBase;
+    const uint32_t x0 = (local % bc.tilesX) * shape.tileW, y0 = (local / bc.tilesX) * shape.tileH;
+    const uint32_t W = bc.cam.width, H = bc.cam.height;
+    for (uint32_t r = 0; r < shape.raysPerLane; r++) {
+      const uint32_t i = lane + 32 * r;
+      const uint32_t x = x0 + i % shape.tileW, y = y0 + i / shape.tileW;
+      if (x >= W || y >= H) continue;
+      float ray[8];
+      eye_ray(bc.cam.proj_inv, bc.cam.world_view_inv, x, y, W, H, bc.cam.tnear, bc.cam.tfar, ray);
+      lrt_hit h;
+      trace_one(c, stack, blockDim.x, shape.stackCap, make_float4(ray[0], ray[1], ray[2], ray[3]),
+                make_float4(ray[4], ray[5], ray[6], ray[7]), h);
+      float4* out = reinterpret_cast<float4*>(hits + bc.rayOffset + uint64_t(y) * W + x);
+      out[0] = make_float4(h.t, __uint_as_float(h.primId), __uint_as_float(h.instId), __uint_as_float(h.geomId));
+      out[1] = make_float4(h.coords[0], h.coords[1], h.coords[2], h.coords[3]);
+    }
+  }
+  if (c.err) atomicOr(err_word, c.err);
+}
+
+cudaError_t launch_trace_cameras(const DevScene& S, const DevBatchCamera* cams, uint32_t ncams, uint32_t ntiles,
+                                 const DevBatchShape& shape, lrt_hit* hits, unsigned long long* work_counter,
+                                 uint32_t* err_word, int grid, cudaStream_t stream)
+{
+  const size_t smem = size_t(shape.stackCap) * kTraceThreads * sizeof(uint32_t);
+  k_trace_cameras<<<grid, kTraceThreads, smem, stream>>>(S, cams, ncams, ntiles, shape, hits, work_counter, err_word);
+  return cudaGetLastError();
+}
+
+cudaError_t cameras_occupancy(uint32_t stack_cap, int* blocks_per_sm)
+{
+  const size_t smem = size_t(stack_cap) * kTraceThreads * sizeof(uint32_t);
+  cudaError_t e = cudaFuncSetAttribute(k_trace_cameras, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int((kMaxStackDev + 1) * kTraceThreads * sizeof(uint32_t)));
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_trace_cameras, kTraceThreads, smem);
+}
+
 // Eye rays of one camera (MultiRenderer::initEyeRay), row-major pixels.
 __global__ void k_eye_rays(DevCamera cam, float4* __restrict__ rays)
 {

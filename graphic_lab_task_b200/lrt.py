@@ -12,9 +12,9 @@ import os
 
 import numpy as np
 
-from ._abi import (HIT_DTYPE, LRT_COUNTER_COUNT, LRT_TRACE_COUNT_WORK, LRT_TRACE_DEVICE_POINTERS,
-                   LRT_TRACE_FAST_MATH, STATUS_NAMES, Preset, SceneArrays, arrays_to_struct, parity_preset,
-                   struct_to_arrays)
+from ._abi import (HIT_DTYPE, LRT_BATCH_NO_GRAPH, LRT_COUNTER_COUNT, LRT_TRACE_COUNT_WORK,
+                   LRT_TRACE_DEVICE_POINTERS, LRT_TRACE_FAST_MATH, STATUS_NAMES, BatchShape, Camera, Preset,
+                   SceneArrays, TuneEntry, arrays_to_struct, parity_preset, struct_to_arrays)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liblrt_b200.so")
@@ -26,7 +26,9 @@ EXPORTED = (
     "lrt_add_geom_sdf_svs", "lrt_add_geom_sdf_sbs", "lrt_clear_scene", "lrt_add_instance", "lrt_commit_scene",
     "lrt_scene_upload", "lrt_scene_export", "lrt_trace_nearest", "lrt_trace_sync", "lrt_ray_query_nearest_hit",
     "lrt_ray_query_any_hit", "lrt_get_work_counters", "lrt_generate_eye_rays", "lrt_set_voxel_step_limit",
-    "lrt_trace_nearest_noalloc",
+    "lrt_trace_nearest_noalloc", "lrt_batch_create", "lrt_batch_destroy", "lrt_batch_ray_offsets",
+    "lrt_batch_update_cameras", "lrt_batch_set_shape", "lrt_batch_get_shape", "lrt_batch_trace", "lrt_batch_sync",
+    "lrt_batch_autotune",
     "lrt_wl_noisy_sphere", "lrt_wl_spheres", "lrt_wl_sphere_sdf", "lrt_wl_sbs_from_spheres",
     "lrt_wl_frame_octree_from_spheres", "lrt_wl_svs_from_spheres",
 )
@@ -70,6 +72,15 @@ def lib():
         "lrt_scene_export": [vp, P(SceneArrays)],
         "lrt_trace_nearest": [vp, vp, vp, u64, vp, u32],
         "lrt_trace_nearest_noalloc": [vp, vp, vp, u64, vp, u32],
+        "lrt_batch_create": [vp, vp, u32, P(vp)],
+        "lrt_batch_destroy": [vp],
+        "lrt_batch_ray_offsets": [vp, vp],
+        "lrt_batch_update_cameras": [vp, vp],
+        "lrt_batch_set_shape": [vp, P(BatchShape)],
+        "lrt_batch_get_shape": [vp, P(BatchShape)],
+        "lrt_batch_trace": [vp, vp, vp, u32],
+        "lrt_batch_sync": [vp, vp],
+        "lrt_batch_autotune": [vp, vp, vp, u32, vp, u32, P(u32)],
         "lrt_trace_sync": [vp, vp, C.c_int32],
         "lrt_ray_query_nearest_hit": [vp, vp, vp, vp],
         "lrt_ray_query_any_hit": [vp, vp, vp, P(C.c_int32)],
@@ -255,3 +266,59 @@ class SceneRT:
     def generate_eye_rays(self, camera, rays_ptr, stream=0):
         self._check(lib().lrt_generate_eye_rays(self.h, C.byref(camera), C.c_void_p(rays_ptr),
                                                 C.c_void_p(stream) if stream else None))
+
+
+class CameraBatch:
+    """Batched multi-camera trace over a committed SceneRT (lrt_batch_*):
+    one persistent launch for all cameras, replayed from a CUDA graph."""
+
+    def __init__(self, scene, cameras):
+        self.scene = scene
+        self.n = len(cameras)
+        arr = (Camera * self.n)(*cameras)
+        h = C.c_void_p()
+        scene._check(lib().lrt_batch_create(scene.h, arr, self.n, C.byref(h)))
+        self.h = h
+        off = np.zeros(self.n + 1, np.uint64)
+        scene._check(lib().lrt_batch_ray_offsets(self.h, off.ctypes.data))
+        self.offsets = off
+        self.total_rays = int(off[-1])
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().lrt_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def update_cameras(self, cameras):
+        arr = (Camera * self.n)(*cameras)
+        self.scene._check(lib().lrt_batch_update_cameras(self.h, arr))
+
+    @property
+    def shape(self):
+        s = BatchShape()
+        self.scene._check(lib().lrt_batch_get_shape(self.h, C.byref(s)))
+        return s.as_tuple()
+
+    def set_shape(self, tile_w, tile_h, rays_per_lane, stack_cap):
+        s = BatchShape(tile_w, tile_h, rays_per_lane, stack_cap)
+        self.scene._check(lib().lrt_batch_set_shape(self.h, C.byref(s)))
+
+    def trace(self, hits_ptr, stream=0, graph=True):
+        self.scene._check(lib().lrt_batch_trace(self.h, C.c_void_p(hits_ptr), C.c_void_p(stream) if stream else None,
+                                                0 if graph else LRT_BATCH_NO_GRAPH))
+
+    def sync(self, stream=0):
+        self.scene._check(lib().lrt_batch_sync(self.h, C.c_void_p(stream) if stream else None))
+
+    def autotune(self, hits_ptr, stream=0, reps=3):
+        table = (TuneEntry * 64)()
+        n = C.c_uint32()
+        self.scene._check(lib().lrt_batch_autotune(self.h, C.c_void_p(hits_ptr), C.c_void_p(stream) if stream else None,
+                                                   reps, table, 64, C.byref(n)))
+        return [(table[i].shape.as_tuple(), float(table[i].ms)) for i in range(n.value)]

@@ -354,6 +354,57 @@ typedef struct lrt_camera {
  * memory `rays_dev`. */
 lrt_status lrt_generate_eye_rays(lrt_scene* scene, const lrt_camera* camera, float* rays_dev, void* stream);
 
+/* ------------------------------------------------------------------------ */
+/* Batched multi-camera form                                                */
+/* ------------------------------------------------------------------------ */
+/* The reference renders cameras one at a time (UpdateCamera + Render per
+ * camera, render_CLI/offscreen_render.cpp:222-235).  A camera batch traces
+ * the primary rays of many cameras of uneven sizes in ONE persistent launch:
+ * each pixel's ray is generated in the kernel exactly as
+ * lrt_generate_eye_rays does and traced exactly as lrt_trace_nearest does, so
+ * every hit equals the per-camera path's.  The camera-table upload and the
+ * launch are captured in a CUDA graph on first use and replayed afterwards.
+ * Hits of camera i are at hits[offsets[i] + y*width + x]. */
+typedef struct lrt_camera_batch lrt_camera_batch;
+
+/* Launch shape: tiles of tile_w x tile_h pixels (tile_w * tile_h must be
+ * 32 * rays_per_lane) taken by one warp at a time, each lane tracing
+ * rays_per_lane pixels; stack_cap traversal-stack entries per thread in
+ * shared memory (at least the scene's BLAS depth + 1, at most 81). */
+typedef struct lrt_batch_shape {
+  uint32_t tile_w;
+  uint32_t tile_h;
+  uint32_t rays_per_lane;
+  uint32_t stack_cap;
+} lrt_batch_shape;
+
+typedef struct lrt_batch_tune_entry {
+  lrt_batch_shape shape;
+  float ms; /* mean time of one batched trace with this shape */
+} lrt_batch_tune_entry;
+
+#define LRT_BATCH_NO_GRAPH 0x1u /* lrt_batch_trace: launch directly instead of replaying the graph */
+
+lrt_status lrt_batch_create(lrt_scene* scene, const lrt_camera* cams, uint32_t count, lrt_camera_batch** out);
+lrt_status lrt_batch_destroy(lrt_camera_batch* batch);
+/* count + 1 prefix offsets of the cameras' hits. */
+lrt_status lrt_batch_ray_offsets(const lrt_camera_batch* batch, uint64_t* offsets);
+/* New camera matrices (same image sizes); picked up by the next replay. */
+lrt_status lrt_batch_update_cameras(lrt_camera_batch* batch, const lrt_camera* cams);
+lrt_status lrt_batch_set_shape(lrt_camera_batch* batch, const lrt_batch_shape* shape);
+lrt_status lrt_batch_get_shape(const lrt_camera_batch* batch, lrt_batch_shape* shape);
+/* Asynchronous on `stream`; hits_dev: device memory for offsets[count] hits,
+ * 16-byte aligned. */
+lrt_status lrt_batch_trace(lrt_camera_batch* batch, lrt_hit* hits_dev, void* stream, uint32_t flags);
+/* Waits for `stream`; LRT_ERR_DEVICE_LIMIT if a batched trace hit a bounded-loop limit. */
+lrt_status lrt_batch_sync(lrt_camera_batch* batch, void* stream);
+/* The project autotuner: times every candidate shape (tiles 32x1, 16x2, 8x4,
+ * 4x8 at 1 ray per lane, 16x4 and 8x8 at 2, 16x8 and 8x16 at 4; stack
+ * capacities depth+1 and 81) over `reps` launches each on `stream`, keeps the
+ * fastest, and reports every timing in `table` (up to table_cap entries). */
+lrt_status lrt_batch_autotune(lrt_camera_batch* batch, lrt_hit* hits_dev, void* stream, uint32_t reps,
+                              lrt_batch_tune_entry* table, uint32_t table_cap, uint32_t* table_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,86 @@
+"""Batched multi-camera form: one persistent launch (replayed from a CUDA
+graph) gives exactly the hits of per-camera eye-ray generation + trace."""
+import numpy as np
+import pytest
+
+from graphic_lab_task_b200 import SceneRT, workloads as wl
+from graphic_lab_task_b200.lrt import CameraBatch, LrtError
+
+pytestmark = pytest.mark.gpu
+
+
+def _sbs_scene(grid=128):
+    sph = wl.spheres(64, seed=1)
+    hdr, nodes, vals, vf = wl.sbs_from_spheres(sph, grid_res=grid)
+    sc = SceneRT()
+    sc.AddInstance(sc.AddGeom_SdfSBS(hdr, nodes, vals, vf), wl.IDENTITY)
+    sc.CommitScene()
+    return sc
+
+
+def _plain(torch, sc, cams):
+    """The per-camera path: lrt_generate_eye_rays + lrt_trace_nearest per camera."""
+    out = []
+    for cam in cams:
+        n = cam.width * cam.height
+        R = torch.empty(n * 8, dtype=torch.float32, device="cuda")
+        H = torch.empty(n * 8, dtype=torch.float32, device="cuda")
+        sc.generate_eye_rays(cam, R.data_ptr())
+        sc.trace_device(R.data_ptr(), H.data_ptr(), n)
+        out.append(H)
+    sc.sync()
+    return torch.cat(out)
+
+
+def test_batched_equals_per_camera(cuda):
+    torch = cuda
+    sc = _sbs_scene()
+    sizes = [(37, 53), (128, 128), (200, 75), (1, 1), (96, 33), (257, 129), (64, 64), (5, 300)]
+    cams = []
+    for i, (w, h) in enumerate(sizes):
+        eye = np.array([np.sin(i), 0.3, np.cos(i)])
+        cams.append(wl.camera(3.0 * eye / np.linalg.norm(eye), width=w, height=h))
+    want = _plain(torch, sc, cams)
+    b = CameraBatch(sc, cams)
+    assert b.total_rays == sum(w * h for w, h in sizes)
+    assert np.array_equal(b.offsets[1:] - b.offsets[:-1], [w * h for w, h in sizes])
+    H = torch.zeros(b.total_rays * 8, dtype=torch.float32, device="cuda")
+    for graph in (True, False, True):
+        H.zero_()
+        b.trace(H.data_ptr(), graph=graph)
+        b.sync()
+        assert torch.equal(H.view(torch.int32), want.view(torch.int32))
+    table = b.autotune(H.data_ptr(), reps=1)
+    assert len(table) >= 8 and all(ms > 0 for _, ms in table)
+    shape = b.shape
+    assert shape in [s for s, _ in table]
+    H.zero_()
+    b.trace(H.data_ptr())
+    b.sync()
+    assert torch.equal(H.view(torch.int32), want.view(torch.int32))
+
+
+def test_batched_every_shape_and_camera_update(cuda):
+    torch = cuda
+    sc = _sbs_scene(64)
+    cams = wl.sphere_cameras(6, res_min=16, res_max=90, seed=5)
+    want = _plain(torch, sc, cams)
+    b = CameraBatch(sc, cams)
+    H = torch.zeros(b.total_rays * 8, dtype=torch.float32, device="cuda")
+    for tw, th, rpl in ((32, 1, 1), (16, 2, 1), (8, 4, 1), (4, 8, 1), (16, 4, 2), (8, 8, 2), (16, 8, 4), (8, 16, 4)):
+        for cap in (b.shape[3], 81):
+            b.set_shape(tw, th, rpl, cap)
+            H.zero_()
+            b.trace(H.data_ptr())
+            b.sync()
+            assert torch.equal(H.view(torch.int32), want.view(torch.int32)), (tw, th, rpl, cap)
+    # new camera matrices, same sizes: the graph replays with the new table
+    cams2 = wl.sphere_cameras(6, res_min=16, res_max=90, seed=5)
+    for c in cams2:
+        c.world_view_inv[12] += 0.05
+    b.update_cameras(cams2)
+    b.trace(H.data_ptr())
+    b.sync()
+    assert torch.equal(H.view(torch.int32), _plain(torch, sc, cams2).view(torch.int32))
+    with pytest.raises(LrtError):
+        b.set_shape(8, 8, 1, b.shape[3])  # 8*8 != 32*1
