@@ -35,6 +35,7 @@ SOURCES = {
     "trace_fast.cu": ["-fmad=true", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
     "device.cu": [],
     "batch.cu": [],
+    "adjoint.cu": [],
     "scene.cpp": None,
     "layout.cpp": None,
     "workloads.cpp": None,

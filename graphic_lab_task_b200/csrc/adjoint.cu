@@ -1,0 +1,165 @@
+// adjoint.cu — differentiable form of the SBS ray query (C-ABI lrt_render_lambert,
+// lrt_adjoint_lambert_sbs, lrt_sbs_update_values).
+//
+// The reference has no differentiable renderer (its SparseDR sources are
+// absent); this is the project's adjoint sphere tracer: the forward pass
+// renders Lambert images through the same traversal as lrt_trace_nearest, the
+// adjoint pass recomputes the march and scatters dLoss/d(SBS float values)
+// by implicit differentiation at the hit (k_adjoint_lambert).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "device_scene.h"
+#include "trace_api.h"
+
+namespace lrt {
+namespace {
+
+// Re-resolves the dense corner grid and the surface-voxel mask of every brick
+// of one indexed SBS model from the (new) float values.  One block per brick.
+__global__ void k_sbs_rebuild(const lrt_sdf_sbs_node* __restrict__ nodes, const uint32_t* __restrict__ data,
+                              const float* __restrict__ dataF, DevSbs sb, uint32_t root, float* __restrict__ dense,
+                              uint32_t* __restrict__ mask)
+{
+  const uint32_t k = blockIdx.x;
+  const uint32_t bs = sb.brick_size, V1 = bs + 1, P = sb.pad, V = sb.vsize;
+  const uint32_t off = nodes[root + k].data_offset;
+  float* g = dense + sb.denseBase + uint64_t(k) * sb.denseStride;
+  for (uint32_t c = threadIdx.x; c < sb.denseStride; c += blockDim.x) {
+    const uint32_t x = c / (V1 * V1), y = (c / V1) % V1, z = c % V1;
+    g[c] = dataF[data[off + ((x + P) * V + (y + P)) * V + (z + P)]];
+  }
+  __syncthreads();
+  uint32_t* m = mask + sb.maskBase + uint64_t(k) * sb.maskStride;
+  for (uint32_t w = threadIdx.x; w < sb.maskStride; w += blockDim.x) m[w] = 0;
+  __syncthreads();
+  for (uint32_t v = threadIdx.x; v < bs * bs * bs; v += blockDim.x) {
+    const uint32_t x = v / (bs * bs), y = (v / bs) % bs, z = v % bs;
+    float vmin = 1e6f;
+    for (int c = 0; c < 8; c++) {
+      const float val = g[((x + ((c & 4) >> 2)) * V1 + (y + ((c & 2) >> 1))) * V1 + (z + (c & 1))];
+      vmin = (val < vmin) ? val : vmin; // load_distance_values' reduction
+    }
+    if (vmin <= 0.0f) {
+      atomicOr(m + 1 + v / 32, 1u << (v % 32));
+      atomicOr(m, 1u);
+    }
+  }
+}
+
+lrt_status check_rays(lrt_scene* s, const void* p)
+{
+  if (!p || (reinterpret_cast<uintptr_t>(p) & 15))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "rays/outputs must be non-NULL 16-byte aligned device memory");
+  return LRT_OK;
+}
+
+lrt_status begin(lrt_scene* s, cudaStream_t stream, StreamSlot** slot, DevScene* S)
+{
+  if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  if (!s->committed || !s->dev) return fail(s, LRT_ERR_NOT_COMMITTED, "render before CommitScene/upload");
+  lrt_status st = check_preset(s);
+  if (st != LRT_OK) return st;
+  // a dedicated slot past the per-stream ones is not needed: render and
+  // adjoint use the slot of their stream like lrt_trace_nearest
+  DeviceScene* d = s->dev;
+  auto it = d->slotOf.find(stream);
+  int idx;
+  if (it == d->slotOf.end()) {
+    if (int(d->slotOf.size()) >= kMaxStreams)
+      return fail(s, LRT_ERR_INVALID_ARGUMENT, "more than %d streams used with one scene", kMaxStreams);
+    idx = int(d->slotOf.size());
+    d->slotOf[stream] = idx;
+  } else {
+    idx = it->second;
+  }
+  *slot = d->slots + idx;
+  *S = d->S;
+  S->flags = preset_flags(s->preset);
+  S->voxelStepCap = s->voxelStepCap ? s->voxelStepCap : kMaxVoxelSteps;
+  cudaError_t e = cudaMemsetAsync(&(*slot)->work, 0, sizeof(unsigned long long), stream);
+  return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "cudaMemsetAsync");
+}
+
+} // namespace
+} // namespace lrt
+
+using namespace lrt;
+
+extern "C" {
+
+lrt_status lrt_sbs_update_values(lrt_scene* s, const float* values_f, uint64_t count, void* stream_p,
+                                 uint32_t flags)
+{
+  if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  if (!s->committed || !s->dev) return fail(s, LRT_ERR_NOT_COMMITTED, "lrt_sbs_update_values before upload");
+  DeviceScene* d = s->dev;
+  if (count != s->h.sdfSBSDataF.size() || !values_f)
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_sbs_update_values: %llu values, the scene holds %zu",
+                (unsigned long long)count, s->h.sdfSBSDataF.size());
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_p);
+  float* dst = const_cast<float*>(d->S.sbsDataF);
+  cudaError_t e = cudaMemcpyAsync(dst, values_f, count * sizeof(float),
+                                  (flags & LRT_TRACE_DEVICE_POINTERS) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                  stream);
+  if (e != cudaSuccess) return cuda_fail(s, e, "lrt_sbs_update_values copy");
+  // re-derive dense bricks and masks of the indexed models on the device
+  for (size_t g = 0; g < s->h.geomData.size(); g++) {
+    if (s->h.geomTags[g] != LRT_TAG_SDF_BRICK) continue;
+    const uint32_t sid = s->h.geomData[g].offset[0];
+    const DevSbs& sb = d->sbsHost[sid];
+    if (!sb.colorLayout || sb.nodeCount == 0) continue;
+    k_sbs_rebuild<<<sb.nodeCount, 128, 0, stream>>>(d->S.sbsNodes, d->S.sbsData, d->S.sbsDataF, sb,
+                                                    s->h.sdfSBSRoots[sid], const_cast<float*>(d->S.sbsDense),
+                                                    const_cast<uint32_t*>(d->S.sbsMask));
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(s, e, "brick rebuild");
+  }
+  // the pruned node pairs were derived from the old masks: trace the
+  // unpruned pairs from now on
+  d->S.pairs = d->pairsOrig;
+  return LRT_OK;
+}
+
+lrt_status lrt_render_lambert(lrt_scene* s, const float* rays_dev, uint64_t n, const float light[3], float* image_dev,
+                              void* stream_p)
+{
+  StreamSlot* slot = nullptr;
+  DevScene S;
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_p);
+  lrt_status st = begin(s, stream, &slot, &S);
+  if (st != LRT_OK) return st;
+  if (!light) return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_render_lambert: NULL light");
+  if ((st = check_rays(s, rays_dev)) != LRT_OK || (st = check_rays(s, image_dev)) != LRT_OK) return st;
+  if (n == 0) return LRT_OK;
+  DeviceScene* d = s->dev;
+  const int grid = int(std::min<uint64_t>(uint64_t(d->grid), (n + kTraceThreads - 1) / kTraceThreads));
+  cudaError_t e = lrt_exact::launch_render_lambert(S, reinterpret_cast<const float4*>(rays_dev), n,
+                                                   make_float3(light[0], light[1], light[2]), image_dev, &slot->work,
+                                                   &slot->err, d->stackCap, std::max(1, grid), stream);
+  return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "render launch");
+}
+
+lrt_status lrt_adjoint_lambert_sbs(lrt_scene* s, const float* rays_dev, uint64_t n, const float light[3],
+                                   const float* dimage_dev, float* grad_dev, void* stream_p)
+{
+  StreamSlot* slot = nullptr;
+  DevScene S;
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_p);
+  lrt_status st = begin(s, stream, &slot, &S);
+  if (st != LRT_OK) return st;
+  if (!light || !dimage_dev || !grad_dev)
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_adjoint_lambert_sbs: NULL argument");
+  if ((st = check_rays(s, rays_dev)) != LRT_OK) return st;
+  if (n == 0) return LRT_OK;
+  DeviceScene* d = s->dev;
+  const int grid = int(std::min<uint64_t>(uint64_t(d->grid), (n + kTraceThreads - 1) / kTraceThreads));
+  cudaError_t e = lrt_exact::launch_adjoint_lambert(S, reinterpret_cast<const float4*>(rays_dev), n,
+                                                    make_float3(light[0], light[1], light[2]), dimage_dev, grad_dev,
+                                                    &slot->work, &slot->err, d->stackCap, std::max(1, grid), stream);
+  return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "adjoint launch");
+}
+
+} // extern "C"

@@ -152,6 +152,16 @@ lrt_status device_upload(lrt_scene* s)
   UP(sbsDense, dense, float, "SBS dense bricks")
   UP(sbsMask, mask, uint32_t, "SBS surface-voxel masks")
   UP(sbs, sbs, DevSbs, "SBS table")
+  if (st == LRT_OK) {
+    if (h.sdfSBSNodes.empty()) {
+      d->pairsOrig = S.pairs; // nothing was pruned
+    } else {
+      const lrt_bvh_node_pair* p = nullptr;
+      st = upload_vec(s, d, h.allNodePairs.data(), h.allNodePairs.size(), &p, "unpruned node pairs");
+      d->pairsOrig = p;
+    }
+  }
+  d->sbsHost = sbs;
 #undef UP
   if (st != LRT_OK) {
     device_release(s);

@@ -75,6 +75,8 @@ struct DevSbs {
   uint32_t nodeCount;   // nodes of this model (leaves naming a node past it are skipped)
   uint32_t maskStride;  // words per brick in sbsMask: 1 + ceil(brick_size^3 / 32)
   uint64_t maskBase;    // first word of node `root` in sbsMask
+  uint32_t pad;         // brick_pad
+  uint32_t vsize;       // brick_size + 2*pad + 1
 };
 
 // sbsMask, per brick: word 0 is nonzero iff some voxel can start a sphere

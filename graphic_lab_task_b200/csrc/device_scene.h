@@ -28,6 +28,8 @@ struct DeviceScene {
   int grid = 0;
   StreamSlot* slots = nullptr; // device, kMaxStreams
   std::map<cudaStream_t, int> slotOf;
+  const lrt_bvh_node_pair* pairsOrig = nullptr; // unpruned node pairs (used once SBS values change)
+  std::vector<DevSbs> sbsHost;                  // host copy of the SBS model table
   // staging buffers for host-pointer calls
   float4* rays = nullptr;
   lrt_hit* hits = nullptr;

@@ -166,6 +166,8 @@ void build_sbs_dense(const HostArrays& h, std::vector<DevSbs>& sbs, std::vector<
     d.denseStride = V1 * V1 * V1;
     d.brick_size = hd.brick_size;
     d.v3 = v * v * v;
+    d.pad = hd.brick_pad;
+    d.vsize = v;
     const uint32_t layout = hd.aux_data & LRT_SBS_LAYOUT_MASK;
     d.colorLayout = (layout == LRT_SBS_LAYOUT_ID32F_IRGB32F || layout == LRT_SBS_LAYOUT_ID32F_IRGB32F_IN) ? 1u : 0u;
     total += counts[i] * d.denseStride;

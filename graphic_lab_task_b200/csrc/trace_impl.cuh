@@ -29,15 +29,37 @@ struct Counters {
   uint32_t c[LRT_COUNTER_COUNT];
 };
 
-template <bool COUNT>
+// What the adjoint needs about the final hit when it lies on an indexed SBS
+// brick: the 8 corner values and their indices in the float value array,
+// the voxel-local hit point, the object-space direction and the voxel size.
+struct HitRecord {
+  float t;          // hit.t when recorded (the record is valid iff it equals the final hit.t)
+  float values[8];
+  uint32_t idx[8];
+  f3 p;
+  f3 dir;
+  float d;
+  bool sbs;         // set by octree_brick for the indexed layouts
+};
+
+// Traversal context.  COUNT adds the work counters, RECORD the hit record;
+// the plain trace kernel instantiates neither.
+template <bool COUNT, bool RECORD = false>
 struct Ctx {
+  static constexpr bool kCount = COUNT;
+  static constexpr bool kRecord = RECORD;
   const DevScene& S;
   Counters cnt;
   uint32_t err;
+  HitRecord rec;
   __device__ explicit Ctx(const DevScene& s) : S(s), err(0)
   {
 #pragma unroll
     for (int i = 0; i < LRT_COUNTER_COUNT; i++) cnt.c[i] = 0;
+    if (RECORD) {
+      rec.t = -1.0f;
+      rec.sbs = false;
+    }
   }
   __device__ __forceinline__ void inc(int k, uint32_t v = 1)
   {
@@ -47,8 +69,8 @@ struct Ctx {
 
 __device__ __forceinline__ f3 ld3(const float4 v) { return mk3(v.x, v.y, v.z); }
 
-template <bool COUNT>
-__device__ void local_surface(Ctx<COUNT>& c, uint32_t type, f3 ray_dir, uint32_t instId, uint32_t geomId,
+template <class CTX>
+__device__ void local_surface(CTX& c, uint32_t type, f3 ray_dir, uint32_t instId, uint32_t geomId,
                               const float* values, uint32_t primId, float d, float qNear, float qFar, f2 fNearFar,
                               f3 start_q, lrt_hit& hit)
 {
@@ -104,6 +126,15 @@ __device__ void local_surface(Ctx<COUNT>& c, uint32_t type, f3 ray_dir, uint32_t
       c.inc(kCntNormals);
     }
     const f2 en = encode_normal(norm);
+    if (CTX::kRecord) {
+      c.rec.t = tReal;
+#pragma unroll
+      for (int i = 0; i < 8; i++) c.rec.values[i] = values[i];
+      c.rec.p = start_q + t * ray_dir;
+      c.rec.dir = ray_dir;
+      c.rec.d = d;
+      c.rec.sbs = false; // octree_brick marks its own hits
+    }
     hit.t = tReal;
     hit.primId = (S.flags & kFlagStIterations) ? iter : primId;
     hit.instId = instId;
@@ -115,8 +146,8 @@ __device__ void local_surface(Ctx<COUNT>& c, uint32_t type, f3 ray_dir, uint32_t
   }
 }
 
-template <bool COUNT>
-__device__ void octree_node(Ctx<COUNT>& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, float tNear, uint32_t instId,
+template <class CTX>
+__device__ void octree_node(CTX& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, float tNear, uint32_t instId,
                             uint32_t geomId, uint32_t bvhNodeId, lrt_hit& hit)
 {
   const DevScene& S = c.S;
@@ -161,8 +192,8 @@ __device__ void octree_node(Ctx<COUNT>& c, const DevGeom& g, f3 ray_pos, f3 ray_
   local_surface(c, g.type, ray_dir, instId, geomId, values, primId, d, qNear, qFar, fNearFar, start_q, hit);
 }
 
-template <bool COUNT>
-__device__ void octree_brick(Ctx<COUNT>& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, float tNear, uint32_t instId,
+template <class CTX>
+__device__ void octree_brick(CTX& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, float tNear, uint32_t instId,
                              uint32_t geomId, uint32_t bvhNodeId, lrt_hit& hit)
 {
   const DevScene& S = c.S;
@@ -225,6 +256,16 @@ __device__ void octree_brick(Ctx<COUNT>& c, const DevGeom& g, f3 ray_pos, f3 ray
       const f3 start_q = (start_pos - min_pos) * scale;
       const float qFar = (fNearFar.y - fNearFar.x) * scale;
       local_surface(c, g.type, ray_dir, instId, geomId, values, primId, d, 0.0f, qFar, fNearFar, start_q, hit);
+      if (CTX::kRecord && hit.t < old_t && sb.colorLayout) {
+        // indices of the 8 corner values in the float array (indexed layouts)
+        const uint32_t V = sb.vsize, P = sb.pad;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          const uint32_t vId = ((vx + ((i & 4) >> 2) + P) * V + (vy + ((i & 2) >> 1) + P)) * V + (vz + (i & 1) + P);
+          c.rec.idx[i] = __ldg(S.sbsData + node.z + vId);
+        }
+        c.rec.sbs = true;
+      }
     }
     bnf.x += smax(0.0f, fNearFar.y - bnf.x) + 1e-6f;
   }
@@ -251,8 +292,8 @@ __device__ void octree_brick(Ctx<COUNT>& c, const DevGeom& g, f3 ray_pos, f3 ray
   }
 }
 
-template <bool COUNT>
-__device__ void triangles(Ctx<COUNT>& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, float tNear, uint32_t instId,
+template <class CTX>
+__device__ void triangles(CTX& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, float tNear, uint32_t instId,
                           uint32_t geomId, uint32_t a_start, uint32_t a_count, lrt_hit& hit)
 {
   const DevScene& S = c.S;
@@ -290,8 +331,8 @@ __device__ void triangles(Ctx<COUNT>& c, const DevGeom& g, f3 ray_pos, f3 ray_di
 }
 
 // IntersectAllPrimitivesInLeaf: returns the tag if the hit moved closer.
-template <bool COUNT>
-__device__ __forceinline__ uint32_t leaf(Ctx<COUNT>& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, float tNear,
+template <class CTX>
+__device__ __forceinline__ uint32_t leaf(CTX& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, float tNear,
                                          uint32_t aabbId, uint32_t instId, uint32_t geomId, lrt_hit& hit)
 {
   const float tPrev = hit.t;
@@ -309,8 +350,8 @@ __device__ __forceinline__ uint32_t leaf(Ctx<COUNT>& c, const DevGeom& g, f3 ray
 }
 
 // BVH2TraverseF32 with the stack in shared memory (thread-strided).
-template <bool COUNT>
-__device__ void blas(Ctx<COUNT>& c, uint32_t* stack, uint32_t stride, uint32_t cap, f3 ray_pos, f3 ray_dir,
+template <class CTX>
+__device__ void blas(CTX& c, uint32_t* stack, uint32_t stride, uint32_t cap, f3 ray_pos, f3 ray_dir,
                      float tNear, uint32_t instId, uint32_t geomId, bool stopOnFirstHit, lrt_hit& hit)
 {
   const DevScene& S = c.S;
@@ -358,8 +399,8 @@ __device__ void blas(Ctx<COUNT>& c, uint32_t* stack, uint32_t stride, uint32_t c
 }
 
 // RayQuery_NearestHit for one ray.
-template <bool COUNT>
-__device__ void trace_one(Ctx<COUNT>& c, uint32_t* stack, uint32_t stride, uint32_t cap, float4 pn, float4 df,
+template <class CTX>
+__device__ void trace_one(CTX& c, uint32_t* stack, uint32_t stride, uint32_t cap, float4 pn, float4 df,
                           lrt_hit& hit)
 {
   const DevScene& S = c.S;
@@ -514,6 +555,150 @@ cudaError_t cameras_occupancy(uint32_t stack_cap, int* blocks_per_sm)
                                        int((kMaxStackDev + 1) * kTraceThreads * sizeof(uint32_t)));
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_trace_cameras, kTraceThreads, smem);
+}
+
+// Lambert shading of a hit, MultiRenderer::ResolveCommon for
+// LAMBERT_NO_TEX with one directional light of unit colour and albedo 1
+// (MultiRenderer_resolve.cpp:617-666): max(0, n . L) with n decoded from the
+// hit's octahedral normal (loadNormalTcFromGbuffer, :27-75); background 0.
+// Triangle normals are decoded too and turned towards the viewer.
+__device__ __forceinline__ float lambert(const lrt_hit& h, f3 dir, f3 L)
+{
+  if (h.primId == 0xFFFFFFFFu) return 0.0f;
+  f3 n = decode_normal(mk2(h.coords[2], h.coords[3]));
+  if ((h.geomId >> 24) == LRT_TYPE_MESH_TRIANGLE) n = ssign(dot(-1.0f * dir, n)) * n;
+  return smax(0.0f, dot(n, L));
+}
+
+// Forward render: image[i] = Lambert shade of ray i's nearest hit.
+__global__ void __launch_bounds__(kTraceThreads) k_render_lambert(DevScene S, const float4* __restrict__ rays,
+                                                                  uint64_t n, float3 light, float* __restrict__ image,
+                                                                  unsigned long long* __restrict__ work_counter,
+                                                                  uint32_t* __restrict__ err_word, uint32_t stack_cap)
+{
+  extern __shared__ uint32_t smem_stack[];
+  uint32_t* stack = smem_stack + threadIdx.x;
+  const uint32_t lane = threadIdx.x & 31;
+  Ctx<false> c(S);
+  const f3 L = mk3(light.x, light.y, light.z);
+  for (;;) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(work_counter, 32ull);
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    if (base >= n) break;
+    const uint64_t i = base + lane;
+    if (i < n) {
+      const float4 pn = __ldg(rays + 2 * i), df = __ldg(rays + 2 * i + 1);
+      lrt_hit h;
+      trace_one(c, stack, blockDim.x, stack_cap, pn, df, h);
+      image[i] = lambert(h, mk3(df.x, df.y, df.z), L);
+    }
+  }
+  if (c.err) atomicOr(err_word, c.err);
+}
+
+// Adjoint of the render with respect to the SBS float values.  The march is
+// recomputed (same traversal, recording the hit voxel), then at the hit
+// point p (voxel units) of the trilinear field f(p; theta):
+//   g = grad_p f,  n = M g / |M g|  (M = transformInvTransposed),
+//   dt/dtheta_i = -w_i(p) / (g . dir)            (implicit differentiation),
+//   dI/dtheta_i = [n.L > 0] * ( u . grad w_i(p) + (u^T H dir) dt/dtheta_i ),
+//   u = M^T (1 - n n^T) L / |M g|,  H = Hessian of f at p (mixed terms only),
+// and dLoss/dI * dI/dtheta_i is added to grad[idx_i] for the 8 corners.
+// Rays whose dLoss/dI is 0 are skipped.  Hits off indexed SBS bricks
+// contribute nothing.
+__global__ void __launch_bounds__(kTraceThreads) k_adjoint_lambert(DevScene S, const float4* __restrict__ rays,
+                                                                   uint64_t n, float3 light,
+                                                                   const float* __restrict__ dimage,
+                                                                   float* __restrict__ grad,
+                                                                   unsigned long long* __restrict__ work_counter,
+                                                                   uint32_t* __restrict__ err_word, uint32_t stack_cap)
+{
+  extern __shared__ uint32_t smem_stack[];
+  uint32_t* stack = smem_stack + threadIdx.x;
+  const uint32_t lane = threadIdx.x & 31;
+  const f3 L = mk3(light.x, light.y, light.z);
+  uint32_t err = 0;
+  for (;;) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(work_counter, 32ull);
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    if (base >= n) break;
+    const uint64_t i = base + lane;
+    if (i >= n) continue;
+    const float dLdI = __ldg(dimage + i);
+    if (dLdI == 0.0f) continue;
+    Ctx<false, true> c(S);
+    const float4 pn = __ldg(rays + 2 * i), df = __ldg(rays + 2 * i + 1);
+    lrt_hit h;
+    trace_one(c, stack, blockDim.x, stack_cap, pn, df, h);
+    err |= c.err;
+    if (h.primId == 0xFFFFFFFFu || !c.rec.sbs || c.rec.t != h.t) continue;
+    if (lambert(h, mk3(df.x, df.y, df.z), L) <= 0.0f) continue; // max(0, .) is flat there
+    const HitRecord& r = c.rec;
+    const float* M = S.instances[h.instId].transformInvTransposed;
+    const f3 p = r.p;
+    // trilinear gradient and mixed second derivatives at p
+    f3 g = mk3(0, 0, 0);
+    float hxy = 0, hxz = 0, hyz = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const float sx = (k & 4) ? 1.0f : -1.0f, sy = (k & 2) ? 1.0f : -1.0f, sz = (k & 1) ? 1.0f : -1.0f;
+      const float wx = (k & 4) ? p.x : 1.0f - p.x, wy = (k & 2) ? p.y : 1.0f - p.y, wz = (k & 1) ? p.z : 1.0f - p.z;
+      const float v = r.values[k];
+      g = g + v * mk3(sx * wy * wz, wx * sy * wz, wx * wy * sz);
+      hxy += v * sx * sy * wz;
+      hxz += v * sx * wy * sz;
+      hyz += v * wx * sy * sz;
+    }
+    const f3 m = matmul4(M, g, 0.0f);
+    const float inv_len = 1.0f / sqrtf(dot(m, m));
+    const f3 nn = inv_len * m;
+    const f3 q = inv_len * (L - dot(nn, L) * nn); // (1 - n n^T) L / |M g|
+    // u = M^T q (M column-major: M^T q has components dot(column_k, q))
+    const f3 u = mk3(M[0] * q.x + M[1] * q.y + M[2] * q.z, M[4] * q.x + M[5] * q.y + M[6] * q.z,
+                     M[8] * q.x + M[9] * q.y + M[10] * q.z);
+    const f3 dir = r.dir;
+    const f3 Hd = mk3(hxy * dir.y + hxz * dir.z, hxy * dir.x + hyz * dir.z, hxz * dir.x + hyz * dir.y);
+    const float uHd = dot(u, Hd);
+    const float gd = dot(g, dir);
+    if (gd == 0.0f) continue;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const float sx = (k & 4) ? 1.0f : -1.0f, sy = (k & 2) ? 1.0f : -1.0f, sz = (k & 1) ? 1.0f : -1.0f;
+      const float wx = (k & 4) ? p.x : 1.0f - p.x, wy = (k & 2) ? p.y : 1.0f - p.y, wz = (k & 1) ? p.z : 1.0f - p.z;
+      const float w = wx * wy * wz;
+      const f3 dw = mk3(sx * wy * wz, wx * sy * wz, wx * wy * sz);
+      const float dI = dot(u, dw) - uHd * w / gd;
+      atomicAdd(grad + r.idx[k], dLdI * dI);
+    }
+  }
+  if (err) atomicOr(err_word, err);
+}
+
+cudaError_t launch_render_lambert(const DevScene& S, const float4* rays, uint64_t n, float3 light, float* image,
+                                  unsigned long long* work_counter, uint32_t* err_word, uint32_t stack_cap, int grid,
+                                  cudaStream_t stream)
+{
+  const size_t smem = size_t(stack_cap) * kTraceThreads * sizeof(uint32_t);
+  cudaError_t e = cudaFuncSetAttribute(k_render_lambert, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int((kMaxStackDev + 1) * kTraceThreads * sizeof(uint32_t)));
+  if (e != cudaSuccess) return e;
+  k_render_lambert<<<grid, kTraceThreads, smem, stream>>>(S, rays, n, light, image, work_counter, err_word, stack_cap);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint_lambert(const DevScene& S, const float4* rays, uint64_t n, float3 light,
+                                   const float* dimage, float* grad, unsigned long long* work_counter,
+                                   uint32_t* err_word, uint32_t stack_cap, int grid, cudaStream_t stream)
+{
+  const size_t smem = size_t(stack_cap) * kTraceThreads * sizeof(uint32_t);
+  cudaError_t e = cudaFuncSetAttribute(k_adjoint_lambert, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int((kMaxStackDev + 1) * kTraceThreads * sizeof(uint32_t)));
+  if (e != cudaSuccess) return e;
+  k_adjoint_lambert<<<grid, kTraceThreads, smem, stream>>>(S, rays, n, light, dimage, grad, work_counter, err_word,
+                                                           stack_cap);
+  return cudaGetLastError();
 }
 
 // Eye rays of one camera (MultiRenderer::initEyeRay), row-major pixels.

@@ -28,7 +28,7 @@ EXPORTED = (
     "lrt_ray_query_any_hit", "lrt_get_work_counters", "lrt_generate_eye_rays", "lrt_set_voxel_step_limit",
     "lrt_trace_nearest_noalloc", "lrt_batch_create", "lrt_batch_destroy", "lrt_batch_ray_offsets",
     "lrt_batch_update_cameras", "lrt_batch_set_shape", "lrt_batch_get_shape", "lrt_batch_trace", "lrt_batch_sync",
-    "lrt_batch_autotune",
+    "lrt_batch_autotune", "lrt_render_lambert", "lrt_adjoint_lambert_sbs", "lrt_sbs_update_values",
     "lrt_wl_noisy_sphere", "lrt_wl_spheres", "lrt_wl_sphere_sdf", "lrt_wl_sbs_from_spheres",
     "lrt_wl_frame_octree_from_spheres", "lrt_wl_svs_from_spheres",
 )
@@ -72,6 +72,9 @@ def lib():
         "lrt_scene_export": [vp, P(SceneArrays)],
         "lrt_trace_nearest": [vp, vp, vp, u64, vp, u32],
         "lrt_trace_nearest_noalloc": [vp, vp, vp, u64, vp, u32],
+        "lrt_render_lambert": [vp, vp, u64, vp, vp, vp],
+        "lrt_adjoint_lambert_sbs": [vp, vp, u64, vp, vp, vp, vp],
+        "lrt_sbs_update_values": [vp, vp, u64, vp, u32],
         "lrt_batch_create": [vp, vp, u32, P(vp)],
         "lrt_batch_destroy": [vp],
         "lrt_batch_ray_offsets": [vp, vp],
@@ -244,6 +247,22 @@ class SceneRT:
 
     def sync(self, stream=0, read_counters=False):
         self._check(lib().lrt_trace_sync(self.h, C.c_void_p(stream) if stream else None, int(read_counters)))
+
+    # -- differentiable form (SBS distances) ------------------------------
+    def render_lambert(self, rays_ptr, n, light, image_ptr, stream=0):
+        L = (C.c_float * 3)(*[float(x) for x in light])
+        self._check(lib().lrt_render_lambert(self.h, C.c_void_p(rays_ptr), n, L, C.c_void_p(image_ptr),
+                                             C.c_void_p(stream) if stream else None))
+
+    def adjoint_lambert(self, rays_ptr, n, light, dimage_ptr, grad_ptr, stream=0):
+        L = (C.c_float * 3)(*[float(x) for x in light])
+        self._check(lib().lrt_adjoint_lambert_sbs(self.h, C.c_void_p(rays_ptr), n, L, C.c_void_p(dimage_ptr),
+                                                  C.c_void_p(grad_ptr), C.c_void_p(stream) if stream else None))
+
+    def update_sbs_values(self, values_ptr, count, device=True, stream=0):
+        self._check(lib().lrt_sbs_update_values(self.h, C.c_void_p(values_ptr), count,
+                                                C.c_void_p(stream) if stream else None,
+                                                LRT_TRACE_DEVICE_POINTERS if device else 0))
 
     def set_voxel_step_limit(self, steps):
         self._check(lib().lrt_set_voxel_step_limit(self.h, steps))

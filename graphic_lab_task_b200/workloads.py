@@ -210,6 +210,25 @@ def sphere_cameras(n, radius=3.0, res_min=128, res_max=2048, seed=3, fixed_res=N
     return cams
 
 
+LIGHT = (0.577, 0.577, 0.577)
+
+
+def adjoint_workload(grid_res=256, views=16, res=512, noise=0.01, seed=4, n_spheres=64, sphere_seed=1):
+    """Differentiable-render workload: the sphere-union SBS at `grid_res`^3,
+    `views` cameras of res x res on a radius-3 sphere, and target values =
+    the distances plus N(0, noise) per voxel value (palette untouched).
+    Returns (header, nodes, values, values_f, target_values_f, cameras, rays)."""
+    sph = spheres(n_spheres, seed=sphere_seed)
+    hdr, nodes, vals, vf = sbs_from_spheres(sph, grid_res=grid_res)
+    rng = np.random.default_rng(seed)
+    target = vf.copy()
+    first = 3 * n_spheres  # the palette precedes the distances
+    target[first:] += rng.normal(0.0, noise, size=len(vf) - first).astype(np.float32)
+    cams = sphere_cameras(views, radius=3.0, seed=seed + 1, fixed_res=res)
+    rays = np.concatenate([eye_rays_host(c) for c in cams])
+    return hdr, nodes, vals, vf, target, cams, rays
+
+
 def random_instances(n, seed=2, scale=(0.05, 0.2), trans=5.0):
     """n column-major transforms: uniform rotation (random unit quaternion),
     uniform scale in `scale`, translation U[-trans, trans]^3."""

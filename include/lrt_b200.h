@@ -355,6 +355,33 @@ typedef struct lrt_camera {
 lrt_status lrt_generate_eye_rays(lrt_scene* scene, const lrt_camera* camera, float* rays_dev, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Differentiable form (SBS distances)                                      */
+/* ------------------------------------------------------------------------ */
+/* No counterpart exists in the reference (its differentiable renderer
+ * sources are absent).  A Lambert image of n rays (device memory, 32 B per
+ * ray) is rendered through the same traversal as lrt_trace_nearest:
+ * image[i] = max(0, n_i . light) for the nearest hit's decoded normal
+ * (MultiRenderer_resolve.cpp:617-666 for LAMBERT_NO_TEX, one directional
+ * light of unit colour, albedo 1), 0 for misses.  Asynchronous on `stream`;
+ * lrt_trace_sync(stream) reports bounded-loop limits. */
+lrt_status lrt_render_lambert(lrt_scene* scene, const float* rays_dev, uint64_t n, const float light[3],
+                              float* image_dev, void* stream);
+
+/* Adjoint of lrt_render_lambert with respect to the scene's SBS float values
+ * (the sdfSBSDataF array of the indexed layouts): grad_dev[j] +=
+ * sum_i dimage_dev[i] * d image[i] / d values_f[j], by implicit
+ * differentiation at each hit with the march recomputed (not stored).
+ * grad_dev holds sdfSBSDataF_count floats and is accumulated into. */
+lrt_status lrt_adjoint_lambert_sbs(lrt_scene* scene, const float* rays_dev, uint64_t n, const float light[3],
+                                   const float* dimage_dev, float* grad_dev, void* stream);
+
+/* Replaces the scene's SBS float values (count must equal the uploaded
+ * sdfSBSDataF count; host memory, or device memory with
+ * LRT_TRACE_DEVICE_POINTERS) and re-derives the device brick layouts. */
+lrt_status lrt_sbs_update_values(lrt_scene* scene, const float* values_f, uint64_t count, void* stream,
+                                 uint32_t flags);
+
+/* ------------------------------------------------------------------------ */
 /* Batched multi-camera form                                                */
 /* ------------------------------------------------------------------------ */
 /* The reference renders cameras one at a time (UpdateCamera + Render per

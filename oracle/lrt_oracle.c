@@ -126,11 +126,23 @@ static inline float trilinear(const float v[8], f3 dp)
          (dp.x) * (dp.y) * (1 - dp.z) * v[6] + (dp.x) * (dp.y) * (dp.z) * v[7];
 }
 
+/* The hit voxel of an SBS hit, recorded for the adjoint (project-written:
+ * the reference has no differentiable renderer). */
+typedef struct {
+  float t;
+  float values[8];
+  uint32_t idx[8];
+  f3 p, dir;
+  float d;
+  int sbs;
+} hit_record_t;
+
 typedef struct {
   const lrt_scene_arrays* a;
   const lrt_preset* p;
   uint64_t* cnt;   /* LRT_COUNTER_COUNT entries (thread-local) */
   uint64_t limits; /* bounded-loop / bounds events */
+  hit_record_t* rec; /* NULL unless recording */
 } ctx_t;
 
 /* BVHRT::need_normal, BVH2Common.cpp:19-32 */
@@ -200,6 +212,14 @@ static void local_surface(ctx_t* c, uint32_t type, f3 ray_dir, uint32_t instId, 
       c->cnt[C_NORMALS]++;
     }
     const f2 en = encode_normal(norm);
+    if (c->rec) {
+      c->rec->t = tReal;
+      for (int i = 0; i < 8; i++) c->rec->values[i] = values[i];
+      c->rec->p = add3(start_q, scl3(t, ray_dir));
+      c->rec->dir = ray_dir;
+      c->rec->d = d;
+      c->rec->sbs = 0;
+    }
     hit->t = tReal;
     hit->primId = primId;
     hit->instId = instId;
@@ -342,6 +362,17 @@ static void octree_brick(ctx_t* c, uint32_t type, f3 ray_pos, f3 ray_dir, float 
       const f3 start_q = scl3(scale, sub3(start_pos, min_pos));
       const float qFar = (fNearFar.y - fNearFar.x) * scale;
       local_surface(c, type, ray_dir, instId, geomId, values, primId, d, 0.0f, qFar, fNearFar, start_q, hit);
+      const uint32_t layout = h.aux_data & LRT_SBS_LAYOUT_MASK;
+      if (c->rec && hit->t < old_t &&
+          (layout == LRT_SBS_LAYOUT_ID32F_IRGB32F || layout == LRT_SBS_LAYOUT_ID32F_IRGB32F_IN)) {
+        const uint32_t vx = (uint32_t)voxelPos.x, vy = (uint32_t)voxelPos.y, vz = (uint32_t)voxelPos.z;
+        for (int i = 0; i < 8; i++) {
+          const uint32_t vId = ((vx + ((i & 4) >> 2) + h.brick_pad) * v_size + (vy + ((i & 2) >> 1) + h.brick_pad)) *
+                                   v_size + (vz + (i & 1) + h.brick_pad);
+          c->rec->idx[i] = A->sdfSBSData[n->data_offset + vId];
+        }
+        c->rec->sbs = 1;
+      }
     }
     bnf.x += smax(0.0f, fNearFar.y - bnf.x) + 1e-6f;
   }
@@ -576,5 +607,105 @@ void lrto_trace_counted(const lrt_scene_arrays* arrays, const lrt_preset* preset
     ctx_t c = {arrays, preset, per_ray_counters + i * LRT_COUNTER_COUNT, 0};
     memset(c.cnt, 0, sizeof(uint64_t) * LRT_COUNTER_COUNT);
     hits[i] = nearest_hit(&c, rays + 8 * i, rays + 8 * i + 4);
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Lambert render and its FP64 adjoint (project-written; the reference has  */
+/* no differentiable renderer).                                             */
+/* ------------------------------------------------------------------------ */
+
+/* decode_normal, utils/raytracing/render_common.h:257-266 */
+static f3 decode_normal(float ex, float ey)
+{
+  f3 v = mk3(ex, ey, 1.0f - fabsf(ex) - fabsf(ey));
+  if (v.z < 0) {
+    const float vx = v.x;
+    v.x = (1.0f - fabsf(v.y)) * ((v.x >= 0.0f) ? +1.0f : -1.0f);
+    v.y = (1.0f - fabsf(vx)) * ((v.y >= 0.0f) ? +1.0f : -1.0f);
+  }
+  return normalize3(v);
+}
+
+/* ResolveCommon for LAMBERT_NO_TEX, one directional light of unit colour,
+ * albedo 1 (MultiRenderer_resolve.cpp:617-666); triangle normals turned to
+ * face the viewer as loadNormalTcFromGbuffer does (:58-59). */
+static float lambert(const lrt_hit* h, f3 dir, f3 L)
+{
+  if (h->primId == 0xFFFFFFFFu) return 0.0f;
+  f3 n = decode_normal(h->coords[2], h->coords[3]);
+  if ((h->geomId >> 24) == LRT_TYPE_MESH_TRIANGLE) n = scl3(ssign(dot3(scl3(-1.0f, dir), n)), n);
+  return smax(0.0f, dot3(n, L));
+}
+
+void lrto_render_lambert(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* rays, uint64_t n,
+                         const float light[3], float* image, int threads)
+{
+  (void)threads;
+  const f3 L = mk3(light[0], light[1], light[2]);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 256) num_threads(threads > 0 ? threads : 1)
+#endif
+  for (int64_t i = 0; i < (int64_t)n; i++) {
+    uint64_t cnt[LRT_COUNTER_COUNT];
+    ctx_t c = {arrays, preset, cnt, 0, NULL};
+    const lrt_hit h = nearest_hit(&c, rays + 8 * i, rays + 8 * i + 4);
+    image[i] = lambert(&h, ld3(rays + 8 * i + 4), L);
+  }
+}
+
+/* FP64 reference adjoint: for every ray with dimage[i] != 0 whose nearest hit
+ * lies on an indexed SBS brick, grad[idx_k] += dimage[i] * dI/dvalue_k with
+ * the implicit-differentiation formula of the GPU kernel evaluated in double
+ * (hit point, values and direction from the float march). */
+void lrto_adjoint_lambert_fp64(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* rays,
+                               uint64_t n, const float light[3], const float* dimage, double* grad)
+{
+  const f3 Lf = mk3(light[0], light[1], light[2]);
+  const double L[3] = {light[0], light[1], light[2]};
+  for (uint64_t i = 0; i < n; i++) {
+    if (dimage[i] == 0.0f) continue;
+    uint64_t cnt[LRT_COUNTER_COUNT];
+    hit_record_t rec;
+    rec.t = -1.0f;
+    rec.sbs = 0;
+    ctx_t c = {arrays, preset, cnt, 0, &rec};
+    const lrt_hit h = nearest_hit(&c, rays + 8 * i, rays + 8 * i + 4);
+    if (h.primId == 0xFFFFFFFFu || !rec.sbs || rec.t != h.t) continue;
+    if (lambert(&h, ld3(rays + 8 * i + 4), Lf) <= 0.0f) continue;
+    const float* Mf = arrays->instanceData[h.instId].transformInvTransposed;
+    double M[16];
+    for (int k = 0; k < 16; k++) M[k] = Mf[k];
+    const double p[3] = {rec.p.x, rec.p.y, rec.p.z}, dir[3] = {rec.dir.x, rec.dir.y, rec.dir.z};
+    double g[3] = {0, 0, 0}, hxy = 0, hxz = 0, hyz = 0, w[8], dw[8][3];
+    for (int k = 0; k < 8; k++) {
+      const double sx = (k & 4) ? 1 : -1, sy = (k & 2) ? 1 : -1, sz = (k & 1) ? 1 : -1;
+      const double wx = (k & 4) ? p[0] : 1 - p[0], wy = (k & 2) ? p[1] : 1 - p[1], wz = (k & 1) ? p[2] : 1 - p[2];
+      const double v = rec.values[k];
+      w[k] = wx * wy * wz;
+      dw[k][0] = sx * wy * wz;
+      dw[k][1] = wx * sy * wz;
+      dw[k][2] = wx * wy * sz;
+      for (int a = 0; a < 3; a++) g[a] += v * dw[k][a];
+      hxy += v * sx * sy * wz;
+      hxz += v * sx * wy * sz;
+      hyz += v * wx * sy * sz;
+    }
+    double m[3];
+    for (int r = 0; r < 3; r++) m[r] = M[r] * g[0] + M[4 + r] * g[1] + M[8 + r] * g[2];
+    const double len = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+    const double nn[3] = {m[0] / len, m[1] / len, m[2] / len};
+    const double nl = nn[0] * L[0] + nn[1] * L[1] + nn[2] * L[2];
+    const double q[3] = {(L[0] - nl * nn[0]) / len, (L[1] - nl * nn[1]) / len, (L[2] - nl * nn[2]) / len};
+    const double u[3] = {M[0] * q[0] + M[1] * q[1] + M[2] * q[2], M[4] * q[0] + M[5] * q[1] + M[6] * q[2],
+                         M[8] * q[0] + M[9] * q[1] + M[10] * q[2]};
+    const double Hd[3] = {hxy * dir[1] + hxz * dir[2], hxy * dir[0] + hyz * dir[2], hxz * dir[0] + hyz * dir[1]};
+    const double uHd = u[0] * Hd[0] + u[1] * Hd[1] + u[2] * Hd[2];
+    const double gd = g[0] * dir[0] + g[1] * dir[1] + g[2] * dir[2];
+    if (gd == 0.0) continue;
+    for (int k = 0; k < 8; k++) {
+      const double dI = u[0] * dw[k][0] + u[1] * dw[k][1] + u[2] * dw[k][2] - uHd * w[k] / gd;
+      grad[rec.idx[k]] += (double)dimage[i] * dI;
+    }
   }
 }

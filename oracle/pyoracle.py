@@ -182,6 +182,44 @@ class RefScene:
         return hits
 
 
+def port_render_lambert(arrays, rays, light, preset=None, threads=os.cpu_count()):
+    """Float Lambert image of the rays (the restatement of the GPU forward)."""
+    lib = port_lib()
+    if not hasattr(lib, "_render_bound"):
+        lib.lrto_render_lambert.restype = None
+        lib.lrto_render_lambert.argtypes = [C.POINTER(SceneArrays), C.POINTER(Preset), C.c_void_p, C.c_uint64,
+                                            C.c_void_p, C.c_void_p, C.c_int]
+        lib.lrto_adjoint_lambert_fp64.restype = None
+        lib.lrto_adjoint_lambert_fp64.argtypes = [C.POINTER(SceneArrays), C.POINTER(Preset), C.c_void_p, C.c_uint64,
+                                                  C.c_void_p, C.c_void_p, C.c_void_p]
+        lib._render_bound = True
+    s, keep = arrays_to_struct(arrays)
+    p = preset if preset is not None else parity_preset()
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    L = np.ascontiguousarray(light, dtype=np.float32)
+    img = np.zeros(len(rays), np.float32)
+    lib.lrto_render_lambert(C.byref(s), C.byref(p), rays.ctypes.data, len(rays), L.ctypes.data, img.ctypes.data,
+                            int(threads))
+    del keep
+    return img
+
+
+def port_adjoint_fp64(arrays, rays, light, dimage, preset=None):
+    """FP64 adjoint of the Lambert render w.r.t. the SBS float values."""
+    port_render_lambert(arrays, np.zeros((0, 8), np.float32), light, preset)  # binds the signatures
+    lib = port_lib()
+    s, keep = arrays_to_struct(arrays)
+    p = preset if preset is not None else parity_preset()
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    L = np.ascontiguousarray(light, dtype=np.float32)
+    di = np.ascontiguousarray(dimage, dtype=np.float32)
+    grad = np.zeros(len(arrays["sdfSBSDataF"]), np.float64)
+    lib.lrto_adjoint_lambert_fp64(C.byref(s), C.byref(p), rays.ctypes.data, len(rays), L.ctypes.data,
+                                  di.ctypes.data, grad.ctypes.data)
+    del keep
+    return grad
+
+
 def ref_trace(arrays, rays, preset=None, threads=1, fast=False):
     """Trace already-flattened arrays with the reference BVHRT."""
     sc = RefScene(fast=fast, preset=preset)
