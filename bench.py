@@ -316,6 +316,7 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_extras:
         del rays, hits, flush
         out["batched"] = batched_cameras(sc, dev, args)
+        out["adjoint"] = adjoint_section(dev, args)
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(sc, None, n)
     print(json.dumps(out))
@@ -382,6 +383,134 @@ def batched_cameras(sc, dev, args):
             "identical_hits": identical, "shape": {"tile_w": shape[0], "tile_h": shape[1],
                                                    "rays_per_lane": shape[2], "stack_cap": shape[3]},
             "autotune_s": tune_s, "autotune_candidates": len(table), "steps": steps}
+
+
+def adjoint_section(dev, args):
+    """Differentiable form: SBS at a virtual 256^3 grid, 16 views of 512x512
+    on a radius-3 sphere, Lambert under light (0.577,0.577,0.577), targets
+    rendered from the values plus N(0, 0.01); loss = mean L2 over all pixels.
+    Times the forward render and the adjoint pass (march recomputed), checks
+    the gradient by central differences (h = 1e-3) on 256 seeded voxels and
+    against the FP64 CPU adjoint on two views."""
+    import torch
+    from graphic_lab_task_b200 import SceneRT, workloads as wl
+    hdr, nodes, vals, vf, target, cams, rays = wl.adjoint_workload(grid_res=256, views=16, res=512)
+    sc = SceneRT()
+    sc.AddInstance(sc.AddGeom_SdfSBS(hdr, nodes, vals, vf), wl.IDENTITY)
+    sc.CommitScene()
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    n = len(rays)
+    R = torch.from_numpy(rays).to(dev)
+    V = torch.from_numpy(vf).to(dev)
+    T = torch.from_numpy(target).to(dev)
+    img = torch.empty(n, dtype=torch.float32, device=dev)
+    timg = torch.empty(n, dtype=torch.float32, device=dev)
+    grad = torch.zeros(len(vf), dtype=torch.float32, device=dev)
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    L = wl.LIGHT
+
+    def render(values, out):
+        sc.update_sbs_values(values.data_ptr(), values.numel(), stream=sp)
+        sc.render_lambert(R.data_ptr(), n, L, out.data_ptr(), stream=sp)
+
+    render(T, timg)
+    render(V, img)
+    dimage = (2.0 / n) * (img - timg)
+    steps = max(3, min(args.steps, 20))
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize(dev)
+        tot = 0.0
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            tot += e0.elapsed_time(e1)
+        return tot / steps
+
+    fwd_ms = timed(lambda: sc.render_lambert(R.data_ptr(), n, L, img.data_ptr(), stream=sp))
+
+    def adj():
+        grad.zero_()
+        sc.adjoint_lambert(R.data_ptr(), n, L, dimage.data_ptr(), grad.data_ptr(), stream=sp)
+
+    adj_ms = timed(adj)
+    upd_ms = timed(lambda: sc.update_sbs_values(V.data_ptr(), V.numel(), stream=sp))
+    sc.sync(stream=sp)
+    loss0 = float(((img - timg).double() ** 2).mean())
+    g = grad.cpu().numpy()
+    # central differences on 256 seeded voxels with a nonzero gradient
+    rng = np.random.default_rng(7)
+    cand = np.nonzero(g != 0)[0]
+    pick = rng.choice(cand, size=min(256, len(cand)), replace=False)
+    h = 1e-3
+    tmp = torch.empty(n, dtype=torch.float32, device=dev)
+
+    def loss_at(k, delta):
+        V[k] += delta
+        render(V, tmp)
+        V[k] -= delta
+        return float(((tmp - timg).double() ** 2).mean())
+
+    t0 = time.perf_counter()
+    fd1 = np.array([(loss_at(int(k), h) - loss_at(int(k), -h)) / (2 * h) for k in pick])
+    fd2 = np.array([(loss_at(int(k), h / 2) - loss_at(int(k), -h / 2)) / h for k in pick])
+    fd_s = time.perf_counter() - t0
+    render(V, img)
+    ga = g[pick].astype(np.float64)
+    # A jump of the loss (a pixel switching between hit and miss or between
+    # voxels) makes fd(h/2) about twice fd(h); smooth voxels agree to O(h^2).
+    smooth = np.abs(fd1 - fd2) <= 0.25 * np.maximum(np.abs(fd1), np.abs(fd2))
+    fdr = (4 * fd2 - fd1) / 3  # Richardson: cancels the h^2 term
+
+    def stats(fd, m):
+        if not m.any():
+            return None
+        per = np.abs(fd[m] - ga[m]) / np.maximum(np.maximum(np.abs(fd[m]), np.abs(ga[m])), 1e-30)
+        return {"rel_l2": float(np.linalg.norm(fd[m] - ga[m]) / np.linalg.norm(fd[m])),
+                "median_rel": float(np.median(per)), "p90_rel": float(np.quantile(per, 0.9)),
+                "frac_within_1e-3": float((per <= 1e-3).mean())}
+
+    allm = np.ones(len(pick), bool)
+    out = {"grid": 256, "views": len(cams), "res": 512, "rays": n, "bricks": int(len(nodes)),
+           "values": int(len(vf)), "loss": loss0, "forward_ms": fwd_ms, "adjoint_ms": adj_ms,
+           "adjoint_over_forward": adj_ms / fwd_ms, "update_values_ms": upd_ms,
+           "forward_mrays_s": n / fwd_ms / 1e3, "nonzero_grad_values": int(len(cand)),
+           "fd": {"voxels": int(len(pick)), "h": h, "smooth_voxels": int(smooth.sum()),
+                  "all_h": stats(fd1, allm), "smooth_h": stats(fd1, smooth),
+                  "smooth_richardson": stats(fdr, smooth), "seconds": fd_s}}
+    # FP64 CPU adjoint on two views (oracle, checker only)
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    try:
+        import pyoracle as po
+        k = 2 * 512 * 512
+        sub = torch.zeros(len(vf), dtype=torch.float32, device=dev)
+        sc.adjoint_lambert(R.data_ptr(), k, L, dimage.data_ptr(), sub.data_ptr(), stream=sp)
+        sc.sync(stream=sp)
+        t0 = time.perf_counter()
+        g64 = po.port_adjoint_fp64(sc.export_arrays(), rays[:k], L, dimage[:k].cpu().numpy())
+        gs = sub.cpu().numpy().astype(np.float64)
+        out["fp64_cpu"] = {"views": 2, "rel_l2": float(np.linalg.norm(gs - g64) / np.linalg.norm(g64)),
+                           "seconds": time.perf_counter() - t0}
+        # central differences (h = 1e-6, double) of the FP64 surface model of
+        # every hit voxel, on the same 256 values, all views
+        t0 = time.perf_counter()
+        fdm = po.port_fd_model_fp64(sc.export_arrays(), rays, L, dimage.cpu().numpy(), pick)
+        per = np.abs(fdm - ga) / np.maximum(np.maximum(np.abs(fdm), np.abs(ga)), 1e-30)
+        out["fd"]["fp64_model"] = {"h": 1e-6, "rel_l2": float(np.linalg.norm(fdm - ga) / np.linalg.norm(fdm)),
+                                   "median_rel": float(np.median(per)), "max_rel": float(per.max()),
+                                   "frac_within_1e-3": float((per <= 1e-3).mean()),
+                                   "seconds": time.perf_counter() - t0}
+    except Exception as e:  # the checker is optional on a box without the oracle build
+        out["fp64_cpu"] = {"unavailable": str(e)}
+    sc.close()
+    return out
 
 
 def cpu_baseline(sc, rays_dev, n):

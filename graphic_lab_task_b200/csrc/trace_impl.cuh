@@ -40,6 +40,9 @@ struct HitRecord {
   f3 dir;
   float d;
   bool sbs;         // set by octree_brick for the indexed layouts
+  bool early;       // the field was already <= EPS where the ray entered the
+                    // voxel: the hit is that entry point, which does not move
+                    // with the values (no dt/dtheta term)
 };
 
 // Traversal context.  COUNT adds the work counters, RECORD the hit record;
@@ -134,6 +137,7 @@ __device__ void local_surface(CTX& c, uint32_t type, f3 ray_dir, uint32_t instId
       c.rec.dir = ray_dir;
       c.rec.d = d;
       c.rec.sbs = false; // octree_brick marks its own hits
+      c.rec.early = early_hit;
     }
     hit.t = tReal;
     hit.primId = (S.flags & kFlagStIterations) ? iter : primId;
@@ -660,16 +664,16 @@ __global__ void __launch_bounds__(kTraceThreads) k_adjoint_lambert(DevScene S, c
                      M[8] * q.x + M[9] * q.y + M[10] * q.z);
     const f3 dir = r.dir;
     const f3 Hd = mk3(hxy * dir.y + hxz * dir.z, hxy * dir.x + hyz * dir.z, hxz * dir.x + hyz * dir.y);
-    const float uHd = dot(u, Hd);
     const float gd = dot(g, dir);
-    if (gd == 0.0f) continue;
+    if (gd == 0.0f && !r.early) continue;
+    const float uHd = r.early ? 0.0f : dot(u, Hd); // early hits: the hit point is fixed
 #pragma unroll
     for (int k = 0; k < 8; k++) {
       const float sx = (k & 4) ? 1.0f : -1.0f, sy = (k & 2) ? 1.0f : -1.0f, sz = (k & 1) ? 1.0f : -1.0f;
       const float wx = (k & 4) ? p.x : 1.0f - p.x, wy = (k & 2) ? p.y : 1.0f - p.y, wz = (k & 1) ? p.z : 1.0f - p.z;
       const float w = wx * wy * wz;
       const f3 dw = mk3(sx * wy * wz, wx * sy * wz, wx * wy * sz);
-      const float dI = dot(u, dw) - uHd * w / gd;
+      const float dI = r.early ? dot(u, dw) : dot(u, dw) - uHd * w / gd;
       atomicAdd(grad + r.idx[k], dLdI * dI);
     }
   }

@@ -135,6 +135,7 @@ typedef struct {
   f3 p, dir;
   float d;
   int sbs;
+  int early; /* hit at the voxel entry (field already <= EPS there): fixed point */
 } hit_record_t;
 
 typedef struct {
@@ -219,6 +220,7 @@ static void local_surface(ctx_t* c, uint32_t type, f3 ray_dir, uint32_t instId, 
       c->rec->dir = ray_dir;
       c->rec->d = d;
       c->rec->sbs = 0;
+      c->rec->early = early_hit;
     }
     hit->t = tReal;
     hit->primId = primId;
@@ -702,10 +704,96 @@ void lrto_adjoint_lambert_fp64(const lrt_scene_arrays* arrays, const lrt_preset*
     const double Hd[3] = {hxy * dir[1] + hxz * dir[2], hxy * dir[0] + hyz * dir[2], hxz * dir[0] + hyz * dir[1]};
     const double uHd = u[0] * Hd[0] + u[1] * Hd[1] + u[2] * Hd[2];
     const double gd = g[0] * dir[0] + g[1] * dir[1] + g[2] * dir[2];
-    if (gd == 0.0) continue;
+    if (gd == 0.0 && !rec.early) continue;
     for (int k = 0; k < 8; k++) {
-      const double dI = u[0] * dw[k][0] + u[1] * dw[k][1] + u[2] * dw[k][2] - uHd * w[k] / gd;
+      const double dn = u[0] * dw[k][0] + u[1] * dw[k][1] + u[2] * dw[k][2];
+      const double dI = rec.early ? dn : dn - uHd * w[k] / gd; /* early hits: the hit point is fixed */
       grad[rec.idx[k]] += (double)dimage[i] * dI;
+    }
+  }
+}
+
+/* Lambert intensity of the FP64 surface model of one hit voxel: the root of
+ * the trilinear field along the ray next to the recorded hit point (Newton),
+ * or the recorded point itself for an early hit (the voxel entry point the
+ * march stopped at), its normal M grad f / |M grad f| and max(0, n . L). */
+static double model_intensity(const double v[8], const double p0[3], const double dir[3], const double M[16],
+                              const double L[3], int early)
+{
+  double s = 0.0, p[3] = {p0[0], p0[1], p0[2]}, g[3];
+  for (int it = 0; it < (early ? 1 : 50); it++) {
+    p[0] = p0[0] + s * dir[0];
+    p[1] = p0[1] + s * dir[1];
+    p[2] = p0[2] + s * dir[2];
+    double f = 0;
+    g[0] = g[1] = g[2] = 0;
+    for (int k = 0; k < 8; k++) {
+      const double wx = (k & 4) ? p[0] : 1 - p[0], wy = (k & 2) ? p[1] : 1 - p[1], wz = (k & 1) ? p[2] : 1 - p[2];
+      const double sx = (k & 4) ? 1 : -1, sy = (k & 2) ? 1 : -1, sz = (k & 1) ? 1 : -1;
+      f += v[k] * wx * wy * wz;
+      g[0] += v[k] * sx * wy * wz;
+      g[1] += v[k] * wx * sy * wz;
+      g[2] += v[k] * wx * wy * sz;
+    }
+    const double df = g[0] * dir[0] + g[1] * dir[1] + g[2] * dir[2];
+    if (df == 0.0) break;
+    const double step = f / df;
+    s -= step;
+    if (fabs(step) < 1e-15) break;
+  }
+  double m[3];
+  for (int r = 0; r < 3; r++) m[r] = M[r] * g[0] + M[4 + r] * g[1] + M[8 + r] * g[2];
+  const double len = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+  const double nl = (m[0] * L[0] + m[1] * L[1] + m[2] * L[2]) / len;
+  return nl > 0 ? nl : 0.0;
+}
+
+/* Central differences (step h, in double) of sum_i dimage[i] * I_i with
+ * respect to the value indices `keys` (sorted ascending), where I_i is the
+ * FP64 surface model of ray i's hit voxel.  This checks the implicit-
+ * differentiation formula without the rounding noise of the float32 march. */
+void lrto_fd_model_fp64(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* rays, uint64_t n,
+                        const float light[3], const float* dimage, const uint32_t* keys, uint64_t nkeys, double h,
+                        double* out, int threads)
+{
+  const f3 Lf = mk3(light[0], light[1], light[2]);
+  const double L[3] = {light[0], light[1], light[2]};
+  (void)threads;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1024) num_threads(threads > 0 ? threads : 1)
+#endif
+  for (int64_t i = 0; i < (int64_t)n; i++) {
+    if (dimage[i] == 0.0f) continue;
+    uint64_t cnt[LRT_COUNTER_COUNT];
+    hit_record_t rec;
+    rec.t = -1.0f;
+    rec.sbs = 0;
+    ctx_t c = {arrays, preset, cnt, 0, &rec};
+    const lrt_hit hh = nearest_hit(&c, rays + 8 * i, rays + 8 * i + 4);
+    if (hh.primId == 0xFFFFFFFFu || !rec.sbs || rec.t != hh.t) continue;
+    if (lambert(&hh, ld3(rays + 8 * i + 4), Lf) <= 0.0f) continue;
+    const float* Mf = arrays->instanceData[hh.instId].transformInvTransposed;
+    double M[16], v[8];
+    for (int k = 0; k < 16; k++) M[k] = Mf[k];
+    for (int k = 0; k < 8; k++) v[k] = rec.values[k];
+    const double p0[3] = {rec.p.x, rec.p.y, rec.p.z}, dir[3] = {rec.dir.x, rec.dir.y, rec.dir.z};
+    for (int k = 0; k < 8; k++) {
+      uint64_t lo = 0, hi = nkeys;
+      while (lo < hi) {
+        const uint64_t mid = (lo + hi) / 2;
+        if (keys[mid] < rec.idx[k]) lo = mid + 1; else hi = mid;
+      }
+      if (lo >= nkeys || keys[lo] != rec.idx[k]) continue;
+      double vp[8], vm[8];
+      for (int j = 0; j < 8; j++) vp[j] = vm[j] = v[j];
+      vp[k] += h;
+      vm[k] -= h;
+      const double d =
+          (model_intensity(vp, p0, dir, M, L, rec.early) - model_intensity(vm, p0, dir, M, L, rec.early)) / (2 * h);
+#ifdef _OPENMP
+#pragma omp atomic
+#endif
+      out[lo] += (double)dimage[i] * d;
     }
   }
 }

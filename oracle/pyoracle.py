@@ -220,6 +220,32 @@ def port_adjoint_fp64(arrays, rays, light, dimage, preset=None):
     return grad
 
 
+def port_fd_model_fp64(arrays, rays, light, dimage, keys, h=1e-6, preset=None, threads=os.cpu_count()):
+    """Central differences (FP64 surface model of each hit voxel) of
+    sum_i dimage[i] * I_i w.r.t. the value indices `keys`."""
+    lib = port_lib()
+    if not hasattr(lib, "_fd_bound"):
+        lib.lrto_fd_model_fp64.restype = None
+        lib.lrto_fd_model_fp64.argtypes = [C.POINTER(SceneArrays), C.POINTER(Preset), C.c_void_p, C.c_uint64,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_double, C.c_void_p,
+                                           C.c_int]
+        lib._fd_bound = True
+    s, keep = arrays_to_struct(arrays)
+    p = preset if preset is not None else parity_preset()
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    L = np.ascontiguousarray(light, dtype=np.float32)
+    di = np.ascontiguousarray(dimage, dtype=np.float32)
+    order = np.argsort(keys)
+    k = np.ascontiguousarray(np.asarray(keys, np.uint32)[order])
+    out = np.zeros(len(k), np.float64)
+    lib.lrto_fd_model_fp64(C.byref(s), C.byref(p), rays.ctypes.data, len(rays), L.ctypes.data, di.ctypes.data,
+                           k.ctypes.data, len(k), float(h), out.ctypes.data, int(threads))
+    del keep
+    res = np.empty_like(out)
+    res[order] = out
+    return res
+
+
 def ref_trace(arrays, rays, preset=None, threads=1, fast=False):
     """Trace already-flattened arrays with the reference BVHRT."""
     sc = RefScene(fast=fast, preset=preset)
