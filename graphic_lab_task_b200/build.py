@@ -36,6 +36,7 @@ SOURCES = {
     "device.cu": [],
     "batch.cu": [],
     "adjoint.cu": [],
+    "wavefront.cu": [],
     "scene.cpp": None,
     "layout.cpp": None,
     "workloads.cpp": None,

@@ -29,6 +29,7 @@ EXPORTED = (
     "lrt_trace_nearest_noalloc", "lrt_batch_create", "lrt_batch_destroy", "lrt_batch_ray_offsets",
     "lrt_batch_update_cameras", "lrt_batch_set_shape", "lrt_batch_get_shape", "lrt_batch_trace", "lrt_batch_sync",
     "lrt_batch_autotune", "lrt_render_lambert", "lrt_adjoint_lambert_sbs", "lrt_sbs_update_values",
+    "lrt_generate_bounce_rays",
     "lrt_wl_noisy_sphere", "lrt_wl_spheres", "lrt_wl_sphere_sdf", "lrt_wl_sbs_from_spheres",
     "lrt_wl_frame_octree_from_spheres", "lrt_wl_svs_from_spheres",
 )
@@ -73,6 +74,7 @@ def lib():
         "lrt_trace_nearest": [vp, vp, vp, u64, vp, u32],
         "lrt_trace_nearest_noalloc": [vp, vp, vp, u64, vp, u32],
         "lrt_render_lambert": [vp, vp, u64, vp, vp, vp],
+        "lrt_generate_bounce_rays": [vp, vp, vp, u64, u64, C.c_float, C.c_float, vp, vp],
         "lrt_adjoint_lambert_sbs": [vp, vp, u64, vp, vp, vp, vp],
         "lrt_sbs_update_values": [vp, vp, u64, vp, u32],
         "lrt_batch_create": [vp, vp, u32, P(vp)],
@@ -247,6 +249,11 @@ class SceneRT:
 
     def sync(self, stream=0, read_counters=False):
         self._check(lib().lrt_trace_sync(self.h, C.c_void_p(stream) if stream else None, int(read_counters)))
+
+    def generate_bounce_rays(self, rays_ptr, hits_ptr, n, seed, out_ptr, tnear=1e-4, tfar=1e9, stream=0):
+        self._check(lib().lrt_generate_bounce_rays(self.h, C.c_void_p(rays_ptr), C.c_void_p(hits_ptr), n, seed,
+                                                   tnear, tfar, C.c_void_p(out_ptr),
+                                                   C.c_void_p(stream) if stream else None))
 
     # -- differentiable form (SBS distances) ------------------------------
     def render_lambert(self, rays_ptr, n, light, image_ptr, stream=0):

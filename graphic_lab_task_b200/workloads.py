@@ -212,6 +212,31 @@ def sphere_cameras(n, radius=3.0, res_min=128, res_max=2048, seed=3, fixed_res=N
 
 LIGHT = (0.577, 0.577, 0.577)
 
+# Incoherent two-level workload: eye far enough out to see the instance cloud
+INSTANCED_EYE = (0.0, 0.0, 12.0)
+
+
+def build_instanced(scene, mesh_tris=(50000, 200000, 500000), octree_depth=8, n_instances=1024, seed=2,
+                    n_spheres=64, sphere_seed=1):
+    """Adds three noisy-sphere meshes (about `mesh_tris` triangles) and two
+    frame-octree SDF objects of the sphere union (depth `octree_depth`) to
+    `scene`, then `n_instances` instances with random similarity transforms
+    (uniform rotation, scale U[0.05, 0.2], translation U[-5, 5]^3), instance i
+    of geometry i % 5.  The two octree geometries hold the same octree: the
+    reference keeps one global origNodes array, overwritten by every
+    AddGeom_SdfFrameOctree (BVH2Common_host.cpp:531), so distinct octrees
+    would make the first one read the second one's boxes."""
+    geoms = []
+    for n in mesh_tris:
+        v, t = noisy_sphere(segments_for_triangles(n), seed=n)
+        geoms.append(scene.AddGeom_Triangles3f(v, t))
+    nodes = frame_octree_from_spheres(spheres(n_spheres, seed=sphere_seed), octree_depth)
+    geoms.append(scene.AddGeom_SdfFrameOctree(nodes))
+    geoms.append(scene.AddGeom_SdfFrameOctree(nodes))
+    for i, m in enumerate(random_instances(n_instances, seed=seed)):
+        scene.AddInstance(geoms[i % len(geoms)], m)
+    return geoms
+
 
 def adjoint_workload(grid_res=256, views=16, res=512, noise=0.01, seed=4, n_spheres=64, sphere_seed=1):
     """Differentiable-render workload: the sphere-union SBS at `grid_res`^3,

@@ -354,6 +354,17 @@ typedef struct lrt_camera {
  * memory `rays_dev`. */
 lrt_status lrt_generate_eye_rays(lrt_scene* scene, const lrt_camera* camera, float* rays_dev, void* stream);
 
+/* One cosine-weighted diffuse bounce ray per ray of a traced batch (a second
+ * wavefront): origin at the hit point, direction from
+ * MapSampleToCosineDistribution with power 1 (utils/raytracing/
+ * render_common.h:75-113) around the hit's decoded normal turned towards the
+ * incoming ray, two uniforms from a PCG hash of (ray index, seed), interval
+ * [tnear, tfar].  Rays whose primary ray missed get a NaN origin (a NaN ray
+ * misses everything; callers may drop them).  All buffers are device memory,
+ * 16-byte aligned; asynchronous on `stream`. */
+lrt_status lrt_generate_bounce_rays(lrt_scene* scene, const float* rays_dev, const lrt_hit* hits_dev, uint64_t n,
+                                    uint64_t seed, float tnear, float tfar, float* bounce_rays_dev, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Differentiable form (SBS distances)                                      */
 /* ------------------------------------------------------------------------ */
