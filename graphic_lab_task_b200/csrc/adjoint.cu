@@ -77,7 +77,7 @@ lrt_status begin(lrt_scene* s, cudaStream_t stream, StreamSlot** slot, DevScene*
   }
   *slot = d->slots + idx;
   *S = d->S;
-  S->flags = preset_flags(s->preset);
+  S->flags = launch_flags(s);
   S->voxelStepCap = s->voxelStepCap ? s->voxelStepCap : kMaxVoxelSteps;
   cudaError_t e = cudaMemsetAsync(&(*slot)->work, 0, sizeof(unsigned long long), stream);
   return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "cudaMemsetAsync");

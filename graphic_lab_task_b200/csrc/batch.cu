@@ -99,7 +99,7 @@ lrt_status set_shape(lrt_camera_batch* b, const DevBatchShape& sh)
 DevScene scene_params(lrt_scene* s)
 {
   DevScene S = s->dev->S;
-  S.flags = preset_flags(s->preset);
+  S.flags = launch_flags(s);
   S.voxelStepCap = s->voxelStepCap ? s->voxelStepCap : kMaxVoxelSteps;
   return S;
 }

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <vector>
@@ -33,7 +34,23 @@ uint32_t preset_flags(const lrt_preset& p)
   return f;
 }
 
+uint32_t launch_flags(const lrt_scene* s)
+{
+  return preset_flags(s->preset) | (s->dev->cleanBoxes ? kFlagCleanBoxes : 0u);
+}
+
 namespace {
+
+// True if every box of the nodes has either no NaN coordinate or six.
+bool boxes_clean(const lrt_bvh_node* n, size_t count)
+{
+  for (size_t i = 0; i < count; i++) {
+    int nans = 0;
+    for (int k = 0; k < 3; k++) nans += std::isnan(n[i].boxMin[k]) + std::isnan(n[i].boxMax[k]);
+    if (nans != 0 && nans != 6) return false;
+  }
+  return true;
+}
 
 template <class T>
 lrt_status upload_vec(lrt_scene* s, DeviceScene* d, const T* src, size_t count, const T** out, const char* name)
@@ -72,7 +89,7 @@ lrt_status launch(lrt_scene* s, const float4* rays, lrt_hit* hits, uint64_t n, c
 {
   DeviceScene* d = s->dev;
   DevScene S = d->S;
-  S.flags = preset_flags(s->preset);
+  S.flags = launch_flags(s);
   S.voxelStepCap = s->voxelStepCap ? s->voxelStepCap : kMaxVoxelSteps;
   const bool count = (flags & LRT_TRACE_COUNT_WORK) != 0;
   cudaError_t e = cudaMemsetAsync(&slot->work, 0, count ? offsetof(StreamSlot, err) : sizeof(unsigned long long),
@@ -162,6 +179,9 @@ lrt_status device_upload(lrt_scene* s)
     }
   }
   d->sbsHost = sbs;
+  d->cleanBoxes = boxes_clean(h.nodesTLAS.data(), h.nodesTLAS.size()) &&
+                  boxes_clean(reinterpret_cast<const lrt_bvh_node*>(pairs.data()), 2 * pairs.size()) &&
+                  boxes_clean(reinterpret_cast<const lrt_bvh_node*>(h.allNodePairs.data()), 2 * h.allNodePairs.size());
 #undef UP
   if (st != LRT_OK) {
     device_release(s);
@@ -387,7 +407,7 @@ extern "C" lrt_status lrt_trace_nearest_noalloc(lrt_scene* s, const float* rays,
   cudaStream_t stream = static_cast<cudaStream_t>(stream_p);
   DeviceScene* d = s->dev;
   DevScene S = d->S;
-  S.flags = preset_flags(s->preset);
+  S.flags = launch_flags(s);
   S.voxelStepCap = s->voxelStepCap ? s->voxelStepCap : kMaxVoxelSteps;
   // the array keeps the previous call's contents: the ray counter and the
   // error word must start at zero

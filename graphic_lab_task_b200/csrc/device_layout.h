@@ -32,6 +32,9 @@ constexpr uint32_t kFlagNeedNormal = 1u;
 constexpr uint32_t kFlagStIterations = 2u;
 constexpr uint32_t kFlagSurfaceMode = 4u; // REPRESENTATION_MODE_SURFACE
 constexpr uint32_t kFlagBBoxMode = 8u;    // SDF_OCTREE_NODE_INTERSECT_BBOX
+// every TLAS/BLAS node box has either no NaN coordinate or six (pruned pairs):
+// node tests may use ray_box_nodes for rays with finite origin, direction and inverse
+constexpr uint32_t kFlagCleanBoxes = 16u;
 
 // error bits of the per-launch error word
 constexpr uint32_t kErrStackOverflow = 1u;

@@ -30,6 +30,7 @@ struct DeviceScene {
   std::map<cudaStream_t, int> slotOf;
   const lrt_bvh_node_pair* pairsOrig = nullptr; // unpruned node pairs (used once SBS values change)
   std::vector<DevSbs> sbsHost;                  // host copy of the SBS model table
+  bool cleanBoxes = false;                      // every node box has 0 or 6 NaN coordinates
   // staging buffers for host-pointer calls
   float4* rays = nullptr;
   lrt_hit* hits = nullptr;
@@ -44,6 +45,7 @@ struct DeviceScene {
 
 // device.cu
 uint32_t preset_flags(const lrt_preset& p);
+uint32_t launch_flags(const lrt_scene* s); // preset flags + the uploaded scene's own
 lrt_status cuda_fail(lrt_scene* s, cudaError_t e, const char* what);
 
 } // namespace lrt

@@ -85,6 +85,28 @@ LRT_HD f2 ray_box(f3 o, f3 inv, f3 bmin, f3 bmax)
   return mk2(smax(tmin, smin(lo2, hi2)), smin(tmax, smax(lo2, hi2)));
 }
 
+// RayBoxIntersection2 with one-instruction min/max, for node tests only.
+// std::min/max differ from fminf/fmaxf only when an operand is NaN (and in
+// which zero they return for +0/-0).  A slab value inv*(b - o) is NaN only if
+// an inverse-direction component is infinite (SafeInverse of an exactly zero
+// component), so for rays with a finite inverse this returns the same
+// interval up to the sign of zeros — and node tests only compare the
+// interval ends (<=, <, >), where +0 == -0.  The caller checks finiteness.
+LRT_HD f2 ray_box_nodes(f3 o, f3 inv, f3 bmin, f3 bmax)
+{
+  const float lo = inv.x * (bmin.x - o.x);
+  const float hi = inv.x * (bmax.x - o.x);
+  const float lo1 = inv.y * (bmin.y - o.y);
+  const float hi1 = inv.y * (bmax.y - o.y);
+  const float lo2 = inv.z * (bmin.z - o.z);
+  const float hi2 = inv.z * (bmax.z - o.z);
+  const float tmin = fmaxf(fminf(lo, hi), fminf(lo1, hi1));
+  const float tmax = fminf(fmaxf(lo, hi), fmaxf(lo1, hi1));
+  return mk2(fmaxf(tmin, fminf(lo2, hi2)), fminf(tmax, fmaxf(lo2, hi2)));
+}
+
+LRT_HD bool finite3(f3 v) { return fabsf(v.x) < INFINITY && fabsf(v.y) < INFINITY && fabsf(v.z) < INFINITY; }
+
 // encode_normal, utils/raytracing/intersection_common.h:96-101 (octahedral)
 LRT_HD f2 encode_normal(f3 v)
 {

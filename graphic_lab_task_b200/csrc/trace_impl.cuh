@@ -353,6 +353,57 @@ __device__ __forceinline__ uint32_t leaf(CTX& c, const DevGeom& g, f3 ray_pos, f
   return (hit.t >= tPrev) ? LRT_TAG_NONE : g.tag;
 }
 
+// Node box test: the literal RayBoxIntersection2 or, when the caller has
+// established the conditions under which it decides the same, ray_box_nodes.
+template <bool FAST>
+__device__ __forceinline__ f2 node_box(f3 o, f3 inv, f3 bmin, f3 bmax)
+{
+  return FAST ? ray_box_nodes(o, inv, bmin, bmax) : ray_box(o, inv, bmin, bmax);
+}
+
+// Rays for which ray_box_nodes decides every node test like ray_box: finite
+// origin and direction (so a finite, non-zero inverse never meets an
+// infinite difference) and finite inverse, in a scene whose boxes are clean.
+__device__ __forceinline__ bool fast_nodes(const DevScene& S, f3 o, f3 d, f3 inv)
+{
+  return (S.flags & kFlagCleanBoxes) && finite3(o) && finite3(d) && finite3(inv);
+}
+
+// The descent of BVH2TraverseF32 (BVH2Common.cpp:3256-3284) down to the next
+// leaf; false if the stack would overflow.
+template <bool FAST, class CTX>
+__device__ __forceinline__ bool blas_descend(CTX& c, const float4* pairs, uint32_t* stack, uint32_t stride,
+                                             uint32_t cap, f3 ray_pos, f3 inv, float tNear, float tHit, int& top,
+                                             uint32_t& leftNodeOffset)
+{
+  while (top >= 0 && ((leftNodeOffset & kLeafBit) == 0)) {
+    c.inc(kCntBlasPairs);
+    const float4* p = pairs + 4 * uint64_t(leftNodeOffset);
+    const float4 l0 = __ldg(p), l1 = __ldg(p + 1), r0 = __ldg(p + 2), r1 = __ldg(p + 3);
+    const uint32_t n0 = __float_as_uint(l0.w), n1 = __float_as_uint(r0.w);
+    const f2 tm0 = node_box<FAST>(ray_pos, inv, ld3(l0), ld3(l1));
+    const f2 tm1 = node_box<FAST>(ray_pos, inv, ld3(r0), ld3(r1));
+    const bool h0 = (tm0.x <= tm0.y) && (tm0.y >= tNear) && (tm0.x <= tHit);
+    const bool h1 = (tm1.x <= tm1.y) && (tm1.y >= tNear) && (tm1.x <= tHit);
+    leftNodeOffset = h0 ? n0 : n1;
+    if (h0 && h1) {
+      if (uint32_t(top) >= cap) {
+        c.err |= kErrStackOverflow;
+        return false;
+      }
+      const bool nearFirst = tm0.x <= tm1.x;
+      leftNodeOffset = nearFirst ? n0 : n1;
+      stack[top * stride] = nearFirst ? n1 : n0;
+      top++;
+    }
+    if (!h0 && !h1) {
+      top--;
+      leftNodeOffset = stack[(top > 0 ? top : 0) * stride];
+    }
+  }
+  return true;
+}
+
 // BVH2TraverseF32 with the stack in shared memory (thread-strided).
 template <class CTX>
 __device__ void blas(CTX& c, uint32_t* stack, uint32_t stride, uint32_t cap, f3 ray_pos, f3 ray_dir,
@@ -366,32 +417,13 @@ __device__ void blas(CTX& c, uint32_t* stack, uint32_t stride, uint32_t cap, f3 
   bool hitFound = false;
   stack[0] = 0;
   const f3 inv = safe_inverse(ray_dir);
+  const bool fast = fast_nodes(S, ray_pos, ray_dir, inv);
   while (top >= 0 && !hitFound) {
-    while (top >= 0 && ((leftNodeOffset & kLeafBit) == 0)) {
-      c.inc(kCntBlasPairs);
-      const float4* p = pairs + 4 * uint64_t(leftNodeOffset);
-      const float4 l0 = __ldg(p), l1 = __ldg(p + 1), r0 = __ldg(p + 2), r1 = __ldg(p + 3);
-      const uint32_t n0 = __float_as_uint(l0.w), n1 = __float_as_uint(r0.w);
-      const f2 tm0 = ray_box(ray_pos, inv, ld3(l0), ld3(l1));
-      const f2 tm1 = ray_box(ray_pos, inv, ld3(r0), ld3(r1));
-      const bool h0 = (tm0.x <= tm0.y) && (tm0.y >= tNear) && (tm0.x <= hit.t);
-      const bool h1 = (tm1.x <= tm1.y) && (tm1.y >= tNear) && (tm1.x <= hit.t);
-      leftNodeOffset = h0 ? n0 : n1;
-      if (h0 && h1) {
-        if (uint32_t(top) >= cap) {
-          c.err |= kErrStackOverflow;
-          return;
-        }
-        const bool nearFirst = tm0.x <= tm1.x;
-        leftNodeOffset = nearFirst ? n0 : n1;
-        stack[top * stride] = nearFirst ? n1 : n0;
-        top++;
-      }
-      if (!h0 && !h1) {
-        top--;
-        leftNodeOffset = stack[(top > 0 ? top : 0) * stride];
-      }
-    }
+    const bool ok = fast ? blas_descend<true>(c, pairs, stack, stride, cap, ray_pos, inv, tNear, hit.t, top,
+                                              leftNodeOffset)
+                         : blas_descend<false>(c, pairs, stack, stride, cap, ray_pos, inv, tNear, hit.t, top,
+                                               leftNodeOffset);
+    if (!ok) return;
     if (top >= 0 && leftNodeOffset != 0xFFFFFFFFu) {
       const float tNearSdf = smax(tNear, 0.01f); // SDF_BIAS (BVH2Common.cpp:3306-3307)
       const uint32_t tag = leaf(c, g, ray_pos, ray_dir, tNearSdf, leftNodeOffset & 0x0FFFFFFFu, instId, geomId, hit);
@@ -400,6 +432,26 @@ __device__ void blas(CTX& c, uint32_t* stack, uint32_t stride, uint32_t cap, f3 
     top--;
     leftNodeOffset = stack[(top > 0 ? top : 0) * stride];
   }
+}
+
+// The stackless TLAS walk of RayQuery_NearestHit (BVH2Common.cpp:3346-3358)
+// up to the next intersected leaf or the end of the escape chain.
+template <bool FAST, class CTX>
+__device__ __forceinline__ void tlas_walk(CTX& c, f3 pos, f3 inv, float tmin, float tHit, uint32_t& nodeIdx,
+                                          uint32_t& travFlags, uint32_t& leftOffset)
+{
+  do {
+    c.inc(kCntTlasNodes);
+    const float4* np = reinterpret_cast<const float4*>(c.S.tlas + nodeIdx);
+    const float4 a = __ldg(np), b = __ldg(np + 1);
+    const f2 bh = node_box<FAST>(pos, inv, ld3(a), ld3(b));
+    const uint32_t intersects = (bh.x <= bh.y) && (bh.y > tmin) && (bh.x < tHit);
+    const uint32_t lo = __float_as_uint(a.w);
+    travFlags = (lo & kLeafBit) | intersects;
+    leftOffset = lo;
+    const bool leafOrNot = (travFlags & kLeafBit) != 0 || (travFlags & 1) == 0;
+    nodeIdx = leafOrNot ? __float_as_uint(b.w) : leftOffset;
+  } while (travFlags != (kLeafBit | 1u) && nodeIdx != 0 && nodeIdx < 0xFFFFFFFEu);
 }
 
 // RayQuery_NearestHit for one ray.
@@ -423,20 +475,13 @@ __device__ void trace_one(CTX& c, uint32_t* stack, uint32_t stride, uint32_t cap
   hit.coords[2] = 0.0f;
   hit.coords[3] = 0.0f;
   uint32_t nodeIdx = 0;
+  const bool fast = fast_nodes(S, pos, dir, inv);
   do {
     uint32_t travFlags = 0, leftOffset = 0;
-    do {
-      c.inc(kCntTlasNodes);
-      const float4* np = reinterpret_cast<const float4*>(S.tlas + nodeIdx);
-      const float4 a = __ldg(np), b = __ldg(np + 1);
-      const f2 bh = ray_box(pos, inv, ld3(a), ld3(b));
-      const uint32_t intersects = (bh.x <= bh.y) && (bh.y > tmin) && (bh.x < hit.t);
-      const uint32_t lo = __float_as_uint(a.w);
-      travFlags = (lo & kLeafBit) | intersects;
-      leftOffset = lo;
-      const bool leafOrNot = (travFlags & kLeafBit) != 0 || (travFlags & 1) == 0;
-      nodeIdx = leafOrNot ? __float_as_uint(b.w) : leftOffset;
-    } while (travFlags != (kLeafBit | 1u) && nodeIdx != 0 && nodeIdx < 0xFFFFFFFEu);
+    if (fast)
+      tlas_walk<true>(c, pos, inv, tmin, hit.t, nodeIdx, travFlags, leftOffset);
+    else
+      tlas_walk<false>(c, pos, inv, tmin, hit.t, nodeIdx, travFlags, leftOffset);
     if (travFlags == (kLeafBit | 1u)) {
       const uint32_t instId = leftOffset & 0x0FFFFFFFu;
       const DevInstance& I = S.instances[instId];

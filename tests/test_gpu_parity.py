@@ -126,6 +126,64 @@ def test_instanced_mixed_scene(cuda):
     assert {0, 3, 5, 11} <= types
 
 
+def _axis_parallel_mix(rays, seed):
+    """Every third ray gets one or two direction components set to exactly
+    zero (an infinite inverse component); some origins become NaN."""
+    rng = np.random.default_rng(seed)
+    out = rays.copy()
+    sel = np.arange(0, len(out), 3)
+    for i in sel:
+        d = out[i, 4:7].astype(np.float64)
+        zero = rng.choice(3, size=rng.integers(1, 3), replace=False)
+        d[zero] = 0.0
+        if not np.any(d):
+            d[2] = -1.0
+        out[i, 4:7] = (d / np.linalg.norm(d)).astype(np.float32)
+        out[i, 4 + zero] = 0.0
+    out[1::97, 0] = np.nan
+    return out
+
+
+def test_mixed_warps_of_axis_parallel_rays(cuda):
+    """Node tests use one-instruction min/max only for rays with a finite
+    origin, direction and inverse; warps that mix both kinds of ray, in a
+    two-level scene of all leaf types, equal the oracle bit for bit."""
+    sph = wl.spheres(32, seed=4)
+    sc = SceneRT()
+    v, t = wl.noisy_sphere(60, seed=2)
+    gm = sc.AddGeom_Triangles3f(v, t)
+    go = sc.AddGeom_SdfFrameOctree(wl.frame_octree_from_spheres(sph, 6))
+    gs = sc.AddGeom_SdfSVS(wl.svs_from_spheres(sph, 6))
+    hdr, nodes, vals, vf = wl.sbs_from_spheres(sph, grid_res=64)
+    gb = sc.AddGeom_SdfSBS(hdr, nodes, vals, vf)
+    for i, m in enumerate(wl.random_instances(48, seed=9, scale=(0.1, 0.4), trans=1.5)):
+        sc.AddInstance([gm, go, gs, gb][i % 4], m)
+    sc.AddInstance(gm, wl.IDENTITY)  # identity transform keeps the zero components in object space
+    sc.CommitScene()
+    rays = _axis_parallel_mix(wl.eye_rays_host(wl.camera((0.5, 0.7, 3.5), width=160, height=120)), seed=5)
+    got = _oracle_check(sc, rays)
+    zero_dir = np.any(rays[:, 4:7] == 0, axis=1)
+    assert np.any(got["primId"][zero_dir] != MISS) and np.any(got["primId"][~zero_dir] != MISS)
+
+
+def test_partially_nan_node_boxes(cuda):
+    """A node box with some but not all coordinates NaN makes the literal
+    std::min/std::max order matter: such a scene takes the literal node tests
+    for every ray and still equals the oracle on the same arrays."""
+    arrays, rays, _, preset = load_golden("mesh_small")
+    pairs = arrays["allNodePairs"].copy()
+    assert len(pairs) > 8
+    for k in range(1, len(pairs), 5):
+        pairs[k]["left"]["boxMin"][k % 3] = np.nan
+        pairs[k]["right"]["boxMax"][(k + 1) % 3] = np.nan
+    arrays = dict(arrays, allNodePairs=pairs)
+    sc = SceneRT(preset=preset)
+    sc.upload_arrays(arrays)
+    got = sc.RayQuery_NearestHitBatch(rays)
+    want = po.port_trace(arrays, rays, preset=preset)
+    assert bit_equal(got, want).all(), hit_summary(got, want)
+
+
 def test_device_eye_rays_equal_host(cuda):
     torch = cuda
     v, t = wl.noisy_sphere(10)
