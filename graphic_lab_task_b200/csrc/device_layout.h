@@ -15,6 +15,7 @@
 //                 and SDF ids the traversal needs (one load per BLAS entry).
 // Values are copied bit for bit, so results do not depend on the layout.
 #pragma once
+#include <stddef.h>
 #include <stdint.h>
 #include <vector_types.h>
 
@@ -23,6 +24,14 @@
 namespace lrt {
 
 constexpr int kTraceThreads = 128;
+// Per-thread shared-memory words after the traversal stack: the inputs of the
+// deferred SDF normal (sign, sample point, 8 corner values).
+constexpr uint32_t kNormalWords = 12;
+// Dynamic shared memory of a trace kernel with stack_cap stack entries per thread.
+constexpr size_t trace_smem_bytes(uint32_t stack_cap)
+{
+  return size_t(stack_cap + kNormalWords) * kTraceThreads * sizeof(uint32_t);
+}
 constexpr uint32_t kMaxStackDev = 80; // STACK_SIZE of raytrace_common.h:36
 constexpr uint32_t kLeafBit = 0x80000000u;
 constexpr uint32_t kMaxVoxelSteps = 4096u; // voxel-march cap per brick (the reference loop is unbounded)

@@ -46,16 +46,19 @@ struct HitRecord {
 };
 
 // Traversal context.  COUNT adds the work counters, RECORD the hit record;
-// the plain trace kernel instantiates neither.
+// the plain trace kernel instantiates neither.  nrec points at this thread's
+// kNormalWords shared-memory words (thread-strided), where a sphere-traced
+// hit leaves what its normal is computed from once the traversal has ended.
 template <bool COUNT, bool RECORD = false>
 struct Ctx {
   static constexpr bool kCount = COUNT;
   static constexpr bool kRecord = RECORD;
   const DevScene& S;
+  float* nrec;
   Counters cnt;
   uint32_t err;
   HitRecord rec;
-  __device__ explicit Ctx(const DevScene& s) : S(s), err(0)
+  __device__ Ctx(const DevScene& s, float* normal_rec) : S(s), nrec(normal_rec), err(0)
   {
 #pragma unroll
     for (int i = 0; i < LRT_COUNTER_COUNT; i++) cnt.c[i] = 0;
@@ -71,6 +74,47 @@ struct Ctx {
 };
 
 __device__ __forceinline__ f3 ld3(const float4 v) { return mk3(v.x, v.y, v.z); }
+
+// This thread's deferred-normal words: after a stack of stack_cap entries.
+__device__ __forceinline__ float* normal_words(uint32_t* smem, uint32_t stack_cap)
+{
+  return reinterpret_cast<float*>(smem + stack_cap * blockDim.x) + threadIdx.x;
+}
+
+// The normal of LocalSurfaceIntersection (BVH2Common.cpp:652-680) from the
+// words a hit left: sign, sample point (start_q in the BBOX mode) and corner
+// values; normalised in world space and octahedrally encoded.
+template <class CTX>
+__device__ __forceinline__ f2 deferred_normal(CTX& c, uint32_t instId)
+{
+  const DevScene& S = c.S;
+  const uint32_t st = blockDim.x;
+  const float* w = c.nrec;
+  const float start_sign = w[0];
+  const f3 q = mk3(w[st], w[2 * st], w[3 * st]);
+  f3 norm;
+  if (S.flags & kFlagBBoxMode) { // every hit is an early hit in this mode
+    const f3 v = mk3(smax(q.x, 1 - q.x), smax(q.y, 1 - q.y), smax(q.z, 1 - q.z));
+    const float qa[3] = {q.x, q.y, q.z};
+    int dim = 0;
+    if (v.y > v.x && v.y > v.z) dim = 1;
+    else if (v.z > v.x && v.z > v.y) dim = 2;
+    float nn[3] = {0, 0, 0};
+    nn[dim] = qa[dim] < 0.5f ? -1.0f : 1.0f;
+    norm = mk3(nn[0], nn[1], nn[2]);
+  } else {
+    float values[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) values[i] = w[(4 + i) * st];
+    const float h = 0.001f;
+    const float ddx = (trilinear(values, q + mk3(h, 0, 0)) - trilinear(values, q + mk3(-h, 0, 0))) / (2 * h);
+    const float ddy = (trilinear(values, q + mk3(0, h, 0)) - trilinear(values, q + mk3(0, -h, 0))) / (2 * h);
+    const float ddz = (trilinear(values, q + mk3(0, 0, h)) - trilinear(values, q + mk3(0, 0, -h))) / (2 * h);
+    norm = start_sign * mk3(ddx, ddy, ddz);
+  }
+  norm = normalize(matmul4(S.instances[instId].transformInvTransposed, norm, 1.0f));
+  return encode_normal(norm);
+}
 
 template <class CTX>
 __device__ void local_surface(CTX& c, uint32_t type, f3 ray_dir, uint32_t instId, uint32_t geomId,
@@ -103,32 +147,23 @@ __device__ void local_surface(CTX& c, uint32_t type, f3 ray_dir, uint32_t instId
   }
   const float tReal = fNearFar.x + d * t;
   if (t <= qFar && hitf && tReal < hit.t) {
-    f3 norm = mk3(0, 0, 1);
+    // The normal is evaluated once the traversal has ended (trace_one), from
+    // what it depends on, kept here: lanes whose hits are found in different
+    // iterations of the surrounding loops then compute their normals together.
+    f2 en = encode_normal(mk3(0, 0, 1));
     if (S.flags & kFlagNeedNormal) {
-      if (early_hit && (S.flags & kFlagBBoxMode)) {
-        const float q[3] = {start_q.x, start_q.y, start_q.z};
-        const f3 v = mk3(smax(start_q.x, 1 - start_q.x), smax(start_q.y, 1 - start_q.y), smax(start_q.z, 1 - start_q.z));
-        int dim = 0;
-        if (v.y > v.x && v.y > v.z) dim = 1;
-        else if (v.z > v.x && v.z > v.y) dim = 2;
-        float nn[3] = {0, 0, 0};
-        nn[dim] = q[dim] < 0.5f ? -1.0f : 1.0f;
-        norm = mk3(nn[0], nn[1], nn[2]);
-      } else {
-        const f3 p0 = start_q + t * ray_dir;
-        const float h = 0.001f;
-        const float ddx =
-            (trilinear(values, p0 + mk3(h, 0, 0)) - trilinear(values, p0 + mk3(-h, 0, 0))) / (2 * h);
-        const float ddy =
-            (trilinear(values, p0 + mk3(0, h, 0)) - trilinear(values, p0 + mk3(0, -h, 0))) / (2 * h);
-        const float ddz =
-            (trilinear(values, p0 + mk3(0, 0, h)) - trilinear(values, p0 + mk3(0, 0, -h))) / (2 * h);
-        norm = start_sign * mk3(ddx, ddy, ddz);
-      }
-      norm = normalize(matmul4(S.instances[instId].transformInvTransposed, norm, 1.0f));
+      const uint32_t st = blockDim.x;
+      // the sample point: start_q itself for the BBOX mode's early hits
+      const f3 q = (S.flags & kFlagBBoxMode) ? start_q : start_q + t * ray_dir;
+      c.nrec[0] = start_sign;
+      c.nrec[st] = q.x;
+      c.nrec[2 * st] = q.y;
+      c.nrec[3 * st] = q.z;
+#pragma unroll
+      for (int i = 0; i < 8; i++) c.nrec[(4 + i) * st] = values[i];
+      en = mk2(0.0f, 0.0f);
       c.inc(kCntNormals);
     }
-    const f2 en = encode_normal(norm);
     if (CTX::kRecord) {
       c.rec.t = tReal;
 #pragma unroll
@@ -492,6 +527,12 @@ __device__ void trace_one(CTX& c, uint32_t* stack, uint32_t stride, uint32_t cap
       if (c.err & kErrStackOverflow) break;
     }
   } while (nodeIdx < 0xFFFFFFFEu && !(stopOnFirstHit && hit.primId != 0xFFFFFFFFu));
+  // the normal of a sphere-traced final hit (all other hits carry theirs)
+  if ((S.flags & kFlagNeedNormal) && hit.geomId < 0xFFFFFFFFu && ((hit.geomId >> 24) != LRT_TYPE_MESH_TRIANGLE)) {
+    const f2 en = deferred_normal(c, hit.instId);
+    hit.coords[2] = en.x;
+    hit.coords[3] = en.y;
+  }
   if (hit.geomId < 0xFFFFFFFFu && ((hit.geomId >> 24) == LRT_TYPE_MESH_TRIANGLE)) {
     const DevGeom& g = S.geoms[hit.geomId & 0x00FFFFFFu];
     hit.primId = __ldg(S.primIndices + g.triBase + hit.primId);
@@ -503,7 +544,7 @@ __device__ void trace_one(CTX& c, uint32_t* stack, uint32_t stride, uint32_t cap
 // (persistent grid of ~one wave).  Stacks live in shared memory,
 // stack[i * blockDim + tid].
 template <bool COUNT>
-__global__ void __launch_bounds__(kTraceThreads) k_trace(DevScene S, const float4* __restrict__ rays,
+__global__ void __launch_bounds__(kTraceThreads, 6) k_trace(DevScene S, const float4* __restrict__ rays,
                                                          lrt_hit* __restrict__ hits, uint64_t n,
                                                          unsigned long long* __restrict__ work_counter,
                                                          unsigned long long* __restrict__ counters,
@@ -512,7 +553,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_trace(DevScene S, const float
   extern __shared__ uint32_t smem_stack[];
   uint32_t* stack = smem_stack + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
-  Ctx<COUNT> c(S);
+  Ctx<COUNT> c(S, normal_words(smem_stack, stack_cap));
   for (;;) {
     unsigned long long base = 0;
     if (lane == 0) base = atomicAdd(work_counter, 32ull);
@@ -545,7 +586,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_trace(DevScene S, const float
 // finds its camera by binary search over the tile bases, and each lane
 // generates (lrt::eye_ray, the function k_eye_rays uses) and traces its
 // raysPerLane pixels, so every hit equals the plain per-camera path's.
-__global__ void __launch_bounds__(kTraceThreads) k_trace_cameras(DevScene S, const DevBatchCamera* __restrict__ cams,
+__global__ void __launch_bounds__(kTraceThreads, 6) k_trace_cameras(DevScene S, const DevBatchCamera* __restrict__ cams,
                                                                  uint32_t ncams, uint32_t ntiles, DevBatchShape shape,
                                                                  lrt_hit* __restrict__ hits,
                                                                  unsigned long long* __restrict__ work_counter,
@@ -554,7 +595,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_trace_cameras(DevScene S, con
   extern __shared__ uint32_t smem_stack[];
   uint32_t* stack = smem_stack + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
-  Ctx<false> c(S);
+  Ctx<false> c(S, normal_words(smem_stack, shape.stackCap));
   for (;;) {
     unsigned long long tile = 0;
     if (lane == 0) tile = atomicAdd(work_counter, 1ull);
@@ -592,16 +633,16 @@ cudaError_t launch_trace_cameras(const DevScene& S, const DevBatchCamera* cams, 
                                  const DevBatchShape& shape, lrt_hit* hits, unsigned long long* work_counter,
                                  uint32_t* err_word, int grid, cudaStream_t stream)
 {
-  const size_t smem = size_t(shape.stackCap) * kTraceThreads * sizeof(uint32_t);
+  const size_t smem = trace_smem_bytes(shape.stackCap);
   k_trace_cameras<<<grid, kTraceThreads, smem, stream>>>(S, cams, ncams, ntiles, shape, hits, work_counter, err_word);
   return cudaGetLastError();
 }
 
 cudaError_t cameras_occupancy(uint32_t stack_cap, int* blocks_per_sm)
 {
-  const size_t smem = size_t(stack_cap) * kTraceThreads * sizeof(uint32_t);
+  const size_t smem = trace_smem_bytes(stack_cap);
   cudaError_t e = cudaFuncSetAttribute(k_trace_cameras, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int((kMaxStackDev + 1) * kTraceThreads * sizeof(uint32_t)));
+                                       int(trace_smem_bytes(kMaxStackDev + 1)));
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_trace_cameras, kTraceThreads, smem);
 }
@@ -628,7 +669,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_render_lambert(DevScene S, co
   extern __shared__ uint32_t smem_stack[];
   uint32_t* stack = smem_stack + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
-  Ctx<false> c(S);
+  Ctx<false> c(S, normal_words(smem_stack, stack_cap));
   const f3 L = mk3(light.x, light.y, light.z);
   for (;;) {
     unsigned long long base = 0;
@@ -677,7 +718,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_adjoint_lambert(DevScene S, c
     if (i >= n) continue;
     const float dLdI = __ldg(dimage + i);
     if (dLdI == 0.0f) continue;
-    Ctx<false, true> c(S);
+    Ctx<false, true> c(S, normal_words(smem_stack, stack_cap));
     const float4 pn = __ldg(rays + 2 * i), df = __ldg(rays + 2 * i + 1);
     lrt_hit h;
     trace_one(c, stack, blockDim.x, stack_cap, pn, df, h);
@@ -729,9 +770,9 @@ cudaError_t launch_render_lambert(const DevScene& S, const float4* rays, uint64_
                                   unsigned long long* work_counter, uint32_t* err_word, uint32_t stack_cap, int grid,
                                   cudaStream_t stream)
 {
-  const size_t smem = size_t(stack_cap) * kTraceThreads * sizeof(uint32_t);
+  const size_t smem = trace_smem_bytes(stack_cap);
   cudaError_t e = cudaFuncSetAttribute(k_render_lambert, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int((kMaxStackDev + 1) * kTraceThreads * sizeof(uint32_t)));
+                                       int(trace_smem_bytes(kMaxStackDev + 1)));
   if (e != cudaSuccess) return e;
   k_render_lambert<<<grid, kTraceThreads, smem, stream>>>(S, rays, n, light, image, work_counter, err_word, stack_cap);
   return cudaGetLastError();
@@ -741,9 +782,9 @@ cudaError_t launch_adjoint_lambert(const DevScene& S, const float4* rays, uint64
                                    const float* dimage, float* grad, unsigned long long* work_counter,
                                    uint32_t* err_word, uint32_t stack_cap, int grid, cudaStream_t stream)
 {
-  const size_t smem = size_t(stack_cap) * kTraceThreads * sizeof(uint32_t);
+  const size_t smem = trace_smem_bytes(stack_cap);
   cudaError_t e = cudaFuncSetAttribute(k_adjoint_lambert, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int((kMaxStackDev + 1) * kTraceThreads * sizeof(uint32_t)));
+                                       int(trace_smem_bytes(kMaxStackDev + 1)));
   if (e != cudaSuccess) return e;
   k_adjoint_lambert<<<grid, kTraceThreads, smem, stream>>>(S, rays, n, light, dimage, grad, work_counter, err_word,
                                                            stack_cap);
@@ -768,7 +809,7 @@ cudaError_t launch_trace(const DevScene& S, const float4* rays, lrt_hit* hits, u
                                 unsigned long long* work_counter, unsigned long long* counters, uint32_t* err_word,
                                 uint32_t stack_cap, int grid, cudaStream_t stream, bool count)
 {
-  const size_t smem = size_t(stack_cap) * kTraceThreads * sizeof(uint32_t);
+  const size_t smem = trace_smem_bytes(stack_cap);
   if (count)
     k_trace<true><<<grid, kTraceThreads, smem, stream>>>(S, rays, hits, n, work_counter, counters, err_word, stack_cap);
   else
@@ -779,7 +820,7 @@ cudaError_t launch_trace(const DevScene& S, const float4* rays, lrt_hit* hits, u
 
 cudaError_t set_trace_smem(uint32_t stack_cap)
 {
-  const int smem = int(stack_cap * kTraceThreads * sizeof(uint32_t));
+  const int smem = int(trace_smem_bytes(stack_cap));
   cudaError_t e = cudaFuncSetAttribute(k_trace<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_trace<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -787,7 +828,7 @@ cudaError_t set_trace_smem(uint32_t stack_cap)
 
 cudaError_t trace_occupancy(uint32_t stack_cap, int* blocks_per_sm)
 {
-  const size_t smem = size_t(stack_cap) * kTraceThreads * sizeof(uint32_t);
+  const size_t smem = trace_smem_bytes(stack_cap);
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_trace<false>, kTraceThreads, smem);
 }
 
