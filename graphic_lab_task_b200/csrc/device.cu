@@ -125,6 +125,98 @@ lrt_status finish(lrt_scene* s, cudaStream_t stream, StreamSlot* slot, bool coun
   return LRT_OK;
 }
 
+// Chunk sizes of the pipeline: kPipeChunkMin, doubling up to kPipeChunk,
+// chunks of at most kPipeChunk, and the ramp again in reverse, so that the
+// first copy in and the last trace and copy out, which nothing overlaps, are
+// short.  Inputs too small for the ramps get chunks of kPipeChunkMin.
+void pipeline_chunks(uint64_t n, std::vector<uint64_t>& out)
+{
+  out.clear();
+  std::vector<uint64_t> up;
+  uint64_t ramp = 0;
+  for (uint64_t m = kPipeChunkMin; m < kPipeChunk; m *= 2) {
+    up.push_back(m);
+    ramp += m;
+  }
+  if (n <= 2 * ramp) {
+    for (uint64_t off = 0; off < n; off += kPipeChunkMin) out.push_back(std::min(kPipeChunkMin, n - off));
+    return;
+  }
+  out = up;
+  const uint64_t mid = n - 2 * ramp;
+  const uint64_t parts = (mid + kPipeChunk - 1) / kPipeChunk;
+  for (uint64_t i = 0; i < parts; i++) out.push_back(mid / parts + (i < mid % parts ? 1 : 0));
+  out.insert(out.end(), up.rbegin(), up.rend());
+}
+
+// Host-pointer trace in chunks (staging buffers already hold n rays): chunk c
+// is copied in on kPipeIn, traced on trace stream c mod kPipeTraceStreams
+// once its copy is done, and copied out on kPipeOut once its trace is done.
+// The copies of consecutive chunks run back to back in both directions while
+// the traces of several chunks run at the same time.  The pipeline starts
+// after the work already queued on the caller's stream, and the caller's
+// stream waits for it.  Events are re-recorded once per chunk: a wait takes
+// the record made before it.
+lrt_status trace_host_pipelined(lrt_scene* s, const float* rays, lrt_hit* hits, uint64_t n, cudaStream_t stream,
+                                uint32_t flags)
+{
+  DeviceScene* d = s->dev;
+  cudaError_t e = cudaSuccess;
+  if (!d->pipeStart) {
+    for (int p = 0; p < kPipeStreams && e == cudaSuccess; p++) {
+      e = cudaStreamCreateWithFlags(&d->pipe[p], cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&d->pipeEv[p], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&d->pipeStart, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_fail(s, e, "pipeline streams");
+  }
+  cudaStream_t in = d->pipe[kPipeIn], out = d->pipe[kPipeOut];
+  StreamSlot* slots[kPipeTraceStreams];
+  for (int k = 0; k < kPipeTraceStreams; k++) {
+    lrt_status st = slot_for(s, d->pipe[kPipeTrace + k], &slots[k]);
+    if (st != LRT_OK) return st;
+  }
+  e = cudaEventRecord(d->pipeStart, stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(in, d->pipeStart, 0);
+  if (e != cudaSuccess) return cuda_fail(s, e, "pipeline start");
+  lrt_status st = LRT_OK;
+  std::vector<uint64_t> chunks;
+  pipeline_chunks(n, chunks);
+  for (uint64_t off = 0, c = 0; c < chunks.size(); off += chunks[c], c++) {
+    const uint64_t m = chunks[c];
+    const int k = int(c % kPipeTraceStreams);
+    cudaStream_t tr = d->pipe[kPipeTrace + k];
+    e = cudaMemcpyAsync(d->rays + 2 * off, rays + 8 * off, m * 32, cudaMemcpyHostToDevice, in);
+    if (e == cudaSuccess) e = cudaEventRecord(d->pipeEv[kPipeIn], in);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(tr, d->pipeEv[kPipeIn], 0);
+    if (e != cudaSuccess) {
+      st = cuda_fail(s, e, "rays host->device");
+      break;
+    }
+    st = launch(s, d->rays + 2 * off, d->hits + off, m, tr, flags, slots[k]);
+    if (st != LRT_OK) break;
+    e = cudaEventRecord(d->pipeEv[kPipeTrace + k], tr);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(out, d->pipeEv[kPipeTrace + k], 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(hits + off, d->hits + off, m * sizeof(lrt_hit), cudaMemcpyDeviceToHost, out);
+    if (e != cudaSuccess) {
+      st = cuda_fail(s, e, "hits device->host");
+      break;
+    }
+  }
+  // the caller's stream waits for the last copy out; every stream is drained
+  // (and each trace stream's error word read) also after a failure
+  if (cudaEventRecord(d->pipeEv[kPipeOut], out) == cudaSuccess) cudaStreamWaitEvent(stream, d->pipeEv[kPipeOut], 0);
+  cudaStreamSynchronize(in);
+  for (int k = 0; k < kPipeTraceStreams; k++) {
+    const lrt_status sf = finish(s, d->pipe[kPipeTrace + k], slots[k], false);
+    if (st == LRT_OK) st = sf;
+  }
+  e = cudaStreamSynchronize(out);
+  if (st == LRT_OK && e != cudaSuccess) st = cuda_fail(s, e, "hits device->host");
+  return st;
+}
+
 } // namespace
 
 lrt_status device_upload(lrt_scene* s)
@@ -253,6 +345,7 @@ lrt_status lrt_trace_nearest(lrt_scene* s, const float* rays, lrt_hit* hits, uin
     if (e != cudaSuccess) return cuda_fail(s, e, "staging buffers");
     d->cap = n;
   }
+  if (n >= kPipeMinRays && !(flags & LRT_TRACE_COUNT_WORK)) return trace_host_pipelined(s, rays, hits, n, stream, flags);
   cudaError_t e = cudaMemcpyAsync(d->rays, rays, n * 32, cudaMemcpyHostToDevice, stream);
   if (e != cudaSuccess) return cuda_fail(s, e, "rays host->device");
   st = launch(s, d->rays, d->hits, n, stream, flags, slot);

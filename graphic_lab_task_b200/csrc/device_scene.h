@@ -20,6 +20,16 @@ struct StreamSlot {
   uint32_t _pad[5];
 };
 constexpr int kMaxStreams = 64;
+// Host-pointer traces of at least kPipeMinRays rays run in chunks as a
+// pipeline: host->device copies on one stream, device->host copies on
+// another, and the traces round-robin over kPipeTraceStreams streams, so
+// that both copy directions and the kernels of several chunks overlap.
+constexpr int kPipeTraceStreams = 4;
+constexpr int kPipeIn = 0, kPipeOut = 1, kPipeTrace = 2; // traces: kPipeTrace + k
+constexpr int kPipeStreams = kPipeTrace + kPipeTraceStreams;
+constexpr uint64_t kPipeChunk = 262144;   // 8 MiB of rays in, 8 MiB of hits out
+constexpr uint64_t kPipeChunkMin = 32768; // first and last chunks
+constexpr uint64_t kPipeMinRays = 262144;
 
 struct DeviceScene {
   std::vector<void*> allocs;
@@ -35,8 +45,19 @@ struct DeviceScene {
   float4* rays = nullptr;
   lrt_hit* hits = nullptr;
   uint64_t cap = 0;
+  // streams of the chunked host-pointer pipeline (created on first use);
+  // pipeEv[p] orders stream p's chunk before the next stage, pipeStart the
+  // pipeline after the work already queued on the caller's stream
+  cudaStream_t pipe[kPipeStreams] = {};
+  cudaEvent_t pipeEv[kPipeStreams] = {};
+  cudaEvent_t pipeStart = nullptr;
   ~DeviceScene()
   {
+    for (int p = 0; p < kPipeStreams; p++) {
+      if (pipe[p]) cudaStreamDestroy(pipe[p]);
+      if (pipeEv[p]) cudaEventDestroy(pipeEv[p]);
+    }
+    if (pipeStart) cudaEventDestroy(pipeStart);
     for (void* p : allocs) cudaFree(p);
     if (rays) cudaFree(rays);
     if (hits) cudaFree(hits);

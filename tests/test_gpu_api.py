@@ -36,6 +36,41 @@ def test_device_pointer_traces_on_two_streams(cuda):
         assert bit_equal(got, want).all()
 
 
+@pytest.mark.parametrize("memory", ["pinned", "pageable"])
+@pytest.mark.parametrize("n", [262144, 300001, 1000003])
+def test_host_buffer_traces_equal_device_trace(cuda, n, memory):
+    """Host-buffer traces of 262144 rays or more run as a chunked
+    copy/trace/copy pipeline over several streams: chunks of 32768 rays for
+    the smaller n (the last one ragged for 300001), chunk sizes ramping
+    32768 -> 262144 and back for n = 1000003.  Every hit equals the
+    single-launch device-pointer trace and the oracle."""
+    torch = cuda
+    import pyoracle as po
+    from graphic_lab_task_b200 import HIT_DTYPE
+    sph = wl.spheres(16, seed=3)
+    hdr, nodes, vals, vf = wl.sbs_from_spheres(sph, grid_res=64)
+    sc = SceneRT()
+    sc.AddInstance(sc.AddGeom_SdfSBS(hdr, nodes, vals, vf), wl.IDENTITY)
+    sc.CommitScene()
+    rays = wl.eye_rays_host(wl.camera((0, 0, 3), width=1000, height=1002))[:n]
+    rays = np.ascontiguousarray(rays)
+    if memory == "pinned":
+        host_rays = torch.from_numpy(rays).pin_memory()
+        host_hits = torch.zeros(n * 8, dtype=torch.float32).pin_memory()
+        sc.trace_host(host_rays.data_ptr(), host_hits.data_ptr(), n)
+        got = host_hits.numpy().view(HIT_DTYPE)
+    else:
+        got = sc.RayQuery_NearestHitBatch(rays)
+    R = torch.from_numpy(rays).cuda()
+    H = torch.zeros(n * 8, dtype=torch.float32, device="cuda")
+    sc.trace_device(R.data_ptr(), H.data_ptr(), n)
+    sc.sync()
+    assert bit_equal(got, H.cpu().numpy().view(HIT_DTYPE)).all()
+    idx = np.unique(np.linspace(0, n - 1, 4096).astype(np.int64))
+    assert bit_equal(got[idx], po.port_trace(sc.export_arrays(), rays[idx])).all()
+    assert (got["primId"] != 0xFFFFFFFF).sum() > 1000
+
+
 def test_misaligned_device_pointer_is_rejected(cuda):
     torch = cuda
     sc, rays, _ = _sbs_scene()
