@@ -107,6 +107,41 @@ LRT_HD f2 ray_box_nodes(f3 o, f3 inv, f3 bmin, f3 bmax)
 
 LRT_HD bool finite3(f3 v) { return fabsf(v.x) < INFINITY && fabsf(v.y) < INFINITY && fabsf(v.z) < INFINITY; }
 
+// The six slab values of RayBoxIntersection2, and its two results computed
+// from them separately (near = .x, far = .y of ray_box), in the literal
+// std::min/max form or (FAST) the one-instruction form.  For a finite box
+// and a ray with finite origin, direction and inverse no slab value is NaN,
+// so the two forms give the same numbers up to the sign of a zero result.
+struct Slabs {
+  float lo, hi, lo1, hi1, lo2, hi2;
+};
+
+LRT_HD Slabs slabs(f3 o, f3 inv, f3 bmin, f3 bmax)
+{
+  Slabs s;
+  s.lo = inv.x * (bmin.x - o.x);
+  s.hi = inv.x * (bmax.x - o.x);
+  s.lo1 = inv.y * (bmin.y - o.y);
+  s.hi1 = inv.y * (bmax.y - o.y);
+  s.lo2 = inv.z * (bmin.z - o.z);
+  s.hi2 = inv.z * (bmax.z - o.z);
+  return s;
+}
+
+template <bool FAST>
+LRT_HD float slab_near(const Slabs& s)
+{
+  if (FAST) return fmaxf(fmaxf(fminf(s.lo, s.hi), fminf(s.lo1, s.hi1)), fminf(s.lo2, s.hi2));
+  return smax(smax(smin(s.lo, s.hi), smin(s.lo1, s.hi1)), smin(s.lo2, s.hi2));
+}
+
+template <bool FAST>
+LRT_HD float slab_far(const Slabs& s)
+{
+  if (FAST) return fminf(fminf(fmaxf(s.lo, s.hi), fmaxf(s.lo1, s.hi1)), fmaxf(s.lo2, s.hi2));
+  return smin(smin(smax(s.lo, s.hi), smax(s.lo1, s.hi1)), smax(s.lo2, s.hi2));
+}
+
 // encode_normal, utils/raytracing/intersection_common.h:96-101 (octahedral)
 LRT_HD f2 encode_normal(f3 v)
 {

@@ -186,8 +186,8 @@ __device__ void local_surface(CTX& c, uint32_t type, f3 ray_dir, uint32_t instId
 }
 
 template <class CTX>
-__device__ void octree_node(CTX& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, float tNear, uint32_t instId,
-                            uint32_t geomId, uint32_t bvhNodeId, lrt_hit& hit)
+__device__ void octree_node(CTX& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, f3 inv_dir, float tNear,
+                            uint32_t instId, uint32_t geomId, uint32_t bvhNodeId, lrt_hit& hit)
 {
   const DevScene& S = c.S;
   float values[8];
@@ -221,7 +221,7 @@ __device__ void octree_node(CTX& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, fl
     }
   }
   const f3 size = max_pos - min_pos;
-  const f2 fNearFar = ray_box(ray_pos, safe_inverse(ray_dir), min_pos, max_pos);
+  const f2 fNearFar = ray_box(ray_pos, inv_dir, min_pos, max_pos); // inv_dir = SafeInverse(ray_dir)
   const f3 start_pos = ray_pos + fNearFar.x * ray_dir;
   const float d = smax(size.x, smax(size.y, size.z));
   const f3 start_q = (start_pos - min_pos) / d;
@@ -231,9 +231,15 @@ __device__ void octree_node(CTX& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, fl
   local_surface(c, g.type, ray_dir, instId, geomId, values, primId, d, qNear, qFar, fNearFar, start_q, hit);
 }
 
-template <class CTX>
-__device__ void octree_brick(CTX& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, float tNear, uint32_t instId,
-                             uint32_t geomId, uint32_t bvhNodeId, lrt_hit& hit)
+// FAST: the ray's origin, direction and inverse are finite, so the brick
+// and voxel boxes (finite) give no NaN slab value and the one-instruction
+// min/max form may be used: a voxel's entry distance is only read when it
+// exceeds tNear >= 0.01 (a nonzero value, the same in both forms), and the
+// march advance smax(0, far - t) + 1e-6 and the clamped voxel coordinates
+// do not depend on the sign of a zero, so every hit is unchanged.
+template <bool FAST, class CTX>
+__device__ void octree_brick(CTX& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, f3 inv_dir, float tNear,
+                             uint32_t instId, uint32_t geomId, uint32_t bvhNodeId, lrt_hit& hit)
 {
   const DevScene& S = c.S;
   const DevSbs& sb = S.sbs[g.sdfId];
@@ -253,8 +259,8 @@ __device__ void octree_brick(CTX& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, f
   const float d = 2.0f / (sz * bs);
   const f3 brick_min_pos = mk3(-1, -1, -1) + sz_inv * mk3(px, py, pz);
   const f3 brick_max_pos = brick_min_pos + sz_inv * mk3(1, 1, 1);
-  const f3 inv_dir = safe_inverse(ray_dir);
-  f2 bnf = ray_box(ray_pos, inv_dir, brick_min_pos, brick_max_pos);
+  const Slabs bsl = slabs(ray_pos, inv_dir, brick_min_pos, brick_max_pos); // inv_dir = SafeInverse(ray_dir)
+  f2 bnf = mk2(slab_near<FAST>(bsl), slab_far<FAST>(bsl));
   const float old_t = hit.t;
   const float scale = 0.5f * sz * bs;
   const float hiClamp = bs - 1e-6f;
@@ -278,8 +284,12 @@ __device__ void octree_brick(CTX& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, f
     const uint32_t vid = (vx * bs + vy) * bs + vz;
     // surface bit == (min of the 8 corner values <= 0), precomputed
     const bool surface = (__ldg(mask + 1 + (vid >> 5)) >> (vid & 31)) & 1u;
-    const f2 fNearFar = ray_box(ray_pos, inv_dir, min_pos, max_pos);
-    if (tNear < fNearFar.x && surface) {
+    // the voxel's exit always (for the advance), its entry only where a
+    // sphere trace may start
+    const Slabs vsl = slabs(ray_pos, inv_dir, min_pos, max_pos);
+    const float vfar = slab_far<FAST>(vsl);
+    if (surface && tNear < slab_near<FAST>(vsl)) {
+      const f2 fNearFar = mk2(slab_near<FAST>(vsl), vfar);
       c.inc(kCntVoxelLoads);
       // 8 corners of the voxel from the dense (bs+1)^3 grid, x-major
       const float* base = dense + (vx * V1 + vy) * V1 + vz;
@@ -306,7 +316,7 @@ __device__ void octree_brick(CTX& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, f
         c.rec.sbs = true;
       }
     }
-    bnf.x += smax(0.0f, fNearFar.y - bnf.x) + 1e-6f;
+    bnf.x += smax(0.0f, vfar - bnf.x) + 1e-6f;
   }
   if (hit.t < old_t && sb.colorLayout) {
     // colour of the hit for the indexed layouts (BVH2Common.cpp:1081-1110)
@@ -370,9 +380,12 @@ __device__ void triangles(CTX& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, floa
 }
 
 // IntersectAllPrimitivesInLeaf: returns the tag if the hit moved closer.
+// inv = SafeInverse(ray_dir); fast: the ray qualifies for the one-instruction
+// box tests (fast_nodes).
 template <class CTX>
-__device__ __forceinline__ uint32_t leaf(CTX& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, float tNear,
-                                         uint32_t aabbId, uint32_t instId, uint32_t geomId, lrt_hit& hit)
+__device__ __forceinline__ uint32_t leaf(CTX& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, f3 inv, bool fast,
+                                         float tNear, uint32_t aabbId, uint32_t instId, uint32_t geomId,
+                                         lrt_hit& hit)
 {
   const float tPrev = hit.t;
   c.inc(kCntLeafCalls);
@@ -381,8 +394,13 @@ __device__ __forceinline__ uint32_t leaf(CTX& c, const DevGeom& g, f3 ray_pos, f
   const uint32_t a_count = (packed & 0x70000000u) >> 28;
   switch (g.tag) {
     case LRT_TAG_TRIANGLE: triangles(c, g, ray_pos, ray_dir, tNear, instId, geomId, a_start, a_count, hit); break;
-    case LRT_TAG_SDF_NODE: octree_node(c, g, ray_pos, ray_dir, tNear, instId, geomId, a_start, hit); break;
-    case LRT_TAG_SDF_BRICK: octree_brick(c, g, ray_pos, ray_dir, tNear, instId, geomId, a_start, hit); break;
+    case LRT_TAG_SDF_NODE: octree_node(c, g, ray_pos, ray_dir, inv, tNear, instId, geomId, a_start, hit); break;
+    case LRT_TAG_SDF_BRICK:
+      if (fast)
+        octree_brick<true>(c, g, ray_pos, ray_dir, inv, tNear, instId, geomId, a_start, hit);
+      else
+        octree_brick<false>(c, g, ray_pos, ray_dir, inv, tNear, instId, geomId, a_start, hit);
+      break;
     default: break;
   }
   return (hit.t >= tPrev) ? LRT_TAG_NONE : g.tag;
@@ -461,7 +479,8 @@ __device__ void blas(CTX& c, uint32_t* stack, uint32_t stride, uint32_t cap, f3 
     if (!ok) return;
     if (top >= 0 && leftNodeOffset != 0xFFFFFFFFu) {
       const float tNearSdf = smax(tNear, 0.01f); // SDF_BIAS (BVH2Common.cpp:3306-3307)
-      const uint32_t tag = leaf(c, g, ray_pos, ray_dir, tNearSdf, leftNodeOffset & 0x0FFFFFFFu, instId, geomId, hit);
+      const uint32_t tag =
+          leaf(c, g, ray_pos, ray_dir, inv, fast, tNearSdf, leftNodeOffset & 0x0FFFFFFFu, instId, geomId, hit);
       hitFound = (tag != 0) && (tag != LRT_TAG_TRIANGLE || stopOnFirstHit);
     }
     top--;
