@@ -37,6 +37,9 @@ LRT_HD f3 operator/(f3 a, float s) { return mk3(a.x / s, a.y / s, a.z / s); }
 LRT_HD float smin(float a, float b) { return (b < a) ? b : a; }   // std::min
 LRT_HD float smax(float a, float b) { return (a < b) ? b : a; }   // std::max
 LRT_HD float sclamp(float u, float a, float b) { return smin(smax(a, u), b); } // LiteMath clamp
+// LiteMath clamp for bounds 0 < a <= b: equal to fminf(fmaxf(u, a), b) for
+// every u (a NaN u gives a in both forms; a zero u of either sign gives a).
+LRT_HD float sclamp_pos(float u, float a, float b) { return fminf(fmaxf(u, a), b); }
 LRT_HD float ssign(float x) { return x == 0.0f ? 0.0f : (x < 0.0f ? -1.0f : 1.0f); } // LiteMath.h:133-138
 
 LRT_HD float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }

@@ -276,8 +276,9 @@ __device__ void octree_brick(CTX& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, f
     c.inc(kCntVoxels);
     const f3 hit_pos = ray_pos + bnf.x * ray_dir;
     const f3 local_pos = (hit_pos - brick_min_pos) * scale;
-    const f3 voxelPos = mk3(floorf(sclamp(local_pos.x, 1e-6f, hiClamp)), floorf(sclamp(local_pos.y, 1e-6f, hiClamp)),
-                            floorf(sclamp(local_pos.z, 1e-6f, hiClamp)));
+    const f3 voxelPos = mk3(floorf(sclamp_pos(local_pos.x, 1e-6f, hiClamp)),
+                            floorf(sclamp_pos(local_pos.y, 1e-6f, hiClamp)),
+                            floorf(sclamp_pos(local_pos.z, 1e-6f, hiClamp)));
     const f3 min_pos = brick_min_pos + d * voxelPos;
     const f3 max_pos = min_pos + d * mk3(1, 1, 1);
     const uint32_t vx = uint32_t(voxelPos.x), vy = uint32_t(voxelPos.y), vz = uint32_t(voxelPos.z);
