@@ -60,7 +60,7 @@ lrt_status begin(lrt_scene* s, cudaStream_t stream, StreamSlot** slot, DevScene*
 {
   if (!s) return LRT_ERR_INVALID_ARGUMENT;
   if (!s->committed || !s->dev) return fail(s, LRT_ERR_NOT_COMMITTED, "render before CommitScene/upload");
-  lrt_status st = check_preset(s);
+  lrt_status st = check_preset(s, true);
   if (st != LRT_OK) return st;
   // a dedicated slot past the per-stream ones is not needed: render and
   // adjoint use the slot of their stream like lrt_trace_nearest

@@ -131,7 +131,7 @@ lrt_status lrt_batch_create(lrt_scene* s, const lrt_camera* cams, uint32_t count
   if (!s || !out) return LRT_ERR_INVALID_ARGUMENT;
   if (!cams || count == 0) return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_batch_create: no cameras");
   if (!s->committed || !s->dev) return fail(s, LRT_ERR_NOT_COMMITTED, "lrt_batch_create before CommitScene/upload");
-  lrt_status st = check_preset(s);
+  lrt_status st = check_preset(s, true);
   if (st != LRT_OK) return st;
   lrt_camera_batch* b = new lrt_camera_batch();
   b->scene = s;
@@ -213,7 +213,7 @@ lrt_status lrt_batch_trace(lrt_camera_batch* b, lrt_hit* hits_dev, void* stream_
   lrt_scene* s = b->scene;
   if (reinterpret_cast<uintptr_t>(hits_dev) & 15)
     return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_batch_trace: hits must be 16-byte aligned");
-  lrt_status st = check_preset(s);
+  lrt_status st = check_preset(s, true);
   if (st != LRT_OK) return st;
   cudaStream_t stream = static_cast<cudaStream_t>(stream_p);
   cudaError_t e;

@@ -31,6 +31,7 @@ uint32_t preset_flags(const lrt_preset& p)
   if (m == LRT_RENDER_MODE_ST_ITERATIONS) f |= kFlagStIterations;
   if (p.representation_mode == 0) f |= kFlagSurfaceMode;
   if (p.sdf_node_intersect == 3) f |= kFlagBBoxMode;
+  f |= (p.sdf_node_intersect & 7u) << kFlagSolverShift;
   return f;
 }
 

@@ -44,6 +44,9 @@ constexpr uint32_t kFlagBBoxMode = 8u;    // SDF_OCTREE_NODE_INTERSECT_BBOX
 // every TLAS/BLAS node box has either no NaN coordinate or six (pruned pairs):
 // node tests may use ray_box_nodes for rays with finite origin, direction and inverse
 constexpr uint32_t kFlagCleanBoxes = 16u;
+// bits 8..10: the preset's sdf_node_intersect (0 ST, 1 ANALYTIC, 2 NEWTON, 3 BBOX, 4 IT)
+constexpr uint32_t kFlagSolverShift = 8u;
+constexpr uint32_t kSolverST = 0, kSolverAnalytic = 1, kSolverNewton = 2, kSolverBBox = 3, kSolverIT = 4;
 
 // error bits of the per-launch error word
 constexpr uint32_t kErrStackOverflow = 1u;

@@ -578,15 +578,19 @@ lrt_status validate(lrt_scene* s, SceneInfo* info)
   return LRT_OK;
 }
 
-// Presets the kernels implement: sphere tracing (or BBOX), trilinear,
-// geometric triangle normals; any render mode.
-lrt_status check_preset(lrt_scene* s)
+// Presets the kernels implement: the ST, ANALYTIC, NEWTON, BBOX and IT node
+// solvers (only ST and BBOX where sphere_tracing_only: the batched, render
+// and adjoint kernels), trilinear, geometric triangle normals; any render mode.
+lrt_status check_preset(lrt_scene* s, bool sphere_tracing_only)
 {
   const lrt_preset& p = s->preset;
   const SceneInfo& I = s->info;
   const bool sdf = I.hasSbs || I.hasFrameOctree || I.hasSvs;
-  if (sdf && p.sdf_node_intersect != 0 && p.sdf_node_intersect != 3)
-    return fail(s, LRT_ERR_UNSUPPORTED, "sdf_node_intersect %u: only ST (0) and BBOX (3) are implemented",
+  if (sdf && p.sdf_node_intersect > 4)
+    return fail(s, LRT_ERR_UNSUPPORTED, "sdf_node_intersect %u is not a node solver (0..4)", p.sdf_node_intersect);
+  if (sdf && sphere_tracing_only && p.sdf_node_intersect != 0 && p.sdf_node_intersect != 3)
+    return fail(s, LRT_ERR_UNSUPPORTED,
+                "sdf_node_intersect %u: this call implements ST (0) and BBOX (3); lrt_trace_nearest has all five",
                 p.sdf_node_intersect);
   if (I.hasSbs && p.interpolation_mode != 0)
     return fail(s, LRT_ERR_UNSUPPORTED, "interpolation_mode %u: only TRILINEAR is implemented", p.interpolation_mode);

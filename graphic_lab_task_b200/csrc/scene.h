@@ -77,7 +77,7 @@ struct lrt_scene {
 namespace lrt {
 // scene.cpp
 lrt_status validate(lrt_scene* s, SceneInfo* info);
-lrt_status check_preset(lrt_scene* s);
+lrt_status check_preset(lrt_scene* s, bool sphere_tracing_only = false);
 lrt_status fail(lrt_scene* s, lrt_status code, const char* fmt, ...);
 // device.cu
 lrt_status device_upload(lrt_scene* s);

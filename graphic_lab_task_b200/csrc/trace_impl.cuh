@@ -45,14 +45,16 @@ struct HitRecord {
                     // with the values (no dt/dtheta term)
 };
 
-// Traversal context.  COUNT adds the work counters, RECORD the hit record;
-// the plain trace kernel instantiates neither.  nrec points at this thread's
+// Traversal context.  COUNT adds the work counters, RECORD the hit record,
+// SOLVERS the ANALYTIC / NEWTON / IT node solvers (ST and BBOX are always
+// there); the plain trace kernel instantiates none.  nrec points at this thread's
 // kNormalWords shared-memory words (thread-strided), where a sphere-traced
 // hit leaves what its normal is computed from once the traversal has ended.
-template <bool COUNT, bool RECORD = false>
+template <bool COUNT, bool RECORD = false, bool SOLVERS = false>
 struct Ctx {
   static constexpr bool kCount = COUNT;
   static constexpr bool kRecord = RECORD;
+  static constexpr bool kSolvers = SOLVERS;
   const DevScene& S;
   float* nrec;
   Counters cnt;
@@ -116,6 +118,127 @@ __device__ __forceinline__ f2 deferred_normal(CTX& c, uint32_t instId)
   return encode_normal(norm);
 }
 
+// The cubic c3 t^3 + c2 t^2 + c1 t + c0 whose root is the trilinear surface
+// along the ray inside one voxel, in voxel units (BVH2Common.cpp:395-436).
+__device__ __forceinline__ void sdf_cubic(const float* values, float d_inv, f3 o, f3 d3, float* c)
+{
+  const float s000 = values[0] * d_inv, s001 = values[1] * d_inv, s010 = values[2] * d_inv;
+  const float s011 = values[3] * d_inv, s100 = values[4] * d_inv, s101 = values[5] * d_inv;
+  const float s110 = values[6] * d_inv, s111 = values[7] * d_inv;
+  const float tmp = s101 - s001;
+  const float k0 = s000;
+  const float k1 = s100 - s000;
+  const float k2 = s010 - s000;
+  const float k3 = s110 - s010 - k1;
+  const float k4 = k0 - s001;
+  const float k5 = k1 - tmp;
+  const float k6 = k2 - (s011 - s001);
+  const float k7 = k3 - (s111 - s011 - tmp);
+  const float m0 = o.x * o.y;
+  const float m1 = d3.x * d3.y;
+  const float m2 = o.x * d3.y + o.y * d3.x;
+  const float m3 = k5 * o.z - k1;
+  const float m4 = k6 * o.z - k2;
+  const float m5 = k7 * o.z - k3;
+  c[0] = (k4 * o.z - k0) + o.x * m3 + o.y * m4 + m0 * m5;
+  c[1] = d3.x * m3 + d3.y * m4 + m2 * m5 + d3.z * (k4 + k5 * o.x + k6 * o.y + k7 * m0);
+  c[2] = m1 * m5 + d3.z * (k5 * d3.x + k6 * d3.y + k7 * m2);
+  c[3] = k7 * m1 * d3.z;
+}
+
+// ANALYTIC (BVH2Common.cpp:441-505): the smallest non-negative real root.
+// The reference's unqualified sqrt is the C library's double sqrt, so the
+// expressions containing it are evaluated in double; acos, pow and cos are
+// CUDA's, which may differ from the host library's in the last bit.
+__device__ __forceinline__ float sdf_root_analytic(const float* c, float EPS)
+{
+  const float c0 = c[0], c1 = c[1], c2 = c[2], c3 = c[3];
+  const float kPi = 3.14159265358979323846f; // LiteMath::M_PI, a float
+  float x1 = 1000, x2 = 1000, x3 = 1000;
+  if (fabsf(c3) > 1e-5f) {
+    const float a = c2 / c3, b = c1 / c3, cc = c0 / c3;
+    const float Q = (a * a - 3 * b) / 9;
+    const float R = (2 * a * a * a - 9 * a * b + 27 * cc) / 54;
+    const float Q3 = Q * Q * Q;
+    if (R * R < Q3) {
+      const float theta = float(acos(double(R) / sqrt(double(Q3))));
+      const double sQ = -2.0 * sqrt(double(Q));
+      x1 = float(sQ * double(cosf(theta / 3)) - double(a / 3));
+      x2 = float(sQ * double(cosf((theta + 2 * kPi) / 3)) - double(a / 3));
+      x3 = float(sQ * double(cosf((theta - 2 * kPi) / 3)) - double(a / 3));
+    } else {
+      const float A = float(double(-ssign(R)) * pow(double(fabsf(R)) + sqrt(double(R * R - Q3)),
+                                                     double(1.0f / 3.0f)));
+      const float B = fabsf(A) > EPS ? Q / A : 0;
+      x1 = A + B - a / 3;
+    }
+  } else if (fabsf(c2) > 1e-7f) {
+    const float a = c2, b = c1, cc = c0;
+    const float D = b * b - 4 * a * cc;
+    if (D > 0) {
+      const float q = -0.5f * (b + ssign(b) * sqrtf(D));
+      x1 = q / a;
+      if (fabsf(q) > EPS) x2 = cc / q;
+    }
+  } else if (fabsf(c1) > EPS) {
+    x1 = -c0 / c1;
+  }
+  x1 = x1 < 0 ? 1000 : x1;
+  x2 = x2 < 0 ? 1000 : x2;
+  x3 = x3 < 0 ? 1000 : x3;
+  return smin(x1, smin(x2, x3));
+}
+
+// NEWTON (BVH2Common.cpp:507-587): a sign change of the cubic bracketed by
+// 0, the roots of its derivative and qFar, then at most 10 Newton steps.
+__device__ __forceinline__ bool sdf_root_newton(const float* c, float qFar, float EPS, float& t)
+{
+  const float c0 = c[0], c1 = c[1], c2 = c[2], c3 = c[3];
+  const float a = 3 * c3, b = 2 * c2, cc = c1;
+  const float t0 = 0;
+  float t1 = qFar, t2 = qFar;
+  const float t3 = qFar;
+  const float D = b * b - 4 * a * cc;
+  if (D >= 0) {
+    const float q = -0.5f * (b + ssign(b) * sqrtf(D));
+    t1 = fabsf(a) > EPS ? q / a : t0;
+    t2 = fabsf(q) > EPS ? cc / q : qFar;
+    const float min_t = smin(t1, t2);
+    t2 = smax(t1, t2);
+    t1 = min_t;
+    t1 = sclamp(t1, t0, t3);
+    t2 = sclamp(t2, t0, t3);
+  }
+  const bool s0 = c0 > 0;
+  const bool s1 = (c0 + t1 * (c1 + t1 * (c2 + t1 * c3))) > 0;
+  const bool s2 = (c0 + t2 * (c1 + t2 * (c2 + t2 * c3))) > 0;
+  const bool s3 = (c0 + t3 * (c1 + t3 * (c2 + t3 * c3))) > 0;
+  float nwt_min = t0, nwt_max = t0;
+  if (s0 != s1) {
+    nwt_min = t0;
+    nwt_max = t1;
+  } else if (s1 != s2) {
+    nwt_min = t1;
+    nwt_max = t2;
+  } else if (s2 != s3) {
+    nwt_min = t2;
+    nwt_max = t3;
+  }
+  if (!(nwt_min < nwt_max)) return false;
+  unsigned nwt_iter = 0;
+  float rtn = 0.5f * (nwt_min + nwt_max);
+  float f = 1000;
+  while (nwt_iter < 10 && fabsf(f) >= EPS) {
+    f = c0 + rtn * (c1 + rtn * (c2 + rtn * c3));
+    const float df = c1 + rtn * (2 * c2 + rtn * 3 * c3);
+    const float dx = f / (df + ssign(df) * 1e-9f);
+    rtn -= dx;
+    nwt_iter++;
+  }
+  t = rtn;
+  return rtn >= 0 && rtn <= qFar && fabsf(f) < EPS;
+}
+
 template <class CTX>
 __device__ void local_surface(CTX& c, uint32_t type, f3 ray_dir, uint32_t instId, uint32_t geomId,
                               const float* values, uint32_t primId, float d, float qNear, float qFar, f2 fNearFar,
@@ -132,10 +255,11 @@ __device__ void local_surface(CTX& c, uint32_t type, f3 ray_dir, uint32_t instId
   c.inc(kCntStSteps);
   if (S.flags & kFlagSurfaceMode) start_sign = ssign(start_dist);
   start_dist *= start_sign;
+  const uint32_t solver = CTX::kSolvers ? (S.flags >> kFlagSolverShift) & 7u : kSolverST;
   if (start_dist <= EPS || (S.flags & kFlagBBoxMode)) {
     early_hit = true;
     hitf = true;
-  } else {
+  } else if (solver == kSolverST) {
     float dist = start_dist;
     while (t < qFar && dist > EPS && iter < 256) {
       t += dist * d_inv;
@@ -144,6 +268,35 @@ __device__ void local_surface(CTX& c, uint32_t type, f3 ray_dir, uint32_t instId
     }
     c.inc(kCntStSteps, iter);
     hitf = (dist <= EPS);
+  } else {
+    float cf[4];
+    sdf_cubic(values, d_inv, start_q, ray_dir, cf);
+    if (solver == kSolverAnalytic) {
+      t = sdf_root_analytic(cf, EPS);
+      hitf = (t >= 0 && t <= qFar);
+    } else if (solver == kSolverNewton) {
+      hitf = sdf_root_newton(cf, qFar, EPS, t);
+    } else { // IT: interval tracing bounded by the cubic's derivative (:588-618)
+      const float c1 = cf[1], c2 = cf[2], c3 = cf[3];
+      const float k = 2;
+      float e = 0.1f * qFar;
+      const float t_max = fabsf(c3) < EPS ? 1e6f : -c2 / (3 * c3);
+      const float df_max = 3 * c3 * t_max * t_max + 2 * c2 * t_max + c1;
+      float dist = start_dist;
+      while (t < qFar && dist > EPS && iter < 256) {
+        const float df_1 = 3 * c3 * t * t + 2 * c2 * t + c1;
+        const float df_2 = 3 * c3 * (t + e) * (t + e) + 2 * c2 * (t + e) + c1;
+        float L = (t_max > t && t_max < t + e) ? smax(df_max, smax(df_1, df_2)) : smax(df_1, df_2);
+        L = smax(L, EPS);
+        const float st = smin((dist * d_inv) / L, e);
+        t += st;
+        e = k * st;
+        dist = start_sign * trilinear(values, start_q + t * ray_dir);
+        iter++;
+      }
+      c.inc(kCntStSteps, iter);
+      hitf = (dist <= EPS);
+    }
   }
   const float tReal = fNearFar.x + d * t;
   if (t <= qFar && hitf && tReal < hit.t) {
@@ -563,7 +716,7 @@ __device__ void trace_one(CTX& c, uint32_t* stack, uint32_t stride, uint32_t cap
 // One thread per ray; warps fetch 32-ray batches from a global counter
 // (persistent grid of ~one wave).  Stacks live in shared memory,
 // stack[i * blockDim + tid].
-template <bool COUNT>
+template <bool COUNT, bool SOLVERS>
 __global__ void __launch_bounds__(kTraceThreads, 6) k_trace(DevScene S, const float4* __restrict__ rays,
                                                          lrt_hit* __restrict__ hits, uint64_t n,
                                                          unsigned long long* __restrict__ work_counter,
@@ -573,7 +726,7 @@ __global__ void __launch_bounds__(kTraceThreads, 6) k_trace(DevScene S, const fl
   extern __shared__ uint32_t smem_stack[];
   uint32_t* stack = smem_stack + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
-  Ctx<COUNT> c(S, normal_words(smem_stack, stack_cap));
+  Ctx<COUNT, false, SOLVERS> c(S, normal_words(smem_stack, stack_cap));
   for (;;) {
     unsigned long long base = 0;
     if (lane == 0) base = atomicAdd(work_counter, 32ull);
@@ -830,26 +983,39 @@ cudaError_t launch_trace(const DevScene& S, const float4* rays, lrt_hit* hits, u
                                 uint32_t stack_cap, int grid, cudaStream_t stream, bool count)
 {
   const size_t smem = trace_smem_bytes(stack_cap);
-  if (count)
-    k_trace<true><<<grid, kTraceThreads, smem, stream>>>(S, rays, hits, n, work_counter, counters, err_word, stack_cap);
+  // the ANALYTIC / NEWTON / IT node solvers live in their own instantiation,
+  // so that the sphere-tracing kernel keeps its registers
+  const uint32_t solver = (S.flags >> kFlagSolverShift) & 7u;
+  const bool solvers = solver != kSolverST && solver != kSolverBBox;
+  if (count && solvers)
+    k_trace<true, true><<<grid, kTraceThreads, smem, stream>>>(S, rays, hits, n, work_counter, counters, err_word,
+                                                               stack_cap);
+  else if (count)
+    k_trace<true, false><<<grid, kTraceThreads, smem, stream>>>(S, rays, hits, n, work_counter, counters, err_word,
+                                                                stack_cap);
+  else if (solvers)
+    k_trace<false, true><<<grid, kTraceThreads, smem, stream>>>(S, rays, hits, n, work_counter, counters, err_word,
+                                                                stack_cap);
   else
-    k_trace<false><<<grid, kTraceThreads, smem, stream>>>(S, rays, hits, n, work_counter, counters, err_word,
-                                                          stack_cap);
+    k_trace<false, false><<<grid, kTraceThreads, smem, stream>>>(S, rays, hits, n, work_counter, counters, err_word,
+                                                                 stack_cap);
   return cudaGetLastError();
 }
 
 cudaError_t set_trace_smem(uint32_t stack_cap)
 {
   const int smem = int(trace_smem_bytes(stack_cap));
-  cudaError_t e = cudaFuncSetAttribute(k_trace<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = cudaFuncSetAttribute(k_trace<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_trace<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_trace<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_trace<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  return cudaFuncSetAttribute(k_trace<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
 cudaError_t trace_occupancy(uint32_t stack_cap, int* blocks_per_sm)
 {
   const size_t smem = trace_smem_bytes(stack_cap);
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_trace<false>, kTraceThreads, smem);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_trace<false, false>, kTraceThreads, smem);
 }
 
 cudaError_t launch_eye_rays(const DevCamera& cam, float4* rays, cudaStream_t stream)

@@ -126,7 +126,7 @@ typedef struct lrt_sdf_sbs_header {
 /* MultiRenderPreset, core/render_settings.h:116-137 (60 bytes). */
 typedef struct lrt_preset {
   uint32_t render_mode;
-  uint32_t sdf_node_intersect;
+  uint32_t sdf_node_intersect; /* SDF_OCTREE_NODE_INTERSECT_*: 0 ST, 1 ANALYTIC, 2 NEWTON, 3 BBOX, 4 IT (render_settings.h:54-58) */
   uint32_t normal_mode;
   uint32_t ray_gen_mode;
   uint32_t interpolation_mode;

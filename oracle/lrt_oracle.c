@@ -50,6 +50,7 @@ typedef struct { float x, y; } f2;
 static inline float smin(float a, float b) { return (b < a) ? b : a; }
 static inline float smax(float a, float b) { return (a < b) ? b : a; }
 static inline float sclamp(float u, float a, float b) { return smin(smax(a, u), b); }
+#define LRT_PI_F 3.14159265358979323846f /* LiteMath::M_PI, a float (LiteMath.h:60) */
 static inline float ssign(float x) { return x == 0.0f ? 0.0f : (x < 0.0f ? -1.0f : 1.0f); }
 
 static inline f3 mk3(float x, float y, float z) { f3 r = {x, y, z}; return r; }
@@ -154,9 +155,133 @@ static int need_normal(const lrt_preset* p)
          m == 11 || m == 27;
 }
 
-/* LocalSurfaceIntersection, ST + BBOX branches, trilinear (BVH2Common.cpp:345-391, 618-690).
- * is_surface_node is always false on this path (OctreeNodeIntersect and
- * OctreeBrickIntersect pass false), so EPS is the base 1e-6. */
+/* The cubic c3 t^3 + c2 t^2 + c1 t + c0 whose root is the trilinear
+ * surface along the ray inside one voxel, in voxel units (BVH2Common.cpp:395-436,
+ * after "Ray Tracing of Signed Distance Function Grids", JCGT 11(3), 2022). */
+static void sdf_cubic(const float values[8], float d_inv, f3 o, f3 d3, float c[4])
+{
+  const float s000 = values[0] * d_inv, s001 = values[1] * d_inv, s010 = values[2] * d_inv;
+  const float s011 = values[3] * d_inv, s100 = values[4] * d_inv, s101 = values[5] * d_inv;
+  const float s110 = values[6] * d_inv, s111 = values[7] * d_inv;
+  const float tmp = s101 - s001;
+  const float k0 = s000;
+  const float k1 = s100 - s000;
+  const float k2 = s010 - s000;
+  const float k3 = s110 - s010 - k1;
+  const float k4 = k0 - s001;
+  const float k5 = k1 - tmp;
+  const float k6 = k2 - (s011 - s001);
+  const float k7 = k3 - (s111 - s011 - tmp);
+  const float m0 = o.x * o.y;
+  const float m1 = d3.x * d3.y;
+  const float m2 = o.x * d3.y + o.y * d3.x;
+  const float m3 = k5 * o.z - k1;
+  const float m4 = k6 * o.z - k2;
+  const float m5 = k7 * o.z - k3;
+  c[0] = (k4 * o.z - k0) + o.x * m3 + o.y * m4 + m0 * m5;
+  c[1] = d3.x * m3 + d3.y * m4 + m2 * m5 + d3.z * (k4 + k5 * o.x + k6 * o.y + k7 * m0);
+  c[2] = m1 * m5 + d3.z * (k5 * d3.x + k6 * d3.y + k7 * m2);
+  c[3] = k7 * m1 * d3.z;
+}
+
+/* ANALYTIC: the smallest non-negative real root of the cubic (Vieta /
+ * Cardano for a cubic, the stable quadratic formula, the linear root),
+ * roots below 0 replaced by 1000 (BVH2Common.cpp:441-505).  The reference's
+ * unqualified sqrt there is the C library's double sqrt, so the expressions
+ * that contain it are evaluated in double and rounded to float on
+ * assignment; std::sqrt, std::cos of a float and M_PI (LiteMath's float)
+ * stay in float. */
+static float sdf_root_analytic(const float c[4], float EPS)
+{
+  const float c0 = c[0], c1 = c[1], c2 = c[2], c3 = c[3];
+  float x1 = 1000, x2 = 1000, x3 = 1000;
+  if (fabsf(c3) > 1e-5f) {
+    const float a = c2 / c3, b = c1 / c3, cc = c0 / c3;
+    const float Q = (a * a - 3 * b) / 9;
+    const float R = (2 * a * a * a - 9 * a * b + 27 * cc) / 54;
+    const float Q3 = Q * Q * Q;
+    if (R * R < Q3) {
+      const float theta = (float)acos(R / sqrt(Q3));
+      x1 = (float)(-2 * sqrt(Q) * cosf(theta / 3) - a / 3);
+      x2 = (float)(-2 * sqrt(Q) * cosf((theta + 2 * LRT_PI_F) / 3) - a / 3);
+      x3 = (float)(-2 * sqrt(Q) * cosf((theta - 2 * LRT_PI_F) / 3) - a / 3);
+    } else {
+      const float A = (float)(-ssign(R) * pow(fabsf(R) + sqrt(R * R - Q3), 1.0f / 3.0f));
+      const float B = fabsf(A) > EPS ? Q / A : 0;
+      x1 = A + B - a / 3;
+    }
+  } else if (fabsf(c2) > 1e-7f) {
+    const float a = c2, b = c1, cc = c0;
+    const float D = b * b - 4 * a * cc;
+    if (D > 0) {
+      const float q = -0.5f * (b + ssign(b) * sqrtf(D));
+      x1 = q / a;
+      if (fabsf(q) > EPS) x2 = cc / q;
+    }
+  } else if (fabsf(c1) > EPS) {
+    x1 = -c0 / c1;
+  }
+  x1 = x1 < 0 ? 1000 : x1;
+  x2 = x2 < 0 ? 1000 : x2;
+  x3 = x3 < 0 ? 1000 : x3;
+  return smin(x1, smin(x2, x3));
+}
+
+/* NEWTON: bracket a sign change of the cubic between 0, the roots of its
+ * derivative and qFar, then at most 10 Newton steps from the middle of the
+ * bracket (BVH2Common.cpp:507-587).  Returns the hit flag; *t the root. */
+static int sdf_root_newton(const float c[4], float qFar, float EPS, float* t)
+{
+  const float c0 = c[0], c1 = c[1], c2 = c[2], c3 = c[3];
+  const float a = 3 * c3, b = 2 * c2, cc = c1;
+  const float t0 = 0;
+  float t1 = qFar, t2 = qFar;
+  const float t3 = qFar;
+  const float D = b * b - 4 * a * cc;
+  if (D >= 0) {
+    const float q = -0.5f * (b + ssign(b) * sqrtf(D));
+    t1 = fabsf(a) > EPS ? q / a : t0;
+    t2 = fabsf(q) > EPS ? cc / q : qFar;
+    const float min_t = smin(t1, t2);
+    t2 = smax(t1, t2);
+    t1 = min_t;
+    t1 = sclamp(t1, t0, t3);
+    t2 = sclamp(t2, t0, t3);
+  }
+  const int s0 = c0 > 0;
+  const int s1 = (c0 + t1 * (c1 + t1 * (c2 + t1 * c3))) > 0;
+  const int s2 = (c0 + t2 * (c1 + t2 * (c2 + t2 * c3))) > 0;
+  const int s3 = (c0 + t3 * (c1 + t3 * (c2 + t3 * c3))) > 0;
+  float nwt_min = t0, nwt_max = t0;
+  if (s0 != s1) {
+    nwt_min = t0;
+    nwt_max = t1;
+  } else if (s1 != s2) {
+    nwt_min = t1;
+    nwt_max = t2;
+  } else if (s2 != s3) {
+    nwt_min = t2;
+    nwt_max = t3;
+  }
+  if (!(nwt_min < nwt_max)) return 0;
+  unsigned nwt_iter = 0;
+  float rtn = 0.5f * (nwt_min + nwt_max);
+  float f = 1000;
+  while (nwt_iter < 10 && fabsf(f) >= EPS) {
+    f = c0 + rtn * (c1 + rtn * (c2 + rtn * c3));
+    const float df = c1 + rtn * (2 * c2 + rtn * 3 * c3);
+    const float dx = f / (df + ssign(df) * 1e-9f);
+    rtn -= dx;
+    nwt_iter++;
+  }
+  *t = rtn;
+  return rtn >= 0 && rtn <= qFar && fabsf(f) < EPS;
+}
+
+/* LocalSurfaceIntersection, trilinear (BVH2Common.cpp:345-690): the ST,
+ * BBOX, ANALYTIC, NEWTON and IT node solvers.  is_surface_node is always
+ * false on this path (OctreeNodeIntersect and OctreeBrickIntersect pass
+ * false), so EPS is the base 1e-6. */
 static void local_surface(ctx_t* c, uint32_t type, f3 ray_dir, uint32_t instId, uint32_t geomId,
                           const float values[8], uint32_t primId, float d, float qNear, float qFar, f2 fNearFar,
                           f3 start_q, lrt_hit* hit)
@@ -175,7 +300,7 @@ static void local_surface(ctx_t* c, uint32_t type, f3 ray_dir, uint32_t instId, 
   if (start_dist <= EPS || P->sdf_node_intersect == 3 /* BBOX */) {
     early_hit = 1;
     hitf = 1;
-  } else {
+  } else if (P->sdf_node_intersect == 0 /* ST */) {
     float dist = start_dist;
     while (t < qFar && dist > EPS && iter < 256) {
       t += dist * d_inv;
@@ -184,6 +309,35 @@ static void local_surface(ctx_t* c, uint32_t type, f3 ray_dir, uint32_t instId, 
     }
     c->cnt[C_ST_STEPS] += iter;
     hitf = (dist <= EPS);
+  } else {
+    float cf[4];
+    sdf_cubic(values, d_inv, start_q, ray_dir, cf);
+    if (P->sdf_node_intersect == 1 /* ANALYTIC */) {
+      t = sdf_root_analytic(cf, EPS);
+      hitf = (t >= 0 && t <= qFar);
+    } else if (P->sdf_node_intersect == 2 /* NEWTON */) {
+      hitf = sdf_root_newton(cf, qFar, EPS, &t);
+    } else { /* IT: interval tracing with the cubic's derivative as a Lipschitz bound (:588-618) */
+      const float c1 = cf[1], c2 = cf[2], c3 = cf[3];
+      const float k = 2;
+      float e = 0.1f * qFar;
+      const float t_max = fabsf(c3) < EPS ? 1e6f : -c2 / (3 * c3);
+      const float df_max = 3 * c3 * t_max * t_max + 2 * c2 * t_max + c1;
+      float dist = start_dist;
+      while (t < qFar && dist > EPS && iter < 256) {
+        const float df_1 = 3 * c3 * t * t + 2 * c2 * t + c1;
+        const float df_2 = 3 * c3 * (t + e) * (t + e) + 2 * c2 * (t + e) + c1;
+        float L = (t_max > t && t_max < t + e) ? smax(df_max, smax(df_1, df_2)) : smax(df_1, df_2);
+        L = smax(L, EPS);
+        const float st = smin((dist * d_inv) / L, e);
+        t += st;
+        e = k * st;
+        dist = start_sign * trilinear(values, add3(start_q, scl3(t, ray_dir)));
+        iter++;
+      }
+      c->cnt[C_ST_STEPS] += iter;
+      hitf = (dist <= EPS);
+    }
   }
   const float tReal = fNearFar.x + d * t;
   if (t <= qFar && hitf && tReal < hit->t) {

@@ -178,6 +178,27 @@ def instanced_mix():
     save("instanced_mix", ref, rays, "frame octree + SVS + mesh, 9 instances")
 
 
+def node_solvers():
+    """The same frame-octree + SVS + SBS scene under the ANALYTIC (the
+    reference's default), NEWTON and IT node solvers of
+    LocalSurfaceIntersection (BVH2Common.cpp:392-618)."""
+    sph = wl.spheres(16, seed=6)
+    hdr, nodes, vals, vf = wl.sbs_from_spheres(sph, grid_res=32, brick_size=4, brick_pad=1)
+    for mode, name in ((1, "solver_analytic"), (2, "solver_newton"), (4, "solver_it")):
+        p = parity_preset()
+        p.sdf_node_intersect = mode
+        ref = po.RefScene(preset=p)
+        gb = ref.add_sbs(hdr, nodes, vals, vf)
+        go = ref.add_frame_octree(wl.frame_octree_from_spheres(sph, 4))
+        gs = ref.add_svs(wl.svs_from_spheres(sph, 4))
+        for i, m in enumerate(wl.random_instances(9, seed=21, scale=(0.4, 0.9), trans=1.2)):
+            ref.add_instance([gb, go, gs][i % 3], m)
+        ref.commit()
+        rays = np.concatenate([camera_rays((0, 0, 4), 48, 48), random_rays(1024, 22, spread=2.0, origin_radius=4.0),
+                               any_hit(random_rays(128, 23, spread=2.0, origin_radius=4.0))])
+        save(name, ref, rays, "SBS + frame octree + SVS, 9 instances, sdf_node_intersect %d" % mode)
+
+
 def read_u32(f):
     return int(np.frombuffer(f.read(4), np.uint32)[0])
 
@@ -255,6 +276,7 @@ def main():
     mesh_small()
     sbs_small()
     instanced_mix()
+    node_solvers()
     if os.path.isdir(REF):
         ref_frame_octree()
         ref_svs()

@@ -82,8 +82,22 @@ def test_misaligned_device_pointer_is_rejected(cuda):
 
 
 def test_unsupported_preset_is_refused(cuda):
+    """The plain trace implements all five node solvers (the reference's
+    default preset uses ANALYTIC); the batched, render and adjoint calls
+    implement ST and BBOX and refuse the others; a solver id outside 0..4 is
+    refused everywhere."""
+    torch = cuda
     sc, rays, _ = _sbs_scene()
-    sc.SetPreset(default_preset())  # ANALYTIC node intersection is not on the path
+    sc.SetPreset(default_preset())
+    sc.RayQuery_NearestHitBatch(rays[:8])
+    R = torch.from_numpy(np.ascontiguousarray(rays[:64])).cuda()
+    img = torch.empty(64, dtype=torch.float32, device="cuda")
+    with pytest.raises(LrtError) as e:
+        sc.render_lambert(R.data_ptr(), 64, wl.LIGHT, img.data_ptr())
+    assert e.value.status == 6 and "sdf_node_intersect" in str(e.value)
+    p = parity_preset()
+    p.sdf_node_intersect = 7
+    sc.SetPreset(p)
     with pytest.raises(LrtError) as e:
         sc.RayQuery_NearestHitBatch(rays[:8])
     assert e.value.status == 6 and "sdf_node_intersect" in str(e.value)

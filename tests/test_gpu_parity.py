@@ -28,7 +28,14 @@ def test_uploaded_reference_arrays_match_reference_hits(cuda, name):
     sc = SceneRT(preset=preset)
     sc.upload_arrays(arrays)
     got = sc.RayQuery_NearestHitBatch(rays)
-    assert bit_equal(got, want).all(), hit_summary(got, want)
+    if preset.sdf_node_intersect == 1:
+        # ANALYTIC evaluates acos, cos and pow, whose CUDA and host-library
+        # results may differ in the last bit: the specification's tolerances
+        rep = tolerance_report(got, want)
+        assert rep["id_mismatch"] <= max(1, len(rays) // 1000), rep
+        assert rep["max_rel_t"] <= 1e-5 and rep["max_normal_err"] <= 1e-3, rep
+    else:
+        assert bit_equal(got, want).all(), hit_summary(got, want)
     fast = sc.RayQuery_NearestHitBatch(rays, fast_math=True)
     rep = tolerance_report(fast, want)
     assert rep["id_mismatch"] <= max(1, len(rays) // 1000), rep
@@ -229,3 +236,33 @@ def test_sbs_counters_equal_oracle_where_work_is_not_skipped(cuda):
         assert gpu[names.index(k)] == cnt[names.index(k)], k
     for k in ("blas_pairs", "leaf_calls", "bricks", "voxels"):
         assert gpu[names.index(k)] <= cnt[names.index(k)], k
+
+
+@pytest.mark.parametrize("solver", [1, 2, 4])
+def test_node_solvers_match_oracle(cuda, solver):
+    """ANALYTIC (the reference's default preset), NEWTON and IT inside SBS,
+    frame-octree and SVS leaves of a 48-instance scene: NEWTON and IT bit for
+    bit; ANALYTIC within the specification's tolerances (its acos, cos and
+    pow come from CUDA on the device and from the C library in the oracle)."""
+    from graphic_lab_task_b200 import parity_preset
+    p = parity_preset()
+    p.sdf_node_intersect = solver
+    sph = wl.spheres(32, seed=4)
+    sc = SceneRT(preset=p)
+    go = sc.AddGeom_SdfFrameOctree(wl.frame_octree_from_spheres(sph, 6))
+    gs = sc.AddGeom_SdfSVS(wl.svs_from_spheres(sph, 6))
+    hdr, nodes, vals, vf = wl.sbs_from_spheres(sph, grid_res=64)
+    gb = sc.AddGeom_SdfSBS(hdr, nodes, vals, vf)
+    for i, m in enumerate(wl.random_instances(48, seed=7, scale=(0.1, 0.4), trans=1.5)):
+        sc.AddInstance([go, gs, gb][i % 3], m)
+    sc.CommitScene()
+    rays = wl.eye_rays_host(wl.camera((0.5, 0.7, 3.5), width=200, height=150))
+    got = sc.RayQuery_NearestHitBatch(rays)
+    want = po.port_trace(sc.export_arrays(), rays, preset=p)
+    assert (want["primId"] != MISS).sum() > 3000
+    if solver == 1:
+        rep = tolerance_report(got, want)
+        assert rep["id_mismatch"] <= len(rays) // 1000, rep
+        assert rep["max_rel_t"] <= 1e-5 and rep["max_normal_err"] <= 1e-3, rep
+    else:
+        assert bit_equal(got, want).all(), hit_summary(got, want)

@@ -14,7 +14,7 @@ GOLDEN = golden_names()
 
 def test_golden_set_is_complete():
     for name in ("hand_triangle", "hand_brick", "mesh_small", "sbs_small", "instanced_mix", "ref_frame_octree",
-                 "ref_svs_crop", "ref_sbs_crop"):
+                 "ref_svs_crop", "ref_sbs_crop", "solver_analytic", "solver_newton", "solver_it"):
         assert name in GOLDEN
 
 
@@ -71,4 +71,28 @@ def test_port_matches_reference_on_fresh_scenes(seed):
     rays = np.concatenate([rays, rays[::3] * np.array([1, 1, 1, 1, 1, 1, 1, -1], np.float32)])
     want = ref.trace(rays)
     got = po.port_trace(ref.export(), rays)
+    assert bit_equal(got, want).all(), hit_summary(got, want)
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference build absent (make -C oracle ref)")
+@pytest.mark.parametrize("solver", [0, 1, 2, 3, 4])
+def test_port_matches_reference_for_every_node_solver(solver):
+    """ST, ANALYTIC (the reference's default), NEWTON, BBOX and IT inside
+    SBS, frame-octree and SVS leaves, on a fresh scene."""
+    from graphic_lab_task_b200._abi import parity_preset
+    p = parity_preset()
+    p.sdf_node_intersect = solver
+    sph = wl.spheres(20, seed=40 + solver)
+    hdr, nodes, vals, vf = wl.sbs_from_spheres(sph, grid_res=48, brick_size=4, brick_pad=1)
+    ref = po.RefScene(preset=p)
+    gb = ref.add_sbs(hdr, nodes, vals, vf)
+    go = ref.add_frame_octree(wl.frame_octree_from_spheres(sph, 5))
+    gs = ref.add_svs(wl.svs_from_spheres(sph, 5))
+    for i, m in enumerate(wl.random_instances(9, seed=50 + solver, scale=(0.4, 0.9), trans=1.2)):
+        ref.add_instance([gb, go, gs][i % 3], m)
+    ref.commit()
+    rays = wl.eye_rays_host(wl.camera((0.2, 0.4, 4.0), width=96, height=96))
+    want = ref.trace(rays, threads=4)
+    got = po.port_trace(ref.export(), rays, preset=p)
+    assert (want["primId"] != MISS).sum() > 500
     assert bit_equal(got, want).all(), hit_summary(got, want)
