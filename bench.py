@@ -315,11 +315,60 @@ def run_ours(args, rank, world, local_rank):
     }
     if not args.no_extras:
         del rays, hits, flush
+        out["render"] = fused_render(sc, dev, args)
         out["batched"] = batched_cameras(sc, dev, args)
         out["adjoint"] = adjoint_section(dev, args)
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(sc, None, n)
     print(json.dumps(out))
+
+
+def fused_render(sc, dev, args):
+    """MultiRenderer::Render on the benchmark scene and camera as one launch
+    (lrt_render_rgba8: eye rays, nearest hit, LAMBERT_NO_TEX resolve with a
+    direct and an ambient light, tonemap to RGBA8) against the G-buffer path
+    of separate launches (lrt_generate_eye_rays + lrt_trace_nearest into a
+    hit buffer, before any resolve).  L2 flushed before every timed step."""
+    import torch
+    from graphic_lab_task_b200 import LIGHT_AMBIENT, LIGHT_DIRECT, LIGHT_DTYPE
+    _, cam = workload_scene_camera_only()
+    n = cam.width * cam.height
+    lights = np.zeros(2, LIGHT_DTYPE)
+    lights[0] = ((0.577, 0.577, 0.577), LIGHT_DIRECT, (1.0, 1.0, 1.0), 0)
+    lights[1] = ((0, 0, 0), LIGHT_AMBIENT, (0.1, 0.1, 0.1), 0)
+    img = torch.zeros(n, dtype=torch.int32, device=dev)
+    rays = torch.empty(n * 8, dtype=torch.float32, device=dev)
+    hits = torch.empty(n * 8, dtype=torch.float32, device=dev)
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    steps = max(3, min(args.steps, 50))
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize(dev)
+        tot = 0.0
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            tot += e0.elapsed_time(e1)
+        return tot / steps
+
+    fused_ms = timed(lambda: sc.render_rgba8(cam, lights, (0, 0, 0, 1), img.data_ptr(), stream=sp))
+
+    def gbuffer():
+        sc.generate_eye_rays(cam, rays.data_ptr(), sp)
+        sc.trace_device(rays.data_ptr(), hits.data_ptr(), n, stream=sp)
+
+    gbuf_ms = timed(gbuffer)
+    sc.sync(stream=sp)
+    return {"pixels": n, "fused_ms": fused_ms, "fused_mpix_s": n / fused_ms / 1e3, "gbuffer_path_ms": gbuf_ms,
+            "gbuffer_path_mpix_s": n / gbuf_ms / 1e3, "gbuffer_bytes_avoided": n * 64, "steps": steps}
 
 
 def batched_cameras(sc, dev, args):

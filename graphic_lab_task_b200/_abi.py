@@ -29,6 +29,10 @@ SBS_NODE_DTYPE = np.dtype([("pos_xy", "<u4"), ("pos_z_lod_size", "<u4"), ("data_
 SBS_HEADER_DTYPE = np.dtype([("brick_size", "<u4"), ("brick_pad", "<u4"), ("bytes_per_value", "<u4"),
                              ("aux_data", "<u4")])
 
+# Light, core/IRenderer.h:72-78 (lrt_light)
+LIGHT_DTYPE = np.dtype([("space", "<f4", (3,)), ("type", "<u4"), ("color", "<f4", (3,)), ("_pad", "<u4")])
+LIGHT_DIRECT, LIGHT_POINT, LIGHT_AMBIENT = 0, 1, 2
+assert LIGHT_DTYPE.itemsize == 32
 assert HIT_DTYPE.itemsize == 32 and BVH_NODE_DTYPE.itemsize == 32 and BVH_PAIR_DTYPE.itemsize == 64
 assert GEOM_DATA_DTYPE.itemsize == 64 and INSTANCE_DTYPE.itemsize == 256
 assert FRAME_OCTREE_NODE_DTYPE.itemsize == 36 and SVS_NODE_DTYPE.itemsize == 16

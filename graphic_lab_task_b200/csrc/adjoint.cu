@@ -123,6 +123,41 @@ lrt_status lrt_sbs_update_values(lrt_scene* s, const float* values_f, uint64_t c
   return LRT_OK;
 }
 
+lrt_status lrt_render_rgba8(lrt_scene* s, const lrt_camera* camera, const lrt_light* lights, uint32_t light_count,
+                            const float background[4], uint32_t* image_dev, void* stream_p)
+{
+  StreamSlot* slot = nullptr;
+  DevScene S;
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_p);
+  lrt_status st = begin(s, stream, &slot, &S);
+  if (st != LRT_OK) return st;
+  if (!camera || !background || !image_dev || (light_count && !lights))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_render_rgba8: NULL camera, background, lights or image");
+  if (light_count > LRT_MAX_LIGHTS)
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_render_rgba8: %u lights (at most %d)", light_count, LRT_MAX_LIGHTS);
+  if (s->preset.render_mode != LRT_RENDER_MODE_LAMBERT_NO_TEX)
+    return fail(s, LRT_ERR_UNSUPPORTED, "lrt_render_rgba8 renders the LAMBERT_NO_TEX mode (1), the preset has %u",
+                s->preset.render_mode);
+  if (camera->width == 0 || camera->height == 0) return LRT_OK;
+  DevCamera cam;
+  std::memcpy(cam.proj_inv, camera->proj_inv, sizeof(cam.proj_inv));
+  std::memcpy(cam.world_view_inv, camera->world_view_inv, sizeof(cam.world_view_inv));
+  cam.width = camera->width;
+  cam.height = camera->height;
+  cam.tnear = camera->tnear;
+  cam.tfar = camera->tfar;
+  DevLights L{};
+  if (light_count) std::memcpy(L.light, lights, light_count * sizeof(lrt_light));
+  L.count = light_count;
+  std::memcpy(L.background, background, sizeof(L.background));
+  DeviceScene* d = s->dev;
+  const uint64_t tiles = uint64_t((cam.width + 7) / 8) * ((cam.height + 3) / 4);
+  const int grid = int(std::min<uint64_t>(uint64_t(d->grid), (tiles * 32 + kTraceThreads - 1) / kTraceThreads));
+  const cudaError_t e =
+      lrt_exact::launch_render_rgba8(S, cam, L, image_dev, &slot->work, &slot->err, d->stackCap, grid, stream);
+  return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "render launch");
+}
+
 lrt_status lrt_render_lambert(lrt_scene* s, const float* rays_dev, uint64_t n, const float light[3], float* image_dev,
                               void* stream_p)
 {

@@ -131,6 +131,15 @@ struct DevCamera {
   float tnear, tfar;
 };
 
+// Lights and background of the fused camera render (lrt_light is Light of
+// core/IRenderer.h:72-78).
+typedef lrt_light DevLight;
+struct DevLights {
+  DevLight light[LRT_MAX_LIGHTS];
+  uint32_t count;
+  float background[4];
+};
+
 // One camera of a batched multi-camera trace: its rays are generated in the
 // kernel, tile by tile; hits go to out[rayOffset + y*width + x].
 struct DevBatchCamera {

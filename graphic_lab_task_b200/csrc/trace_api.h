@@ -17,6 +17,9 @@
                                    unsigned long long* work_counter, uint32_t* err_word, int grid,              \
                                    cudaStream_t stream);                                                        \
   cudaError_t cameras_occupancy(uint32_t stack_cap, int* blocks_per_sm);                                        \
+  cudaError_t launch_render_rgba8(const lrt::DevScene& S, const lrt::DevCamera& cam, const lrt::DevLights& lights,\
+                                  uint32_t* image, unsigned long long* work_counter, uint32_t* err_word,        \
+                                  uint32_t stack_cap, int grid, cudaStream_t stream);                           \
   cudaError_t launch_render_lambert(const lrt::DevScene& S, const float4* rays, uint64_t n, float3 light,       \
                                     float* image, unsigned long long* work_counter, uint32_t* err_word,         \
                                     uint32_t stack_cap, int grid, cudaStream_t stream);                         \

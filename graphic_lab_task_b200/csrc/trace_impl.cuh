@@ -59,6 +59,7 @@ struct Ctx {
   float* nrec;
   Counters cnt;
   uint32_t err;
+  uint32_t triLocal; // a triangle hit's primId before the m_primIndices remap (its triSoup record)
   HitRecord rec;
   __device__ Ctx(const DevScene& s, float* normal_rec) : S(s), nrec(normal_rec), err(0)
   {
@@ -708,6 +709,7 @@ __device__ void trace_one(CTX& c, uint32_t* stack, uint32_t stride, uint32_t cap
   }
   if (hit.geomId < 0xFFFFFFFFu && ((hit.geomId >> 24) == LRT_TYPE_MESH_TRIANGLE)) {
     const DevGeom& g = S.geoms[hit.geomId & 0x00FFFFFFu];
+    c.triLocal = hit.primId;
     hit.primId = __ldg(S.primIndices + g.triBase + hit.primId);
   }
   if (hit.primId != 0xFFFFFFFFu) c.inc(kCntHits);
@@ -833,6 +835,88 @@ __device__ __forceinline__ float lambert(const lrt_hit& h, f3 dir, f3 L)
   return smax(0.0f, dot(n, L));
 }
 
+// MultiRenderer::Render for MULTI_RENDER_MODE_LAMBERT_NO_TEX with one sample
+// per pixel and no transparency (MultiRenderer.cpp:14-60), fused into one
+// launch: per pixel initEyeRay (the eye_ray of lrt_generate_eye_rays), the
+// nearest hit, ResolveCommon (MultiRenderer_resolve.cpp:580-666: white albedo,
+// direct / point / ambient lights, triangle normals recomputed from the
+// triangle and turned towards the viewer as in loadNormalTcFromGbuffer :27-75,
+// SDF normals decoded from the hit) and Tonemap (:536-542) into RGBA8.  A warp
+// takes 8x4-pixel tiles from a global counter.
+__device__ __forceinline__ uint32_t tonemap_rgba8(float r, float g, float b, float a)
+{
+  // uint4(255 * clamp(color, 0, 1)): clamp as LiteMath's min(max(a, u), b)
+  const uint32_t x = uint32_t(255.0f * sclamp(r, 0.0f, 1.0f));
+  const uint32_t y = uint32_t(255.0f * sclamp(g, 0.0f, 1.0f));
+  const uint32_t z = uint32_t(255.0f * sclamp(b, 0.0f, 1.0f));
+  const uint32_t w = uint32_t(255.0f * sclamp(a, 0.0f, 1.0f));
+  return (w << 24) | (z << 16) | (y << 8) | x;
+}
+
+__global__ void __launch_bounds__(kTraceThreads) k_render_rgba8(DevScene S, DevCamera cam, DevLights L,
+                                                                uint32_t* __restrict__ image,
+                                                                unsigned long long* __restrict__ work_counter,
+                                                                uint32_t* __restrict__ err_word, uint32_t stack_cap)
+{
+  extern __shared__ uint32_t smem_stack[];
+  uint32_t* stack = smem_stack + threadIdx.x;
+  const uint32_t lane = threadIdx.x & 31;
+  Ctx<false> c(S, normal_words(smem_stack, stack_cap));
+  const uint32_t tilesX = (cam.width + 7) / 8, ntiles = tilesX * ((cam.height + 3) / 4);
+  for (;;) {
+    unsigned long long tile = 0;
+    if (lane == 0) tile = atomicAdd(work_counter, 1ull);
+    tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
+    if (tile >= ntiles) break;
+    const uint32_t x = uint32_t(tile % tilesX) * 8 + (lane & 7), y = uint32_t(tile / tilesX) * 4 + (lane >> 3);
+    if (x >= cam.width || y >= cam.height) continue;
+    float r[8];
+    eye_ray(cam.proj_inv, cam.world_view_inv, x, y, cam.width, cam.height, cam.tnear, cam.tfar, r);
+    lrt_hit h;
+    trace_one(c, stack, blockDim.x, stack_cap, make_float4(r[0], r[1], r[2], r[3]), make_float4(r[4], r[5], r[6], r[7]),
+              h);
+    uint32_t px;
+    if (h.primId == 0xFFFFFFFFu) {
+      px = tonemap_rgba8(L.background[0], L.background[1], L.background[2], L.background[3]);
+    } else {
+      const f3 rayPos = mk3(r[0], r[1], r[2]), rayDir = mk3(r[4], r[5], r[6]);
+      f3 norm;
+      if ((h.geomId >> 24) == LRT_TYPE_MESH_TRIANGLE) {
+        const DevGeom& g = S.geoms[h.geomId & 0x00FFFFFFu];
+        const float4* tri = S.triSoup + 3 * (uint64_t(g.triBase) + c.triLocal);
+        const f3 raw = cross(ld3(__ldg(tri + 1)), ld3(__ldg(tri + 2)));
+        norm = normalize(matmul4(S.instances[h.instId].transformInvTransposed, raw, 1.0f));
+        norm = ssign(dot(-1.0f * rayDir, norm)) * norm;
+      } else {
+        norm = decode_normal(mk2(h.coords[2], h.coords[3]));
+      }
+      const f3 color = mk3(1, 1, 1);
+      f3 fc = mk3(0, 0, 0);
+      for (uint32_t i = 0; i < L.count; i++) {
+        const DevLight& l = L.light[i];
+        const f3 lc = mk3(l.color[0], l.color[1], l.color[2]);
+        const f3 sp = mk3(l.space[0], l.space[1], l.space[2]);
+        if (l.type == LRT_LIGHT_DIRECT) {
+          const float q = smax(0.0f, dot(norm, sp));
+          fc = fc + (lc * color) * q;
+        } else if (l.type == LRT_LIGHT_POINT) {
+          const f3 surf = rayPos + h.t * rayDir;
+          f3 dir = sp - surf;
+          const float len = sqrtf(dot(dir, dir));
+          dir = mk3(dir.x / len, dir.y / len, dir.z / len);
+          const float q = smax(0.0f, dot(norm, dir));
+          fc = fc + ((lc * color) * q) / (len * len);
+        } else {
+          fc = fc + lc * color;
+        }
+      }
+      px = tonemap_rgba8(fc.x, fc.y, fc.z, 1.0f);
+    }
+    image[uint64_t(y) * cam.width + x] = px;
+  }
+  if (c.err) atomicOr(err_word, c.err);
+}
+
 // Forward render: image[i] = Lambert shade of ray i's nearest hit.
 __global__ void __launch_bounds__(kTraceThreads) k_render_lambert(DevScene S, const float4* __restrict__ rays,
                                                                   uint64_t n, float3 light, float* __restrict__ image,
@@ -937,6 +1021,18 @@ __global__ void __launch_bounds__(kTraceThreads) k_adjoint_lambert(DevScene S, c
     }
   }
   if (err) atomicOr(err_word, err);
+}
+
+cudaError_t launch_render_rgba8(const DevScene& S, const DevCamera& cam, const DevLights& lights, uint32_t* image,
+                                unsigned long long* work_counter, uint32_t* err_word, uint32_t stack_cap, int grid,
+                                cudaStream_t stream)
+{
+  const size_t smem = trace_smem_bytes(stack_cap);
+  cudaError_t e = cudaFuncSetAttribute(k_render_rgba8, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(trace_smem_bytes(kMaxStackDev + 1)));
+  if (e != cudaSuccess) return e;
+  k_render_rgba8<<<grid, kTraceThreads, smem, stream>>>(S, cam, lights, image, work_counter, err_word, stack_cap);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_render_lambert(const DevScene& S, const float4* rays, uint64_t n, float3 light, float* image,

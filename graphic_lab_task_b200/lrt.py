@@ -12,7 +12,7 @@ import os
 
 import numpy as np
 
-from ._abi import (HIT_DTYPE, LRT_BATCH_NO_GRAPH, LRT_COUNTER_COUNT, LRT_TRACE_COUNT_WORK,
+from ._abi import (HIT_DTYPE, LIGHT_DTYPE, LRT_BATCH_NO_GRAPH, LRT_COUNTER_COUNT, LRT_TRACE_COUNT_WORK,
                    LRT_TRACE_DEVICE_POINTERS, LRT_TRACE_FAST_MATH, STATUS_NAMES, BatchShape, Camera, Preset,
                    SceneArrays, TuneEntry, arrays_to_struct, parity_preset, struct_to_arrays)
 
@@ -29,7 +29,7 @@ EXPORTED = (
     "lrt_trace_nearest_noalloc", "lrt_batch_create", "lrt_batch_destroy", "lrt_batch_ray_offsets",
     "lrt_batch_update_cameras", "lrt_batch_set_shape", "lrt_batch_get_shape", "lrt_batch_trace", "lrt_batch_sync",
     "lrt_batch_autotune", "lrt_render_lambert", "lrt_adjoint_lambert_sbs", "lrt_sbs_update_values",
-    "lrt_generate_bounce_rays",
+    "lrt_generate_bounce_rays", "lrt_render_rgba8",
     "lrt_wl_noisy_sphere", "lrt_wl_spheres", "lrt_wl_sphere_sdf", "lrt_wl_sbs_from_spheres",
     "lrt_wl_frame_octree_from_spheres", "lrt_wl_svs_from_spheres",
 )
@@ -74,6 +74,7 @@ def lib():
         "lrt_trace_nearest": [vp, vp, vp, u64, vp, u32],
         "lrt_trace_nearest_noalloc": [vp, vp, vp, u64, vp, u32],
         "lrt_render_lambert": [vp, vp, u64, vp, vp, vp],
+        "lrt_render_rgba8": [vp, vp, vp, u32, vp, vp, vp],
         "lrt_generate_bounce_rays": [vp, vp, vp, u64, u64, C.c_float, C.c_float, vp, vp],
         "lrt_adjoint_lambert_sbs": [vp, vp, u64, vp, vp, vp, vp],
         "lrt_sbs_update_values": [vp, vp, u64, vp, u32],
@@ -261,6 +262,15 @@ class SceneRT:
         L = (C.c_float * 3)(*[float(x) for x in light])
         self._check(lib().lrt_render_lambert(self.h, C.c_void_p(rays_ptr), n, L, C.c_void_p(image_ptr),
                                              C.c_void_p(stream) if stream else None))
+
+    def render_rgba8(self, camera, lights, background, image_ptr, stream=0):
+        """Fused Render (eye rays, nearest hit, LAMBERT_NO_TEX resolve with
+        `lights` — a LIGHT_DTYPE array —, tonemap) of `camera` into
+        width*height RGBA8 pixels of device memory."""
+        lt = np.ascontiguousarray(lights, dtype=LIGHT_DTYPE)
+        bg = (C.c_float * 4)(*[float(x) for x in background])
+        self._check(lib().lrt_render_rgba8(self.h, C.byref(camera), lt.ctypes.data if len(lt) else None, len(lt), bg,
+                                           C.c_void_p(image_ptr), C.c_void_p(stream) if stream else None))
 
     def adjoint_lambert(self, rays_ptr, n, light, dimage_ptr, grad_ptr, stream=0):
         L = (C.c_float * 3)(*[float(x) for x in light])

@@ -378,6 +378,30 @@ lrt_status lrt_generate_bounce_rays(lrt_scene* scene, const float* rays_dev, con
 lrt_status lrt_render_lambert(lrt_scene* scene, const float* rays_dev, uint64_t n, const float light[3],
                               float* image_dev, void* stream);
 
+/* Light, core/IRenderer.h:72-78 (32 bytes).  space is the direction of a
+ * LRT_LIGHT_DIRECT light (normalised by the caller, as create_direct_light
+ * does) or the position of a LRT_LIGHT_POINT one; color includes intensity. */
+typedef struct lrt_light {
+  float space[3];
+  uint32_t type; /* LIGHT_TYPE_*, core/IRenderer.h:16-18 */
+  float color[3];
+  uint32_t _pad;
+} lrt_light;
+enum { LRT_LIGHT_DIRECT = 0, LRT_LIGHT_POINT = 1, LRT_LIGHT_AMBIENT = 2 };
+#define LRT_MAX_LIGHTS 16
+
+/* MultiRenderer::Render (MultiRenderer.cpp:14-60) for the
+ * MULTI_RENDER_MODE_LAMBERT_NO_TEX preset, one sample per pixel, no
+ * transparency, fused into one launch: initEyeRay, RayQuery_NearestHit,
+ * ResolveCommon (MultiRenderer_resolve.cpp:580-666: white albedo, the given
+ * lights, `background` for misses) and Tonemap (:536-542).  Writes
+ * width*height RGBA8 pixels (row-major) to device memory image_dev;
+ * asynchronous on `stream`, lrt_trace_sync(stream) reports bounded-loop
+ * limits.  No counterpart call in the reference (it renders through a
+ * G-buffer); the node solver must be ST or BBOX. */
+lrt_status lrt_render_rgba8(lrt_scene* scene, const lrt_camera* camera, const lrt_light* lights,
+                            uint32_t light_count, const float background[4], uint32_t* image_dev, void* stream);
+
 /* Adjoint of lrt_render_lambert with respect to the scene's SBS float values
  * (the sdfSBSDataF array of the indexed layouts): grad_dev[j] +=
  * sum_i dimage_dev[i] * d image[i] / d values_f[j], by implicit

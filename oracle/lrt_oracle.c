@@ -145,6 +145,7 @@ typedef struct {
   uint64_t* cnt;   /* LRT_COUNTER_COUNT entries (thread-local) */
   uint64_t limits; /* bounded-loop / bounds events */
   hit_record_t* rec; /* NULL unless recording */
+  uint32_t tri_local; /* a triangle hit's primId before the m_primIndices remap */
 } ctx_t;
 
 /* BVHRT::need_normal, BVH2Common.cpp:19-32 */
@@ -717,6 +718,7 @@ static lrt_hit nearest_hit(ctx_t* c, const float pn[4], const float dfar[4])
 done:
   if (hit.geomId < 0xFFFFFFFFu && ((hit.geomId >> 24) == LRT_TYPE_MESH_TRIANGLE)) {
     const uint32_t g = hit.geomId & 0x00FFFFFFu;
+    c->tri_local = hit.primId;
     hit.primId = A->primIndices[A->geomData[g].offset[0] / 3 + hit.primId];
   }
   if (hit.primId != 0xFFFFFFFFu) c->cnt[C_HITS]++;
@@ -949,5 +951,81 @@ void lrto_fd_model_fp64(const lrt_scene_arrays* arrays, const lrt_preset* preset
 #endif
       out[lo] += (double)dimage[i] * d;
     }
+  }
+}
+
+
+/* ------------------------------------------------------------------------ */
+/* MultiRenderer::Render for LAMBERT_NO_TEX, one sample, no transparency    */
+/* (MultiRenderer.cpp:14-60): ResolveCommon + Tonemap of each eye ray.      */
+/* ------------------------------------------------------------------------ */
+
+/* Tonemap, MultiRenderer_resolve.cpp:536-542: uint4(255 * clamp(c, 0, 1)). */
+static uint32_t tonemap_rgba8(float r, float g, float b, float a)
+{
+  const uint32_t x = (uint32_t)(255.0f * sclamp(r, 0.0f, 1.0f));
+  const uint32_t y = (uint32_t)(255.0f * sclamp(g, 0.0f, 1.0f));
+  const uint32_t z = (uint32_t)(255.0f * sclamp(b, 0.0f, 1.0f));
+  const uint32_t w = (uint32_t)(255.0f * sclamp(a, 0.0f, 1.0f));
+  return (w << 24) | (z << 16) | (y << 8) | x;
+}
+
+/* rays: the eye rays of the image in row-major pixel order (initEyeRay). */
+void lrto_render_rgba8(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* rays, uint64_t n,
+                       const lrt_light* lights, uint32_t light_count, const float background[4], uint32_t* image,
+                       int threads)
+{
+  (void)threads;
+#ifdef _OPENMP
+#pragma omp parallel for num_threads(threads > 0 ? threads : 1) schedule(dynamic, 256)
+#endif
+  for (int64_t i = 0; i < (int64_t)n; i++) {
+    uint64_t cnt[LRT_COUNTER_COUNT];
+    ctx_t c = {arrays, preset, cnt, 0, NULL, 0};
+    const float* r = rays + 8 * i;
+    const lrt_hit h = nearest_hit(&c, r, r + 4);
+    if (h.primId == 0xFFFFFFFFu) {
+      image[i] = tonemap_rgba8(background[0], background[1], background[2], background[3]);
+      continue;
+    }
+    const f3 rayPos = mk3(r[0], r[1], r[2]), rayDir = mk3(r[4], r[5], r[6]);
+    f3 norm;
+    if ((h.geomId >> 24) == LRT_TYPE_MESH_TRIANGLE) {
+      /* loadNormalTcFromGbuffer, NORMAL_MODE_GEOMETRY (:33-59) */
+      const uint32_t g = h.geomId & 0x00FFFFFFu;
+      const uint32_t base = arrays->geomData[g].offset[0] + 3 * c.tri_local;
+      const float* vA = arrays->vertPos + 4 * (uint64_t)(arrays->geomData[g].offset[1] + arrays->indices[base + 0]);
+      const float* vB = arrays->vertPos + 4 * (uint64_t)(arrays->geomData[g].offset[1] + arrays->indices[base + 1]);
+      const float* vC = arrays->vertPos + 4 * (uint64_t)(arrays->geomData[g].offset[1] + arrays->indices[base + 2]);
+      const f3 A = mk3(vA[0], vA[1], vA[2]), B = mk3(vB[0], vB[1], vB[2]), C = mk3(vC[0], vC[1], vC[2]);
+      const f3 raw = cross3(sub3(B, A), sub3(C, A));
+      norm = normalize3(matmul4(arrays->instanceData[h.instId].transformInvTransposed, raw, 1.0f));
+      norm = scl3(ssign(dot3(scl3(-1.0f, rayDir), norm)), norm);
+    } else {
+      norm = decode_normal(h.coords[2], h.coords[3]);
+    }
+    /* ResolveCommon, LAMBERT_NO_TEX (:617-666): white albedo */
+    const f3 color = mk3(1, 1, 1);
+    f3 fc = mk3(0, 0, 0);
+    for (uint32_t k = 0; k < light_count; k++) {
+      const lrt_light* l = &lights[k];
+      const f3 lc = mk3(l->color[0], l->color[1], l->color[2]);
+      const f3 sp = mk3(l->space[0], l->space[1], l->space[2]);
+      if (l->type == LRT_LIGHT_DIRECT) {
+        const float q = smax(0.0f, dot3(norm, sp));
+        fc = add3(fc, scl3(q, mul3(lc, color)));
+      } else if (l->type == LRT_LIGHT_POINT) {
+        const f3 surf = add3(rayPos, scl3(h.t, rayDir));
+        f3 dir = sub3(sp, surf);
+        const float len = sqrtf(dot3(dir, dir));
+        dir = mk3(dir.x / len, dir.y / len, dir.z / len);
+        const float q = smax(0.0f, dot3(norm, dir));
+        const f3 lq = scl3(q, mul3(lc, color));
+        fc = add3(fc, mk3(lq.x / (len * len), lq.y / (len * len), lq.z / (len * len)));
+      } else {
+        fc = add3(fc, mul3(lc, color));
+      }
+    }
+    image[i] = tonemap_rgba8(fc.x, fc.y, fc.z, 1.0f);
   }
 }

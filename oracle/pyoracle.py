@@ -204,6 +204,28 @@ def port_render_lambert(arrays, rays, light, preset=None, threads=os.cpu_count()
     return img
 
 
+def port_render_rgba8(arrays, rays, lights, background, preset=None, threads=os.cpu_count()):
+    """RGBA8 image of the eye rays `rays` (row-major pixels): nearest hit,
+    LAMBERT_NO_TEX resolve with `lights` (LIGHT_DTYPE) and tonemap."""
+    from graphic_lab_task_b200._abi import LIGHT_DTYPE
+    lib = port_lib()
+    if not hasattr(lib, "_rgba8_bound"):
+        lib.lrto_render_rgba8.restype = None
+        lib.lrto_render_rgba8.argtypes = [C.POINTER(SceneArrays), C.POINTER(Preset), C.c_void_p, C.c_uint64,
+                                          C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int]
+        lib._rgba8_bound = True
+    s, keep = arrays_to_struct(arrays)
+    p = preset if preset is not None else parity_preset()
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    lt = np.ascontiguousarray(lights, dtype=LIGHT_DTYPE)
+    bg = np.ascontiguousarray(background, dtype=np.float32)
+    img = np.zeros(len(rays), np.uint32)
+    lib.lrto_render_rgba8(C.byref(s), C.byref(p), rays.ctypes.data, len(rays), lt.ctypes.data if len(lt) else None,
+                          len(lt), bg.ctypes.data, img.ctypes.data, int(threads))
+    del keep
+    return img
+
+
 def port_adjoint_fp64(arrays, rays, light, dimage, preset=None):
     """FP64 adjoint of the Lambert render w.r.t. the SBS float values."""
     port_render_lambert(arrays, np.zeros((0, 8), np.float32), light, preset)  # binds the signatures

@@ -1,0 +1,70 @@
+"""Fused camera render (lrt_render_rgba8): eye rays, nearest hit, the
+LAMBERT_NO_TEX resolve with direct, point and ambient lights, and the tonemap
+in one launch, bit-identical to the oracle's restatement of MultiRenderer's
+Render on the same scene arrays."""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from graphic_lab_task_b200 import (LIGHT_AMBIENT, LIGHT_DIRECT, LIGHT_DTYPE, LIGHT_POINT, LrtError, SceneRT,
+                                   parity_preset, workloads as wl)
+
+pytestmark = pytest.mark.gpu
+
+
+def _lights():
+    lt = np.zeros(3, LIGHT_DTYPE)
+    d = np.array([0.4, 0.8, 0.45], np.float32)
+    lt[0] = (d / np.linalg.norm(d), LIGHT_DIRECT, (0.9, 0.85, 0.7), 0)
+    lt[1] = ((1.5, 2.0, 2.5), LIGHT_POINT, (4.0, 3.0, 2.0), 0)
+    lt[2] = ((0, 0, 0), LIGHT_AMBIENT, (0.05, 0.06, 0.08), 0)
+    return lt
+
+
+def _mixed_scene():
+    sph = wl.spheres(32, seed=4)
+    sc = SceneRT()
+    v, t = wl.noisy_sphere(60, seed=2)
+    gm = sc.AddGeom_Triangles3f(v, t)
+    go = sc.AddGeom_SdfFrameOctree(wl.frame_octree_from_spheres(sph, 6))
+    gs = sc.AddGeom_SdfSVS(wl.svs_from_spheres(sph, 6))
+    hdr, nodes, vals, vf = wl.sbs_from_spheres(sph, grid_res=64)
+    gb = sc.AddGeom_SdfSBS(hdr, nodes, vals, vf)
+    for i, m in enumerate(wl.random_instances(40, seed=7, scale=(0.1, 0.4), trans=1.5)):
+        sc.AddInstance([gm, go, gs, gb][i % 4], m)
+    sc.CommitScene()
+    return sc
+
+
+@pytest.mark.parametrize("size", [(200, 150), (256, 128)])
+def test_render_rgba8_matches_oracle(cuda, size):
+    torch = cuda
+    sc = _mixed_scene()
+    cam = wl.camera((0.5, 0.7, 3.5), width=size[0], height=size[1])
+    bg = (0.1, 0.2, 0.3, 1.0)
+    img = torch.zeros(size[0] * size[1], dtype=torch.int32, device="cuda")
+    sc.render_rgba8(cam, _lights(), bg, img.data_ptr())
+    sc.sync()
+    got = img.cpu().numpy().view(np.uint32)
+    want = po.port_render_rgba8(sc.export_arrays(), wl.eye_rays_host(cam), _lights(), bg)
+    assert np.array_equal(got, want), "%d of %d pixels differ" % ((got != want).sum(), len(got))
+    bgpx = (255 << 24) | (int(255 * 0.3) << 16) | (int(255 * 0.2) << 8) | int(255 * 0.1)
+    assert 0.05 < (got != bgpx).mean() < 0.95  # both hits and background in view
+    assert len(np.unique(got)) > 100
+
+
+def test_render_rgba8_refusals(cuda):
+    torch = cuda
+    sc = _mixed_scene()
+    cam = wl.camera((0.5, 0.7, 3.5), width=16, height=16)
+    img = torch.zeros(256, dtype=torch.int32, device="cuda")
+    many = np.zeros(17, LIGHT_DTYPE)
+    with pytest.raises(LrtError) as e:
+        sc.render_rgba8(cam, many, (0, 0, 0, 1), img.data_ptr())
+    assert e.value.status == 1
+    p = parity_preset()
+    p.render_mode = 0
+    sc.SetPreset(p)
+    with pytest.raises(LrtError) as e:
+        sc.render_rgba8(cam, _lights(), (0, 0, 0, 1), img.data_ptr())
+    assert e.value.status == 6 and "LAMBERT_NO_TEX" in str(e.value)
