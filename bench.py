@@ -262,6 +262,17 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize(dev)
     sc.sync(stream=sp)
     kernel_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    # the same rays traced in 8x4-pixel tiles (lrt_trace_nearest_image): as
+    # the reference's kernel1D_FillGbuffer walks pixels in packed tiles
+    tile_ms = []
+    for i in range(min(args.steps, 50)):
+        flush.zero_()
+        starts[i].record(stream)
+        sc.trace_image(rays.data_ptr(), hits.data_ptr(), WIDTH, HEIGHT, stream=sp)
+        ends[i].record(stream)
+    torch.cuda.synchronize(dev)
+    sc.sync(stream=sp)
+    tile_ms = [starts[i].elapsed_time(ends[i]) for i in range(min(args.steps, 50))]
     # end to end through the public API with pinned host buffers
     host_rays = torch.empty(n * 8, dtype=torch.float32, pin_memory=True)
     host_rays.copy_(rays.cpu())
@@ -309,6 +320,9 @@ def run_ours(args, rank, world, local_rank):
                      "bytes_per_ray": bytes_per_launch / n, "kernel": "k_trace (exact build)"},
         "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * 32,
                 "ms_per_step": total_e2e_ms / args.steps},
+        "image_tile_order": {"ms_per_step": sum(tile_ms) / len(tile_ms),
+                             "value": n / (sum(tile_ms) / len(tile_ms)) / 1e3, "unit": "Mrays/s",
+                             "call": "lrt_trace_nearest_image (same rays, 8x4-pixel tiles per warp)"},
         "clocks": clk,
         "gpu_launches": 2 * args.steps,
         "work_counters": {k: int(v) for k, v in zip(COUNTER_NAMES, counters)},

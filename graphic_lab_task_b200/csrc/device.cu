@@ -85,8 +85,10 @@ lrt_status slot_for(lrt_scene* s, cudaStream_t stream, StreamSlot** out)
   return LRT_OK;
 }
 
+// img_w > 0: the n = img_w * img_h rays are an image in row-major order,
+// traced in 8x4-pixel tiles.
 lrt_status launch(lrt_scene* s, const float4* rays, lrt_hit* hits, uint64_t n, cudaStream_t stream, uint32_t flags,
-                  StreamSlot* slot)
+                  StreamSlot* slot, uint32_t img_w = 0, uint32_t img_h = 0)
 {
   DeviceScene* d = s->dev;
   DevScene S = d->S;
@@ -96,14 +98,14 @@ lrt_status launch(lrt_scene* s, const float4* rays, lrt_hit* hits, uint64_t n, c
   cudaError_t e = cudaMemsetAsync(&slot->work, 0, count ? offsetof(StreamSlot, err) : sizeof(unsigned long long),
                                   stream);
   if (e != cudaSuccess) return cuda_fail(s, e, "cudaMemsetAsync");
-  const uint64_t warps = (n + 31) / 32;
+  const uint64_t warps = img_w ? uint64_t((img_w + 7) / 8) * ((img_h + 3) / 4) : (n + 31) / 32;
   const int grid = int(std::min<uint64_t>(uint64_t(d->grid), (warps * 32 + kTraceThreads - 1) / kTraceThreads));
   if (flags & LRT_TRACE_FAST_MATH)
     e = lrt_fast::launch_trace(S, rays, hits, n, &slot->work, slot->counters, &slot->err, d->stackCap, grid, stream,
-                               count);
+                               count, img_w, img_h);
   else
     e = lrt_exact::launch_trace(S, rays, hits, n, &slot->work, slot->counters, &slot->err, d->stackCap, grid,
-                                stream, count);
+                                stream, count, img_w, img_h);
   if (e != cudaSuccess) return cuda_fail(s, e, "trace launch");
   return LRT_OK;
 }
@@ -354,6 +356,24 @@ lrt_status lrt_trace_nearest(lrt_scene* s, const float* rays, lrt_hit* hits, uin
   e = cudaMemcpyAsync(hits, d->hits, n * sizeof(lrt_hit), cudaMemcpyDeviceToHost, stream);
   if (e != cudaSuccess) return cuda_fail(s, e, "hits device->host");
   return finish(s, stream, slot, (flags & LRT_TRACE_COUNT_WORK) != 0);
+}
+
+lrt_status lrt_trace_nearest_image(lrt_scene* s, const float* rays_dev, lrt_hit* hits_dev, uint32_t width,
+                                   uint32_t height, void* stream_p, uint32_t flags)
+{
+  if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  if (!s->committed || !s->dev) return fail(s, LRT_ERR_NOT_COMMITTED, "trace before CommitScene/upload");
+  if (width == 0 || height == 0) return LRT_OK;
+  if (!rays_dev || !hits_dev || ((reinterpret_cast<uintptr_t>(rays_dev) | reinterpret_cast<uintptr_t>(hits_dev)) & 15))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_trace_nearest_image: rays/hits must be 16-byte aligned device memory");
+  lrt_status st = check_preset(s);
+  if (st != LRT_OK) return st;
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_p);
+  StreamSlot* slot = nullptr;
+  st = slot_for(s, stream, &slot);
+  if (st != LRT_OK) return st;
+  return launch(s, reinterpret_cast<const float4*>(rays_dev), hits_dev, uint64_t(width) * height, stream, flags, slot,
+                width, height);
 }
 
 // Waits for the stream's traces and reports a bounded-loop limit hit by any of

@@ -718,24 +718,39 @@ __device__ void trace_one(CTX& c, uint32_t* stack, uint32_t stride, uint32_t cap
 // One thread per ray; warps fetch 32-ray batches from a global counter
 // (persistent grid of ~one wave).  Stacks live in shared memory,
 // stack[i * blockDim + tid].
+//
+// With img_w > 0 the n = img_w * img_h rays form an image in row-major pixel
+// order and a warp's 32 rays are an 8x4-pixel tile instead of 32 pixels of a
+// row (the reference's kernel1D_FillGbuffer also walks pixels in packed
+// tiles, MultiRenderer.cpp:185-202); each ray's hit is unchanged.
 template <bool COUNT, bool SOLVERS>
 __global__ void __launch_bounds__(kTraceThreads, 6) k_trace(DevScene S, const float4* __restrict__ rays,
                                                          lrt_hit* __restrict__ hits, uint64_t n,
                                                          unsigned long long* __restrict__ work_counter,
                                                          unsigned long long* __restrict__ counters,
-                                                         uint32_t* __restrict__ err_word, uint32_t stack_cap)
+                                                         uint32_t* __restrict__ err_word, uint32_t stack_cap,
+                                                         uint32_t img_w, uint32_t img_h)
 {
   extern __shared__ uint32_t smem_stack[];
   uint32_t* stack = smem_stack + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
   Ctx<COUNT, false, SOLVERS> c(S, normal_words(smem_stack, stack_cap));
+  const uint64_t tilesX = (uint64_t(img_w) + 7) / 8;
+  const uint64_t slots = img_w ? tilesX * ((uint64_t(img_h) + 3) / 4) * 32 : n; // ray slots handed out
   for (;;) {
     unsigned long long base = 0;
     if (lane == 0) base = atomicAdd(work_counter, 32ull);
     base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    if (base >= n) break;
-    const uint64_t i = base + lane;
-    if (i < n) {
+    if (base >= slots) break;
+    uint64_t i = base + lane;
+    bool valid = i < n;
+    if (img_w) {
+      const uint64_t b = base >> 5;
+      const uint32_t x = uint32_t(b % tilesX) * 8 + (lane & 7), y = uint32_t(b / tilesX) * 4 + (lane >> 3);
+      valid = x < img_w && y < img_h;
+      i = uint64_t(y) * img_w + x;
+    }
+    if (valid) {
       const float4 pn = __ldg(rays + 2 * i), df = __ldg(rays + 2 * i + 1);
       lrt_hit h;
       trace_one(c, stack, blockDim.x, stack_cap, pn, df, h);
@@ -1076,7 +1091,8 @@ __global__ void k_eye_rays(DevCamera cam, float4* __restrict__ rays)
 // Host-side launchers (one copy per namespace; declared in trace_api.h).
 cudaError_t launch_trace(const DevScene& S, const float4* rays, lrt_hit* hits, uint64_t n,
                                 unsigned long long* work_counter, unsigned long long* counters, uint32_t* err_word,
-                                uint32_t stack_cap, int grid, cudaStream_t stream, bool count)
+                                uint32_t stack_cap, int grid, cudaStream_t stream, bool count, uint32_t img_w,
+                                uint32_t img_h)
 {
   const size_t smem = trace_smem_bytes(stack_cap);
   // the ANALYTIC / NEWTON / IT node solvers live in their own instantiation,
@@ -1085,16 +1101,16 @@ cudaError_t launch_trace(const DevScene& S, const float4* rays, lrt_hit* hits, u
   const bool solvers = solver != kSolverST && solver != kSolverBBox;
   if (count && solvers)
     k_trace<true, true><<<grid, kTraceThreads, smem, stream>>>(S, rays, hits, n, work_counter, counters, err_word,
-                                                               stack_cap);
+                                                               stack_cap, img_w, img_h);
   else if (count)
     k_trace<true, false><<<grid, kTraceThreads, smem, stream>>>(S, rays, hits, n, work_counter, counters, err_word,
-                                                                stack_cap);
+                                                                stack_cap, img_w, img_h);
   else if (solvers)
     k_trace<false, true><<<grid, kTraceThreads, smem, stream>>>(S, rays, hits, n, work_counter, counters, err_word,
-                                                                stack_cap);
+                                                                stack_cap, img_w, img_h);
   else
     k_trace<false, false><<<grid, kTraceThreads, smem, stream>>>(S, rays, hits, n, work_counter, counters, err_word,
-                                                                 stack_cap);
+                                                                 stack_cap, img_w, img_h);
   return cudaGetLastError();
 }
 

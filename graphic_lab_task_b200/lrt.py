@@ -29,7 +29,7 @@ EXPORTED = (
     "lrt_trace_nearest_noalloc", "lrt_batch_create", "lrt_batch_destroy", "lrt_batch_ray_offsets",
     "lrt_batch_update_cameras", "lrt_batch_set_shape", "lrt_batch_get_shape", "lrt_batch_trace", "lrt_batch_sync",
     "lrt_batch_autotune", "lrt_render_lambert", "lrt_adjoint_lambert_sbs", "lrt_sbs_update_values",
-    "lrt_generate_bounce_rays", "lrt_render_rgba8",
+    "lrt_generate_bounce_rays", "lrt_render_rgba8", "lrt_trace_nearest_image",
     "lrt_wl_noisy_sphere", "lrt_wl_spheres", "lrt_wl_sphere_sdf", "lrt_wl_sbs_from_spheres",
     "lrt_wl_frame_octree_from_spheres", "lrt_wl_svs_from_spheres",
 )
@@ -75,6 +75,7 @@ def lib():
         "lrt_trace_nearest_noalloc": [vp, vp, vp, u64, vp, u32],
         "lrt_render_lambert": [vp, vp, u64, vp, vp, vp],
         "lrt_render_rgba8": [vp, vp, vp, u32, vp, vp, vp],
+        "lrt_trace_nearest_image": [vp, vp, vp, u32, u32, vp, u32],
         "lrt_generate_bounce_rays": [vp, vp, vp, u64, u64, C.c_float, C.c_float, vp, vp],
         "lrt_adjoint_lambert_sbs": [vp, vp, u64, vp, vp, vp, vp],
         "lrt_sbs_update_values": [vp, vp, u64, vp, u32],
@@ -248,6 +249,13 @@ class SceneRT:
             (LRT_TRACE_COUNT_WORK if count_work else 0)
         self._check(lib().lrt_trace_nearest(self.h, C.c_void_p(rays_ptr), C.c_void_p(hits_ptr), n,
                                             C.c_void_p(stream) if stream else None, flags))
+
+    def trace_image(self, rays_ptr, hits_ptr, width, height, stream=0, fast_math=False, count_work=False):
+        """Asynchronous trace of the device rays of a width x height image
+        (row-major pixels), in 8x4-pixel tiles per warp."""
+        flags = (LRT_TRACE_FAST_MATH if fast_math else 0) | (LRT_TRACE_COUNT_WORK if count_work else 0)
+        self._check(lib().lrt_trace_nearest_image(self.h, C.c_void_p(rays_ptr), C.c_void_p(hits_ptr), width, height,
+                                                  C.c_void_p(stream) if stream else None, flags))
 
     def sync(self, stream=0, read_counters=False):
         self._check(lib().lrt_trace_sync(self.h, C.c_void_p(stream) if stream else None, int(read_counters)))

@@ -310,6 +310,16 @@ lrt_status lrt_trace_nearest_noalloc(lrt_scene* scene, const float* rays, lrt_hi
  * LRT_TRACE_COUNT_WORK trace on the stream become readable. */
 lrt_status lrt_trace_sync(lrt_scene* scene, void* stream, int32_t read_counters);
 
+/* lrt_trace_nearest for the width*height rays of one image stored in
+ * row-major pixel order, device pointers only (asynchronous on `stream`,
+ * flags: LRT_TRACE_FAST_MATH, LRT_TRACE_COUNT_WORK).  A warp traces an 8x4
+ * tile of pixels rather than 32 pixels of one row, as the reference's
+ * kernel1D_FillGbuffer walks pixels in packed tiles (MultiRenderer.cpp:
+ * 185-202); every hit equals lrt_trace_nearest's for the same ray.  No
+ * counterpart entry point in the reference. */
+lrt_status lrt_trace_nearest_image(lrt_scene* scene, const float* rays_dev, lrt_hit* hits_dev, uint32_t width,
+                                   uint32_t height, void* stream, uint32_t flags);
+
 /* ISceneObject::RayQuery_NearestHit / RayQuery_AnyHit for one ray
  * (CrossRT.h:145,163).  Synchronous; forwards to a 1-ray batch. */
 lrt_status lrt_ray_query_nearest_hit(lrt_scene* scene, const float pos_and_near[4], const float dir_and_far[4],

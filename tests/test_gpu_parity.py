@@ -266,3 +266,32 @@ def test_node_solvers_match_oracle(cuda, solver):
         assert rep["max_rel_t"] <= 1e-5 and rep["max_normal_err"] <= 1e-3, rep
     else:
         assert bit_equal(got, want).all(), hit_summary(got, want)
+
+
+@pytest.mark.parametrize("size", [(203, 97), (1920, 1080)])
+def test_image_tile_order_equals_linear_trace(cuda, size):
+    """lrt_trace_nearest_image hands out 8x4-pixel tiles instead of 32
+    consecutive rays; every hit (and the work counted) is the same as the
+    linear trace's, ragged image edges included."""
+    torch = cuda
+    from graphic_lab_task_b200 import HIT_DTYPE
+    sph = wl.spheres(64, seed=1)
+    hdr, nodes, vals, vf = wl.sbs_from_spheres(sph, grid_res=128)
+    sc = SceneRT()
+    sc.AddInstance(sc.AddGeom_SdfSBS(hdr, nodes, vals, vf), wl.IDENTITY)
+    sc.CommitScene()
+    w, h = size
+    rays = wl.eye_rays_host(wl.camera((0, 0, 3), width=w, height=h))
+    R = torch.from_numpy(rays).cuda()
+    H1 = torch.zeros(w * h * 8, dtype=torch.float32, device="cuda")
+    H2 = torch.zeros_like(H1)
+    sc.trace_device(R.data_ptr(), H1.data_ptr(), w * h, count_work=True)
+    sc.sync(read_counters=True)
+    c1 = sc.work_counters()
+    sc.trace_image(R.data_ptr(), H2.data_ptr(), w, h, count_work=True)
+    sc.sync(read_counters=True)
+    c2 = sc.work_counters()
+    a, b = H1.cpu().numpy().view(HIT_DTYPE), H2.cpu().numpy().view(HIT_DTYPE)
+    assert bit_equal(a, b).all(), hit_summary(b, a)
+    assert np.array_equal(c1, c2)
+    assert (a["primId"] != MISS).sum() > 0.05 * w * h
