@@ -664,127 +664,141 @@ def configs_table(args):
         d.update({"steps": 10, "l2": "flushed before every timed step", "data": "synthetic (seeded)"})
         print(json.dumps(d), flush=True)
 
-    # 0: triangle mesh, 256x256
-    v, t = wl.noisy_sphere(317, seed=0)
-    sc = SceneRT()
-    sc.AddInstance(sc.AddGeom_Triangles3f(v, t), wl.IDENTITY)
-    sc.CommitScene()
-    rays = wl.eye_rays_host(wl.camera((0, 0, 3), width=256, height=256))
-    n = len(rays)
-    R = torch.from_numpy(rays).to(dev)
-    H = torch.empty(n * 8, dtype=torch.float32, device=dev)
-    ms = timed(lambda: sc.trace_device(R.data_ptr(), H.data_ptr(), n, stream=sp))
-    sc.sync(stream=sp)
-    emit({"config": 0, "workload": "mesh 200k triangles, 256x256", "rays": n, "gpu_ms": ms,
-          "gpu_mrays_s": n / ms / 1e3, "roofline": roofline(sc, R, n, ms), "cpu_reference": cpu(sc, rays)})
-    sc.close()
+    only = {int(x) for x in args.only.split(",") if x.strip()}
 
-    # 1: SBS 1920x1080
-    (hdr, nodes, vals, vf), cam = workload_scene()
-    sc = SceneRT()
-    sc.AddInstance(sc.AddGeom_SdfSBS(hdr, nodes, vals, vf), wl.IDENTITY)
-    sc.CommitScene()
-    rays = wl.eye_rays_host(cam)
-    n = len(rays)
-    R = torch.from_numpy(rays).to(dev)
-    H = torch.empty(n * 8, dtype=torch.float32, device=dev)
-    ms = timed(lambda: sc.trace_device(R.data_ptr(), H.data_ptr(), n, stream=sp))
-    sc.sync(stream=sp)
-    emit({"config": 1, "workload": "SBS 512^3, 1920x1080", "rays": n, "gpu_ms": ms, "gpu_mrays_s": n / ms / 1e3,
-          "roofline": roofline(sc, R, n, ms), "cpu_reference": cpu(sc, rays)})
+    if 0 in only:
+        # 0: triangle mesh, 256x256
+        v, t = wl.noisy_sphere(317, seed=0)
+        sc = SceneRT()
+        sc.AddInstance(sc.AddGeom_Triangles3f(v, t), wl.IDENTITY)
+        sc.CommitScene()
+        rays = wl.eye_rays_host(wl.camera((0, 0, 3), width=256, height=256))
+        n = len(rays)
+        R = torch.from_numpy(rays).to(dev)
+        H = torch.empty(n * 8, dtype=torch.float32, device=dev)
+        ms = timed(lambda: sc.trace_device(R.data_ptr(), H.data_ptr(), n, stream=sp))
+        sc.sync(stream=sp)
+        emit({"config": 0, "workload": "mesh 200k triangles, 256x256", "rays": n, "gpu_ms": ms,
+              "gpu_mrays_s": n / ms / 1e3, "roofline": roofline(sc, R, n, ms), "cpu_reference": cpu(sc, rays)})
+        sc.close()
 
-    # 3: 64 batched cameras on the same scene
-    cams = wl.sphere_cameras(64, radius=3.0, res_min=128, res_max=2048, seed=3)
-    b = CameraBatch(sc, cams)
-    total = b.total_rays
-    hb = torch.zeros(total * 8, dtype=torch.float32, device=dev)
-    b.autotune(hb.data_ptr(), stream=sp, reps=2)
-    bms = timed(lambda: b.trace(hb.data_ptr(), stream=sp))
-    b.sync(stream=sp)
-    maxn = max(c.width * c.height for c in cams)
-    rbuf = torch.empty(maxn * 8, dtype=torch.float32, device=dev)
-    hp = torch.zeros(total * 8, dtype=torch.float32, device=dev)
+    if 1 in only or 3 in only:
+        # 1: SBS 1920x1080
+        (hdr, nodes, vals, vf), cam = workload_scene()
+        sc = SceneRT()
+        sc.AddInstance(sc.AddGeom_SdfSBS(hdr, nodes, vals, vf), wl.IDENTITY)
+        sc.CommitScene()
+        if 1 in only:
+            rays = wl.eye_rays_host(cam)
+            n = len(rays)
+            R = torch.from_numpy(rays).to(dev)
+            H = torch.empty(n * 8, dtype=torch.float32, device=dev)
+            ms = timed(lambda: sc.trace_device(R.data_ptr(), H.data_ptr(), n, stream=sp))
+            sc.sync(stream=sp)
+            emit({"config": 1, "workload": "SBS 512^3, 1920x1080", "rays": n, "gpu_ms": ms, "gpu_mrays_s": n / ms / 1e3,
+                  "roofline": roofline(sc, R, n, ms), "cpu_reference": cpu(sc, rays)})
 
-    def plain():
-        off = 0
-        for c in cams:
-            k = c.width * c.height
-            sc.generate_eye_rays(c, rbuf.data_ptr(), sp)
-            sc.trace_device(rbuf.data_ptr(), hp.data_ptr() + off * 32, k, stream=sp)
-            off += k
+        if 3 in only:
+            # 3: 64 batched cameras on the same scene
+            cams = wl.sphere_cameras(64, radius=3.0, res_min=128, res_max=2048, seed=3)
+            b = CameraBatch(sc, cams)
+            total = b.total_rays
+            hb = torch.zeros(total * 8, dtype=torch.float32, device=dev)
+            b.autotune(hb.data_ptr(), stream=sp, reps=2)
+            bms = timed(lambda: b.trace(hb.data_ptr(), stream=sp))
+            b.sync(stream=sp)
+            maxn = max(c.width * c.height for c in cams)
+            rbuf = torch.empty(maxn * 8, dtype=torch.float32, device=dev)
+            hp = torch.zeros(total * 8, dtype=torch.float32, device=dev)
 
-    pms = timed(plain)
-    sc.sync(stream=sp)
-    identical = bool(torch.equal(hb.view(torch.int32), hp.view(torch.int32)))
-    b.close()
-    # CPU sample: every 16th pixel of every 4th camera
-    sample = np.concatenate([wl.eye_rays_host(c)[::16] for c in cams[::4]])
-    emit({"config": 3, "workload": "64 cameras, 128..2048 square, SBS 512^3", "rays": total,
-          "gpu_batched_ms": bms, "gpu_batched_mrays_s": total / bms / 1e3, "gpu_plain_ms": pms,
-          "gpu_plain_mrays_s": total / pms / 1e3, "identical_hits": identical,
-          "cpu_reference": cpu(sc, sample)})
-    sc.close()
+            def plain():
+                off = 0
+                for c in cams:
+                    k = c.width * c.height
+                    sc.generate_eye_rays(c, rbuf.data_ptr(), sp)
+                    sc.trace_device(rbuf.data_ptr(), hp.data_ptr() + off * 32, k, stream=sp)
+                    off += k
 
-    # 2: instanced meshes + frame octrees, primary 4096^2 and one bounce
-    sc = SceneRT()
-    wl.build_instanced(sc)
-    sc.CommitScene()
-    cam = wl.camera(wl.INSTANCED_EYE, width=4096, height=4096)
-    n = 4096 * 4096
-    R = torch.empty(n * 8, dtype=torch.float32, device=dev)
-    H = torch.empty_like(R)
-    B = torch.empty_like(R)
-    sc.generate_eye_rays(cam, R.data_ptr(), sp)
-    pms = timed(lambda: sc.trace_device(R.data_ptr(), H.data_ptr(), n, stream=sp), steps=5)
-    sc.generate_bounce_rays(R.data_ptr(), H.data_ptr(), n, 11, B.data_ptr(), stream=sp)
-    torch.cuda.synchronize(dev)
-    bv = B.view(-1, 8)
-    bv = bv[~torch.isnan(bv[:, 0])].contiguous()
-    nb = bv.shape[0]
-    HB = torch.empty(nb * 8, dtype=torch.float32, device=dev)
-    bms = timed(lambda: sc.trace_device(bv.data_ptr(), HB.data_ptr(), nb, stream=sp), steps=5)
+            pms = timed(plain)
+            sc.sync(stream=sp)
+            identical = bool(torch.equal(hb.view(torch.int32), hp.view(torch.int32)))
+            b.close()
+            # CPU sample: every 16th pixel of every 4th camera
+            sample = np.concatenate([wl.eye_rays_host(c)[::16] for c in cams[::4]])
+            emit({"config": 3, "workload": "64 cameras, 128..2048 square, SBS 512^3", "rays": total,
+                  "gpu_batched_ms": bms, "gpu_batched_mrays_s": total / bms / 1e3, "gpu_plain_ms": pms,
+                  "gpu_plain_mrays_s": total / pms / 1e3, "identical_hits": identical,
+                  "cpu_reference": cpu(sc, sample)})
+            sc.close()
 
-    def wave():
-        sc.trace_device(R.data_ptr(), H.data_ptr(), n, stream=sp)
-        sc.generate_bounce_rays(R.data_ptr(), H.data_ptr(), n, 11, B.data_ptr(), stream=sp)
-        x = B.view(-1, 8)
-        x = x[~torch.isnan(x[:, 0])].contiguous()
-        sc.trace_device(x.data_ptr(), HB.data_ptr(), x.shape[0], stream=sp)
+    if 2 in only:
+        # 2: instanced meshes + frame octrees, primary 4096^2 and one bounce
+        sc = SceneRT()
+        wl.build_instanced(sc)
+        sc.CommitScene()
+        cam = wl.camera(wl.INSTANCED_EYE, width=4096, height=4096)
+        n = 4096 * 4096
+        R = torch.empty(n * 8, dtype=torch.float32, device=dev)
+        H = torch.empty_like(R)
+        B = torch.empty_like(R)
+        sc.generate_eye_rays(cam, R.data_ptr(), sp)
+        pms = timed(lambda: sc.trace_device(R.data_ptr(), H.data_ptr(), n, stream=sp), steps=5)
+        idx = torch.empty(n, dtype=torch.int32, device=dev)
+        cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+        sc.generate_bounce_rays_compact(R.data_ptr(), H.data_ptr(), n, 11, B.data_ptr(), idx.data_ptr(), cnt.data_ptr(),
+                                        stream=sp)
+        torch.cuda.synchronize(dev)
+        nb = int(cnt.item())
+        bv = B.view(-1, 8)[:nb]
+        HB = torch.empty(nb * 8, dtype=torch.float32, device=dev)
+        bms = timed(lambda: sc.trace_device(bv.data_ptr(), HB.data_ptr(), nb, stream=sp), steps=5)
+        cms = timed(lambda: sc.generate_bounce_rays_compact(R.data_ptr(), H.data_ptr(), n, 11, B.data_ptr(),
+                                                            idx.data_ptr(), cnt.data_ptr(), stream=sp), steps=5)
 
-    wms = timed(wave, steps=5)
-    sc.sync(stream=sp)
-    prim = R.view(-1, 8)[:: 256].cpu().numpy()
-    bnc = bv[:: max(1, nb // 65536)].cpu().numpy()
-    emit({"config": 2, "workload": "1024 instances (3 meshes, 2 frame octrees), 4096^2 + 1 bounce",
-          "rays": n, "bounce_rays": nb, "gpu_primary_ms": pms, "gpu_primary_mrays_s": n / pms / 1e3,
-          "gpu_bounce_ms": bms, "gpu_bounce_mrays_s": nb / bms / 1e3, "gpu_wavefront_ms": wms,
-          "gpu_wavefront_mrays_s": (n + nb) / wms / 1e3, "roofline_primary": roofline(sc, R, n, pms),
-          "cpu_reference_primary": cpu(sc, prim), "cpu_reference_bounce": cpu(sc, bnc)})
-    sc.close()
-    del R, H, B, HB, bv
+        def wave():
+            # primary trace, compacted bounce rays, bounce trace sized by the device count
+            sc.trace_device(R.data_ptr(), H.data_ptr(), n, stream=sp)
+            sc.generate_bounce_rays_compact(R.data_ptr(), H.data_ptr(), n, 11, B.data_ptr(), idx.data_ptr(),
+                                            cnt.data_ptr(), stream=sp)
+            k = int(cnt.item())
+            sc.trace_device(B.data_ptr(), HB.data_ptr(), k, stream=sp)
 
-    # 4: differentiable render, 16 views of 512^2 at a virtual 256^3 grid
-    hdr, nodes, vals, vf, target, cams, rays = wl.adjoint_workload(grid_res=256, views=16, res=512)
-    sc = SceneRT()
-    sc.AddInstance(sc.AddGeom_SdfSBS(hdr, nodes, vals, vf), wl.IDENTITY)
-    sc.CommitScene()
-    n = len(rays)
-    R = torch.from_numpy(rays).to(dev)
-    img = torch.empty(n, dtype=torch.float32, device=dev)
-    dimg = torch.full((n,), 1.0 / n, dtype=torch.float32, device=dev)
-    grad = torch.zeros(len(vf), dtype=torch.float32, device=dev)
-    fms = timed(lambda: sc.render_lambert(R.data_ptr(), n, wl.LIGHT, img.data_ptr(), stream=sp))
+        wms = timed(wave, steps=5)
+        sc.sync(stream=sp)
+        prim = R.view(-1, 8)[:: 256].cpu().numpy()
+        bnc = bv[:: max(1, nb // 65536)].cpu().numpy()
+        emit({"config": 2, "workload": "1024 instances (3 meshes, 2 frame octrees), 4096^2 + 1 bounce",
+              "rays": n, "bounce_rays": nb, "gpu_primary_ms": pms, "gpu_primary_mrays_s": n / pms / 1e3,
+              "gpu_bounce_ms": bms, "gpu_bounce_mrays_s": nb / bms / 1e3, "gpu_bounce_generate_compact_ms": cms,
+              "gpu_wavefront_ms": wms,
+              "gpu_wavefront_mrays_s": (n + nb) / wms / 1e3, "roofline_primary": roofline(sc, R, n, pms),
+              "cpu_reference_primary": cpu(sc, prim), "cpu_reference_bounce": cpu(sc, bnc)})
+        sc.close()
+        del R, H, B, HB, bv
 
-    def adj():
-        grad.zero_()
-        sc.adjoint_lambert(R.data_ptr(), n, wl.LIGHT, dimg.data_ptr(), grad.data_ptr(), stream=sp)
+    if 4 in only:
+        # 4: differentiable render, 16 views of 512^2 at a virtual 256^3 grid
+        hdr, nodes, vals, vf, target, cams, rays = wl.adjoint_workload(grid_res=256, views=16, res=512)
+        sc = SceneRT()
+        sc.AddInstance(sc.AddGeom_SdfSBS(hdr, nodes, vals, vf), wl.IDENTITY)
+        sc.CommitScene()
+        n = len(rays)
+        R = torch.from_numpy(rays).to(dev)
+        img = torch.empty(n, dtype=torch.float32, device=dev)
+        dimg = torch.full((n,), 1.0 / n, dtype=torch.float32, device=dev)
+        grad = torch.zeros(len(vf), dtype=torch.float32, device=dev)
+        fms = timed(lambda: sc.render_lambert(R.data_ptr(), n, wl.LIGHT, img.data_ptr(), stream=sp))
 
-    ams = timed(adj)
-    sc.sync(stream=sp)
-    emit({"config": 4, "workload": "SBS 256^3, 16 views of 512^2, Lambert forward + adjoint", "rays": n,
-          "gpu_forward_ms": fms, "gpu_forward_mrays_s": n / fms / 1e3, "gpu_adjoint_ms": ams,
-          "adjoint_over_forward": ams / fms, "cpu_reference_trace": cpu(sc, rays[:: 16])})
-    sc.close()
+        def adj():
+            grad.zero_()
+            sc.adjoint_lambert(R.data_ptr(), n, wl.LIGHT, dimg.data_ptr(), grad.data_ptr(), stream=sp)
+
+        ams = timed(adj)
+        sc.sync(stream=sp)
+        emit({"config": 4, "workload": "SBS 256^3, 16 views of 512^2, Lambert forward + adjoint", "rays": n,
+              "gpu_forward_ms": fms, "gpu_forward_mrays_s": n / fms / 1e3, "gpu_adjoint_ms": ams,
+              "adjoint_over_forward": ams / fms, "cpu_reference_trace": cpu(sc, rays[:: 16])})
+        sc.close()
 
 
 def main():
@@ -797,6 +811,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the batched-camera and adjoint sections")
     ap.add_argument("--configs", action="store_true",
                     help="measure every benchmark configuration (GPU and reference CPU), one JSON line each")
+    ap.add_argument("--only", default="0,1,2,3,4", help="with --configs: the configurations to measure")
     args = ap.parse_args()
     if args.configs:
         configs_table(args)

@@ -41,6 +41,9 @@ struct DeviceScene {
   const lrt_bvh_node_pair* pairsOrig = nullptr; // unpruned node pairs (used once SBS values change)
   std::vector<DevSbs> sbsHost;                  // host copy of the SBS model table
   bool cleanBoxes = false;                      // every node box has 0 or 6 NaN coordinates
+  // per-tile hit counts of lrt_generate_bounce_rays_compact
+  uint32_t* tileScratch = nullptr;
+  uint64_t tileCap = 0;
   // staging buffers for host-pointer calls
   float4* rays = nullptr;
   lrt_hit* hits = nullptr;
@@ -61,6 +64,7 @@ struct DeviceScene {
     for (void* p : allocs) cudaFree(p);
     if (rays) cudaFree(rays);
     if (hits) cudaFree(hits);
+    if (tileScratch) cudaFree(tileScratch);
   }
 };
 

@@ -9,6 +9,7 @@
 // tests, and a caller can drop them (origin x != x) before tracing.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "device_scene.h"
@@ -59,29 +60,136 @@ __device__ f3 cosine_sample(float r1, float r2, f3 n)
   return res;
 }
 
+// The bounce ray of traced ray i (which hit): origin at the hit point,
+// cosine-weighted direction around the normal turned towards the ray.
+__device__ __forceinline__ void bounce_ray(const float4 pn, const float4 df, const float4 h0, const float4 h1,
+                                           uint64_t i, uint64_t seed, float tnear, float tfar, float4* out)
+{
+  const f3 dir = mk3(df.x, df.y, df.z);
+  const f3 pos = mk3(pn.x, pn.y, pn.z) + h0.x * dir;
+  f3 nrm = decode_normal(mk2(h1.z, h1.w));
+  if (dot(nrm, dir) > 0.0f) nrm = -1.0f * nrm; // face the incoming ray
+  uint64_t state = (i + 1) * 0x9E3779B97F4A7C15ull ^ seed;
+  pcg_hash(state);
+  const float r1 = uniform01(state), r2 = uniform01(state);
+  const f3 b = normalize(cosine_sample(r1, r2, nrm));
+  out[0] = make_float4(pos.x, pos.y, pos.z, tnear);
+  out[1] = make_float4(b.x, b.y, b.z, tfar);
+}
+
 __global__ void k_bounce(const float4* __restrict__ rays, const lrt_hit* __restrict__ hits, uint64_t n, uint64_t seed,
                          float tnear, float tfar, float4* __restrict__ out)
 {
   for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
-    const float4 pn = rays[2 * i], df = rays[2 * i + 1];
     const float4 h0 = reinterpret_cast<const float4*>(hits + i)[0];
-    const float4 h1 = reinterpret_cast<const float4*>(hits + i)[1];
     if (__float_as_uint(h0.y) == 0xFFFFFFFFu) {
       const float qnan = __int_as_float(0x7fc00000);
       out[2 * i] = make_float4(qnan, qnan, qnan, tnear);
       out[2 * i + 1] = make_float4(0.0f, 0.0f, 1.0f, tfar);
       continue;
     }
-    const f3 dir = mk3(df.x, df.y, df.z);
-    const f3 pos = mk3(pn.x, pn.y, pn.z) + h0.x * dir;
-    f3 nrm = decode_normal(mk2(h1.z, h1.w));
-    if (dot(nrm, dir) > 0.0f) nrm = -1.0f * nrm; // face the incoming ray
-    uint64_t state = (i + 1) * 0x9E3779B97F4A7C15ull ^ seed;
-    pcg_hash(state);
-    const float r1 = uniform01(state), r2 = uniform01(state);
-    const f3 b = normalize(cosine_sample(r1, r2, nrm));
-    out[2 * i] = make_float4(pos.x, pos.y, pos.z, tnear);
-    out[2 * i + 1] = make_float4(b.x, b.y, b.z, tfar);
+    const float4 h1 = reinterpret_cast<const float4*>(hits + i)[1];
+    bounce_ray(rays[2 * i], rays[2 * i + 1], h0, h1, i, seed, tnear, tfar, out + 2 * i);
+  }
+}
+
+// Stream compaction of the hits in three passes over tiles of kTile rays
+// (kCompactThreads threads x kCompactItems rays, ray k*kCompactThreads + tid
+// of the tile for item k): count the hits of each tile, scan the tile
+// counts, then write each hit's bounce ray at its rank, so the output keeps
+// the order of the traced rays.
+constexpr int kCompactThreads = 256, kCompactItems = 8, kTile = kCompactThreads * kCompactItems;
+
+__device__ __forceinline__ bool is_hit(const lrt_hit* hits, uint64_t i, uint64_t n)
+{
+  return i < n && __ldg(&hits[i].primId) != 0xFFFFFFFFu;
+}
+
+__global__ void __launch_bounds__(kCompactThreads) k_count_hits(const lrt_hit* __restrict__ hits, uint64_t n,
+                                                                uint32_t* __restrict__ tile_count)
+{
+  __shared__ uint32_t warp_sum[kCompactThreads / 32];
+  const uint64_t base = uint64_t(blockIdx.x) * kTile;
+  uint32_t c = 0;
+#pragma unroll
+  for (int k = 0; k < kCompactItems; k++) c += is_hit(hits, base + k * kCompactThreads + threadIdx.x, n);
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, o);
+  if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < kCompactThreads / 32; w++) t += warp_sum[w];
+    tile_count[blockIdx.x] = t;
+  }
+}
+
+// Exclusive scan of the tile counts (one block); count_out = the total.
+__global__ void __launch_bounds__(1024) k_scan_tiles(uint32_t* __restrict__ tile, uint32_t ntiles,
+                                                     unsigned long long* __restrict__ count_out)
+{
+  __shared__ uint32_t warp_sum[32];
+  __shared__ unsigned long long carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (uint32_t start = 0; start < ntiles; start += 1024) {
+    const uint32_t t = start + threadIdx.x;
+    const uint32_t v = t < ntiles ? tile[t] : 0;
+    uint32_t x = v; // inclusive warp scan
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+      if ((threadIdx.x & 31) >= uint32_t(o)) x += y;
+    }
+    if ((threadIdx.x & 31) == 31) warp_sum[threadIdx.x >> 5] = x;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      uint32_t w = warp_sum[threadIdx.x];
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+        if (threadIdx.x >= uint32_t(o)) w += y;
+      }
+      warp_sum[threadIdx.x] = w; // inclusive over warps
+    }
+    __syncthreads();
+    const uint32_t before = (threadIdx.x >= 32 ? warp_sum[(threadIdx.x >> 5) - 1] : 0) + (x - v);
+    if (t < ntiles) tile[t] = uint32_t(carry) + before;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += warp_sum[31];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *count_out = carry;
+}
+
+__global__ void __launch_bounds__(kCompactThreads)
+    k_bounce_compact(const float4* __restrict__ rays, const lrt_hit* __restrict__ hits, uint64_t n, uint64_t seed,
+                     float tnear, float tfar, const uint32_t* __restrict__ tile_offset, float4* __restrict__ out,
+                     uint32_t* __restrict__ index)
+{
+  __shared__ uint32_t warp_sum[kCompactThreads / 32];
+  const uint64_t base = uint64_t(blockIdx.x) * kTile;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t rank = tile_offset[blockIdx.x];
+#pragma unroll 1
+  for (int k = 0; k < kCompactItems; k++) {
+    const uint64_t i = base + k * kCompactThreads + threadIdx.x;
+    const bool h = is_hit(hits, i, n);
+    const uint32_t m = __ballot_sync(0xFFFFFFFFu, h);
+    if (lane == 0) warp_sum[warp] = __popc(m);
+    __syncthreads();
+    uint32_t before = 0, total = 0;
+    for (int w = 0; w < kCompactThreads / 32; w++) {
+      const uint32_t c = warp_sum[w];
+      before += (w < int(warp)) ? c : 0;
+      total += c;
+    }
+    if (h) {
+      const uint32_t pos = rank + before + __popc(m & ((1u << lane) - 1u));
+      const float4 h0 = reinterpret_cast<const float4*>(hits + i)[0];
+      const float4 h1 = reinterpret_cast<const float4*>(hits + i)[1];
+      bounce_ray(rays[2 * i], rays[2 * i + 1], h0, h1, i, seed, tnear, tfar, out + 2 * uint64_t(pos));
+      index[pos] = uint32_t(i);
+    }
+    rank += total;
+    __syncthreads();
   }
 }
 
@@ -105,4 +213,43 @@ extern "C" lrt_status lrt_generate_bounce_rays(lrt_scene* s, const float* rays_d
                                                                seed, tnear, tfar, reinterpret_cast<float4*>(bounce_dev));
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? LRT_OK : (s ? cuda_fail(s, e, "bounce rays") : LRT_ERR_CUDA);
+}
+
+extern "C" lrt_status lrt_generate_bounce_rays_compact(lrt_scene* s, const float* rays_dev, const lrt_hit* hits_dev,
+                                                       uint64_t n, uint64_t seed, float tnear, float tfar,
+                                                       float* bounce_dev, uint32_t* index_dev, uint64_t* count_dev,
+                                                       void* stream_p)
+{
+  if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  if (!s->dev) return fail(s, LRT_ERR_NOT_COMMITTED, "lrt_generate_bounce_rays_compact before CommitScene/upload");
+  if (!rays_dev || !hits_dev || !bounce_dev || !index_dev || !count_dev)
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_generate_bounce_rays_compact: NULL buffer");
+  if ((reinterpret_cast<uintptr_t>(rays_dev) | reinterpret_cast<uintptr_t>(hits_dev) |
+       reinterpret_cast<uintptr_t>(bounce_dev)) & 15 || (reinterpret_cast<uintptr_t>(count_dev) & 7))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_generate_bounce_rays_compact: misaligned buffer");
+  if (n > 0xFFFFFFFFull)
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_generate_bounce_rays_compact: more than 2^32 - 1 rays");
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_p);
+  DeviceScene* d = s->dev;
+  const uint64_t ntiles = (n + kTile - 1) / kTile;
+  if (ntiles > d->tileCap) {
+    if (d->tileScratch) cudaFree(d->tileScratch);
+    d->tileScratch = nullptr;
+    d->tileCap = 0;
+    const cudaError_t e = cudaMalloc(&d->tileScratch, std::max<uint64_t>(ntiles, 1) * sizeof(uint32_t));
+    if (e != cudaSuccess) return cuda_fail(s, e, "compaction scratch");
+    d->tileCap = std::max<uint64_t>(ntiles, 1);
+  }
+  unsigned long long* cnt = reinterpret_cast<unsigned long long*>(count_dev);
+  if (n == 0) {
+    const cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), stream);
+    return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "cudaMemsetAsync");
+  }
+  k_count_hits<<<uint32_t(ntiles), kCompactThreads, 0, stream>>>(hits_dev, n, d->tileScratch);
+  k_scan_tiles<<<1, 1024, 0, stream>>>(d->tileScratch, uint32_t(ntiles), cnt);
+  k_bounce_compact<<<uint32_t(ntiles), kCompactThreads, 0, stream>>>(
+      reinterpret_cast<const float4*>(rays_dev), hits_dev, n, seed, tnear, tfar, d->tileScratch,
+      reinterpret_cast<float4*>(bounce_dev), index_dev);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "bounce compaction");
 }

@@ -29,7 +29,7 @@ EXPORTED = (
     "lrt_trace_nearest_noalloc", "lrt_batch_create", "lrt_batch_destroy", "lrt_batch_ray_offsets",
     "lrt_batch_update_cameras", "lrt_batch_set_shape", "lrt_batch_get_shape", "lrt_batch_trace", "lrt_batch_sync",
     "lrt_batch_autotune", "lrt_render_lambert", "lrt_adjoint_lambert_sbs", "lrt_sbs_update_values",
-    "lrt_generate_bounce_rays", "lrt_render_rgba8", "lrt_trace_nearest_image",
+    "lrt_generate_bounce_rays", "lrt_generate_bounce_rays_compact", "lrt_render_rgba8", "lrt_trace_nearest_image",
     "lrt_wl_noisy_sphere", "lrt_wl_spheres", "lrt_wl_sphere_sdf", "lrt_wl_sbs_from_spheres",
     "lrt_wl_frame_octree_from_spheres", "lrt_wl_svs_from_spheres",
 )
@@ -77,6 +77,7 @@ def lib():
         "lrt_render_rgba8": [vp, vp, vp, u32, vp, vp, vp],
         "lrt_trace_nearest_image": [vp, vp, vp, u32, u32, vp, u32],
         "lrt_generate_bounce_rays": [vp, vp, vp, u64, u64, C.c_float, C.c_float, vp, vp],
+        "lrt_generate_bounce_rays_compact": [vp, vp, vp, u64, u64, C.c_float, C.c_float, vp, vp, vp, vp],
         "lrt_adjoint_lambert_sbs": [vp, vp, u64, vp, vp, vp, vp],
         "lrt_sbs_update_values": [vp, vp, u64, vp, u32],
         "lrt_batch_create": [vp, vp, u32, P(vp)],
@@ -266,6 +267,15 @@ class SceneRT:
                                                    C.c_void_p(stream) if stream else None))
 
     # -- differentiable form (SBS distances) ------------------------------
+    def generate_bounce_rays_compact(self, rays_ptr, hits_ptr, n, seed, out_ptr, index_ptr, count_ptr, tnear=1e-4,
+                                     tfar=1e9, stream=0):
+        """Bounce rays of the hits only, in ray order; index_ptr (uint32) maps
+        them to the traced rays, count_ptr (device uint64) receives their number."""
+        self._check(lib().lrt_generate_bounce_rays_compact(self.h, C.c_void_p(rays_ptr), C.c_void_p(hits_ptr), n,
+                                                           seed, tnear, tfar, C.c_void_p(out_ptr),
+                                                           C.c_void_p(index_ptr), C.c_void_p(count_ptr),
+                                                           C.c_void_p(stream) if stream else None))
+
     def render_lambert(self, rays_ptr, n, light, image_ptr, stream=0):
         L = (C.c_float * 3)(*[float(x) for x in light])
         self._check(lib().lrt_render_lambert(self.h, C.c_void_p(rays_ptr), n, L, C.c_void_p(image_ptr),

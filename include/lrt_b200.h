@@ -375,6 +375,17 @@ lrt_status lrt_generate_eye_rays(lrt_scene* scene, const lrt_camera* camera, flo
 lrt_status lrt_generate_bounce_rays(lrt_scene* scene, const float* rays_dev, const lrt_hit* hits_dev, uint64_t n,
                                     uint64_t seed, float tnear, float tfar, float* bounce_rays_dev, void* stream);
 
+/* lrt_generate_bounce_rays without the rays whose primary ray missed: the
+ * bounce rays of the hits, in increasing order of the traced ray, packed
+ * into bounce_dev[0 .. *count_dev), with index_dev[k] the traced ray of
+ * bounce ray k (each bounce ray equals lrt_generate_bounce_rays's for that
+ * ray).  count_dev: one uint64 in device memory, written on `stream` (read it
+ * back, or size the next trace by it).  At most 2^32 - 1 rays.  Three
+ * launches (count per tile, scan, write), no host synchronisation. */
+lrt_status lrt_generate_bounce_rays_compact(lrt_scene* scene, const float* rays_dev, const lrt_hit* hits_dev,
+                                            uint64_t n, uint64_t seed, float tnear, float tfar, float* bounce_dev,
+                                            uint32_t* index_dev, uint64_t* count_dev, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Differentiable form (SBS distances)                                      */
 /* ------------------------------------------------------------------------ */

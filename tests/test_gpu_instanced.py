@@ -66,3 +66,34 @@ def test_instanced_primary_and_bounce(cuda, scale):
     if len(nan_rays):
         got = sc.RayQuery_NearestHitBatch(nan_rays)
         assert np.all(got["primId"] == MISS)
+
+
+@pytest.mark.parametrize("n", [1, 2047, 2049, 300001])
+def test_compacted_bounce_rays_equal_the_full_generator(cuda, n):
+    """lrt_generate_bounce_rays_compact packs the bounce rays of the hits in
+    ray order: they equal the full generator's rays at the hit positions,
+    the index map is the list of hit rays and the device count their number."""
+    torch = cuda
+    sc = SceneRT()
+    wl.build_instanced(sc, mesh_tris=(2000, 8000, 20000), octree_depth=6, n_instances=256)
+    sc.CommitScene()
+    rays = wl.eye_rays_host(wl.camera(wl.INSTANCED_EYE, width=600, height=501))[:n]
+    R = torch.from_numpy(np.ascontiguousarray(rays)).cuda()
+    H = torch.empty(n * 8, dtype=torch.float32, device="cuda")
+    sc.trace_device(R.data_ptr(), H.data_ptr(), n)
+    full = torch.empty(n * 8, dtype=torch.float32, device="cuda")
+    sc.generate_bounce_rays(R.data_ptr(), H.data_ptr(), n, 5, full.data_ptr())
+    comp = torch.full((n * 8,), -7.0, dtype=torch.float32, device="cuda")
+    idx = torch.zeros(n, dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    sc.generate_bounce_rays_compact(R.data_ptr(), H.data_ptr(), n, 5, comp.data_ptr(), idx.data_ptr(), cnt.data_ptr())
+    sc.sync()
+    hits = H.cpu().numpy().view(HIT_DTYPE)
+    want_idx = np.nonzero(hits["primId"] != MISS)[0]
+    k = int(cnt.item())
+    assert k == len(want_idx)
+    assert np.array_equal(idx.cpu().numpy()[:k].astype(np.int64), want_idx)
+    f = full.cpu().numpy().reshape(-1, 8)
+    c = comp.cpu().numpy().reshape(-1, 8)
+    assert np.array_equal(c[:k].view(np.uint32), f[want_idx].view(np.uint32))
+    assert np.all(c[k:] == -7.0)  # nothing written past the count
