@@ -35,6 +35,28 @@ EXPORTED = (
 )
 
 
+# Host-buffer traces of PIPE_MIN_RAYS rays or more are staged in chunks
+# (csrc/device.cu, pipeline_chunks): sizes ramp PIPE_CHUNK_MIN -> PIPE_CHUNK
+# and back down, one trace launch per chunk.
+PIPE_MIN_RAYS, PIPE_CHUNK, PIPE_CHUNK_MIN = 262144, 262144, 32768
+
+
+def pipeline_chunks(n):
+    """The chunk sizes of a host-buffer trace of n rays (one launch each)."""
+    if n < PIPE_MIN_RAYS:
+        return [n] if n else []
+    up, m = [], PIPE_CHUNK_MIN
+    while m < PIPE_CHUNK:
+        up.append(m)
+        m *= 2
+    ramp = sum(up)
+    if n <= 2 * ramp:
+        return [min(PIPE_CHUNK_MIN, n - o) for o in range(0, n, PIPE_CHUNK_MIN)]
+    mid = n - 2 * ramp
+    parts = (mid + PIPE_CHUNK - 1) // PIPE_CHUNK
+    return up + [mid // parts + (1 if i < mid % parts else 0) for i in range(parts)] + up[::-1]
+
+
 class LrtError(RuntimeError):
     def __init__(self, status, message):
         super().__init__("%s: %s" % (STATUS_NAMES.get(status, status), message))

@@ -80,3 +80,14 @@ def test_hit_layout():
     h = np.zeros(1, HIT_DTYPE)
     assert h.itemsize == 32
     assert HIT_DTYPE.fields["coords"][1] == 16
+
+
+def test_pipeline_chunk_schedule_mirror():
+    """graphic_lab_task_b200.lrt.pipeline_chunks mirrors the library's chunk
+    schedule of host-buffer traces: sizes sum to n, ramp up and down."""
+    from graphic_lab_task_b200.lrt import PIPE_CHUNK, PIPE_CHUNK_MIN, pipeline_chunks
+    for n in (1, 1000, 262144, 300001, 1000003, 2073600, 16777216):
+        c = pipeline_chunks(n)
+        assert sum(c) == n and all(0 < x <= PIPE_CHUNK for x in c)
+    c = pipeline_chunks(2073600)
+    assert c[0] == PIPE_CHUNK_MIN and c[-1] == PIPE_CHUNK_MIN and len(c) == 13
