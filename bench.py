@@ -762,8 +762,9 @@ def configs_table(args):
                                                             idx.data_ptr(), cnt.data_ptr(), stream=sp), steps=5)
 
         def wave():
-            # primary trace, compacted bounce rays, bounce trace sized by the device count
-            sc.trace_device(R.data_ptr(), H.data_ptr(), n, stream=sp)
+            # primary trace (the eye rays are an image: tile order), compacted
+            # bounce rays, bounce trace sized by the device count
+            sc.trace_image(R.data_ptr(), H.data_ptr(), 4096, 4096, stream=sp)
             sc.generate_bounce_rays_compact(R.data_ptr(), H.data_ptr(), n, 11, B.data_ptr(), idx.data_ptr(),
                                             cnt.data_ptr(), stream=sp)
             k = int(cnt.item())
