@@ -724,7 +724,7 @@ __device__ void trace_one(CTX& c, uint32_t* stack, uint32_t stride, uint32_t cap
 // row (the reference's kernel1D_FillGbuffer also walks pixels in packed
 // tiles, MultiRenderer.cpp:185-202); each ray's hit is unchanged.
 template <bool COUNT, bool SOLVERS>
-__global__ void __launch_bounds__(kTraceThreads, 6) k_trace(DevScene S, const float4* __restrict__ rays,
+__global__ void __launch_bounds__(kTraceThreads, 7) k_trace(DevScene S, const float4* __restrict__ rays,
                                                          lrt_hit* __restrict__ hits, uint64_t n,
                                                          unsigned long long* __restrict__ work_counter,
                                                          unsigned long long* __restrict__ counters,
@@ -776,7 +776,7 @@ __global__ void __launch_bounds__(kTraceThreads, 6) k_trace(DevScene S, const fl
 // finds its camera by binary search over the tile bases, and each lane
 // generates (lrt::eye_ray, the function k_eye_rays uses) and traces its
 // raysPerLane pixels, so every hit equals the plain per-camera path's.
-__global__ void __launch_bounds__(kTraceThreads, 6) k_trace_cameras(DevScene S, const DevBatchCamera* __restrict__ cams,
+__global__ void __launch_bounds__(kTraceThreads, 7) k_trace_cameras(DevScene S, const DevBatchCamera* __restrict__ cams,
                                                                  uint32_t ncams, uint32_t ntiles, DevBatchShape shape,
                                                                  lrt_hit* __restrict__ hits,
                                                                  unsigned long long* __restrict__ work_counter,
@@ -868,7 +868,7 @@ __device__ __forceinline__ uint32_t tonemap_rgba8(float r, float g, float b, flo
   return (w << 24) | (z << 16) | (y << 8) | x;
 }
 
-__global__ void __launch_bounds__(kTraceThreads) k_render_rgba8(DevScene S, DevCamera cam, DevLights L,
+__global__ void __launch_bounds__(kTraceThreads, 7) k_render_rgba8(DevScene S, DevCamera cam, DevLights L,
                                                                 uint32_t* __restrict__ image,
                                                                 unsigned long long* __restrict__ work_counter,
                                                                 uint32_t* __restrict__ err_word, uint32_t stack_cap)
