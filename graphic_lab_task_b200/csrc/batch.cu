@@ -35,6 +35,7 @@ struct lrt_camera_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   lrt_hit* graphHits = nullptr; // hits pointer baked into the graph
+  lrt::DevScene graphScene{};   // scene parameters baked into the graph
   ~lrt_camera_batch()
   {
     if (exec) cudaGraphExecDestroy(exec);
@@ -221,7 +222,10 @@ lrt_status lrt_batch_trace(lrt_camera_batch* b, lrt_hit* hits_dev, void* stream_
     e = enqueue(b, hits_dev, stream);
     return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "batched trace");
   }
-  if (!b->exec || b->graphHits != hits_dev) {
+  // re-capture when the hits buffer or anything the kernel reads from the
+  // scene changed (preset, voxel limit, new SBS values, updated instances)
+  const DevScene S = scene_params(s);
+  if (!b->exec || b->graphHits != hits_dev || std::memcmp(&S, &b->graphScene, sizeof(S)) != 0) {
     if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
     if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
     e = cudaStreamBeginCapture(b->capStream, cudaStreamCaptureModeThreadLocal);
@@ -233,6 +237,7 @@ lrt_status lrt_batch_trace(lrt_camera_batch* b, lrt_hit* hits_dev, void* stream_
     e = cudaGraphInstantiate(&b->exec, b->graph, 0);
     if (e != cudaSuccess) return cuda_fail(s, e, "cudaGraphInstantiate");
     b->graphHits = hits_dev;
+    b->graphScene = S;
   }
   e = cudaGraphLaunch(b->exec, stream);
   return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "cudaGraphLaunch");

@@ -274,9 +274,11 @@ lrt_status device_upload(lrt_scene* s)
     }
   }
   d->sbsHost = sbs;
-  d->cleanBoxes = boxes_clean(h.nodesTLAS.data(), h.nodesTLAS.size()) &&
-                  boxes_clean(reinterpret_cast<const lrt_bvh_node*>(pairs.data()), 2 * pairs.size()) &&
+  d->pairsClean = boxes_clean(reinterpret_cast<const lrt_bvh_node*>(pairs.data()), 2 * pairs.size()) &&
                   boxes_clean(reinterpret_cast<const lrt_bvh_node*>(h.allNodePairs.data()), 2 * h.allNodePairs.size());
+  d->cleanBoxes = d->pairsClean && boxes_clean(h.nodesTLAS.data(), h.nodesTLAS.size());
+  d->tlasCount = h.nodesTLAS.size();
+  d->instCount = h.instanceData.size();
 #undef UP
   if (st != LRT_OK) {
     device_release(s);
@@ -301,6 +303,44 @@ lrt_status device_upload(lrt_scene* s)
     return st;
   }
   d->grid = std::max(1, perSm) * sms;
+  return LRT_OK;
+}
+
+// After a commit that changed only instances (UpdateInstance, or ClearScene
+// and AddInstance over the same geometry): write the new TLAS and instances
+// into their buffers (new buffers where the counts changed) and leave every
+// BLAS, brick and mask array on the device as it is.
+lrt_status device_update_instances(lrt_scene* s)
+{
+  DeviceScene* d = s->dev;
+  const HostArrays& h = s->h;
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev != s->device)
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "commit on device %d of a scene uploaded to device %d", dev, s->device);
+  lrt_status st = LRT_OK;
+  auto put = [&](const void* src, size_t count, size_t elem, size_t& have, const void** ptr, const char* name) {
+    if (st != LRT_OK) return;
+    if (count != have) {
+      void* p = nullptr;
+      e = cudaMalloc(&p, count * elem);
+      if (e != cudaSuccess) {
+        st = cuda_fail(s, e, name);
+        return;
+      }
+      d->allocs.push_back(p);
+      *ptr = p; // the old buffer stays listed in allocs and is freed with the scene
+      have = count;
+    }
+    e = cudaMemcpy(const_cast<void*>(*ptr), src, count * elem, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) st = cuda_fail(s, e, name);
+  };
+  put(h.nodesTLAS.data(), h.nodesTLAS.size(), sizeof(lrt_bvh_node), d->tlasCount,
+      reinterpret_cast<const void**>(&d->S.tlas), "TLAS nodes");
+  put(h.instanceData.data(), h.instanceData.size(), sizeof(lrt_instance_data), d->instCount,
+      reinterpret_cast<const void**>(&d->S.instances), "instances");
+  if (st != LRT_OK) return st;
+  d->cleanBoxes = d->pairsClean && boxes_clean(h.nodesTLAS.data(), h.nodesTLAS.size());
   return LRT_OK;
 }
 

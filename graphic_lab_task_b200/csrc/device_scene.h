@@ -41,6 +41,8 @@ struct DeviceScene {
   const lrt_bvh_node_pair* pairsOrig = nullptr; // unpruned node pairs (used once SBS values change)
   std::vector<DevSbs> sbsHost;                  // host copy of the SBS model table
   bool cleanBoxes = false;                      // every node box has 0 or 6 NaN coordinates
+  bool pairsClean = false;                      // the BLAS part of cleanBoxes
+  size_t tlasCount = 0, instCount = 0;          // sizes of the TLAS and instance buffers
   // per-tile hit counts of lrt_generate_bounce_rays_compact
   uint32_t* tileScratch = nullptr;
   uint64_t tileCap = 0;

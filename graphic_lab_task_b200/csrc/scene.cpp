@@ -676,6 +676,7 @@ lrt_status lrt_set_preset(lrt_scene* s, const lrt_preset* p)
 lrt_status lrt_clear_geom(lrt_scene* s)
 {
   if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  s->geomVersion++;
   const lrt_preset keep = s->preset;
   s->h = HostArrays();
   s->preset = keep;
@@ -688,6 +689,7 @@ lrt_status lrt_add_geom_triangles3f(lrt_scene* s, const float* vpos, size_t nver
 {
   (void)flags;
   if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  s->geomVersion++;
   if (!vpos || !tri || nvert == 0 || nidx == 0 || nidx % 3 != 0)
     return fail(s, LRT_ERR_INVALID_ARGUMENT, "AddGeom_Triangles3f: empty input or index count %zu not a multiple of 3",
                 nidx);
@@ -767,6 +769,7 @@ lrt_status lrt_add_geom_aabb(lrt_scene* s, uint32_t tag, const float* boxes8, si
 {
   (void)flags;
   if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  s->geomVersion++;
   if (!boxes8 || n == 0) return fail(s, LRT_ERR_INVALID_ARGUMENT, "AddGeom_AABB: no boxes");
   std::vector<Aabb> boxes(n);
   for (size_t i = 0; i < n; i++) boxes[i] = box_of(boxes8 + 8 * i, boxes8 + 8 * i + 4);
@@ -780,6 +783,7 @@ lrt_status lrt_add_geom_sdf_frame_octree(lrt_scene* s, const lrt_sdf_frame_octre
                                          uint32_t* geom_id_out)
 {
   if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  s->geomVersion++;
   if (!nodes || count == 0 || count >= (1u << 28))
     return fail(s, LRT_ERR_INVALID_ARGUMENT, "AddGeom_SdfFrameOctree: %zu nodes", count);
   HostArrays& h = s->h;
@@ -805,6 +809,7 @@ lrt_status lrt_add_geom_sdf_frame_octree(lrt_scene* s, const lrt_sdf_frame_octre
 lrt_status lrt_add_geom_sdf_svs(lrt_scene* s, const lrt_sdf_svs_node* nodes, size_t count, uint32_t* geom_id_out)
 {
   if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  s->geomVersion++;
   if (!nodes || count == 0 || count >= (1u << 28))
     return fail(s, LRT_ERR_INVALID_ARGUMENT, "AddGeom_SdfSVS: %zu nodes", count);
   HostArrays& h = s->h;
@@ -825,6 +830,7 @@ lrt_status lrt_add_geom_sdf_sbs(lrt_scene* s, const lrt_sdf_sbs_header* header, 
                                 size_t values_f_count, uint32_t* geom_id_out)
 {
   if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  s->geomVersion++;
   if (!header || !nodes || count == 0 || !values || values_count == 0 || count >= (1u << 28) ||
       values_count >= (1u << 28))
     return fail(s, LRT_ERR_INVALID_ARGUMENT, "AddGeom_SdfSBS: %zu nodes, %zu values", count, values_count);
@@ -934,9 +940,49 @@ lrt_status lrt_commit_scene(lrt_scene* s, uint32_t flags)
   lrt_status st = validate(s, &s->info);
   if (st != LRT_OK) return st;
   if (flags & LRT_COMMIT_HOST_ONLY) return LRT_OK;
-  st = device_upload(s);
+  if (s->dev && s->uploadedGeomVersion == s->geomVersion) {
+    // only instances changed since the last upload (UpdateInstance,
+    // ClearScene + AddInstance): the BLAS data on the device stays
+    st = device_update_instances(s);
+  } else {
+    st = device_upload(s);
+    if (st == LRT_OK) s->uploadedGeomVersion = s->geomVersion;
+  }
   if (st != LRT_OK) return st;
   s->committed = true;
+  return LRT_OK;
+}
+
+lrt_status lrt_update_instance(lrt_scene* s, uint32_t inst_id, const float* m, uint32_t flags)
+{
+  if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  if (!m) return fail(s, LRT_ERR_INVALID_ARGUMENT, "UpdateInstance: NULL matrix");
+  HostArrays& h = s->h;
+  // the reference accepts inst_id == size (BVH2Common_host.cpp:1305) and writes past the array
+  if (inst_id >= h.instanceData.size())
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "UpdateInstance: instance %u of %zu", inst_id, h.instanceData.size());
+  lrt_instance_data& inst = h.instanceData[inst_id];
+  float inv[16];
+  if (!invert4(m, inv)) return fail(s, LRT_ERR_INVALID_ARGUMENT, "UpdateInstance: singular matrix");
+  // the box of the geometry box's 8 corners (:1311-1329); min/max do not depend on their order
+  const float* bmin = h.geomData[inst.geomId].boxMin;
+  const float* bmax = h.geomData[inst.geomId].boxMax;
+  for (int k = 0; k < 4; k++) { inst.boxMin[k] = FLT_MAX; inst.boxMax[k] = -FLT_MAX; }
+  for (int c = 0; c < 8; c++) {
+    const float v[4] = {(c & 1) ? bmax[0] : bmin[0], (c & 2) ? bmax[1] : bmin[1], (c & 4) ? bmax[2] : bmin[2], 1.0f};
+    for (int r = 0; r < 4; r++) {
+      const float x = v[0] * m[r] + v[1] * m[4 + r] + v[2] * m[8 + r] + v[3] * m[12 + r];
+      inst.boxMin[r] = std::min(inst.boxMin[r], x);
+      inst.boxMax[r] = std::max(inst.boxMax[r], x);
+    }
+  }
+  std::memcpy(inst.transform, m, sizeof(inst.transform));
+  std::memcpy(inst.transformInv, inv, sizeof(inst.transformInv));
+  // the reference leaves transformInvTransposed as it was (:1333-1334)
+  if (flags & LRT_UPDATE_NORMAL_MATRIX)
+    for (int r = 0; r < 4; r++)
+      for (int c = 0; c < 4; c++) inst.transformInvTransposed[c * 4 + r] = inst.transformInv[r * 4 + c];
+  s->committed = false;
   return LRT_OK;
 }
 
@@ -971,10 +1017,12 @@ lrt_status lrt_scene_upload(lrt_scene* s, const lrt_scene_arrays* a)
 #undef CP
   s->h = std::move(h);
   s->committed = false;
+  s->geomVersion++;
   lrt_status st = validate(s, &s->info);
   if (st != LRT_OK) return st;
   st = device_upload(s);
   if (st != LRT_OK) return st;
+  s->uploadedGeomVersion = s->geomVersion;
   s->committed = true;
   return LRT_OK;
 }

@@ -67,6 +67,10 @@ struct lrt_scene {
   uint32_t primsInLeaf = 2;
   uint32_t voxelStepCap = 0; // 0 = kMaxVoxelSteps
   bool committed = false;
+  // geometry changes since the last full upload: a commit that finds none
+  // re-uploads only the instances and the TLAS
+  uint64_t geomVersion = 1;
+  uint64_t uploadedGeomVersion = 0;
   lrt::SceneInfo info;
   lrt::DeviceScene* dev = nullptr;
   int device = -1;
@@ -81,5 +85,6 @@ lrt_status check_preset(lrt_scene* s, bool sphere_tracing_only = false);
 lrt_status fail(lrt_scene* s, lrt_status code, const char* fmt, ...);
 // device.cu
 lrt_status device_upload(lrt_scene* s);
+lrt_status device_update_instances(lrt_scene* s);
 void device_release(lrt_scene* s);
 } // namespace lrt

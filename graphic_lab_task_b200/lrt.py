@@ -30,6 +30,7 @@ EXPORTED = (
     "lrt_batch_update_cameras", "lrt_batch_set_shape", "lrt_batch_get_shape", "lrt_batch_trace", "lrt_batch_sync",
     "lrt_batch_autotune", "lrt_render_lambert", "lrt_adjoint_lambert_sbs", "lrt_sbs_update_values",
     "lrt_generate_bounce_rays", "lrt_generate_bounce_rays_compact", "lrt_render_rgba8", "lrt_trace_nearest_image",
+    "lrt_update_instance",
     "lrt_wl_noisy_sphere", "lrt_wl_spheres", "lrt_wl_sphere_sdf", "lrt_wl_sbs_from_spheres",
     "lrt_wl_frame_octree_from_spheres", "lrt_wl_svs_from_spheres",
 )
@@ -91,6 +92,7 @@ def lib():
         "lrt_clear_scene": [vp],
         "lrt_add_instance": [vp, u32, vp, P(u32)],
         "lrt_commit_scene": [vp, u32],
+        "lrt_update_instance": [vp, u32, vp, u32],
         "lrt_scene_upload": [vp, P(SceneArrays)],
         "lrt_scene_export": [vp, P(SceneArrays)],
         "lrt_trace_nearest": [vp, vp, vp, u64, vp, u32],
@@ -230,6 +232,11 @@ class SceneRT:
         iid = C.c_uint32()
         self._check(lib().lrt_add_instance(self.h, geomId, m.ctypes.data, C.byref(iid)))
         return iid.value
+
+    def UpdateInstance(self, inst_id, matrix_col_major, update_normal_matrix=False):
+        """ISceneObject::UpdateInstance: takes effect at the next CommitScene."""
+        m = np.ascontiguousarray(matrix_col_major, dtype=np.float32).reshape(16)
+        self._check(lib().lrt_update_instance(self.h, inst_id, m.ctypes.data, 1 if update_normal_matrix else 0))
 
     def CommitScene(self, options=4, host_only=False):
         """Builds the TLAS and uploads to the current CUDA device; with

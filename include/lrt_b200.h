@@ -229,6 +229,18 @@ lrt_status lrt_add_instance(lrt_scene* scene, uint32_t geom_id, const float* mat
 #define LRT_COMMIT_HOST_ONLY 0x100u
 lrt_status lrt_commit_scene(lrt_scene* scene, uint32_t build_flags);
 
+/* ISceneObject::UpdateInstance (CrossRT.h:116; BVHRT::UpdateInstance,
+ * MultiRenderer/BVH2Common_host.cpp:1303-1335): the new column-major
+ * transform of instance inst_id, its box recomputed from the geometry's box;
+ * it takes effect at the next lrt_commit_scene, which rebuilds the TLAS and,
+ * when no geometry changed since the last upload, writes only the TLAS and
+ * the instances to the device.  As in the reference, transformInvTransposed
+ * (the normal matrix) keeps its old value unless LRT_UPDATE_NORMAL_MATRIX is
+ * set; inst_id must be below the instance count (the reference also accepts
+ * the count itself and writes past its array). */
+#define LRT_UPDATE_NORMAL_MATRIX 0x1u
+lrt_status lrt_update_instance(lrt_scene* scene, uint32_t inst_id, const float* matrix_col_major16, uint32_t flags);
+
 /* ------------------------------------------------------------------------ */
 /* Drop-in upload of arrays flattened by the reference's BVHRT host code.     */
 /* ------------------------------------------------------------------------ */

@@ -155,3 +155,42 @@ def test_unsupported_presets_are_reported():
     from graphic_lab_task_b200 import default_preset
     sc = SceneRT(preset=default_preset())  # ANALYTIC node intersection, VERTEX normals
     assert sc.GetPreset().sdf_node_intersect == 1
+
+
+def test_update_instance_host_semantics():
+    """UpdateInstance (BVH2Common_host.cpp:1303-1335): new transform, inverse
+    and box; the normal matrix stays unless asked for, as in the reference;
+    the arrays equal a scene built with the new transform from the start
+    (normal matrix refreshed); bad ids and singular matrices are refused."""
+    sc, _ = build_mixed(seed=3)
+    mats = wl.random_instances(8, seed=33, scale=(0.3, 0.8), trans=1.2)
+    before = sc.export_arrays()["instanceData"].copy()
+    sc.UpdateInstance(2, mats[2])
+    sc.CommitScene(host_only=True)
+    after = sc.export_arrays()["instanceData"]
+    assert np.array_equal(after[2]["transform"], np.asarray(mats[2], np.float32))
+    assert np.array_equal(after[2]["transformInvTransposed"], before[2]["transformInvTransposed"])
+    assert not np.array_equal(after[2]["transformInv"], before[2]["transformInv"])
+    sc.UpdateInstance(2, mats[2], update_normal_matrix=True)
+    sc.UpdateInstance(5, mats[5], update_normal_matrix=True)
+    sc.CommitScene(host_only=True)
+    # the same scene built with the final transforms from the start
+    sph = wl.spheres(12, seed=203)
+    fresh = SceneRT()
+    v, t = wl.noisy_sphere(20, seed=3)
+    gm = fresh.AddGeom_Triangles3f(v, t)
+    hdr, nodes, vals, vf = wl.sbs_from_spheres(sph, grid_res=32, brick_size=4, brick_pad=1)
+    gb = fresh.AddGeom_SdfSBS(hdr, nodes, vals, vf)
+    go = fresh.AddGeom_SdfFrameOctree(wl.frame_octree_from_spheres(sph, 4))
+    gs = fresh.AddGeom_SdfSVS(wl.svs_from_spheres(sph, 4))
+    orig = wl.random_instances(8, seed=3, scale=(0.3, 0.8), trans=1.2)
+    for i, m in enumerate(orig):
+        fresh.AddInstance([gm, gb, go, gs][i % 4], mats[i] if i in (2, 5) else m)
+    fresh.CommitScene(host_only=True)
+    a, b = sc.export_arrays(), fresh.export_arrays()
+    for k in ("instanceData", "nodesTLAS"):
+        assert a[k].tobytes() == b[k].tobytes(), k
+    with pytest.raises(LrtError):
+        sc.UpdateInstance(8, mats[0])
+    with pytest.raises(LrtError):
+        sc.UpdateInstance(0, np.zeros(16, np.float32))
