@@ -873,6 +873,91 @@ lrt_status lrt_add_geom_sdf_sbs(lrt_scene* s, const lrt_sdf_sbs_header* header, 
   return LRT_OK;
 }
 
+// ---- SDF model files (the formats of sdf/simple/sdf_simple.cpp:50-142) ----
+namespace {
+struct FileReader {
+  FILE* f = nullptr;
+  long size = 0;
+  explicit FileReader(const char* path)
+  {
+    f = path ? std::fopen(path, "rb") : nullptr;
+    if (f && std::fseek(f, 0, SEEK_END) == 0) {
+      size = std::ftell(f);
+      std::fseek(f, 0, SEEK_SET);
+    }
+  }
+  ~FileReader()
+  {
+    if (f) std::fclose(f);
+  }
+  long left() const { return f ? size - std::ftell(f) : 0; }
+  bool read(void* dst, size_t bytes) { return f && left() >= long(bytes) && std::fread(dst, 1, bytes, f) == bytes; }
+  bool u32(uint32_t* v) { return read(v, sizeof(uint32_t)); }
+};
+} // namespace
+
+// load_sdf_frame_octree (:58-66): u32 count, count 36-byte nodes.
+lrt_status lrt_add_geom_sdf_frame_octree_file(lrt_scene* s, const char* path, uint32_t* geom_id_out)
+{
+  if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  FileReader r(path);
+  uint32_t n = 0;
+  if (!r.f) return fail(s, LRT_ERR_INVALID_ARGUMENT, "frame-octree file %s cannot be opened", path ? path : "(null)");
+  if (!r.u32(&n) || r.left() < long(n) * long(sizeof(lrt_sdf_frame_octree_node)))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "frame-octree file %s is shorter than its %u nodes", path, n);
+  std::vector<lrt_sdf_frame_octree_node> nodes(n);
+  if (n && !r.read(nodes.data(), n * sizeof(lrt_sdf_frame_octree_node)))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "frame-octree file %s: read error", path);
+  return lrt_add_geom_sdf_frame_octree(s, nodes.data(), n, geom_id_out);
+}
+
+// load_sdf_SVS (:88-96): u32 count, count 16-byte nodes.
+lrt_status lrt_add_geom_sdf_svs_file(lrt_scene* s, const char* path, uint32_t* geom_id_out)
+{
+  if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  FileReader r(path);
+  uint32_t n = 0;
+  if (!r.f) return fail(s, LRT_ERR_INVALID_ARGUMENT, "SVS file %s cannot be opened", path ? path : "(null)");
+  if (!r.u32(&n) || r.left() < long(n) * long(sizeof(lrt_sdf_svs_node)))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "SVS file %s is shorter than its %u nodes", path, n);
+  std::vector<lrt_sdf_svs_node> nodes(n);
+  if (n && !r.read(nodes.data(), n * sizeof(lrt_sdf_svs_node)))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "SVS file %s: read error", path);
+  return lrt_add_geom_sdf_svs(s, nodes.data(), n, geom_id_out);
+}
+
+// load_sdf_SBS (:122-142): header, u32 count, nodes, u32 value count, values,
+// then u32 float count and floats; files written before the float trailer
+// existed end after the values.
+lrt_status lrt_add_geom_sdf_sbs_file(lrt_scene* s, const char* path, uint32_t* geom_id_out)
+{
+  if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  FileReader r(path);
+  if (!r.f) return fail(s, LRT_ERR_INVALID_ARGUMENT, "SBS file %s cannot be opened", path ? path : "(null)");
+  lrt_sdf_sbs_header hdr;
+  uint32_t n = 0, cnt = 0, cnt_f = 0;
+  if (!r.read(&hdr, sizeof(hdr)) || !r.u32(&n) || r.left() < long(n) * long(sizeof(lrt_sdf_sbs_node)))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "SBS file %s is shorter than its header and %u nodes", path, n);
+  std::vector<lrt_sdf_sbs_node> nodes(n);
+  if (n && !r.read(nodes.data(), n * sizeof(lrt_sdf_sbs_node)))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "SBS file %s: read error", path);
+  if (!r.u32(&cnt) || r.left() < long(cnt) * 4)
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "SBS file %s is shorter than its %u values", path, cnt);
+  std::vector<uint32_t> values(cnt);
+  if (cnt && !r.read(values.data(), cnt * sizeof(uint32_t)))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "SBS file %s: read error", path);
+  std::vector<float> values_f;
+  if (r.left() >= 4) {
+    if (!r.u32(&cnt_f) || r.left() < long(cnt_f) * 4)
+      return fail(s, LRT_ERR_INVALID_ARGUMENT, "SBS file %s is shorter than its %u float values", path, cnt_f);
+    values_f.resize(cnt_f);
+    if (cnt_f && !r.read(values_f.data(), cnt_f * sizeof(float)))
+      return fail(s, LRT_ERR_INVALID_ARGUMENT, "SBS file %s: read error", path);
+  }
+  return lrt_add_geom_sdf_sbs(s, &hdr, nodes.data(), n, values.data(), values.size(),
+                              values_f.empty() ? nullptr : values_f.data(), values_f.size(), geom_id_out);
+}
+
 lrt_status lrt_clear_scene(lrt_scene* s)
 {
   if (!s) return LRT_ERR_INVALID_ARGUMENT;

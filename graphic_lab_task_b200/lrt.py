@@ -30,7 +30,8 @@ EXPORTED = (
     "lrt_batch_update_cameras", "lrt_batch_set_shape", "lrt_batch_get_shape", "lrt_batch_trace", "lrt_batch_sync",
     "lrt_batch_autotune", "lrt_render_lambert", "lrt_adjoint_lambert_sbs", "lrt_sbs_update_values",
     "lrt_generate_bounce_rays", "lrt_generate_bounce_rays_compact", "lrt_render_rgba8", "lrt_trace_nearest_image",
-    "lrt_update_instance",
+    "lrt_update_instance", "lrt_add_geom_sdf_frame_octree_file", "lrt_add_geom_sdf_svs_file",
+    "lrt_add_geom_sdf_sbs_file",
     "lrt_wl_noisy_sphere", "lrt_wl_spheres", "lrt_wl_sphere_sdf", "lrt_wl_sbs_from_spheres",
     "lrt_wl_frame_octree_from_spheres", "lrt_wl_svs_from_spheres",
 )
@@ -93,6 +94,9 @@ def lib():
         "lrt_add_instance": [vp, u32, vp, P(u32)],
         "lrt_commit_scene": [vp, u32],
         "lrt_update_instance": [vp, u32, vp, u32],
+        "lrt_add_geom_sdf_frame_octree_file": [vp, C.c_char_p, P(u32)],
+        "lrt_add_geom_sdf_svs_file": [vp, C.c_char_p, P(u32)],
+        "lrt_add_geom_sdf_sbs_file": [vp, C.c_char_p, P(u32)],
         "lrt_scene_upload": [vp, P(SceneArrays)],
         "lrt_scene_export": [vp, P(SceneArrays)],
         "lrt_trace_nearest": [vp, vp, vp, u64, vp, u32],
@@ -232,6 +236,15 @@ class SceneRT:
         iid = C.c_uint32()
         self._check(lib().lrt_add_instance(self.h, geomId, m.ctypes.data, C.byref(iid)))
         return iid.value
+
+    def AddGeom_SdfFile(self, kind, path):
+        """Adds an SDF model from a file in the reference's format; kind is
+        "frame_octree", "svs" or "sbs".  Returns the geometry id."""
+        fn = {"frame_octree": lib().lrt_add_geom_sdf_frame_octree_file, "svs": lib().lrt_add_geom_sdf_svs_file,
+              "sbs": lib().lrt_add_geom_sdf_sbs_file}[kind]
+        g = C.c_uint32()
+        self._check(fn(self.h, os.fsencode(path), C.byref(g)))
+        return g.value
 
     def UpdateInstance(self, inst_id, matrix_col_major, update_normal_matrix=False):
         """ISceneObject::UpdateInstance: takes effect at the next CommitScene."""

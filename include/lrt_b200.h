@@ -220,6 +220,15 @@ lrt_status lrt_add_geom_sdf_sbs(lrt_scene* scene, const lrt_sdf_sbs_header* head
 /* ISceneObject::ClearScene / AddInstance / CommitScene (CrossRT.h:101-115;
  * BVH2Common_host.cpp:1230-1301).  matrix: 16 floats, column-major.
  * CommitScene builds the TLAS and uploads everything to the current device. */
+/* The same adders reading the reference's model files (sdf/simple/
+ * sdf_simple.cpp:50-142): frame octree and SVS = u32 node count + nodes; SBS
+ * = header, u32 node count, nodes, u32 value count, values, u32 float count,
+ * floats (older files end after the values).  Files shorter than their counts
+ * are refused with LRT_ERR_INVALID_ARGUMENT. */
+lrt_status lrt_add_geom_sdf_frame_octree_file(lrt_scene* scene, const char* path, uint32_t* geom_id_out);
+lrt_status lrt_add_geom_sdf_svs_file(lrt_scene* scene, const char* path, uint32_t* geom_id_out);
+lrt_status lrt_add_geom_sdf_sbs_file(lrt_scene* scene, const char* path, uint32_t* geom_id_out);
+
 lrt_status lrt_clear_scene(lrt_scene* scene);
 lrt_status lrt_add_instance(lrt_scene* scene, uint32_t geom_id, const float* matrix_col_major16,
                             uint32_t* inst_id_out);

@@ -194,3 +194,53 @@ def test_update_instance_host_semantics():
         sc.UpdateInstance(8, mats[0])
     with pytest.raises(LrtError):
         sc.UpdateInstance(0, np.zeros(16, np.float32))
+
+
+def _write(path, *chunks):
+    with open(path, "wb") as f:
+        for c in chunks:
+            f.write(np.ascontiguousarray(c).tobytes())
+
+
+def test_sdf_model_files_load_like_the_arrays(tmp_path):
+    """The file adders read the reference's model formats
+    (sdf/simple/sdf_simple.cpp): the arrays equal those of the in-memory
+    adders, an SBS file without the float trailer (the older format) loads
+    with its quantised values, and truncated files are refused."""
+    sph = wl.spheres(10, seed=31)
+    oct_nodes = wl.frame_octree_from_spheres(sph, 4)
+    svs = wl.svs_from_spheres(sph, 4)
+    hdr, nodes, vals, vf = wl.sbs_from_spheres(sph, grid_res=32, brick_size=4, brick_pad=1)
+    u32 = lambda x: np.array([x], np.uint32)  # noqa: E731
+    _write(tmp_path / "o.bin", u32(len(oct_nodes)), oct_nodes)
+    _write(tmp_path / "s.bin", u32(len(svs)), svs)
+    _write(tmp_path / "b.bin", hdr, u32(len(nodes)), nodes, u32(len(vals)), vals, u32(len(vf)), vf)
+    a, b = SceneRT(), SceneRT()
+    for sc, from_file in ((a, True), (b, False)):
+        if from_file:
+            g = [sc.AddGeom_SdfFile("frame_octree", tmp_path / "o.bin"), sc.AddGeom_SdfFile("svs", tmp_path / "s.bin"),
+                 sc.AddGeom_SdfFile("sbs", tmp_path / "b.bin")]
+        else:
+            g = [sc.AddGeom_SdfFrameOctree(oct_nodes), sc.AddGeom_SdfSVS(svs), sc.AddGeom_SdfSBS(hdr, nodes, vals, vf)]
+        for i, m in enumerate(wl.random_instances(6, seed=5, scale=(0.3, 0.7), trans=1.0)):
+            sc.AddInstance(g[i % 3], m)
+        sc.CommitScene(host_only=True)
+    xa, xb = a.export_arrays(), b.export_arrays()
+    for k in xa:
+        assert xa[k].tobytes() == xb[k].tobytes(), k
+    # the older SBS format: no float-count trailer; a DX (quantised) layout needs no floats
+    dx = hdr.copy()
+    dx["aux_data"] = 0x01000000  # SDF_SBS_NODE_LAYOUT_DX
+    dx["bytes_per_value"] = 4
+    _write(tmp_path / "old.bin", dx, u32(len(nodes)), nodes, u32(len(vals)), vals)
+    c = SceneRT()
+    c.AddGeom_SdfFile("sbs", tmp_path / "old.bin")
+    # truncated files
+    _write(tmp_path / "t.bin", u32(len(svs) + 5), svs)
+    with pytest.raises(LrtError):
+        SceneRT().AddGeom_SdfFile("svs", tmp_path / "t.bin")
+    _write(tmp_path / "t2.bin", hdr, u32(len(nodes)), nodes, u32(len(vals) + 1), vals)
+    with pytest.raises(LrtError):
+        SceneRT().AddGeom_SdfFile("sbs", tmp_path / "t2.bin")
+    with pytest.raises(LrtError):
+        SceneRT().AddGeom_SdfFile("frame_octree", tmp_path / "missing.bin")
