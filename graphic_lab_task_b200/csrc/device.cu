@@ -98,7 +98,8 @@ lrt_status launch(lrt_scene* s, const float4* rays, lrt_hit* hits, uint64_t n, c
   cudaError_t e = cudaMemsetAsync(&slot->work, 0, count ? offsetof(StreamSlot, err) : sizeof(unsigned long long),
                                   stream);
   if (e != cudaSuccess) return cuda_fail(s, e, "cudaMemsetAsync");
-  const uint64_t warps = img_w ? uint64_t((img_w + 7) / 8) * ((img_h + 3) / 4) : (n + 31) / 32;
+  const uint64_t warps = img_w ? uint64_t((img_w + kImgTileW - 1) / kImgTileW) * ((img_h + kImgTileH - 1) / kImgTileH)
+                               : (n + 31) / 32;
   const int grid = int(std::min<uint64_t>(uint64_t(d->grid), (warps * 32 + kTraceThreads - 1) / kTraceThreads));
   if (flags & LRT_TRACE_FAST_MATH)
     e = lrt_fast::launch_trace(S, rays, hits, n, &slot->work, slot->counters, &slot->err, d->stackCap, grid, stream,

@@ -24,6 +24,8 @@
 namespace lrt {
 
 constexpr int kTraceThreads = 128;
+// pixels of the tile one warp traces in lrt_trace_nearest_image (32 in all)
+constexpr uint32_t kImgTileW = 8, kImgTileH = 4;
 // Per-thread shared-memory words after the traversal stack: the inputs of the
 // deferred SDF normal (sign, sample point, 8 corner values).
 constexpr uint32_t kNormalWords = 12;

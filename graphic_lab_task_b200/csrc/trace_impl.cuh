@@ -735,8 +735,8 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_trace(DevScene S, const fl
   uint32_t* stack = smem_stack + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
   Ctx<COUNT, false, SOLVERS> c(S, normal_words(smem_stack, stack_cap));
-  const uint64_t tilesX = (uint64_t(img_w) + 7) / 8;
-  const uint64_t slots = img_w ? tilesX * ((uint64_t(img_h) + 3) / 4) * 32 : n; // ray slots handed out
+  const uint64_t tilesX = (uint64_t(img_w) + kImgTileW - 1) / kImgTileW;
+  const uint64_t slots = img_w ? tilesX * ((uint64_t(img_h) + kImgTileH - 1) / kImgTileH) * 32 : n; // ray slots
   for (;;) {
     unsigned long long base = 0;
     if (lane == 0) base = atomicAdd(work_counter, 32ull);
@@ -746,7 +746,8 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_trace(DevScene S, const fl
     bool valid = i < n;
     if (img_w) {
       const uint64_t b = base >> 5;
-      const uint32_t x = uint32_t(b % tilesX) * 8 + (lane & 7), y = uint32_t(b / tilesX) * 4 + (lane >> 3);
+      const uint32_t x = uint32_t(b % tilesX) * kImgTileW + (lane % kImgTileW);
+      const uint32_t y = uint32_t(b / tilesX) * kImgTileH + (lane / kImgTileW);
       valid = x < img_w && y < img_h;
       i = uint64_t(y) * img_w + x;
     }
