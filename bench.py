@@ -443,12 +443,21 @@ def batched_cameras(sc, dev, args):
     batched_ms = timed(lambda: b.trace(hb.data_ptr(), stream=sp))
     b.sync(stream=sp)
     identical = bool(torch.equal(hb.view(torch.int32), hp.view(torch.int32)))
+    # the same cameras rendered to RGBA8 images in one launch (eye rays, trace, resolve, tonemap)
+    from graphic_lab_task_b200 import LIGHT_AMBIENT, LIGHT_DIRECT, LIGHT_DTYPE
+    lights = np.zeros(2, LIGHT_DTYPE)
+    lights[0] = ((0.577, 0.577, 0.577), LIGHT_DIRECT, (1.0, 1.0, 1.0), 0)
+    lights[1] = ((0, 0, 0), LIGHT_AMBIENT, (0.1, 0.1, 0.1), 0)
+    imgs = hb.view(torch.int32)[:total]  # reuses the hit buffer's memory for the images
+    render_ms = timed(lambda: b.render_rgba8(lights, (0, 0, 0, 1), imgs.data_ptr(), stream=sp))
+    b.sync(stream=sp)
     shape = b.shape
     b.close()
     return {"cameras": len(cams), "rays": total, "resolutions": [int(c.width) for c in cams],
             "plain_ms": plain_ms, "plain_mrays_s": total / plain_ms / 1e3, "plain_launches": 2 * len(cams),
             "batched_ms": batched_ms, "batched_mrays_s": total / batched_ms / 1e3, "speedup": plain_ms / batched_ms,
-            "identical_hits": identical, "shape": {"tile_w": shape[0], "tile_h": shape[1],
+            "identical_hits": identical, "render_rgba8_ms": render_ms, "render_rgba8_mpix_s": total / render_ms / 1e3,
+            "shape": {"tile_w": shape[0], "tile_h": shape[1],
                                                    "rays_per_lane": shape[2], "stack_cap": shape[3]},
             "autotune_s": tune_s, "autotune_candidates": len(table), "steps": steps}
 

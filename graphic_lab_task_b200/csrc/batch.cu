@@ -105,8 +105,10 @@ DevScene scene_params(lrt_scene* s)
   return S;
 }
 
-// table upload + state reset + launch, on `stream` (captured or not)
-cudaError_t enqueue(lrt_camera_batch* b, lrt_hit* hits, cudaStream_t stream)
+// table upload + state reset + launch, on `stream` (captured or not); with
+// `image`, RGBA8 pixels (resolve with `lights`) instead of hits
+cudaError_t enqueue(lrt_camera_batch* b, lrt_hit* hits, cudaStream_t stream, const DevLights* lights = nullptr,
+                    uint32_t* image = nullptr)
 {
   cudaError_t e = cudaMemcpyAsync(b->devTable, b->hostTable, sizeof(DevBatchCamera) * b->ncams,
                                   cudaMemcpyHostToDevice, stream);
@@ -115,7 +117,8 @@ cudaError_t enqueue(lrt_camera_batch* b, lrt_hit* hits, cudaStream_t stream)
     const DevScene S = scene_params(b->scene);
     const int grid = int(std::min<uint64_t>(uint64_t(b->grid), (uint64_t(b->ntiles) * 32 + kTraceThreads - 1) / kTraceThreads));
     e = lrt_exact::launch_trace_cameras(S, b->devTable, b->ncams, b->ntiles, b->shape, hits, b->state,
-                                        reinterpret_cast<uint32_t*>(b->state + 1), std::max(1, grid), stream);
+                                        reinterpret_cast<uint32_t*>(b->state + 1), std::max(1, grid), stream, lights,
+                                        image);
   }
   return e;
 }
@@ -241,6 +244,29 @@ lrt_status lrt_batch_trace(lrt_camera_batch* b, lrt_hit* hits_dev, void* stream_
   }
   e = cudaGraphLaunch(b->exec, stream);
   return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "cudaGraphLaunch");
+}
+
+lrt_status lrt_batch_render_rgba8(lrt_camera_batch* b, const lrt_light* lights, uint32_t light_count,
+                                  const float background[4], uint32_t* images_dev, void* stream_p)
+{
+  if (!b || !images_dev || !background || (light_count && !lights)) return LRT_ERR_INVALID_ARGUMENT;
+  lrt_scene* s = b->scene;
+  if (reinterpret_cast<uintptr_t>(images_dev) & 3)
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_batch_render_rgba8: images must be 4-byte aligned");
+  if (light_count > LRT_MAX_LIGHTS)
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_batch_render_rgba8: %u lights (at most %d)", light_count,
+                LRT_MAX_LIGHTS);
+  if (s->preset.render_mode != LRT_RENDER_MODE_LAMBERT_NO_TEX)
+    return fail(s, LRT_ERR_UNSUPPORTED, "lrt_batch_render_rgba8 renders the LAMBERT_NO_TEX mode (1), the preset has %u",
+                s->preset.render_mode);
+  lrt_status st = check_preset(s, true);
+  if (st != LRT_OK) return st;
+  DevLights L{};
+  if (light_count) std::memcpy(L.light, lights, light_count * sizeof(lrt_light));
+  L.count = light_count;
+  std::memcpy(L.background, background, sizeof(L.background));
+  const cudaError_t e = enqueue(b, nullptr, static_cast<cudaStream_t>(stream_p), &L, images_dev);
+  return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "batched render");
 }
 
 lrt_status lrt_batch_sync(lrt_camera_batch* b, void* stream_p)

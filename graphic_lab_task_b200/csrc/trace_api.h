@@ -16,7 +16,8 @@
   cudaError_t launch_trace_cameras(const lrt::DevScene& S, const lrt::DevBatchCamera* cams, uint32_t ncams,     \
                                    uint32_t ntiles, const lrt::DevBatchShape& shape, lrt_hit* hits,             \
                                    unsigned long long* work_counter, uint32_t* err_word, int grid,              \
-                                   cudaStream_t stream);                                                        \
+                                   cudaStream_t stream, const lrt::DevLights* lights = nullptr,                 \
+                                   uint32_t* image = nullptr);                                                  \
   cudaError_t cameras_occupancy(uint32_t stack_cap, int* blocks_per_sm);                                        \
   cudaError_t launch_render_rgba8(const lrt::DevScene& S, const lrt::DevCamera& cam, const lrt::DevLights& lights,\
                                   uint32_t* image, unsigned long long* work_counter, uint32_t* err_word,        \

@@ -772,16 +772,77 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_trace(DevScene S, const fl
   }
 }
 
+// Tonemap (MultiRenderer_resolve.cpp:536-542) of one colour to RGBA8.
+__device__ __forceinline__ uint32_t tonemap_rgba8(float r, float g, float b, float a)
+{
+  // uint4(255 * clamp(color, 0, 1)): clamp as LiteMath's min(max(a, u), b)
+  const uint32_t x = uint32_t(255.0f * sclamp(r, 0.0f, 1.0f));
+  const uint32_t y = uint32_t(255.0f * sclamp(g, 0.0f, 1.0f));
+  const uint32_t z = uint32_t(255.0f * sclamp(b, 0.0f, 1.0f));
+  const uint32_t w = uint32_t(255.0f * sclamp(a, 0.0f, 1.0f));
+  return (w << 24) | (z << 16) | (y << 8) | x;
+}
+
+// ResolveCommon for LAMBERT_NO_TEX (white albedo, the lights of L, the
+// background for misses) and Tonemap of one traced eye ray; c.triLocal is
+// the triangle record of a triangle hit (set by trace_one).
+template <class CTX>
+__device__ __forceinline__ uint32_t resolve_rgba8(CTX& c, const DevLights& L, f3 rayPos, f3 rayDir,
+                                                  const lrt_hit& h)
+{
+  const DevScene& S = c.S;
+  if (h.primId == 0xFFFFFFFFu) {
+    return tonemap_rgba8(L.background[0], L.background[1], L.background[2], L.background[3]);
+  } else {
+    f3 norm;
+    if ((h.geomId >> 24) == LRT_TYPE_MESH_TRIANGLE) {
+      const DevGeom& g = S.geoms[h.geomId & 0x00FFFFFFu];
+      const float4* tri = S.triSoup + 3 * (uint64_t(g.triBase) + c.triLocal);
+      const f3 raw = cross(ld3(__ldg(tri + 1)), ld3(__ldg(tri + 2)));
+      norm = normalize(matmul4(S.instances[h.instId].transformInvTransposed, raw, 1.0f));
+      norm = ssign(dot(-1.0f * rayDir, norm)) * norm;
+    } else {
+      norm = decode_normal(mk2(h.coords[2], h.coords[3]));
+    }
+    const f3 color = mk3(1, 1, 1);
+    f3 fc = mk3(0, 0, 0);
+    for (uint32_t i = 0; i < L.count; i++) {
+      const DevLight& l = L.light[i];
+      const f3 lc = mk3(l.color[0], l.color[1], l.color[2]);
+      const f3 sp = mk3(l.space[0], l.space[1], l.space[2]);
+      if (l.type == LRT_LIGHT_DIRECT) {
+        const float q = smax(0.0f, dot(norm, sp));
+        fc = fc + (lc * color) * q;
+      } else if (l.type == LRT_LIGHT_POINT) {
+        const f3 surf = rayPos + h.t * rayDir;
+        f3 dir = sp - surf;
+        const float len = sqrtf(dot(dir, dir));
+        dir = mk3(dir.x / len, dir.y / len, dir.z / len);
+        const float q = smax(0.0f, dot(norm, dir));
+        fc = fc + ((lc * color) * q) / (len * len);
+      } else {
+        fc = fc + lc * color;
+      }
+    }
+    return tonemap_rgba8(fc.x, fc.y, fc.z, 1.0f);
+  }
+}
+
 // Batched multi-camera form: one persistent launch over the pixel tiles of
 // all cameras.  A warp takes one tile at a time from the global counter,
 // finds its camera by binary search over the tile bases, and each lane
 // generates (lrt::eye_ray, the function k_eye_rays uses) and traces its
 // raysPerLane pixels, so every hit equals the plain per-camera path's.
+//
+// RENDER: instead of hits, each pixel's RGBA8 colour (resolve_rgba8: the
+// LAMBERT_NO_TEX resolve with L and the tonemap) goes to image[rayOffset + y*width + x].
+template <bool RENDER>
 __global__ void __launch_bounds__(kTraceThreads, 7) k_trace_cameras(DevScene S, const DevBatchCamera* __restrict__ cams,
                                                                  uint32_t ncams, uint32_t ntiles, DevBatchShape shape,
                                                                  lrt_hit* __restrict__ hits,
                                                                  unsigned long long* __restrict__ work_counter,
-                                                                 uint32_t* __restrict__ err_word)
+                                                                 uint32_t* __restrict__ err_word, DevLights L,
+                                                                 uint32_t* __restrict__ image)
 {
   extern __shared__ uint32_t smem_stack[];
   uint32_t* stack = smem_stack + threadIdx.x;
@@ -812,9 +873,14 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_trace_cameras(DevScene S, 
       lrt_hit h;
       trace_one(c, stack, blockDim.x, shape.stackCap, make_float4(ray[0], ray[1], ray[2], ray[3]),
                 make_float4(ray[4], ray[5], ray[6], ray[7]), h);
-      float4* out = reinterpret_cast<float4*>(hits + bc.rayOffset + uint64_t(y) * W + x);
-      out[0] = make_float4(h.t, __uint_as_float(h.primId), __uint_as_float(h.instId), __uint_as_float(h.geomId));
-      out[1] = make_float4(h.coords[0], h.coords[1], h.coords[2], h.coords[3]);
+      if (RENDER) {
+        image[bc.rayOffset + uint64_t(y) * W + x] =
+            resolve_rgba8(c, L, mk3(ray[0], ray[1], ray[2]), mk3(ray[4], ray[5], ray[6]), h);
+      } else {
+        float4* out = reinterpret_cast<float4*>(hits + bc.rayOffset + uint64_t(y) * W + x);
+        out[0] = make_float4(h.t, __uint_as_float(h.primId), __uint_as_float(h.instId), __uint_as_float(h.geomId));
+        out[1] = make_float4(h.coords[0], h.coords[1], h.coords[2], h.coords[3]);
+      }
     }
   }
   if (c.err) atomicOr(err_word, c.err);
@@ -822,20 +888,30 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_trace_cameras(DevScene S, 
 
 cudaError_t launch_trace_cameras(const DevScene& S, const DevBatchCamera* cams, uint32_t ncams, uint32_t ntiles,
                                  const DevBatchShape& shape, lrt_hit* hits, unsigned long long* work_counter,
-                                 uint32_t* err_word, int grid, cudaStream_t stream)
+                                 uint32_t* err_word, int grid, cudaStream_t stream, const DevLights* lights,
+                                 uint32_t* image)
 {
   const size_t smem = trace_smem_bytes(shape.stackCap);
-  k_trace_cameras<<<grid, kTraceThreads, smem, stream>>>(S, cams, ncams, ntiles, shape, hits, work_counter, err_word);
+  if (image) {
+    cudaError_t e = cudaFuncSetAttribute(k_trace_cameras<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(trace_smem_bytes(kMaxStackDev + 1)));
+    if (e != cudaSuccess) return e;
+    k_trace_cameras<true><<<grid, kTraceThreads, smem, stream>>>(S, cams, ncams, ntiles, shape, hits, work_counter,
+                                                                 err_word, *lights, image);
+  } else {
+    k_trace_cameras<false><<<grid, kTraceThreads, smem, stream>>>(S, cams, ncams, ntiles, shape, hits, work_counter,
+                                                                  err_word, DevLights{}, nullptr);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t cameras_occupancy(uint32_t stack_cap, int* blocks_per_sm)
 {
   const size_t smem = trace_smem_bytes(stack_cap);
-  cudaError_t e = cudaFuncSetAttribute(k_trace_cameras, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(k_trace_cameras<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(trace_smem_bytes(kMaxStackDev + 1)));
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_trace_cameras, kTraceThreads, smem);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_trace_cameras<false>, kTraceThreads, smem);
 }
 
 // Lambert shading of a hit, MultiRenderer::ResolveCommon for
@@ -859,16 +935,6 @@ __device__ __forceinline__ float lambert(const lrt_hit& h, f3 dir, f3 L)
 // triangle and turned towards the viewer as in loadNormalTcFromGbuffer :27-75,
 // SDF normals decoded from the hit) and Tonemap (:536-542) into RGBA8.  A warp
 // takes 8x4-pixel tiles from a global counter.
-__device__ __forceinline__ uint32_t tonemap_rgba8(float r, float g, float b, float a)
-{
-  // uint4(255 * clamp(color, 0, 1)): clamp as LiteMath's min(max(a, u), b)
-  const uint32_t x = uint32_t(255.0f * sclamp(r, 0.0f, 1.0f));
-  const uint32_t y = uint32_t(255.0f * sclamp(g, 0.0f, 1.0f));
-  const uint32_t z = uint32_t(255.0f * sclamp(b, 0.0f, 1.0f));
-  const uint32_t w = uint32_t(255.0f * sclamp(a, 0.0f, 1.0f));
-  return (w << 24) | (z << 16) | (y << 8) | x;
-}
-
 __global__ void __launch_bounds__(kTraceThreads, 7) k_render_rgba8(DevScene S, DevCamera cam, DevLights L,
                                                                 uint32_t* __restrict__ image,
                                                                 unsigned long long* __restrict__ work_counter,
@@ -891,43 +957,7 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_render_rgba8(DevScene S, D
     lrt_hit h;
     trace_one(c, stack, blockDim.x, stack_cap, make_float4(r[0], r[1], r[2], r[3]), make_float4(r[4], r[5], r[6], r[7]),
               h);
-    uint32_t px;
-    if (h.primId == 0xFFFFFFFFu) {
-      px = tonemap_rgba8(L.background[0], L.background[1], L.background[2], L.background[3]);
-    } else {
-      const f3 rayPos = mk3(r[0], r[1], r[2]), rayDir = mk3(r[4], r[5], r[6]);
-      f3 norm;
-      if ((h.geomId >> 24) == LRT_TYPE_MESH_TRIANGLE) {
-        const DevGeom& g = S.geoms[h.geomId & 0x00FFFFFFu];
-        const float4* tri = S.triSoup + 3 * (uint64_t(g.triBase) + c.triLocal);
-        const f3 raw = cross(ld3(__ldg(tri + 1)), ld3(__ldg(tri + 2)));
-        norm = normalize(matmul4(S.instances[h.instId].transformInvTransposed, raw, 1.0f));
-        norm = ssign(dot(-1.0f * rayDir, norm)) * norm;
-      } else {
-        norm = decode_normal(mk2(h.coords[2], h.coords[3]));
-      }
-      const f3 color = mk3(1, 1, 1);
-      f3 fc = mk3(0, 0, 0);
-      for (uint32_t i = 0; i < L.count; i++) {
-        const DevLight& l = L.light[i];
-        const f3 lc = mk3(l.color[0], l.color[1], l.color[2]);
-        const f3 sp = mk3(l.space[0], l.space[1], l.space[2]);
-        if (l.type == LRT_LIGHT_DIRECT) {
-          const float q = smax(0.0f, dot(norm, sp));
-          fc = fc + (lc * color) * q;
-        } else if (l.type == LRT_LIGHT_POINT) {
-          const f3 surf = rayPos + h.t * rayDir;
-          f3 dir = sp - surf;
-          const float len = sqrtf(dot(dir, dir));
-          dir = mk3(dir.x / len, dir.y / len, dir.z / len);
-          const float q = smax(0.0f, dot(norm, dir));
-          fc = fc + ((lc * color) * q) / (len * len);
-        } else {
-          fc = fc + lc * color;
-        }
-      }
-      px = tonemap_rgba8(fc.x, fc.y, fc.z, 1.0f);
-    }
+    const uint32_t px = resolve_rgba8(c, L, mk3(r[0], r[1], r[2]), mk3(r[4], r[5], r[6]), h);
     image[uint64_t(y) * cam.width + x] = px;
   }
   if (c.err) atomicOr(err_word, c.err);

@@ -31,7 +31,7 @@ EXPORTED = (
     "lrt_batch_autotune", "lrt_render_lambert", "lrt_adjoint_lambert_sbs", "lrt_sbs_update_values",
     "lrt_generate_bounce_rays", "lrt_generate_bounce_rays_compact", "lrt_render_rgba8", "lrt_trace_nearest_image",
     "lrt_update_instance", "lrt_add_geom_sdf_frame_octree_file", "lrt_add_geom_sdf_svs_file",
-    "lrt_add_geom_sdf_sbs_file",
+    "lrt_add_geom_sdf_sbs_file", "lrt_batch_render_rgba8",
     "lrt_wl_noisy_sphere", "lrt_wl_spheres", "lrt_wl_sphere_sdf", "lrt_wl_sbs_from_spheres",
     "lrt_wl_frame_octree_from_spheres", "lrt_wl_svs_from_spheres",
 )
@@ -116,6 +116,7 @@ def lib():
         "lrt_batch_get_shape": [vp, P(BatchShape)],
         "lrt_batch_trace": [vp, vp, vp, u32],
         "lrt_batch_sync": [vp, vp],
+        "lrt_batch_render_rgba8": [vp, vp, u32, vp, vp, vp],
         "lrt_batch_autotune": [vp, vp, vp, u32, vp, u32, P(u32)],
         "lrt_trace_sync": [vp, vp, C.c_int32],
         "lrt_ray_query_nearest_hit": [vp, vp, vp, vp],
@@ -409,6 +410,13 @@ class CameraBatch:
     def trace(self, hits_ptr, stream=0, graph=True):
         self.scene._check(lib().lrt_batch_trace(self.h, C.c_void_p(hits_ptr), C.c_void_p(stream) if stream else None,
                                                 0 if graph else LRT_BATCH_NO_GRAPH))
+
+    def render_rgba8(self, lights, background, images_ptr, stream=0):
+        """All cameras' RGBA8 images in one launch (offsets as the rays')."""
+        lt = np.ascontiguousarray(lights, dtype=LIGHT_DTYPE)
+        bg = (C.c_float * 4)(*[float(x) for x in background])
+        self.scene._check(lib().lrt_batch_render_rgba8(self.h, lt.ctypes.data if len(lt) else None, len(lt), bg,
+                                                       C.c_void_p(images_ptr), C.c_void_p(stream) if stream else None))
 
     def sync(self, stream=0):
         self.scene._check(lib().lrt_batch_sync(self.h, C.c_void_p(stream) if stream else None))

@@ -501,6 +501,13 @@ lrt_status lrt_batch_get_shape(const lrt_camera_batch* batch, lrt_batch_shape* s
  * 16-byte aligned. */
 lrt_status lrt_batch_trace(lrt_camera_batch* batch, lrt_hit* hits_dev, void* stream, uint32_t flags);
 /* Waits for `stream`; LRT_ERR_DEVICE_LIMIT if a batched trace hit a bounded-loop limit. */
+/* lrt_render_rgba8 for every camera of the batch in one launch (tiles and
+ * launch shape of the batch): camera c's width*height RGBA8 pixels go to
+ * images_dev + offsets[c] (lrt_batch_ray_offsets), row-major; every pixel
+ * equals lrt_render_rgba8's for that camera.  Launched directly (no graph),
+ * asynchronous on `stream`; lrt_batch_sync reports bounded-loop limits. */
+lrt_status lrt_batch_render_rgba8(lrt_camera_batch* batch, const lrt_light* lights, uint32_t light_count,
+                                  const float background[4], uint32_t* images_dev, void* stream);
 lrt_status lrt_batch_sync(lrt_camera_batch* batch, void* stream);
 /* The project autotuner: times every candidate shape (tiles 32x1, 16x2, 8x4,
  * 4x8 at 1 ray per lane, 16x4 and 8x8 at 2, 16x8 and 8x16 at 4; stack

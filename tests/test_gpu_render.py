@@ -68,3 +68,28 @@ def test_render_rgba8_refusals(cuda):
     with pytest.raises(LrtError) as e:
         sc.render_rgba8(cam, _lights(), (0, 0, 0, 1), img.data_ptr())
     assert e.value.status == 6 and "LAMBERT_NO_TEX" in str(e.value)
+
+
+def test_batched_render_equals_per_camera_render(cuda):
+    """lrt_batch_render_rgba8 renders every camera of a batch in one launch;
+    each image equals lrt_render_rgba8's for that camera."""
+    torch = cuda
+    from graphic_lab_task_b200.lrt import CameraBatch
+    sc = _mixed_scene()
+    cams = wl.sphere_cameras(6, radius=3.5, res_min=40, res_max=130, seed=5)
+    b = CameraBatch(sc, cams)
+    imgs = torch.zeros(b.total_rays, dtype=torch.int32, device="cuda")
+    bg = (0.1, 0.2, 0.3, 1.0)
+    b.render_rgba8(_lights(), bg, imgs.data_ptr())
+    b.sync()
+    got = imgs.cpu().numpy().view(np.uint32)
+    off = 0
+    for c in cams:
+        k = c.width * c.height
+        one = torch.zeros(k, dtype=torch.int32, device="cuda")
+        sc.render_rgba8(c, _lights(), bg, one.data_ptr())
+        sc.sync()
+        assert np.array_equal(got[off:off + k], one.cpu().numpy().view(np.uint32))
+        off += k
+    assert len(np.unique(got)) > 100
+    b.close()
