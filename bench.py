@@ -7,9 +7,13 @@ Workload (one "step"): one plain nearest-hit pass over 1920x1080 primary rays
 of a sparse-brick-set SDF — the union of 64 seeded spheres sampled on a
 virtual 512^3 grid, 8^3-voxel bricks with a 1-voxel border, fp32 distances in
 the indexed layout, camera at (0,0,3) looking at the origin, 60 degree fovy,
-tmin 1e-4.  Rays and the scene are resident in HBM when timing starts; the
-L2 is flushed (a 256 MiB write) before every timed step and each step is
-timed with CUDA events on the launching stream.
+tmin 1e-4.  The rays (the camera's image, row-major) are traced with
+lrt_trace_nearest_image, each warp taking an 8x4-pixel tile as the
+reference's kernel1D_FillGbuffer walks packed tiles; the same rays in row
+order through lrt_trace_nearest are timed beside it ("row_order").  Rays and
+the scene are resident in HBM when timing starts; the L2 is flushed (a
+256 MiB write) before every timed step and each step is timed with CUDA
+events on the launching stream.
 
 Multi-GPU: rays are independent, so N ranks each trace the full workload on
 their own GPU (replicas, weak scaling); the time is the max over ranks.
@@ -60,7 +64,8 @@ def workload_scene_camera_only():
 def config_dict(extra=None):
     d = {"workload": WORKLOAD, "rays_per_step": WIDTH * HEIGHT, "image": [WIDTH, HEIGHT], "virtual_grid": GRID,
          "brick_size": BRICK, "brick_pad": PAD, "spheres": N_SPHERES, "sbs_layout": "ID32F_IRGB32F (fp32)",
-         "preset": "LAMBERT_NO_TEX, ST, GEOMETRY normals, TRILINEAR, VOLUME", "l2": "flushed before every step (256 MiB)"}
+         "preset": "LAMBERT_NO_TEX, ST, GEOMETRY normals, TRILINEAR, VOLUME", "l2": "flushed before every step (256 MiB)",
+         "call": "lrt_trace_nearest_image (the camera's rays in row-major order, 8x4-pixel tiles per warp)"}
     if extra:
         d.update(extra)
     return d
@@ -237,14 +242,18 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream
     sc.generate_eye_rays(cam, rays.data_ptr(), sp)
+    # The rays are one camera's image in row-major order; the timed call is
+    # lrt_trace_nearest_image, which hands each warp an 8x4-pixel tile (as the
+    # reference's kernel1D_FillGbuffer walks packed tiles) and returns the
+    # hits lrt_trace_nearest returns; the row-order call is timed beside it.
     # counting pass (untimed): algorithmic bytes of one launch
-    sc.trace_device(rays.data_ptr(), hits.data_ptr(), n, stream=sp, count_work=True)
+    sc.trace_image(rays.data_ptr(), hits.data_ptr(), WIDTH, HEIGHT, stream=sp, count_work=True)
     sc.sync(stream=sp, read_counters=True)
     counters = sc.work_counters()
     hit_count = int(counters[list(COUNTER_NAMES).index("hits")])
     bytes_per_launch = algorithmic_bytes(counters, n, sbs_colour_hits=hit_count)
     for _ in range(args.warmup):
-        sc.trace_device(rays.data_ptr(), hits.data_ptr(), n, stream=sp)
+        sc.trace_image(rays.data_ptr(), hits.data_ptr(), WIDTH, HEIGHT, stream=sp)
     sc.sync(stream=sp)
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -258,22 +267,21 @@ def run_ours(args, rank, world, local_rank):
     for i in range(args.steps):
         flush.zero_()
         starts[i].record(stream)
-        sc.trace_device(rays.data_ptr(), hits.data_ptr(), n, stream=sp)
-        ends[i].record(stream)
-    torch.cuda.synchronize(dev)
-    sc.sync(stream=sp)
-    kernel_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    # the same rays traced in 8x4-pixel tiles (lrt_trace_nearest_image): as
-    # the reference's kernel1D_FillGbuffer walks pixels in packed tiles
-    tile_ms = []
-    for i in range(min(args.steps, 50)):
-        flush.zero_()
-        starts[i].record(stream)
         sc.trace_image(rays.data_ptr(), hits.data_ptr(), WIDTH, HEIGHT, stream=sp)
         ends[i].record(stream)
     torch.cuda.synchronize(dev)
     sc.sync(stream=sp)
-    tile_ms = [starts[i].elapsed_time(ends[i]) for i in range(min(args.steps, 50))]
+    kernel_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    # the same rays traced in row order (lrt_trace_nearest, 32 consecutive rays per warp)
+    row_ms = []
+    for i in range(min(args.steps, 50)):
+        flush.zero_()
+        starts[i].record(stream)
+        sc.trace_device(rays.data_ptr(), hits.data_ptr(), n, stream=sp)
+        ends[i].record(stream)
+    torch.cuda.synchronize(dev)
+    sc.sync(stream=sp)
+    row_ms = [starts[i].elapsed_time(ends[i]) for i in range(min(args.steps, 50))]
     # end to end through the public API with pinned host buffers
     host_rays = torch.empty(n * 8, dtype=torch.float32, pin_memory=True)
     host_rays.copy_(rays.cpu())
@@ -318,14 +326,14 @@ def run_ours(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": bytes_per_launch,
-                     "bytes_per_ray": bytes_per_launch / n, "kernel": "k_trace (exact build)"},
+                     "bytes_per_ray": bytes_per_launch / n,
+                     "kernel": "k_trace (exact build) via lrt_trace_nearest_image"},
         "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * 32,
                 "ms_per_step": total_e2e_ms / args.steps,
                 "gpu_launches": args.steps * len(pipeline_chunks(n)),
                 "call": "lrt_trace_nearest, pinned host buffers (chunked copy/trace/copy pipeline)"},
-        "image_tile_order": {"ms_per_step": sum(tile_ms) / len(tile_ms),
-                             "value": n / (sum(tile_ms) / len(tile_ms)) / 1e3, "unit": "Mrays/s",
-                             "call": "lrt_trace_nearest_image (same rays, 8x4-pixel tiles per warp)"},
+        "row_order": {"ms_per_step": sum(row_ms) / len(row_ms), "value": n / (sum(row_ms) / len(row_ms)) / 1e3,
+                      "unit": "Mrays/s", "call": "lrt_trace_nearest (same rays, 32 consecutive rays per warp)"},
         "clocks": clk,
         # our kernels in the device-timed region: one k_trace per step (the L2
         # flush between steps is torch's); the e2e region's are under "e2e"
