@@ -37,11 +37,13 @@ SOURCES = {
     "batch.cu": [],
     "adjoint.cu": [],
     "wavefront.cu": [],
+    "lbvh.cu": [],
     "scene.cpp": None,
     "layout.cpp": None,
     "workloads.cpp": None,
 }
-HEADERS = ["trace_impl.cuh", "device_layout.h", "lrt_math.h", "scene.h", "layout.h", "trace_api.h", "device_scene.h"]
+HEADERS = ["trace_impl.cuh", "device_layout.h", "lrt_math.h", "scene.h", "layout.h", "trace_api.h", "device_scene.h",
+           "lbvh.h"]
 
 
 def _stale(obj, src):

@@ -1,0 +1,25 @@
+// lbvh.h — the device tree builder used for the BUILD_LOW build quality.
+#pragma once
+#include <stdint.h>
+
+#include <vector>
+
+namespace lrt {
+
+// Inner node i of the binary radix tree over the Morton-sorted boxes.  kid[c]
+// is an inner node index, or a leaf (a position in the sorted order) with
+// the top bit set.  [first, last] is the node's range of sorted positions;
+// lo/hi its box (the union of its boxes).
+struct LbvhInner {
+  float lo[3], hi[3];
+  uint32_t kid[2];
+  uint32_t first, last;
+};
+
+// Builds the tree over n boxes (n x {lo.xyz, hi.xyz}, host memory) on the
+// current CUDA device and returns it to the host: order[p] is the box at
+// sorted position p, inner has n - 1 nodes with the root at 0 (none when
+// n == 1).  Returns nullptr on success, else a message.
+const char* lbvh_build(const float* boxes6, uint32_t n, std::vector<uint32_t>& order, std::vector<LbvhInner>& inner);
+
+} // namespace lrt

@@ -20,6 +20,7 @@
 #include <cstring>
 #include <new>
 
+#include "lbvh.h"
 #include "scene.h"
 
 namespace lrt {
@@ -162,6 +163,68 @@ struct SahBuilder {
   }
 };
 
+// The BUILD_LOW tree: a linear BVH built on the device (lbvh.cu) in the
+// node form the emitters read (nodes[0] the root, leaf ranges in `ids`).
+// Inner nodes of at most maxLeaf primitives become leaves, as SahBuilder
+// stops at maxLeaf.
+struct RadixTree {
+  std::vector<uint32_t> ids;
+  std::vector<BNode> nodes;
+
+  // nullptr on success, else the device builder's message
+  const char* build(const std::vector<Aabb>& prim, uint32_t maxLeaf)
+  {
+    maxLeaf = std::max(1u, maxLeaf);
+    std::vector<LbvhInner> inner;
+    static_assert(sizeof(Aabb) == 6 * sizeof(float), "Aabb is lo.xyz, hi.xyz");
+    const char* err = lbvh_build(reinterpret_cast<const float*>(prim.data()), uint32_t(prim.size()), ids, inner);
+    if (err) return err;
+    nodes.clear();
+    nodes.reserve(2 * prim.size());
+    nodes.emplace_back();
+    if (inner.empty()) { // one primitive
+      nodes[0].box = prim[ids[0]];
+      nodes[0].count = 1;
+      return nullptr;
+    }
+    // depth-first from the root; `tree` is an inner index or a leaf position with the top bit set
+    struct Item {
+      uint32_t tree;
+      int32_t node;
+    };
+    std::vector<Item> todo{{0u, 0}};
+    while (!todo.empty()) {
+      const Item it = todo.back();
+      todo.pop_back();
+      BNode& n = nodes[it.node];
+      if (it.tree & 0x80000000u) {
+        const uint32_t pos = it.tree & 0x7FFFFFFFu;
+        n.box = prim[ids[pos]];
+        n.start = pos;
+        n.count = 1;
+        continue;
+      }
+      const LbvhInner& in = inner[it.tree];
+      for (int k = 0; k < 3; k++) {
+        n.box.lo[k] = in.lo[k];
+        n.box.hi[k] = in.hi[k];
+      }
+      if (in.last - in.first + 1 <= maxLeaf) {
+        n.start = in.first;
+        n.count = in.last - in.first + 1;
+        continue;
+      }
+      for (int c = 0; c < 2; c++) {
+        const int32_t id = int32_t(nodes.size());
+        nodes[it.node].kid[c] = id; // `n` may move when nodes grows
+        nodes.emplace_back();
+        todo.push_back({in.kid[c], id});
+      }
+    }
+    return nullptr;
+  }
+};
+
 lrt_bvh_node make_node(const Aabb& b, uint32_t left, uint32_t esc)
 {
   lrt_bvh_node n;
@@ -185,8 +248,8 @@ lrt_bvh_node dummy_node()
 // node stored in pair k are pair `leftOffset`).  `leafWord(node)` gives the
 // packed leftOffset of a leaf.  escapeIndex follows the aligned-array
 // convention of AlignNodes2 (left -> its right sibling, right -> parent's).
-template <class LeafWord>
-void emit_pairs(const SahBuilder& B, std::vector<lrt_bvh_node_pair>& out, LeafWord leafWord)
+template <class Tree, class LeafWord>
+void emit_pairs(const Tree& B, std::vector<lrt_bvh_node_pair>& out, LeafWord leafWord)
 {
   const BNode& root = B.nodes[0];
   if (root.leaf()) {
@@ -197,7 +260,7 @@ void emit_pairs(const SahBuilder& B, std::vector<lrt_bvh_node_pair>& out, LeafWo
     return;
   }
   struct Rec {
-    static uint32_t go(const SahBuilder& B, std::vector<lrt_bvh_node_pair>& out, int32_t node, uint32_t base,
+    static uint32_t go(const Tree& B, std::vector<lrt_bvh_node_pair>& out, int32_t node, uint32_t base,
                        uint32_t parentEsc, LeafWord& lw)
     {
       const BNode& n = B.nodes[node];
@@ -224,10 +287,11 @@ void emit_pairs(const SahBuilder& B, std::vector<lrt_bvh_node_pair>& out, LeafWo
 // Emits a built tree as the TLAS node array: aligned pairs in depth-first
 // pre-order, node 0/1 are the root's children, inner nodes point at their
 // left child, escapeIndex gives the next node of a stackless traversal.
-void emit_tlas(const SahBuilder& B, std::vector<lrt_bvh_node>& out)
+template <class Tree>
+void emit_tlas(const Tree& B, std::vector<lrt_bvh_node>& out)
 {
   struct Rec {
-    static void go(const SahBuilder& B, std::vector<lrt_bvh_node>& out, int32_t node, uint32_t parentEsc)
+    static void go(const Tree& B, std::vector<lrt_bvh_node>& out, int32_t node, uint32_t parentEsc)
     {
       const BNode& n = B.nodes[node];
       const uint32_t k = uint32_t(out.size());
@@ -260,12 +324,26 @@ Aabb box_of(const float* mn, const float* mx)
 
 // AddGeom_AABB's BLAS part: one box per leaf, leaf word = Pack(boxIndex, 1)
 // (BuildBVH(boxes), cbvh.cpp:650-660), identity leaf table (:451-453).
-uint32_t add_aabb_blas(lrt_scene* s, uint32_t tag, const std::vector<Aabb>& boxes)
+// BLAS of custom boxes, one box per leaf; BUILD_LOW builds the tree on the
+// device.  ~0u if that build failed (the message is the scene's last error).
+uint32_t add_aabb_blas(lrt_scene* s, uint32_t tag, const std::vector<Aabb>& boxes, uint32_t flags = 0)
 {
   HostArrays& h = s->h;
-  SahBuilder B(boxes, 1);
-  B.build(0, uint32_t(boxes.size()));
-  emit_pairs(B, h.allNodePairs, [&](int32_t node) { return pack_offset_and_size(B.ids[B.nodes[node].start], 1); });
+  auto emit = [&](const auto& B) {
+    emit_pairs(B, h.allNodePairs, [&](int32_t node) { return pack_offset_and_size(B.ids[B.nodes[node].start], 1); });
+  };
+  if (flags & LRT_BUILD_LOW) {
+    RadixTree R;
+    if (const char* err = R.build(boxes, 1)) {
+      fail(s, LRT_ERR_CUDA, "AddGeom_AABB (BUILD_LOW): %s", err);
+      return ~0u;
+    }
+    emit(R);
+  } else {
+    SahBuilder B(boxes, 1);
+    B.build(0, uint32_t(boxes.size()));
+    emit(B);
+  }
   const uint32_t old = uint32_t(h.primIdCount.size());
   for (uint32_t i = 0; i < boxes.size(); i++) h.primIdCount.push_back(i);
   h.startEnd.push_back(old);
@@ -437,10 +515,21 @@ lrt_status validate(lrt_scene* s, SceneInfo* info)
   for (size_t i = 0; i < h.instanceData.size(); i++)
     if (h.instanceData[i].geomId >= G)
       return fail(s, LRT_ERR_BAD_SCENE, "instance %zu names geometry %u of %zu", i, h.instanceData[i].geomId, G);
-  // geometries
-  const size_t P = h.allNodePairs.size();
+  // geometries: checked once per geometry version; a commit after instance
+  // changes only keeps what the last check found
+  const bool geomChecked = s->validatedGeomVersion == s->geomVersion;
+  if (geomChecked) {
+    const SceneInfo& c = s->geomInfo;
+    I.maxBlasDepth = c.maxBlasDepth;
+    I.hasTriangles = c.hasTriangles;
+    I.hasSbs = c.hasSbs;
+    I.hasFrameOctree = c.hasFrameOctree;
+    I.hasSvs = c.hasSvs;
+    I.hasSbsNeighbours = c.hasSbsNeighbours;
+  }
+  const size_t P = geomChecked ? 0 : h.allNodePairs.size();
   std::vector<uint8_t> pairSeen(P, 0);
-  for (size_t g = 0; g < G; g++) {
+  for (size_t g = 0; g < G && !geomChecked; g++) {
     const lrt_geom_data& gd = h.geomData[g];
     const uint32_t tag = h.geomTags[g];
     const uint32_t a0 = h.startEnd[2 * g], a1 = h.startEnd[2 * g + 1];
@@ -574,6 +663,8 @@ lrt_status validate(lrt_scene* s, SceneInfo* info)
   }
   if (I.maxBlasDepth > kMaxStack)
     return fail(s, LRT_ERR_BAD_SCENE, "BLAS depth %u exceeds the %u-entry traversal stack", I.maxBlasDepth, kMaxStack);
+  s->geomInfo = I;
+  s->validatedGeomVersion = s->geomVersion;
   *info = I;
   return LRT_OK;
 }
@@ -687,12 +778,13 @@ lrt_status lrt_clear_geom(lrt_scene* s)
 lrt_status lrt_add_geom_triangles3f(lrt_scene* s, const float* vpos, size_t nvert, const uint32_t* tri,
                                     size_t nidx, uint32_t flags, size_t stride, uint32_t* geom_id_out)
 {
-  (void)flags;
   if (!s) return LRT_ERR_INVALID_ARGUMENT;
   s->geomVersion++;
   if (!vpos || !tri || nvert == 0 || nidx == 0 || nidx % 3 != 0)
     return fail(s, LRT_ERR_INVALID_ARGUMENT, "AddGeom_Triangles3f: empty input or index count %zu not a multiple of 3",
                 nidx);
+  if ((flags & LRT_BUILD_LOW) && nidx / 3 >= (size_t(1) << 28))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "AddGeom_Triangles3f (BUILD_LOW): %zu triangles", nidx / 3);
   if (stride == 0) stride = 12;
   if (stride % 4 != 0 || stride < 12)
     return fail(s, LRT_ERR_INVALID_ARGUMENT, "AddGeom_Triangles3f: vertex byte stride %zu", stride);
@@ -735,21 +827,35 @@ lrt_status lrt_add_geom_triangles3f(lrt_scene* s, const float* vpos, size_t nver
       }
     }
   }
-  SahBuilder B(boxes, s->primsInLeaf);
-  B.build(0, uint32_t(nt));
   // leaves numbered in emission order; each leaf word is Pack(leafId, 1) and
   // its triangle range goes to primIdCount as Pack(start, count)
   // (cbvh.cpp:516-525, AppendTreeData BVH2Common_host.cpp:287-301).
   std::vector<uint32_t> startCount;
   std::vector<uint32_t> reordered;
   reordered.reserve(nt);
-  emit_pairs(B, h.allNodePairs, [&](int32_t node) {
-    const BNode& n = B.nodes[node];
-    const uint32_t leafId = uint32_t(startCount.size());
-    startCount.push_back(pack_offset_and_size(uint32_t(reordered.size()), n.count));
-    for (uint32_t i = n.start; i < n.start + n.count; i++) reordered.push_back(B.ids[i]);
-    return pack_offset_and_size(leafId, 1);
-  });
+  auto emit = [&](const auto& B) {
+    emit_pairs(B, h.allNodePairs, [&](int32_t node) {
+      const BNode& n = B.nodes[node];
+      const uint32_t leafId = uint32_t(startCount.size());
+      startCount.push_back(pack_offset_and_size(uint32_t(reordered.size()), n.count));
+      for (uint32_t i = n.start; i < n.start + n.count; i++) reordered.push_back(B.ids[i]);
+      return pack_offset_and_size(leafId, 1);
+    });
+  };
+  if (flags & LRT_BUILD_LOW) {
+    RadixTree R;
+    if (const char* err = R.build(boxes, s->primsInLeaf)) {
+      h.vertPos.resize(4 * oldV);
+      h.geomData.pop_back();
+      h.geomTags.pop_back();
+      return fail(s, LRT_ERR_CUDA, "AddGeom_Triangles3f (BUILD_LOW): %s", err);
+    }
+    emit(R);
+  } else {
+    SahBuilder B(boxes, s->primsInLeaf);
+    B.build(0, uint32_t(nt));
+    emit(B);
+  }
   h.primIndices.insert(h.primIndices.end(), reordered.begin(), reordered.end());
   h.indices.resize(oldI + 3 * reordered.size());
   for (size_t i = 0; i < reordered.size(); i++)
@@ -767,13 +873,15 @@ lrt_status lrt_add_geom_triangles3f(lrt_scene* s, const float* vpos, size_t nver
 lrt_status lrt_add_geom_aabb(lrt_scene* s, uint32_t tag, const float* boxes8, size_t n, uint32_t flags,
                              uint32_t* geom_id_out)
 {
-  (void)flags;
   if (!s) return LRT_ERR_INVALID_ARGUMENT;
   s->geomVersion++;
   if (!boxes8 || n == 0) return fail(s, LRT_ERR_INVALID_ARGUMENT, "AddGeom_AABB: no boxes");
+  if ((flags & LRT_BUILD_LOW) && n >= (size_t(1) << 28))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "AddGeom_AABB (BUILD_LOW): %zu boxes", n);
   std::vector<Aabb> boxes(n);
   for (size_t i = 0; i < n; i++) boxes[i] = box_of(boxes8 + 8 * i, boxes8 + 8 * i + 4);
-  const uint32_t id = add_aabb_blas(s, tag, boxes);
+  const uint32_t id = add_aabb_blas(s, tag, boxes, flags);
+  if (id == ~0u) return LRT_ERR_CUDA;
   s->committed = false;
   if (geom_id_out) *geom_id_out = id;
   return LRT_OK;
@@ -1008,9 +1116,15 @@ lrt_status lrt_commit_scene(lrt_scene* s, uint32_t flags)
   if (h.instanceData.size() > 1) {
     std::vector<Aabb> boxes(h.instanceData.size());
     for (size_t i = 0; i < boxes.size(); i++) boxes[i] = box_of(h.instanceData[i].boxMin, h.instanceData[i].boxMax);
-    SahBuilder B(boxes, 1);
-    B.build(0, uint32_t(boxes.size()));
-    emit_tlas(B, h.nodesTLAS);
+    if (flags & LRT_BUILD_LOW) {
+      RadixTree R;
+      if (const char* err = R.build(boxes, 1)) return fail(s, LRT_ERR_CUDA, "CommitScene (BUILD_LOW): %s", err);
+      emit_tlas(R, h.nodesTLAS);
+    } else {
+      SahBuilder B(boxes, 1);
+      B.build(0, uint32_t(boxes.size()));
+      emit_tlas(B, h.nodesTLAS);
+    }
   } else {
     // a single instance needs no TLAS: one leaf node (:1245-1252)
     lrt_bvh_node n;

@@ -71,6 +71,8 @@ struct lrt_scene {
   // re-uploads only the instances and the TLAS
   uint64_t geomVersion = 1;
   uint64_t uploadedGeomVersion = 0;
+  uint64_t validatedGeomVersion = 0; // geometry arrays last passed validation at this version
+  lrt::SceneInfo geomInfo;           // what that validation found
   lrt::SceneInfo info;
   lrt::DeviceScene* dev = nullptr;
   int device = -1;

@@ -192,6 +192,19 @@ lrt_status lrt_default_preset(lrt_preset* out);
 /* ISceneObject::ClearGeom (CrossRT.h:60; BVH2Common_host.cpp:128-156). */
 lrt_status lrt_clear_geom(lrt_scene* scene);
 
+/* Build qualities of the reference's BuildOptions (CrossRT/CrossRT.h:14-17).
+ * LRT_BUILD_LOW builds the tree on the current CUDA device (a linear BVH over
+ * Morton-sorted box centres, Karras 2012) instead of the host's binned SAH:
+ * orders of magnitude faster for large meshes, with the same array formats
+ * and a tree that traverses somewhat slower.  It needs a CUDA device (else
+ * LRT_ERR_CUDA) and takes effect in lrt_add_geom_triangles3f,
+ * lrt_add_geom_aabb and, for the TLAS, lrt_commit_scene.  The other values
+ * select the SAH build. */
+#define LRT_BUILD_LOW 0x1u
+#define LRT_BUILD_MEDIUM 0x2u
+#define LRT_BUILD_HIGH 0x4u
+#define LRT_BUILD_REFIT 0x8u
+
 /* ISceneObject::AddGeom_Triangles3f (CrossRT.h:71-72;
  * BVH2Common_host.cpp:307-359).  vertex_byte_stride 0 means 12. */
 lrt_status lrt_add_geom_triangles3f(lrt_scene* scene, const float* vpos3f, size_t vert_count,

@@ -69,3 +69,57 @@ def tolerance_report(got, want, rays=None):
     return {"id_mismatch": int((~ids).sum()), "max_rel_t": float(rel_t.max()) if len(rel_t) else 0.0,
             "max_normal_err": float(dn.max()) if len(dn) else 0.0, "t_fail": int((rel_t > 1e-5).sum()),
             "n_fail": int((dn > 1e-4).sum()), "mismatch_idx": np.nonzero(~ids)[0]}
+
+
+LEAF = 0x80000000
+
+
+def check_blas_layout(arrays, geom, base=None):
+    """The fat-pair BLAS of geometry `geom` (its pairs from `base`, by
+    default its geomData bvhOffset) is a depth-first pre-order tree (every
+    inner pointer points forward, no pair reached twice) whose leaves name
+    each entry of its leaf table once, Pack(id, 1); returns the leaf ids in
+    traversal order."""
+    pairs, gd, se = arrays["allNodePairs"], arrays["geomData"], arrays["startEnd"]
+    base = int(gd["bvhOffset"][geom]) if base is None else base
+    a0, a1 = int(se[geom][0]), int(se[geom][1])
+    seen, ids, stack = set(), [], [0]
+    while stack:
+        k = stack.pop()
+        assert k not in seen
+        seen.add(k)
+        for side in ("left", "right"):
+            lo = int(pairs[base + k][side]["leftOffset"])
+            if lo & LEAF:
+                if lo != 0xFFFFFFFF and lo != LEAF:
+                    assert (lo & 0x0FFFFFFF) < a1 - a0
+                    assert (lo >> 28) & 7 == 1      # Pack(id, 1)
+                    ids.append(lo & 0x0FFFFFFF)
+            else:
+                assert lo > k                       # depth-first pre-order
+                stack.append(lo)
+    assert sorted(ids) == list(range(a1 - a0))
+    return ids
+
+
+def check_tlas_layout(nodes, n_inst):
+    """The escape-index TLAS: aligned sibling pairs, the left one escaping
+    to its sibling and the right one to its parent's escape, each instance
+    in exactly one leaf, and every inner box containing its children."""
+    assert nodes[0]["escapeIndex"] == 1 and nodes[1]["escapeIndex"] == 0xFFFFFFFE
+    leaves = []
+    stack = [(0, 0xFFFFFFFE)]
+    while stack:
+        a, esc = stack.pop()
+        assert nodes[a]["escapeIndex"] == a + 1 and nodes[a + 1]["escapeIndex"] == esc
+        for j in (0, 1):
+            n = nodes[a + j]
+            lo = int(n["leftOffset"])
+            if lo & LEAF:
+                leaves.append(lo & 0x0FFFFFFF)
+            else:
+                assert lo > a
+                for c in (lo, lo + 1):
+                    assert np.all(nodes[c]["boxMin"] >= n["boxMin"]) and np.all(nodes[c]["boxMax"] <= n["boxMax"])
+                stack.append((lo, int(n["escapeIndex"])))
+    assert sorted(leaves) == list(range(n_inst))

@@ -6,9 +6,7 @@ import pytest
 
 import pyoracle as po
 from graphic_lab_task_b200 import LrtError, SceneRT, workloads as wl
-from helpers import MISS, bit_equal, hit_summary
-
-LEAF = 0x80000000
+from helpers import LEAF, MISS, bit_equal, check_blas_layout, check_tlas_layout, hit_summary
 
 
 def build_mixed(seed=0, n_inst=8):
@@ -29,28 +27,9 @@ def build_mixed(seed=0, n_inst=8):
 def test_blas_layout_matches_reference_conventions():
     sc, (v, t) = build_mixed()
     a = sc.export_arrays()
-    pairs, gd, se = a["allNodePairs"], a["geomData"], a["startEnd"]
-    for g in range(len(gd)):
-        base = int(gd["bvhOffset"][g])
-        a0, a1 = int(se[g][0]), int(se[g][1])
-        seen = set()
-        stack = [0]
-        leaves = 0
-        while stack:
-            k = stack.pop()
-            assert k not in seen
-            seen.add(k)
-            for side in ("left", "right"):
-                lo = int(pairs[base + k][side]["leftOffset"])
-                if lo & LEAF:
-                    if lo != 0xFFFFFFFF and lo != LEAF:
-                        leaves += 1
-                        assert (lo & 0x0FFFFFFF) < a1 - a0
-                        assert (lo >> 28) & 7 == 1      # Pack(id, 1)
-                else:
-                    assert lo > k                       # depth-first pre-order
-                    stack.append(lo)
-        assert leaves == a1 - a0
+    se = a["startEnd"]
+    for g in range(len(a["geomData"])):
+        check_blas_layout(a, g)
     # triangle leaves: primIdCount packs (start, count <= primsInLeaf), m_indices is the reordered index buffer
     g = 0
     pc = a["primIdCount"][se[g][0]:se[g][1]]
@@ -61,20 +40,7 @@ def test_blas_layout_matches_reference_conventions():
 
 def test_tlas_escape_layout():
     sc, _ = build_mixed(n_inst=13)
-    nodes = sc.export_arrays()["nodesTLAS"]
-    assert nodes[0]["escapeIndex"] == 1 and nodes[1]["escapeIndex"] == 0xFFFFFFFE
-    leaves = set()
-    stack = [(0, 0xFFFFFFFE)]
-    while stack:
-        a, esc = stack.pop()
-        assert nodes[a]["escapeIndex"] == a + 1 and nodes[a + 1]["escapeIndex"] == esc
-        for j in (0, 1):
-            lo = int(nodes[a + j]["leftOffset"])
-            if lo & LEAF:
-                leaves.add(lo & 0x0FFFFFFF)
-            else:
-                stack.append((lo, int(nodes[a + j]["escapeIndex"])))
-    assert leaves == set(range(13))
+    check_tlas_layout(sc.export_arrays()["nodesTLAS"], 13)
 
 
 def test_single_instance_tlas_is_one_leaf():
@@ -244,3 +210,29 @@ def test_sdf_model_files_load_like_the_arrays(tmp_path):
         SceneRT().AddGeom_SdfFile("sbs", tmp_path / "t2.bin")
     with pytest.raises(LrtError):
         SceneRT().AddGeom_SdfFile("frame_octree", tmp_path / "missing.bin")
+
+
+@pytest.mark.skipif(__import__("torch").cuda.is_available(), reason="checks the error without a CUDA device")
+def test_device_build_without_device_is_an_error():
+    """BUILD_LOW builds the tree on the CUDA device; without one the adder
+    fails with LRT_ERR_CUDA and leaves the scene as it was."""
+    from graphic_lab_task_b200 import BUILD_LOW
+    sc = SceneRT()
+    v, t = wl.noisy_sphere(8)
+    with pytest.raises(LrtError) as e:
+        sc.AddGeom_Triangles3f(v, t, flags=BUILD_LOW)
+    assert e.value.status == 4 and "BUILD_LOW" in str(e.value)
+    with pytest.raises(LrtError) as e:
+        sc.AddGeom_AABB(0, np.array([[0, 0, 0, 1, 1, 1, 1, 1]], np.float32), flags=BUILD_LOW)
+    assert e.value.status == 4
+    g = sc.AddGeom_Triangles3f(v, t)
+    assert g == 0
+    sc.AddInstance(g, wl.IDENTITY)
+    sc.AddInstance(g, wl.IDENTITY)
+    with pytest.raises(LrtError) as e:
+        sc.CommitScene(options=BUILD_LOW, host_only=True)
+    assert e.value.status == 4
+    sc.CommitScene(host_only=True)
+    a = sc.export_arrays()
+    check_blas_layout(a, 0)
+    assert len(a["geomData"]) == 1 and len(a["vertPos"]) == len(v)
