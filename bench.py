@@ -393,9 +393,16 @@ def fused_render(sc, dev, args):
         sc.trace_device(rays.data_ptr(), hits.data_ptr(), n, stream=sp)
 
     gbuf_ms = timed(gbuffer)
+    # kernel1D_FillGbufferWithTransparency on the same camera: SBS_COL hits
+    # keep the (transparent) initial colour, so every pixel's loop traces
+    # through all surfaces along its ray until it misses
+    transp = torch.empty(n * 4, dtype=torch.float32, device=dev)
+    transp_ms = timed(lambda: sc.fill_gbuffer_transparency(cam, (0, 0, 0, 1), transp.data_ptr(), hits.data_ptr(),
+                                                           stream=sp))
     sc.sync(stream=sp)
     return {"pixels": n, "fused_ms": fused_ms, "fused_mpix_s": n / fused_ms / 1e3, "gbuffer_path_ms": gbuf_ms,
-            "gbuffer_path_mpix_s": n / gbuf_ms / 1e3, "gbuffer_bytes_avoided": n * 64, "steps": steps}
+            "gbuffer_path_mpix_s": n / gbuf_ms / 1e3, "gbuffer_bytes_avoided": n * 64, "steps": steps,
+            "transparency_ms": transp_ms, "transparency_mpix_s": n / transp_ms / 1e3}
 
 
 def batched_cameras(sc, dev, args):

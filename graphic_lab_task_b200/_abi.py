@@ -32,6 +32,11 @@ SBS_HEADER_DTYPE = np.dtype([("brick_size", "<u4"), ("brick_pad", "<u4"), ("byte
 # Light, core/IRenderer.h:72-78 (lrt_light)
 LIGHT_DTYPE = np.dtype([("space", "<f4", (3,)), ("type", "<u4"), ("color", "<f4", (3,)), ("_pad", "<u4")])
 LIGHT_DIRECT, LIGHT_POINT, LIGHT_AMBIENT = 0, 1, 2
+# MultiRendererMaterial, core/IRenderer.h:31-38 (lrt_material)
+MATERIAL_DTYPE = np.dtype([("type", "<u4"), ("texId", "<u4"), ("metallic", "<f4"), ("roughness", "<f4"),
+                           ("base_color", "<f4", (4,))])
+MATERIAL_COLORED, MATERIAL_TEXTURED = 0, 1
+assert MATERIAL_DTYPE.itemsize == 32
 # BuildOptions, CrossRT/CrossRT.h:14-17 (LRT_BUILD_*): LOW builds the tree on the device
 BUILD_LOW, BUILD_MEDIUM, BUILD_HIGH, BUILD_REFIT = 0x1, 0x2, 0x4, 0x8
 assert LIGHT_DTYPE.itemsize == 32

@@ -158,6 +158,94 @@ lrt_status lrt_render_rgba8(lrt_scene* s, const lrt_camera* camera, const lrt_li
   return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "render launch");
 }
 
+lrt_status lrt_set_materials(lrt_scene* s, const lrt_material* materials, uint32_t material_count,
+                             const uint32_t* mat_id_by_prim_id, uint64_t mat_id_count, const uint32_t* mat_id_offsets,
+                             uint32_t offset_count)
+{
+  if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  if ((material_count && !materials) || (mat_id_count && !mat_id_by_prim_id) || (offset_count && !mat_id_offsets))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_set_materials: NULL array with a nonzero count");
+  for (uint64_t i = 0; i < mat_id_count; i++)
+    if (mat_id_by_prim_id[i] >= material_count)
+      return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_set_materials: material id %u at %llu of %u materials",
+                  mat_id_by_prim_id[i], (unsigned long long)i, material_count);
+  for (uint32_t g = 0; g < offset_count; g++) {
+    const uint64_t start = mat_id_offsets[2 * g], size = mat_id_offsets[2 * g + 1];
+    if (start + size > mat_id_count)
+      return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_set_materials: geometry %u range [%llu, +%llu) beyond %llu ids", g,
+                  (unsigned long long)start, (unsigned long long)size, (unsigned long long)mat_id_count);
+  }
+  s->mats.assign(materials, materials + material_count);
+  s->matIds.assign(mat_id_by_prim_id, mat_id_by_prim_id + mat_id_count);
+  s->matOffsets.assign(mat_id_offsets, mat_id_offsets + 2 * size_t(offset_count));
+  s->matVersion++;
+  return LRT_OK;
+}
+
+lrt_status lrt_fill_gbuffer_transparency(lrt_scene* s, const lrt_camera* camera, const float background[4],
+                                         float* transparency_dev, lrt_hit* hits_dev, void* stream_p)
+{
+  StreamSlot* slot = nullptr;
+  DevScene S;
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_p);
+  lrt_status st = begin(s, stream, &slot, &S);
+  if (st != LRT_OK) return st;
+  if (!camera || !background || !transparency_dev || !hits_dev)
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_fill_gbuffer_transparency: NULL camera, background or output");
+  if ((st = check_rays(s, transparency_dev)) != LRT_OK || (st = check_rays(s, hits_dev)) != LRT_OK) return st;
+  // every geometry whose hits read a material needs a nonempty range
+  const HostArrays& h = s->h;
+  for (size_t g = 0; g < h.geomData.size(); g++) {
+    const uint32_t type = h.geomData[g].type;
+    if (type == LRT_TYPE_SDF_SBS_COL || type == LRT_TYPE_GRAPHICS_PRIM) continue;
+    if (2 * g + 1 >= s->matOffsets.size() || s->matOffsets[2 * g + 1] == 0)
+      return fail(s, LRT_ERR_INVALID_ARGUMENT,
+                  "lrt_fill_gbuffer_transparency: geometry %zu (type %u) has no material range (lrt_set_materials)", g,
+                  type);
+  }
+  if (camera->width == 0 || camera->height == 0) return LRT_OK;
+  DeviceScene* d = s->dev;
+  if (d->matVersion != s->matVersion) {
+    // copy the tables (synchronous: they change rarely)
+    cudaFree(d->mats);
+    cudaFree(d->matIds);
+    cudaFree(d->matOffsets);
+    d->mats = nullptr;
+    d->matIds = nullptr;
+    d->matOffsets = nullptr;
+    cudaError_t e = cudaMalloc(&d->mats, std::max<size_t>(1, s->mats.size()) * sizeof(lrt_material));
+    if (e == cudaSuccess) e = cudaMalloc(&d->matIds, std::max<size_t>(1, s->matIds.size()) * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&d->matOffsets, std::max<size_t>(1, s->matOffsets.size()) * sizeof(uint32_t));
+    if (e == cudaSuccess && !s->mats.empty())
+      e = cudaMemcpy(d->mats, s->mats.data(), s->mats.size() * sizeof(lrt_material), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !s->matIds.empty())
+      e = cudaMemcpy(d->matIds, s->matIds.data(), s->matIds.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !s->matOffsets.empty())
+      e = cudaMemcpy(d->matOffsets, s->matOffsets.data(), s->matOffsets.size() * sizeof(uint32_t),
+                     cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(s, e, "material tables host->device");
+    d->matVersion = s->matVersion;
+  }
+  DevCamera cam;
+  std::memcpy(cam.proj_inv, camera->proj_inv, sizeof(cam.proj_inv));
+  std::memcpy(cam.world_view_inv, camera->world_view_inv, sizeof(cam.world_view_inv));
+  cam.width = camera->width;
+  cam.height = camera->height;
+  cam.tnear = camera->tnear;
+  cam.tfar = camera->tfar;
+  DevMaterials M;
+  M.mats = d->mats;
+  M.ids = d->matIds;
+  M.offsets = reinterpret_cast<const uint2*>(d->matOffsets);
+  std::memcpy(M.background, background, sizeof(M.background));
+  const uint64_t tiles = uint64_t((cam.width + 7) / 8) * ((cam.height + 3) / 4);
+  const int grid = int(std::min<uint64_t>(uint64_t(d->grid), (tiles * 32 + kTraceThreads - 1) / kTraceThreads));
+  const cudaError_t e = lrt_exact::launch_fill_gbuffer_transparency(S, cam, M, reinterpret_cast<float4*>(transparency_dev),
+                                                                    hits_dev, &slot->work, &slot->err, d->stackCap,
+                                                                    grid, stream);
+  return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "transparency launch");
+}
+
 lrt_status lrt_render_lambert(lrt_scene* s, const float* rays_dev, uint64_t n, const float light[3], float* image_dev,
                               void* stream_p)
 {

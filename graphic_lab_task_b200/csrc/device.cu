@@ -123,7 +123,7 @@ lrt_status finish(lrt_scene* s, cudaStream_t stream, StreamSlot* slot, bool coun
   if (hs.err) {
     cudaMemsetAsync(&slot->err, 0, sizeof(uint32_t), stream);
     cudaStreamSynchronize(stream);
-    return fail(s, LRT_ERR_DEVICE_LIMIT, "trace hit a bounded-loop limit (error bits 0x%x: 1 = stack, 2 = voxel march)",
+    return fail(s, LRT_ERR_DEVICE_LIMIT, "trace hit a bounded-loop limit (error bits 0x%x: 1 = stack, 2 = voxel march, 4 = transparency layers)",
                 hs.err);
   }
   return LRT_OK;
@@ -593,6 +593,6 @@ extern "C" lrt_status lrt_trace_nearest_noalloc(lrt_scene* s, const float* rays,
   if (e != cudaSuccess) return cuda_fail(s, e, "trace");
   if (err)
     return fail(s, LRT_ERR_DEVICE_LIMIT,
-                "trace hit a bounded-loop limit (error bits 0x%x: 1 = stack, 2 = voxel march)", err);
+                "trace hit a bounded-loop limit (error bits 0x%x: 1 = stack, 2 = voxel march, 4 = transparency layers)", err);
   return LRT_OK;
 }

@@ -53,6 +53,7 @@ constexpr uint32_t kSolverST = 0, kSolverAnalytic = 1, kSolverNewton = 2, kSolve
 // error bits of the per-launch error word
 constexpr uint32_t kErrStackOverflow = 1u;
 constexpr uint32_t kErrVoxelCap = 2u;
+constexpr uint32_t kErrLayerCap = 4u; // a transparency loop reached LRT_MAX_TRANSPARENCY_LAYERS
 
 // work counters (same order as LRT_COUNTER_COUNT in lrt_b200.h)
 enum : int {
@@ -139,6 +140,16 @@ typedef lrt_light DevLight;
 struct DevLights {
   DevLight light[LRT_MAX_LIGHTS];
   uint32_t count;
+  float background[4];
+};
+
+// The renderer's material tables for the transparency loop (lrt_material =
+// MultiRendererMaterial, core/IRenderer.h:31-38; offsets = uint2 {start,
+// size} per geometry) and the background colour.
+struct DevMaterials {
+  const lrt_material* mats;
+  const uint32_t* ids;
+  const uint2* offsets;
   float background[4];
 };
 

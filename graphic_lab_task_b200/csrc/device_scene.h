@@ -46,6 +46,12 @@ struct DeviceScene {
   // per-tile hit counts of lrt_generate_bounce_rays_compact
   uint32_t* tileScratch = nullptr;
   uint64_t tileCap = 0;
+  // the renderer's material tables (lrt_set_materials), copied at the first
+  // transparency trace after they changed
+  lrt_material* mats = nullptr;
+  uint32_t* matIds = nullptr;
+  uint2* matOffsets = nullptr;
+  uint64_t matVersion = 0;
   // staging buffers for host-pointer calls
   float4* rays = nullptr;
   lrt_hit* hits = nullptr;
@@ -67,6 +73,9 @@ struct DeviceScene {
     if (rays) cudaFree(rays);
     if (hits) cudaFree(hits);
     if (tileScratch) cudaFree(tileScratch);
+    if (mats) cudaFree(mats);
+    if (matIds) cudaFree(matIds);
+    if (matOffsets) cudaFree(matOffsets);
   }
 };
 

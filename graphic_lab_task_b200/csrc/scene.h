@@ -78,6 +78,10 @@ struct lrt_scene {
   int device = -1;
   std::string err;
   uint64_t counters[LRT_COUNTER_COUNT] = {};
+  // renderer materials (lrt_set_materials), validated; matVersion counts changes
+  std::vector<lrt_material> mats;
+  std::vector<uint32_t> matIds, matOffsets;
+  uint64_t matVersion = 0;
 };
 
 namespace lrt {

@@ -22,6 +22,10 @@
   cudaError_t launch_render_rgba8(const lrt::DevScene& S, const lrt::DevCamera& cam, const lrt::DevLights& lights,\
                                   uint32_t* image, unsigned long long* work_counter, uint32_t* err_word,        \
                                   uint32_t stack_cap, int grid, cudaStream_t stream);                           \
+  cudaError_t launch_fill_gbuffer_transparency(const lrt::DevScene& S, const lrt::DevCamera& cam,               \
+                                               const lrt::DevMaterials& M, float4* transparency, lrt_hit* gbuffer,\
+                                               unsigned long long* work_counter, uint32_t* err_word,            \
+                                               uint32_t stack_cap, int grid, cudaStream_t stream);              \
   cudaError_t launch_render_lambert(const lrt::DevScene& S, const float4* rays, uint64_t n, float3 light,       \
                                     float* image, unsigned long long* work_counter, uint32_t* err_word,         \
                                     uint32_t stack_cap, int grid, cudaStream_t stream);                         \

@@ -963,6 +963,70 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_render_rgba8(DevScene S, D
   if (c.err) atomicOr(err_word, c.err);
 }
 
+// kernel1D_FillGbufferWithTransparency + AnyHit (MultiRenderer.cpp:204-246)
+// for one sample: per pixel of the camera (8x4-pixel tiles per warp) the loop
+// of nearest hits compositing the COLORED materials front to back, each trace
+// starting at the previous hit point with the eye ray's tNear and direction.
+// Misses take the background; SBS_COL (11) and graphics-primitive (17) hits
+// keep the previous colour.  The loop ends when the remaining alpha is at
+// most 0.01 or, unlike the reference's, after kMaxLayers traces (error bit).
+__global__ void __launch_bounds__(kTraceThreads, 7) k_fill_gbuffer_transparency(
+    DevScene S, DevCamera cam, DevMaterials M, float4* __restrict__ transparency, lrt_hit* __restrict__ gbuffer,
+    unsigned long long* __restrict__ work_counter, uint32_t* __restrict__ err_word, uint32_t stack_cap)
+{
+  constexpr uint32_t kMaxLayers = LRT_MAX_TRANSPARENCY_LAYERS;
+  extern __shared__ uint32_t smem_stack[];
+  uint32_t* stack = smem_stack + threadIdx.x;
+  const uint32_t lane = threadIdx.x & 31;
+  Ctx<false> c(S, normal_words(smem_stack, stack_cap));
+  const uint32_t tilesX = (cam.width + 7) / 8, ntiles = tilesX * ((cam.height + 3) / 4);
+  for (;;) {
+    unsigned long long tile = 0;
+    if (lane == 0) tile = atomicAdd(work_counter, 1ull);
+    tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
+    if (tile >= ntiles) break;
+    const uint32_t x = uint32_t(tile % tilesX) * 8 + (lane & 7), y = uint32_t(tile / tilesX) * 4 + (lane >> 3);
+    if (x >= cam.width || y >= cam.height) continue;
+    float r[8];
+    eye_ray(cam.proj_inv, cam.world_view_inv, x, y, cam.width, cam.height, cam.tnear, cam.tfar, r);
+    f3 pos = mk3(r[0], r[1], r[2]);
+    const f3 dir = mk3(r[4], r[5], r[6]);
+    f3 tc = mk3(0.0f, 0.0f, 0.0f);
+    float alpha = 1.0f;
+    float4 color = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    lrt_hit h;
+    for (uint32_t layer = 0;; layer++) {
+      if (layer == kMaxLayers) {
+        c.err |= kErrLayerCap;
+        break;
+      }
+      const float wa = alpha * color.w;
+      tc = mk3(tc.x + wa * color.x, tc.y + wa * color.y, tc.z + wa * color.z);
+      alpha *= (1.0f - color.w);
+      trace_one(c, stack, blockDim.x, stack_cap, make_float4(pos.x, pos.y, pos.z, r[3]),
+                make_float4(r[4], r[5], r[6], r[7]), h);
+      const uint32_t type = h.geomId >> 24, geomId = h.geomId & 0x00FFFFFFu;
+      if (h.primId == 0xFFFFFFFFu) {
+        color = make_float4(M.background[0], M.background[1], M.background[2], M.background[3]);
+      } else if (type != LRT_TYPE_SDF_SBS_COL && type != LRT_TYPE_GRAPHICS_PRIM) {
+        const uint2 o = M.offsets[geomId];
+        const lrt_material& m = M.mats[M.ids[o.x + h.primId % o.y]];
+        color = m.type == LRT_MATERIAL_COLORED
+                    ? make_float4(m.base_color[0], m.base_color[1], m.base_color[2], m.base_color[3])
+                    : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+      }
+      pos = pos + h.t * dir;
+      if (!(alpha > 0.01f)) break;
+    }
+    const uint64_t i = uint64_t(y) * cam.width + x;
+    transparency[i] = make_float4(tc.x, tc.y, tc.z, alpha);
+    float4* out = reinterpret_cast<float4*>(gbuffer + i);
+    out[0] = make_float4(h.t, __uint_as_float(h.primId), __uint_as_float(h.instId), __uint_as_float(h.geomId));
+    out[1] = make_float4(h.coords[0], h.coords[1], h.coords[2], h.coords[3]);
+  }
+  if (c.err) atomicOr(err_word, c.err);
+}
+
 // Forward render: image[i] = Lambert shade of ray i's nearest hit.
 __global__ void __launch_bounds__(kTraceThreads) k_render_lambert(DevScene S, const float4* __restrict__ rays,
                                                                   uint64_t n, float3 light, float* __restrict__ image,
@@ -1078,6 +1142,19 @@ cudaError_t launch_render_rgba8(const DevScene& S, const DevCamera& cam, const D
                                        int(trace_smem_bytes(kMaxStackDev + 1)));
   if (e != cudaSuccess) return e;
   k_render_rgba8<<<grid, kTraceThreads, smem, stream>>>(S, cam, lights, image, work_counter, err_word, stack_cap);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill_gbuffer_transparency(const DevScene& S, const DevCamera& cam, const DevMaterials& M,
+                                             float4* transparency, lrt_hit* gbuffer, unsigned long long* work_counter,
+                                             uint32_t* err_word, uint32_t stack_cap, int grid, cudaStream_t stream)
+{
+  const size_t smem = trace_smem_bytes(stack_cap);
+  cudaError_t e = cudaFuncSetAttribute(k_fill_gbuffer_transparency, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(trace_smem_bytes(kMaxStackDev + 1)));
+  if (e != cudaSuccess) return e;
+  k_fill_gbuffer_transparency<<<grid, kTraceThreads, smem, stream>>>(S, cam, M, transparency, gbuffer, work_counter,
+                                                                     err_word, stack_cap);
   return cudaGetLastError();
 }
 

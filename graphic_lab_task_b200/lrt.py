@@ -12,7 +12,7 @@ import os
 
 import numpy as np
 
-from ._abi import (HIT_DTYPE, LIGHT_DTYPE, LRT_BATCH_NO_GRAPH, LRT_COUNTER_COUNT, LRT_TRACE_COUNT_WORK,
+from ._abi import (HIT_DTYPE, LIGHT_DTYPE, MATERIAL_DTYPE, LRT_BATCH_NO_GRAPH, LRT_COUNTER_COUNT, LRT_TRACE_COUNT_WORK,
                    LRT_TRACE_DEVICE_POINTERS, LRT_TRACE_FAST_MATH, STATUS_NAMES, BatchShape, Camera, Preset,
                    SceneArrays, TuneEntry, arrays_to_struct, parity_preset, struct_to_arrays)
 
@@ -30,6 +30,7 @@ EXPORTED = (
     "lrt_batch_update_cameras", "lrt_batch_set_shape", "lrt_batch_get_shape", "lrt_batch_trace", "lrt_batch_sync",
     "lrt_batch_autotune", "lrt_render_lambert", "lrt_adjoint_lambert_sbs", "lrt_sbs_update_values",
     "lrt_generate_bounce_rays", "lrt_generate_bounce_rays_compact", "lrt_render_rgba8", "lrt_trace_nearest_image",
+    "lrt_set_materials", "lrt_fill_gbuffer_transparency",
     "lrt_update_instance", "lrt_add_geom_sdf_frame_octree_file", "lrt_add_geom_sdf_svs_file",
     "lrt_add_geom_sdf_sbs_file", "lrt_batch_render_rgba8",
     "lrt_wl_noisy_sphere", "lrt_wl_spheres", "lrt_wl_sphere_sdf", "lrt_wl_sbs_from_spheres",
@@ -103,6 +104,8 @@ def lib():
         "lrt_trace_nearest_noalloc": [vp, vp, vp, u64, vp, u32],
         "lrt_render_lambert": [vp, vp, u64, vp, vp, vp],
         "lrt_render_rgba8": [vp, vp, vp, u32, vp, vp, vp],
+        "lrt_set_materials": [vp, vp, u32, vp, u64, vp, u32],
+        "lrt_fill_gbuffer_transparency": [vp, vp, vp, vp, vp, vp],
         "lrt_trace_nearest_image": [vp, vp, vp, u32, u32, vp, u32],
         "lrt_generate_bounce_rays": [vp, vp, vp, u64, u64, C.c_float, C.c_float, vp, vp],
         "lrt_generate_bounce_rays_compact": [vp, vp, vp, u64, u64, C.c_float, C.c_float, vp, vp, vp, vp],
@@ -332,6 +335,23 @@ class SceneRT:
         bg = (C.c_float * 4)(*[float(x) for x in background])
         self._check(lib().lrt_render_rgba8(self.h, C.byref(camera), lt.ctypes.data if len(lt) else None, len(lt), bg,
                                            C.c_void_p(image_ptr), C.c_void_p(stream) if stream else None))
+
+    def set_materials(self, materials, mat_id_by_prim_id, mat_id_offsets):
+        """MultiRenderer's m_materials (MATERIAL_DTYPE), m_matIdbyPrimId and
+        m_matIdOffsets ({start, size} per geometry), copied."""
+        m = np.ascontiguousarray(materials, dtype=MATERIAL_DTYPE)
+        ids = np.ascontiguousarray(mat_id_by_prim_id, dtype=np.uint32).reshape(-1)
+        offs = np.ascontiguousarray(mat_id_offsets, dtype=np.uint32).reshape(-1)
+        self._check(lib().lrt_set_materials(self.h, m.ctypes.data if len(m) else None, len(m),
+                                            ids.ctypes.data if len(ids) else None, len(ids),
+                                            offs.ctypes.data if len(offs) else None, len(offs) // 2))
+
+    def fill_gbuffer_transparency(self, camera, background, transparency_ptr, hits_ptr, stream=0):
+        """kernel1D_FillGbufferWithTransparency for `camera`: float4
+        {rgb, alpha} and the last hit per pixel, in device memory."""
+        bg = (C.c_float * 4)(*[float(x) for x in background])
+        self._check(lib().lrt_fill_gbuffer_transparency(self.h, C.byref(camera), bg, C.c_void_p(transparency_ptr),
+                                                        C.c_void_p(hits_ptr), C.c_void_p(stream) if stream else None))
 
     def adjoint_lambert(self, rays_ptr, n, light, dimage_ptr, grad_ptr, stream=0):
         L = (C.c_float * 3)(*[float(x) for x in light])

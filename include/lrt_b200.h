@@ -149,6 +149,7 @@ typedef struct lrt_preset {
 #define LRT_TYPE_SDF_SBS 6u
 #define LRT_TYPE_SDF_SBS_TEX 10u
 #define LRT_TYPE_SDF_SBS_COL 11u
+#define LRT_TYPE_GRAPHICS_PRIM 17u
 #define LRT_TAG_NONE 0u            /* MultiRenderer/BVH2Common.h:30-43 */
 #define LRT_TAG_TRIANGLE 1u
 #define LRT_TAG_SDF_BRICK 4u
@@ -456,6 +457,41 @@ enum { LRT_LIGHT_DIRECT = 0, LRT_LIGHT_POINT = 1, LRT_LIGHT_AMBIENT = 2 };
  * G-buffer); the node solver must be ST or BBOX. */
 lrt_status lrt_render_rgba8(lrt_scene* scene, const lrt_camera* camera, const lrt_light* lights,
                             uint32_t light_count, const float background[4], uint32_t* image_dev, void* stream);
+
+/* MultiRendererMaterial (core/IRenderer.h:31-38), 32 bytes. */
+typedef struct lrt_material {
+  uint32_t type; /* MULTI_RENDER_MATERIAL_TYPE_*, core/IRenderer.h:21-22 */
+  uint32_t texId;
+  float metallic;
+  float roughness;
+  float base_color[4];
+} lrt_material;
+enum { LRT_MATERIAL_COLORED = 0, LRT_MATERIAL_TEXTURED = 1 };
+
+/* The renderer's materials (MultiRenderer::m_materials, m_matIdbyPrimId,
+ * m_matIdOffsets: MultiRenderer.h:255-258), copied to the device: primitive
+ * p of geometry g has material mat_id_by_prim_id[start_g + p % size_g] with
+ * {start_g, size_g} = mat_id_offsets[2g .. 2g+1].  Every id must name a
+ * material and every range lie inside mat_id_by_prim_id
+ * (LRT_ERR_INVALID_ARGUMENT otherwise); a count of 0 clears them. */
+lrt_status lrt_set_materials(lrt_scene* scene, const lrt_material* materials, uint32_t material_count,
+                             const uint32_t* mat_id_by_prim_id, uint64_t mat_id_count, const uint32_t* mat_id_offsets,
+                             uint32_t offset_count);
+
+/* MultiRenderer::kernel1D_FillGbufferWithTransparency with AnyHit
+ * (MultiRenderer.cpp:204-246), one sample of `camera`: per pixel the loop of
+ * nearest hits that composites COLORED materials' base colours front to back
+ * (misses take `background`; SBS_COL and graphics-primitive hits keep the
+ * previous colour, as in the reference) until the remaining alpha is at most
+ * 0.01, each ray restarting at the previous hit point.  Writes the float4
+ * {rgb, alpha} to transparency_dev and the last hit to hits_dev (row-major
+ * pixels, device memory); asynchronous on `stream`.  Every mesh geometry of
+ * the scene needs a material range of size >= 1.  The reference's loop has
+ * no bound; here a pixel stops after LRT_MAX_TRANSPARENCY_LAYERS traces and
+ * lrt_trace_sync(stream) reports LRT_ERR_DEVICE_LIMIT. */
+#define LRT_MAX_TRANSPARENCY_LAYERS 256
+lrt_status lrt_fill_gbuffer_transparency(lrt_scene* scene, const lrt_camera* camera, const float background[4],
+                                         float* transparency_dev, lrt_hit* hits_dev, void* stream);
 
 /* Adjoint of lrt_render_lambert with respect to the scene's SBS float values
  * (the sdfSBSDataF array of the indexed layouts): grad_dev[j] +=

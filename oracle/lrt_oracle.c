@@ -1029,3 +1029,66 @@ void lrto_render_rgba8(const lrt_scene_arrays* arrays, const lrt_preset* preset,
     image[i] = tonemap_rgba8(fc.x, fc.y, fc.z, 1.0f);
   }
 }
+
+/* MultiRenderer::AnyHit (MultiRenderer.cpp:223-246) as
+ * kernel1D_FillGbufferWithTransparency (:204-221) calls it per eye ray:
+ * nearest hits composited front to back, each trace restarting at the
+ * previous hit point; offsets are {start, size} per geometry.  The loop is
+ * the reference's, bounded by max_layers traces (the reference has no bound);
+ * returns how many rays reached that bound. */
+uint64_t lrto_fill_gbuffer_transparency(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* rays,
+                                        uint64_t n, const lrt_material* materials, const uint32_t* mat_ids,
+                                        const uint32_t* mat_offsets, const float background[4], uint32_t max_layers,
+                                        float* transparency, lrt_hit* hits, int threads)
+{
+  uint64_t capped = 0;
+  (void)threads;
+#ifdef _OPENMP
+#pragma omp parallel for num_threads(threads > 0 ? threads : 1) schedule(dynamic, 256) reduction(+ : capped)
+#endif
+  for (int64_t i = 0; i < (int64_t)n; i++) {
+    uint64_t cnt[LRT_COUNTER_COUNT];
+    ctx_t c = {arrays, preset, cnt, 0, NULL, 0};
+    const float* r = rays + 8 * i;
+    float pn[4] = {r[0], r[1], r[2], r[3]};
+    f3 tc = mk3(0, 0, 0);
+    float alpha = 1.0f;
+    float color[4] = {0, 0, 0, 0};
+    lrt_hit h;
+    uint32_t layer = 0;
+    do {
+      if (layer++ == max_layers) {
+        capped++;
+        break;
+      }
+      /* transparencyColor += alpha * color.w * to_float3(color) */
+      const float wa = alpha * color[3];
+      tc = mk3(tc.x + wa * color[0], tc.y + wa * color[1], tc.z + wa * color[2]);
+      alpha *= (1.0f - color[3]);
+      h = nearest_hit(&c, pn, r + 4);
+      const uint32_t type = h.geomId >> 24, geomId = h.geomId & 0x00FFFFFFu;
+      if (h.primId == 0xFFFFFFFFu) {
+        memcpy(color, background, sizeof(color));
+      } else if (type != LRT_TYPE_SDF_SBS_COL && type != LRT_TYPE_GRAPHICS_PRIM) {
+        const uint32_t matId = mat_ids[mat_offsets[2 * geomId] + h.primId % mat_offsets[2 * geomId + 1]];
+        const lrt_material* m = &materials[matId];
+        if (m->type == LRT_MATERIAL_COLORED) {
+          memcpy(color, m->base_color, sizeof(color));
+        } else {
+          color[0] = color[1] = color[2] = 0.0f;
+          color[3] = 1.0f;
+        }
+      }
+      /* rayPos = to_float3(rayPosAndNear) + to_float3(rayDirAndFar) * hit->t */
+      pn[0] = pn[0] + r[4] * h.t;
+      pn[1] = pn[1] + r[5] * h.t;
+      pn[2] = pn[2] + r[6] * h.t;
+    } while (alpha > 0.01f);
+    transparency[4 * i + 0] = tc.x;
+    transparency[4 * i + 1] = tc.y;
+    transparency[4 * i + 2] = tc.z;
+    transparency[4 * i + 3] = alpha;
+    hits[i] = h;
+  }
+  return capped;
+}

@@ -226,6 +226,36 @@ def port_render_rgba8(arrays, rays, lights, background, preset=None, threads=os.
     return img
 
 
+def port_fill_gbuffer_transparency(arrays, rays, materials, mat_ids, mat_offsets, background, max_layers=256,
+                                   preset=None, threads=os.cpu_count()):
+    """AnyHit's transparency loop per eye ray (rays: row-major pixels).
+    Returns (transparency float4 per ray, last hits, rays that hit the layer bound)."""
+    from graphic_lab_task_b200._abi import MATERIAL_DTYPE
+    lib = port_lib()
+    if not hasattr(lib, "_transp_bound"):
+        lib.lrto_fill_gbuffer_transparency.restype = C.c_uint64
+        lib.lrto_fill_gbuffer_transparency.argtypes = [C.POINTER(SceneArrays), C.POINTER(Preset), C.c_void_p,
+                                                       C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                       C.c_uint32, C.c_void_p, C.c_void_p, C.c_int]
+        lib._transp_bound = True
+    s, keep = arrays_to_struct(arrays)
+    p = preset if preset is not None else parity_preset()
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    mats = np.ascontiguousarray(materials, dtype=MATERIAL_DTYPE)
+    ids = np.ascontiguousarray(mat_ids, dtype=np.uint32)
+    offs = np.ascontiguousarray(mat_offsets, dtype=np.uint32).reshape(-1)
+    bg = np.ascontiguousarray(background, dtype=np.float32)
+    transp = np.zeros((len(rays), 4), np.float32)
+    hits = np.zeros(len(rays), HIT_DTYPE)
+    capped = lib.lrto_fill_gbuffer_transparency(C.byref(s), C.byref(p), rays.ctypes.data, len(rays),
+                                                mats.ctypes.data if len(mats) else None,
+                                                ids.ctypes.data if len(ids) else None,
+                                                offs.ctypes.data if len(offs) else None, bg.ctypes.data,
+                                                int(max_layers), transp.ctypes.data, hits.ctypes.data, int(threads))
+    del keep
+    return transp, hits, int(capped)
+
+
 def port_adjoint_fp64(arrays, rays, light, dimage, preset=None):
     """FP64 adjoint of the Lambert render w.r.t. the SBS float values."""
     port_render_lambert(arrays, np.zeros((0, 8), np.float32), light, preset)  # binds the signatures

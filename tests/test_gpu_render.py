@@ -6,8 +6,9 @@ import numpy as np
 import pytest
 
 import pyoracle as po
-from graphic_lab_task_b200 import (LIGHT_AMBIENT, LIGHT_DIRECT, LIGHT_DTYPE, LIGHT_POINT, LrtError, SceneRT,
-                                   parity_preset, workloads as wl)
+from graphic_lab_task_b200 import (HIT_DTYPE, LIGHT_AMBIENT, LIGHT_DIRECT, LIGHT_DTYPE, LIGHT_POINT, LrtError,
+                                   SceneRT, parity_preset, workloads as wl)
+from helpers import bit_equal
 
 pytestmark = pytest.mark.gpu
 
@@ -93,3 +94,60 @@ def test_batched_render_equals_per_camera_render(cuda):
         off += k
     assert len(np.unique(got)) > 100
     b.close()
+
+
+def test_fill_gbuffer_transparency_matches_oracle(cuda):
+    """kernel1D_FillGbufferWithTransparency on the device: the composited
+    float4 and the last hit of every pixel are bit-identical to the oracle's
+    AnyHit loop."""
+    torch = cuda
+    from test_oracle import transparency_tables
+    sc = _mixed_scene()
+    a = sc.export_arrays()
+    mats, ids, offs = transparency_tables(len(a["geomData"]), seed=3)
+    sc.set_materials(mats, ids, offs)
+    cam = wl.camera((0.5, 0.7, 3.5), width=200, height=150)
+    bg = np.array([0.1, 0.2, 0.3, 1.0], np.float32)
+    n = cam.width * cam.height
+    tr = torch.zeros(n * 4, dtype=torch.float32, device="cuda")
+    hits = torch.zeros(n * 8, dtype=torch.float32, device="cuda")
+    sc.fill_gbuffer_transparency(cam, bg, tr.data_ptr(), hits.data_ptr())
+    sc.sync()
+    got_t = tr.cpu().numpy().reshape(-1, 4)
+    got_h = hits.cpu().numpy().view(HIT_DTYPE).reshape(-1)
+    want_t, want_h, capped = po.port_fill_gbuffer_transparency(a, wl.eye_rays_host(cam), mats, ids, offs, bg)
+    assert capped == 0
+    same = (got_t.view(np.uint32) == want_t.view(np.uint32)).all(axis=1) & bit_equal(got_h, want_h)
+    assert same.all(), "%d of %d pixels differ" % ((~same).sum(), n)
+    assert (got_t[:, 3] < 0.99).sum() > 500  # composited layers
+
+
+def test_fill_gbuffer_transparency_refusals_and_layer_bound(cuda):
+    torch = cuda
+    from test_oracle import transparency_tables
+    sc = _mixed_scene()
+    cam = wl.camera((0.5, 0.7, 3.5), width=32, height=32)
+    tr = torch.zeros(32 * 32 * 4, dtype=torch.float32, device="cuda")
+    hits = torch.zeros(32 * 32 * 8, dtype=torch.float32, device="cuda")
+    bg = (0.1, 0.2, 0.3, 1.0)
+    with pytest.raises(LrtError) as e:  # no materials for the mesh
+        sc.fill_gbuffer_transparency(cam, bg, tr.data_ptr(), hits.data_ptr())
+    assert e.value.status == 1 and "material range" in str(e.value)
+    mats, ids, offs = transparency_tables(4)
+    bad = ids.copy()
+    bad[0] = len(mats)
+    with pytest.raises(LrtError) as e:
+        sc.set_materials(mats, bad, offs)
+    assert e.value.status == 1
+    with pytest.raises(LrtError) as e:
+        sc.set_materials(mats, ids, offs + np.array([0, 1000], np.uint32))
+    assert e.value.status == 1
+    # a transparent background never brings alpha down: the reference loops
+    # forever on rays that miss; here they stop at the layer bound
+    sc.set_materials(mats, ids, offs)
+    sc.fill_gbuffer_transparency(cam, (0.1, 0.2, 0.3, 0.0), tr.data_ptr(), hits.data_ptr())
+    with pytest.raises(LrtError) as e:
+        sc.sync()
+    assert e.value.status == 5 and "transparency" in str(e.value)
+    sc.fill_gbuffer_transparency(cam, bg, tr.data_ptr(), hits.data_ptr())
+    sc.sync()

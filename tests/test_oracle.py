@@ -96,3 +96,60 @@ def test_port_matches_reference_for_every_node_solver(solver):
     got = po.port_trace(ref.export(), rays, preset=p)
     assert (want["primId"] != MISS).sum() > 500
     assert bit_equal(got, want).all(), hit_summary(got, want)
+
+
+def transparency_tables(n_geoms_needing, prim_range=64, seed=0):
+    """Materials for the transparency loop: four colours of different alpha,
+    a textured one (composited as opaque black) and an opaque one; geometry g
+    gets its own range of random material ids."""
+    from graphic_lab_task_b200 import MATERIAL_COLORED, MATERIAL_DTYPE, MATERIAL_TEXTURED
+    mats = np.zeros(6, MATERIAL_DTYPE)
+    for k, (rgb, a) in enumerate([((1, 0, 0), 0.5), ((0, 1, 0), 0.3), ((0, 0, 1), 0.8), ((1, 1, 1), 0.05)]):
+        mats[k] = (MATERIAL_COLORED, 0, 0.0, 0.5, (*rgb, a))
+    mats[4] = (MATERIAL_TEXTURED, 3, 0.0, 0.5, (1, 1, 1, 1))
+    mats[5] = (MATERIAL_COLORED, 0, 0.0, 0.5, (1, 1, 0, 1.0))
+    rng = np.random.default_rng(seed)
+    ids, offs = [], []
+    for g in range(n_geoms_needing):
+        size = int(rng.integers(1, prim_range))
+        offs.append((len(ids), size))
+        ids.extend(rng.choice([0, 1, 2, 3, 3, 3, 4, 5], size).tolist())
+    return mats, np.array(ids, np.uint32), np.array(offs, np.uint32)
+
+
+def test_transparency_loop_matches_its_statement():
+    """The oracle's AnyHit loop (MultiRenderer.cpp:223-246) against the same
+    loop written here over the oracle's nearest hit, ray by ray, in float32."""
+    from test_builder import build_mixed
+    sc, _ = build_mixed(seed=1)
+    a = sc.export_arrays()
+    mats, ids, offs = transparency_tables(len(a["geomData"]))
+    bg = np.array([0.1, 0.2, 0.3, 1.0], np.float32)
+    rays = wl.eye_rays_host(wl.camera((0.3, 0.9, 3.2), width=24, height=18))
+    got_t, got_h, capped = po.port_fill_gbuffer_transparency(a, rays, mats, ids, offs, bg, threads=1)
+    assert capped == 0
+    f32 = np.float32
+    for i, r in enumerate(rays):
+        pn = r[:4].copy()
+        tc = np.zeros(3, f32)
+        alpha = f32(1)
+        color = np.zeros(4, f32)
+        while True:
+            wa = f32(alpha * color[3])
+            tc = (tc + wa * color[:3]).astype(f32)
+            alpha = f32(alpha * f32(f32(1) - color[3]))
+            h = po.port_trace(a, np.concatenate([pn, r[4:]])[None, :], threads=1)[0]
+            typ, gid = int(h["geomId"]) >> 24, int(h["geomId"]) & 0xFFFFFF
+            if h["primId"] == MISS:
+                color = bg.copy()
+            elif typ not in (11, 17):
+                m = mats[ids[offs[gid][0] + int(h["primId"]) % offs[gid][1]]]
+                color = m["base_color"].astype(f32) if m["type"] == 0 else np.array([0, 0, 0, 1], f32)
+            pn[:3] = (pn[:3] + r[4:7] * f32(h["t"])).astype(f32)
+            if not alpha > f32(0.01):
+                break
+        want = np.array([*tc, alpha], f32)
+        assert got_t[i].view(np.uint32).tolist() == want.view(np.uint32).tolist(), (i, got_t[i], want)
+        assert bit_equal(got_h[i:i + 1], h.reshape(1)).all()
+    # several layers on some rays: the loop composited more than one surface
+    assert (got_t[:, 3] < 0.99).sum() > 20 and np.unique(got_t[:, :3].round(4), axis=0).shape[0] > 10
