@@ -244,8 +244,10 @@ def run_ours(args, rank, world, local_rank):
     sc.generate_eye_rays(cam, rays.data_ptr(), sp)
     # The rays are one camera's image in row-major order; the timed call is
     # lrt_trace_nearest_image, which hands each warp an 8x4-pixel tile (as the
-    # reference's kernel1D_FillGbuffer walks packed tiles) and returns the
-    # hits lrt_trace_nearest returns; the row-order call is timed beside it.
+    # reference's kernel1D_FillGbuffer walks packed tiles), starting with the
+    # tiles the previous launch on the stream found slowest, and returns the
+    # hits lrt_trace_nearest returns; the row-order call and the image call
+    # in plain tile order are timed beside it.
     # counting pass (untimed): algorithmic bytes of one launch
     sc.trace_image(rays.data_ptr(), hits.data_ptr(), WIDTH, HEIGHT, stream=sp, count_work=True)
     sc.sync(stream=sp, read_counters=True)
@@ -282,6 +284,16 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize(dev)
     sc.sync(stream=sp)
     row_ms = [starts[i].elapsed_time(ends[i]) for i in range(min(args.steps, 50))]
+    # the image-order call with its tiles in plain row order (no longest-first
+    # schedule from the previous launch)
+    for i in range(min(args.steps, 50)):
+        flush.zero_()
+        starts[i].record(stream)
+        sc.trace_image(rays.data_ptr(), hits.data_ptr(), WIDTH, HEIGHT, stream=sp, natural_order=True)
+        ends[i].record(stream)
+    torch.cuda.synchronize(dev)
+    sc.sync(stream=sp)
+    nat_ms = [starts[i].elapsed_time(ends[i]) for i in range(min(args.steps, 50))]
     # end to end through the public API with pinned host buffers
     host_rays = torch.empty(n * 8, dtype=torch.float32, pin_memory=True)
     host_rays.copy_(rays.cpu())
@@ -334,6 +346,10 @@ def run_ours(args, rank, world, local_rank):
                 "call": "lrt_trace_nearest, pinned host buffers (chunked copy/trace/copy pipeline)"},
         "row_order": {"ms_per_step": sum(row_ms) / len(row_ms), "value": n / (sum(row_ms) / len(row_ms)) / 1e3,
                       "unit": "Mrays/s", "call": "lrt_trace_nearest (same rays, 32 consecutive rays per warp)"},
+        "natural_tile_order": {"ms_per_step": sum(nat_ms) / len(nat_ms),
+                               "value": n / (sum(nat_ms) / len(nat_ms)) / 1e3, "unit": "Mrays/s",
+                               "call": "lrt_trace_nearest_image with LRT_TRACE_NATURAL_ORDER (tiles in row order, "
+                                       "no longest-first schedule from the previous launch)"},
         "clocks": clk,
         # our kernels in the device-timed region: one k_trace per step (the L2
         # flush between steps is torch's); the e2e region's are under "e2e"

@@ -153,9 +153,14 @@ lrt_status lrt_render_rgba8(lrt_scene* s, const lrt_camera* camera, const lrt_li
   DeviceScene* d = s->dev;
   const uint64_t tiles = uint64_t((cam.width + 7) / 8) * ((cam.height + 3) / 4);
   const int grid = int(std::min<uint64_t>(uint64_t(d->grid), (tiles * 32 + kTraceThreads - 1) / kTraceThreads));
-  const cudaError_t e =
-      lrt_exact::launch_render_rgba8(S, cam, L, image_dev, &slot->work, &slot->err, d->stackCap, grid, stream);
-  return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "render launch");
+  const uint32_t* rd = nullptr;
+  uint32_t* wr = nullptr;
+  if ((st = sched_prepare(s, stream, cam.width, cam.height, false, &rd, &wr)) != LRT_OK) return st;
+  const cudaError_t e = lrt_exact::launch_render_rgba8(S, cam, L, image_dev, &slot->work, &slot->err, d->stackCap,
+                                                       grid, stream, rd, wr);
+  if (e != cudaSuccess) return cuda_fail(s, e, "render launch");
+  sched_commit(s, stream, false);
+  return LRT_OK;
 }
 
 lrt_status lrt_set_materials(lrt_scene* s, const lrt_material* materials, uint32_t material_count,
@@ -240,10 +245,15 @@ lrt_status lrt_fill_gbuffer_transparency(lrt_scene* s, const lrt_camera* camera,
   std::memcpy(M.background, background, sizeof(M.background));
   const uint64_t tiles = uint64_t((cam.width + 7) / 8) * ((cam.height + 3) / 4);
   const int grid = int(std::min<uint64_t>(uint64_t(d->grid), (tiles * 32 + kTraceThreads - 1) / kTraceThreads));
-  const cudaError_t e = lrt_exact::launch_fill_gbuffer_transparency(S, cam, M, reinterpret_cast<float4*>(transparency_dev),
-                                                                    hits_dev, &slot->work, &slot->err, d->stackCap,
-                                                                    grid, stream);
-  return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "transparency launch");
+  const uint32_t* rd = nullptr;
+  uint32_t* wr = nullptr;
+  if ((st = sched_prepare(s, stream, cam.width, cam.height, false, &rd, &wr)) != LRT_OK) return st;
+  const cudaError_t e = lrt_exact::launch_fill_gbuffer_transparency(
+      S, cam, M, reinterpret_cast<float4*>(transparency_dev), hits_dev, &slot->work, &slot->err, d->stackCap, grid,
+      stream, rd, wr);
+  if (e != cudaSuccess) return cuda_fail(s, e, "transparency launch");
+  sched_commit(s, stream, false);
+  return LRT_OK;
 }
 
 lrt_status lrt_render_lambert(lrt_scene* s, const float* rays_dev, uint64_t n, const float light[3], float* image_dev,

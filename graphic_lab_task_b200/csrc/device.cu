@@ -85,8 +85,53 @@ lrt_status slot_for(lrt_scene* s, cudaStream_t stream, StreamSlot** out)
   return LRT_OK;
 }
 
+} // namespace
+
+lrt_status sched_prepare(lrt_scene* s, cudaStream_t stream, uint32_t width, uint32_t height, bool natural,
+                         const uint32_t** rd, uint32_t** wr)
+{
+  *rd = nullptr;
+  *wr = nullptr;
+  if (natural) return LRT_OK;
+  DeviceScene* d = s->dev;
+  ImageSchedule& q = d->sched[stream];
+  const uint64_t tiles = uint64_t((width + kImgTileW - 1) / kImgTileW) * ((height + kImgTileH - 1) / kImgTileH);
+  const size_t clear = (kSchedHeader + (tiles + 31) / 32) * sizeof(uint32_t); // header + bitmap
+  cudaError_t e = cudaSuccess;
+  if (q.w != width || q.h != height) {
+    for (uint32_t*& b : q.buf) {
+      cudaFree(b);
+      b = nullptr;
+    }
+    q.w = q.h = 0;
+    for (uint32_t*& b : q.buf) {
+      if (e == cudaSuccess) e = cudaMalloc(&b, sched_words(tiles) * sizeof(uint32_t));
+      if (e == cudaSuccess) e = cudaMemsetAsync(b, 0, clear, stream);
+    }
+    if (e != cudaSuccess) return cuda_fail(s, e, "tile schedule buffers");
+    q.w = width;
+    q.h = height;
+    q.rd = 0;
+  }
+  e = cudaMemsetAsync(q.buf[1 - q.rd], 0, clear, stream);
+  if (e != cudaSuccess) return cuda_fail(s, e, "cudaMemsetAsync");
+  *rd = q.buf[q.rd];
+  *wr = q.buf[1 - q.rd];
+  return LRT_OK;
+}
+
+void sched_commit(lrt_scene* s, cudaStream_t stream, bool natural)
+{
+  if (natural) return;
+  ImageSchedule& q = s->dev->sched[stream];
+  q.rd = 1 - q.rd;
+}
+
+namespace {
+
 // img_w > 0: the n = img_w * img_h rays are an image in row-major order,
-// traced in 8x4-pixel tiles.
+// traced in 8x4-pixel tiles, in the stream's tile schedule unless flags has
+// LRT_TRACE_NATURAL_ORDER (or LRT_TRACE_COUNT_WORK).
 lrt_status launch(lrt_scene* s, const float4* rays, lrt_hit* hits, uint64_t n, cudaStream_t stream, uint32_t flags,
                   StreamSlot* slot, uint32_t img_w = 0, uint32_t img_h = 0)
 {
@@ -101,13 +146,19 @@ lrt_status launch(lrt_scene* s, const float4* rays, lrt_hit* hits, uint64_t n, c
   const uint64_t warps = img_w ? uint64_t((img_w + kImgTileW - 1) / kImgTileW) * ((img_h + kImgTileH - 1) / kImgTileH)
                                : (n + 31) / 32;
   const int grid = int(std::min<uint64_t>(uint64_t(d->grid), (warps * 32 + kTraceThreads - 1) / kTraceThreads));
+  const bool natural = !img_w || count || (flags & LRT_TRACE_NATURAL_ORDER);
+  const uint32_t* rd = nullptr;
+  uint32_t* wr = nullptr;
+  lrt_status st = sched_prepare(s, stream, img_w, img_h, natural, &rd, &wr);
+  if (st != LRT_OK) return st;
   if (flags & LRT_TRACE_FAST_MATH)
     e = lrt_fast::launch_trace(S, rays, hits, n, &slot->work, slot->counters, &slot->err, d->stackCap, grid, stream,
-                               count, img_w, img_h);
+                               count, img_w, img_h, rd, wr);
   else
     e = lrt_exact::launch_trace(S, rays, hits, n, &slot->work, slot->counters, &slot->err, d->stackCap, grid,
-                                stream, count, img_w, img_h);
+                                stream, count, img_w, img_h, rd, wr);
   if (e != cudaSuccess) return cuda_fail(s, e, "trace launch");
+  sched_commit(s, stream, natural);
   return LRT_OK;
 }
 

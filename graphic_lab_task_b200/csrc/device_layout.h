@@ -26,6 +26,12 @@ namespace lrt {
 constexpr int kTraceThreads = 128;
 // pixels of the tile one warp traces in lrt_trace_nearest_image (32 in all)
 constexpr uint32_t kImgTileW = 8, kImgTileH = 4;
+
+// Tile schedule of the image-order launches (one per stream and image size,
+// two buffers used alternately): a header {count, maxCost, 0, 0}, a bitmap
+// of the listed tiles, then the list of expensive tiles.
+constexpr uint32_t kSchedHeader = 4;
+inline __host__ __device__ uint64_t sched_words(uint64_t tiles) { return kSchedHeader + (tiles + 31) / 32 + tiles; }
 // Per-thread shared-memory words after the traversal stack: the inputs of the
 // deferred SDF normal (sign, sample point, 8 corner values).
 constexpr uint32_t kNormalWords = 12;

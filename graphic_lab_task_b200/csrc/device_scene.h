@@ -31,6 +31,16 @@ constexpr uint64_t kPipeChunk = 262144;   // 8 MiB of rays in, 8 MiB of hits out
 constexpr uint64_t kPipeChunkMin = 32768; // first and last chunks
 constexpr uint64_t kPipeMinRays = 262144;
 
+// Tile schedule of the image-order launches on one stream (sched_next in
+// trace_impl.cuh): two device buffers of sched_words(tiles) words for a
+// width x height image, the one the next launch reads being buf[rd]; the
+// other is cleared and written by that launch.
+struct ImageSchedule {
+  uint32_t w = 0, h = 0;
+  uint32_t* buf[2] = {nullptr, nullptr};
+  int rd = 0;
+};
+
 struct DeviceScene {
   std::vector<void*> allocs;
   DevScene S{};
@@ -52,6 +62,7 @@ struct DeviceScene {
   uint32_t* matIds = nullptr;
   uint2* matOffsets = nullptr;
   uint64_t matVersion = 0;
+  std::map<cudaStream_t, ImageSchedule> sched; // per stream of image-order launches
   // staging buffers for host-pointer calls
   float4* rays = nullptr;
   lrt_hit* hits = nullptr;
@@ -76,11 +87,20 @@ struct DeviceScene {
     if (mats) cudaFree(mats);
     if (matIds) cudaFree(matIds);
     if (matOffsets) cudaFree(matOffsets);
+    for (auto& kv : sched)
+      for (uint32_t* b : kv.second.buf) cudaFree(b);
   }
 };
 
 // device.cu
 uint32_t preset_flags(const lrt_preset& p);
+// The schedule buffers of the next image-order launch of a width x height
+// image on `stream` (allocated, or reset when the size changed, on first
+// use); *rd = *wr = nullptr when `natural` asks for plain tile order.  The
+// caller launches, then calls sched_commit.
+lrt_status sched_prepare(lrt_scene* s, cudaStream_t stream, uint32_t width, uint32_t height, bool natural,
+                         const uint32_t** rd, uint32_t** wr);
+void sched_commit(lrt_scene* s, cudaStream_t stream, bool natural);
 uint32_t launch_flags(const lrt_scene* s); // preset flags + the uploaded scene's own
 lrt_status cuda_fail(lrt_scene* s, cudaError_t e, const char* what);
 

@@ -9,7 +9,8 @@
   cudaError_t launch_trace(const lrt::DevScene& S, const float4* rays, lrt_hit* hits, uint64_t n,               \
                            unsigned long long* work_counter, unsigned long long* counters, uint32_t* err_word,  \
                            uint32_t stack_cap, int grid, cudaStream_t stream, bool count, uint32_t img_w = 0,   \
-                           uint32_t img_h = 0);                                                                 \
+                           uint32_t img_h = 0, const uint32_t* sched_rd = nullptr,                              \
+                           uint32_t* sched_wr = nullptr);                                                                 \
   cudaError_t set_trace_smem(uint32_t stack_cap);                                                               \
   cudaError_t trace_occupancy(uint32_t stack_cap, int* blocks_per_sm);                                          \
   cudaError_t launch_eye_rays(const lrt::DevCamera& cam, float4* rays, cudaStream_t stream);                    \
@@ -21,11 +22,14 @@
   cudaError_t cameras_occupancy(uint32_t stack_cap, int* blocks_per_sm);                                        \
   cudaError_t launch_render_rgba8(const lrt::DevScene& S, const lrt::DevCamera& cam, const lrt::DevLights& lights,\
                                   uint32_t* image, unsigned long long* work_counter, uint32_t* err_word,        \
-                                  uint32_t stack_cap, int grid, cudaStream_t stream);                           \
+                                  uint32_t stack_cap, int grid, cudaStream_t stream,                            \
+                                  const uint32_t* sched_rd = nullptr, uint32_t* sched_wr = nullptr);            \
   cudaError_t launch_fill_gbuffer_transparency(const lrt::DevScene& S, const lrt::DevCamera& cam,               \
                                                const lrt::DevMaterials& M, float4* transparency, lrt_hit* gbuffer,\
                                                unsigned long long* work_counter, uint32_t* err_word,            \
-                                               uint32_t stack_cap, int grid, cudaStream_t stream);              \
+                                               uint32_t stack_cap, int grid, cudaStream_t stream,               \
+                                               const uint32_t* sched_rd = nullptr,                              \
+                                               uint32_t* sched_wr = nullptr);                                   \
   cudaError_t launch_render_lambert(const lrt::DevScene& S, const float4* rays, uint64_t n, float3 light,       \
                                     float* image, unsigned long long* work_counter, uint32_t* err_word,         \
                                     uint32_t stack_cap, int grid, cudaStream_t stream);                         \

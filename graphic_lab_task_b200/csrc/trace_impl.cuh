@@ -715,6 +715,58 @@ __device__ void trace_one(CTX& c, uint32_t* stack, uint32_t stride, uint32_t cap
   if (hit.primId != 0xFFFFFFFFu) c.inc(kCntHits);
 }
 
+// Longest-first order of the tiles of an image-order launch.  With the
+// schedule of the previous same-size launch on its stream (rd), a launch
+// first takes the tiles that launch listed as expensive (in the order it
+// finished them), then every other tile in natural order; each tile's
+// duration is measured on lane 0 and those of at least a quarter of the
+// previous launch's longest go to the list for the next launch (wr).  Only
+// which warp traces which tile, and when, depends on it.  rd == nullptr:
+// natural order; wr == nullptr: nothing recorded.  The per-warp state lives
+// in shared memory so that the traversal keeps its registers.
+struct WarpClock {
+  long long start;  // clock64 when the warp took its current tile
+  uint32_t tile;    // that tile, ~0u before the first
+  uint32_t longest; // longest tile this warp has reported
+};
+
+// lane 0, after the warp has finished its current tile (if any): records
+// that tile's duration and returns the next tile of `tiles`, ~0u when none
+// is left.
+__device__ __forceinline__ uint32_t sched_next(const uint32_t* __restrict__ rd, uint32_t* wr, uint32_t tiles,
+                                               unsigned long long* counter, WarpClock& wc)
+{
+  if (wr && wc.tile != ~0u) {
+    const long long dt = (clock64() - wc.start) >> 4;
+    const uint32_t cost = uint32_t(dt < 0xFFFFFFFFll ? dt : 0xFFFFFFFFll);
+    if (cost > wc.longest) {
+      wc.longest = cost;
+      atomicMax(wr + 1, cost);
+    }
+    const uint32_t thr = rd ? __ldg(rd + 1) / 4 : 0u;
+    if (thr && cost >= thr) {
+      const uint32_t slot = atomicAdd(wr, 1u);
+      if (slot < tiles) wr[kSchedHeader + (tiles + 31) / 32 + slot] = wc.tile;
+      atomicOr(wr + kSchedHeader + (wc.tile >> 5), 1u << (wc.tile & 31));
+    }
+  }
+  const uint32_t nHard = rd ? min(__ldg(rd), tiles) : 0u;
+  for (;;) {
+    const unsigned long long k = atomicAdd(counter, 1ull);
+    uint32_t tile;
+    if (k < nHard) {
+      tile = __ldg(rd + kSchedHeader + (tiles + 31) / 32 + k);
+      if (tile >= tiles) continue; // a listed tile is always inside the image
+    } else {
+      if (k - nHard >= tiles) return wc.tile = ~0u;
+      tile = uint32_t(k - nHard);
+      if (nHard && ((__ldg(rd + kSchedHeader + (tile >> 5)) >> (tile & 31)) & 1u)) continue; // listed: taken above
+    }
+    wc.start = clock64();
+    return wc.tile = tile;
+  }
+}
+
 // One thread per ray; warps fetch 32-ray batches from a global counter
 // (persistent grid of ~one wave).  Stacks live in shared memory,
 // stack[i * blockDim + tid].
@@ -723,28 +775,44 @@ __device__ void trace_one(CTX& c, uint32_t* stack, uint32_t stride, uint32_t cap
 // order and a warp's 32 rays are an 8x4-pixel tile instead of 32 pixels of a
 // row (the reference's kernel1D_FillGbuffer also walks pixels in packed
 // tiles, MultiRenderer.cpp:185-202); each ray's hit is unchanged.
-template <bool COUNT, bool SOLVERS>
+template <bool COUNT, bool SOLVERS, bool IMG>
 __global__ void __launch_bounds__(kTraceThreads, 7) k_trace(DevScene S, const float4* __restrict__ rays,
                                                          lrt_hit* __restrict__ hits, uint64_t n,
                                                          unsigned long long* __restrict__ work_counter,
                                                          unsigned long long* __restrict__ counters,
                                                          uint32_t* __restrict__ err_word, uint32_t stack_cap,
-                                                         uint32_t img_w, uint32_t img_h)
+                                                         uint32_t img_w, uint32_t img_h,
+                                                         const uint32_t* __restrict__ sched_rd, uint32_t* sched_wr)
 {
   extern __shared__ uint32_t smem_stack[];
   uint32_t* stack = smem_stack + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
   Ctx<COUNT, false, SOLVERS> c(S, normal_words(smem_stack, stack_cap));
+  __shared__ WarpClock wclock[IMG ? kTraceThreads / 32 : 1];
   const uint64_t tilesX = (uint64_t(img_w) + kImgTileW - 1) / kImgTileW;
-  const uint64_t slots = img_w ? tilesX * ((uint64_t(img_h) + kImgTileH - 1) / kImgTileH) * 32 : n; // ray slots
+  if (IMG && lane == 0) {
+    wclock[threadIdx.x >> 5].tile = ~0u;
+    wclock[threadIdx.x >> 5].longest = 0;
+  }
   for (;;) {
     unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(work_counter, 32ull);
-    base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    if (base >= slots) break;
+    if (IMG) { // work counter in tiles
+      __syncwarp();
+      uint32_t tile = 0;
+      if (lane == 0)
+        tile = sched_next(sched_rd, sched_wr, uint32_t(tilesX * ((img_h + kImgTileH - 1) / kImgTileH)), work_counter,
+                          wclock[threadIdx.x >> 5]);
+      tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
+      if (tile == ~0u) break;
+      base = uint64_t(tile) * 32;
+    } else { // in rays
+      if (lane == 0) base = atomicAdd(work_counter, 32ull);
+      base = __shfl_sync(0xFFFFFFFFu, base, 0);
+      if (base >= n) break;
+    }
     uint64_t i = base + lane;
     bool valid = i < n;
-    if (img_w) {
+    if (IMG) {
       const uint64_t b = base >> 5;
       const uint32_t x = uint32_t(b % tilesX) * kImgTileW + (lane % kImgTileW);
       const uint32_t y = uint32_t(b / tilesX) * kImgTileH + (lane / kImgTileW);
@@ -938,27 +1006,36 @@ __device__ __forceinline__ float lambert(const lrt_hit& h, f3 dir, f3 L)
 __global__ void __launch_bounds__(kTraceThreads, 7) k_render_rgba8(DevScene S, DevCamera cam, DevLights L,
                                                                 uint32_t* __restrict__ image,
                                                                 unsigned long long* __restrict__ work_counter,
-                                                                uint32_t* __restrict__ err_word, uint32_t stack_cap)
+                                                                uint32_t* __restrict__ err_word, uint32_t stack_cap,
+                                                                const uint32_t* __restrict__ sched_rd,
+                                                                uint32_t* sched_wr)
 {
   extern __shared__ uint32_t smem_stack[];
   uint32_t* stack = smem_stack + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
   Ctx<false> c(S, normal_words(smem_stack, stack_cap));
   const uint32_t tilesX = (cam.width + 7) / 8, ntiles = tilesX * ((cam.height + 3) / 4);
+  __shared__ WarpClock wclock[kTraceThreads / 32];
+  if (lane == 0) {
+    wclock[threadIdx.x >> 5].tile = ~0u;
+    wclock[threadIdx.x >> 5].longest = 0;
+  }
   for (;;) {
-    unsigned long long tile = 0;
-    if (lane == 0) tile = atomicAdd(work_counter, 1ull);
+    uint32_t tile = 0;
+    __syncwarp();
+    if (lane == 0) tile = sched_next(sched_rd, sched_wr, ntiles, work_counter, wclock[threadIdx.x >> 5]);
     tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
-    if (tile >= ntiles) break;
-    const uint32_t x = uint32_t(tile % tilesX) * 8 + (lane & 7), y = uint32_t(tile / tilesX) * 4 + (lane >> 3);
-    if (x >= cam.width || y >= cam.height) continue;
-    float r[8];
-    eye_ray(cam.proj_inv, cam.world_view_inv, x, y, cam.width, cam.height, cam.tnear, cam.tfar, r);
-    lrt_hit h;
-    trace_one(c, stack, blockDim.x, stack_cap, make_float4(r[0], r[1], r[2], r[3]), make_float4(r[4], r[5], r[6], r[7]),
-              h);
-    const uint32_t px = resolve_rgba8(c, L, mk3(r[0], r[1], r[2]), mk3(r[4], r[5], r[6]), h);
-    image[uint64_t(y) * cam.width + x] = px;
+    if (tile == ~0u) break;
+    const uint32_t x = (tile % tilesX) * 8 + (lane & 7), y = (tile / tilesX) * 4 + (lane >> 3);
+    if (x < cam.width && y < cam.height) {
+      float r[8];
+      eye_ray(cam.proj_inv, cam.world_view_inv, x, y, cam.width, cam.height, cam.tnear, cam.tfar, r);
+      lrt_hit h;
+      trace_one(c, stack, blockDim.x, stack_cap, make_float4(r[0], r[1], r[2], r[3]),
+                make_float4(r[4], r[5], r[6], r[7]), h);
+      const uint32_t px = resolve_rgba8(c, L, mk3(r[0], r[1], r[2]), mk3(r[4], r[5], r[6]), h);
+      image[uint64_t(y) * cam.width + x] = px;
+    }
   }
   if (c.err) atomicOr(err_word, c.err);
 }
@@ -972,7 +1049,8 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_render_rgba8(DevScene S, D
 // most 0.01 or, unlike the reference's, after kMaxLayers traces (error bit).
 __global__ void __launch_bounds__(kTraceThreads, 7) k_fill_gbuffer_transparency(
     DevScene S, DevCamera cam, DevMaterials M, float4* __restrict__ transparency, lrt_hit* __restrict__ gbuffer,
-    unsigned long long* __restrict__ work_counter, uint32_t* __restrict__ err_word, uint32_t stack_cap)
+    unsigned long long* __restrict__ work_counter, uint32_t* __restrict__ err_word, uint32_t stack_cap,
+    const uint32_t* __restrict__ sched_rd, uint32_t* sched_wr)
 {
   constexpr uint32_t kMaxLayers = LRT_MAX_TRANSPARENCY_LAYERS;
   extern __shared__ uint32_t smem_stack[];
@@ -980,49 +1058,56 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_fill_gbuffer_transparency(
   const uint32_t lane = threadIdx.x & 31;
   Ctx<false> c(S, normal_words(smem_stack, stack_cap));
   const uint32_t tilesX = (cam.width + 7) / 8, ntiles = tilesX * ((cam.height + 3) / 4);
+  __shared__ WarpClock wclock[kTraceThreads / 32];
+  if (lane == 0) {
+    wclock[threadIdx.x >> 5].tile = ~0u;
+    wclock[threadIdx.x >> 5].longest = 0;
+  }
   for (;;) {
-    unsigned long long tile = 0;
-    if (lane == 0) tile = atomicAdd(work_counter, 1ull);
+    uint32_t tile = 0;
+    __syncwarp();
+    if (lane == 0) tile = sched_next(sched_rd, sched_wr, ntiles, work_counter, wclock[threadIdx.x >> 5]);
     tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
-    if (tile >= ntiles) break;
-    const uint32_t x = uint32_t(tile % tilesX) * 8 + (lane & 7), y = uint32_t(tile / tilesX) * 4 + (lane >> 3);
-    if (x >= cam.width || y >= cam.height) continue;
-    float r[8];
-    eye_ray(cam.proj_inv, cam.world_view_inv, x, y, cam.width, cam.height, cam.tnear, cam.tfar, r);
-    f3 pos = mk3(r[0], r[1], r[2]);
-    const f3 dir = mk3(r[4], r[5], r[6]);
-    f3 tc = mk3(0.0f, 0.0f, 0.0f);
-    float alpha = 1.0f;
-    float4 color = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    lrt_hit h;
-    for (uint32_t layer = 0;; layer++) {
-      if (layer == kMaxLayers) {
-        c.err |= kErrLayerCap;
-        break;
+    if (tile == ~0u) break;
+    const uint32_t x = (tile % tilesX) * 8 + (lane & 7), y = (tile / tilesX) * 4 + (lane >> 3);
+    if (x < cam.width && y < cam.height) {
+      float r[8];
+      eye_ray(cam.proj_inv, cam.world_view_inv, x, y, cam.width, cam.height, cam.tnear, cam.tfar, r);
+      f3 pos = mk3(r[0], r[1], r[2]);
+      const f3 dir = mk3(r[4], r[5], r[6]);
+      f3 tc = mk3(0.0f, 0.0f, 0.0f);
+      float alpha = 1.0f;
+      float4 color = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      lrt_hit h;
+      for (uint32_t layer = 0;; layer++) {
+        if (layer == kMaxLayers) {
+          c.err |= kErrLayerCap;
+          break;
+        }
+        const float wa = alpha * color.w;
+        tc = mk3(tc.x + wa * color.x, tc.y + wa * color.y, tc.z + wa * color.z);
+        alpha *= (1.0f - color.w);
+        trace_one(c, stack, blockDim.x, stack_cap, make_float4(pos.x, pos.y, pos.z, r[3]),
+                  make_float4(r[4], r[5], r[6], r[7]), h);
+        const uint32_t type = h.geomId >> 24, geomId = h.geomId & 0x00FFFFFFu;
+        if (h.primId == 0xFFFFFFFFu) {
+          color = make_float4(M.background[0], M.background[1], M.background[2], M.background[3]);
+        } else if (type != LRT_TYPE_SDF_SBS_COL && type != LRT_TYPE_GRAPHICS_PRIM) {
+          const uint2 o = M.offsets[geomId];
+          const lrt_material& m = M.mats[M.ids[o.x + h.primId % o.y]];
+          color = m.type == LRT_MATERIAL_COLORED
+                      ? make_float4(m.base_color[0], m.base_color[1], m.base_color[2], m.base_color[3])
+                      : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+        }
+        pos = pos + h.t * dir;
+        if (!(alpha > 0.01f)) break;
       }
-      const float wa = alpha * color.w;
-      tc = mk3(tc.x + wa * color.x, tc.y + wa * color.y, tc.z + wa * color.z);
-      alpha *= (1.0f - color.w);
-      trace_one(c, stack, blockDim.x, stack_cap, make_float4(pos.x, pos.y, pos.z, r[3]),
-                make_float4(r[4], r[5], r[6], r[7]), h);
-      const uint32_t type = h.geomId >> 24, geomId = h.geomId & 0x00FFFFFFu;
-      if (h.primId == 0xFFFFFFFFu) {
-        color = make_float4(M.background[0], M.background[1], M.background[2], M.background[3]);
-      } else if (type != LRT_TYPE_SDF_SBS_COL && type != LRT_TYPE_GRAPHICS_PRIM) {
-        const uint2 o = M.offsets[geomId];
-        const lrt_material& m = M.mats[M.ids[o.x + h.primId % o.y]];
-        color = m.type == LRT_MATERIAL_COLORED
-                    ? make_float4(m.base_color[0], m.base_color[1], m.base_color[2], m.base_color[3])
-                    : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-      }
-      pos = pos + h.t * dir;
-      if (!(alpha > 0.01f)) break;
+      const uint64_t i = uint64_t(y) * cam.width + x;
+      transparency[i] = make_float4(tc.x, tc.y, tc.z, alpha);
+      float4* out = reinterpret_cast<float4*>(gbuffer + i);
+      out[0] = make_float4(h.t, __uint_as_float(h.primId), __uint_as_float(h.instId), __uint_as_float(h.geomId));
+      out[1] = make_float4(h.coords[0], h.coords[1], h.coords[2], h.coords[3]);
     }
-    const uint64_t i = uint64_t(y) * cam.width + x;
-    transparency[i] = make_float4(tc.x, tc.y, tc.z, alpha);
-    float4* out = reinterpret_cast<float4*>(gbuffer + i);
-    out[0] = make_float4(h.t, __uint_as_float(h.primId), __uint_as_float(h.instId), __uint_as_float(h.geomId));
-    out[1] = make_float4(h.coords[0], h.coords[1], h.coords[2], h.coords[3]);
   }
   if (c.err) atomicOr(err_word, c.err);
 }
@@ -1135,26 +1220,28 @@ __global__ void __launch_bounds__(kTraceThreads) k_adjoint_lambert(DevScene S, c
 
 cudaError_t launch_render_rgba8(const DevScene& S, const DevCamera& cam, const DevLights& lights, uint32_t* image,
                                 unsigned long long* work_counter, uint32_t* err_word, uint32_t stack_cap, int grid,
-                                cudaStream_t stream)
+                                cudaStream_t stream, const uint32_t* sched_rd, uint32_t* sched_wr)
 {
   const size_t smem = trace_smem_bytes(stack_cap);
   cudaError_t e = cudaFuncSetAttribute(k_render_rgba8, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(trace_smem_bytes(kMaxStackDev + 1)));
   if (e != cudaSuccess) return e;
-  k_render_rgba8<<<grid, kTraceThreads, smem, stream>>>(S, cam, lights, image, work_counter, err_word, stack_cap);
+  k_render_rgba8<<<grid, kTraceThreads, smem, stream>>>(S, cam, lights, image, work_counter, err_word, stack_cap,
+                                                        sched_rd, sched_wr);
   return cudaGetLastError();
 }
 
 cudaError_t launch_fill_gbuffer_transparency(const DevScene& S, const DevCamera& cam, const DevMaterials& M,
                                              float4* transparency, lrt_hit* gbuffer, unsigned long long* work_counter,
-                                             uint32_t* err_word, uint32_t stack_cap, int grid, cudaStream_t stream)
+                                             uint32_t* err_word, uint32_t stack_cap, int grid, cudaStream_t stream,
+                                             const uint32_t* sched_rd, uint32_t* sched_wr)
 {
   const size_t smem = trace_smem_bytes(stack_cap);
   cudaError_t e = cudaFuncSetAttribute(k_fill_gbuffer_transparency, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(trace_smem_bytes(kMaxStackDev + 1)));
   if (e != cudaSuccess) return e;
   k_fill_gbuffer_transparency<<<grid, kTraceThreads, smem, stream>>>(S, cam, M, transparency, gbuffer, work_counter,
-                                                                     err_word, stack_cap);
+                                                                     err_word, stack_cap, sched_rd, sched_wr);
   return cudaGetLastError();
 }
 
@@ -1200,42 +1287,56 @@ __global__ void k_eye_rays(DevCamera cam, float4* __restrict__ rays)
 cudaError_t launch_trace(const DevScene& S, const float4* rays, lrt_hit* hits, uint64_t n,
                                 unsigned long long* work_counter, unsigned long long* counters, uint32_t* err_word,
                                 uint32_t stack_cap, int grid, cudaStream_t stream, bool count, uint32_t img_w,
-                                uint32_t img_h)
+                                uint32_t img_h, const uint32_t* sched_rd, uint32_t* sched_wr)
 {
   const size_t smem = trace_smem_bytes(stack_cap);
   // the ANALYTIC / NEWTON / IT node solvers live in their own instantiation,
   // so that the sphere-tracing kernel keeps its registers
   const uint32_t solver = (S.flags >> kFlagSolverShift) & 7u;
   const bool solvers = solver != kSolverST && solver != kSolverBBox;
-  if (count && solvers)
-    k_trace<true, true><<<grid, kTraceThreads, smem, stream>>>(S, rays, hits, n, work_counter, counters, err_word,
-                                                               stack_cap, img_w, img_h);
-  else if (count)
-    k_trace<true, false><<<grid, kTraceThreads, smem, stream>>>(S, rays, hits, n, work_counter, counters, err_word,
-                                                                stack_cap, img_w, img_h);
-  else if (solvers)
-    k_trace<false, true><<<grid, kTraceThreads, smem, stream>>>(S, rays, hits, n, work_counter, counters, err_word,
-                                                                stack_cap, img_w, img_h);
-  else
-    k_trace<false, false><<<grid, kTraceThreads, smem, stream>>>(S, rays, hits, n, work_counter, counters, err_word,
-                                                                 stack_cap, img_w, img_h);
+  // image order (IMG) is its own instantiation, so that the tile schedule
+  // costs the row-order kernel nothing
+  auto go = [&](auto kernel) {
+    kernel<<<grid, kTraceThreads, smem, stream>>>(S, rays, hits, n, work_counter, counters, err_word, stack_cap, img_w,
+                                                  img_h, sched_rd, sched_wr);
+  };
+  if (img_w) {
+    if (count && solvers) go(k_trace<true, true, true>);
+    else if (count) go(k_trace<true, false, true>);
+    else if (solvers) go(k_trace<false, true, true>);
+    else go(k_trace<false, false, true>);
+  } else {
+    if (count && solvers) go(k_trace<true, true, false>);
+    else if (count) go(k_trace<true, false, false>);
+    else if (solvers) go(k_trace<false, true, false>);
+    else go(k_trace<false, false, false>);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t set_trace_smem(uint32_t stack_cap)
 {
   const int smem = int(trace_smem_bytes(stack_cap));
-  cudaError_t e = cudaFuncSetAttribute(k_trace<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_trace<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_trace<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_trace<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = cudaSuccess;
+  auto set = [&](auto kernel) {
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  };
+  set(k_trace<true, false, false>);
+  set(k_trace<true, true, false>);
+  set(k_trace<false, true, false>);
+  set(k_trace<false, false, false>);
+  set(k_trace<true, false, true>);
+  set(k_trace<true, true, true>);
+  set(k_trace<false, true, true>);
+  set(k_trace<false, false, true>);
+  return e;
 }
 
 cudaError_t trace_occupancy(uint32_t stack_cap, int* blocks_per_sm)
 {
   const size_t smem = trace_smem_bytes(stack_cap);
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_trace<false, false>, kTraceThreads, smem);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_trace<false, false, false>, kTraceThreads,
+                                                       smem);
 }
 
 cudaError_t launch_eye_rays(const DevCamera& cam, float4* rays, cudaStream_t stream)

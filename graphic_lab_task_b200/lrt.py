@@ -13,7 +13,7 @@ import os
 import numpy as np
 
 from ._abi import (HIT_DTYPE, LIGHT_DTYPE, MATERIAL_DTYPE, LRT_BATCH_NO_GRAPH, LRT_COUNTER_COUNT, LRT_TRACE_COUNT_WORK,
-                   LRT_TRACE_DEVICE_POINTERS, LRT_TRACE_FAST_MATH, STATUS_NAMES, BatchShape, Camera, Preset,
+                   LRT_TRACE_DEVICE_POINTERS, LRT_TRACE_FAST_MATH, LRT_TRACE_NATURAL_ORDER, STATUS_NAMES, BatchShape, Camera, Preset,
                    SceneArrays, TuneEntry, arrays_to_struct, parity_preset, struct_to_arrays)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -297,10 +297,13 @@ class SceneRT:
         self._check(lib().lrt_trace_nearest(self.h, C.c_void_p(rays_ptr), C.c_void_p(hits_ptr), n,
                                             C.c_void_p(stream) if stream else None, flags))
 
-    def trace_image(self, rays_ptr, hits_ptr, width, height, stream=0, fast_math=False, count_work=False):
+    def trace_image(self, rays_ptr, hits_ptr, width, height, stream=0, fast_math=False, count_work=False,
+                    natural_order=False):
         """Asynchronous trace of the device rays of a width x height image
-        (row-major pixels), in 8x4-pixel tiles per warp."""
-        flags = (LRT_TRACE_FAST_MATH if fast_math else 0) | (LRT_TRACE_COUNT_WORK if count_work else 0)
+        (row-major pixels), in 8x4-pixel tiles per warp, the stream's
+        longest-first tile schedule unless natural_order."""
+        flags = (LRT_TRACE_FAST_MATH if fast_math else 0) | (LRT_TRACE_COUNT_WORK if count_work else 0) | \
+            (LRT_TRACE_NATURAL_ORDER if natural_order else 0)
         self._check(lib().lrt_trace_nearest_image(self.h, C.c_void_p(rays_ptr), C.c_void_p(hits_ptr), width, height,
                                                   C.c_void_p(stream) if stream else None, flags))
 

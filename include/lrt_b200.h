@@ -311,6 +311,8 @@ lrt_status lrt_scene_export(const lrt_scene* scene, lrt_scene_arrays* out);
 #define LRT_TRACE_FAST_MATH 0x2u       /* FMA-contracted kernels (tolerance
                                           parity); default is the exact build */
 #define LRT_TRACE_COUNT_WORK 0x4u      /* also accumulate work counters     */
+#define LRT_TRACE_NATURAL_ORDER 0x8u   /* lrt_trace_nearest_image: tiles in
+                                          row order, no tile schedule      */
 
 /* Batched BVHRT::RayQuery_NearestHit.  rays: n x {float4 posAndNear,
  * float4 dirAndFar} (32 bytes per ray), hits: n x lrt_hit.  A ray whose
@@ -347,10 +349,18 @@ lrt_status lrt_trace_sync(lrt_scene* scene, void* stream, int32_t read_counters)
 
 /* lrt_trace_nearest for the width*height rays of one image stored in
  * row-major pixel order, device pointers only (asynchronous on `stream`,
- * flags: LRT_TRACE_FAST_MATH, LRT_TRACE_COUNT_WORK).  A warp traces an 8x4
- * tile of pixels rather than 32 pixels of one row, as the reference's
- * kernel1D_FillGbuffer walks pixels in packed tiles (MultiRenderer.cpp:
- * 185-202); every hit equals lrt_trace_nearest's for the same ray.  No
+ * flags: LRT_TRACE_FAST_MATH, LRT_TRACE_COUNT_WORK, LRT_TRACE_NATURAL_ORDER).
+ * A warp traces an 8x4 tile of pixels rather than 32 pixels of one row, as
+ * the reference's kernel1D_FillGbuffer walks pixels in packed tiles
+ * (MultiRenderer.cpp:185-202); every hit equals lrt_trace_nearest's for the
+ * same ray.  Tiles are scheduled longest first: each launch measures its
+ * tiles' durations, and the next launch of the same image size on the same
+ * stream starts with the tiles that took at least a quarter of the longest
+ * (the rest follow in row order), so that a few slow tiles do not finish
+ * last.  The order never changes a result; the first launch of a size on a
+ * stream allocates that stream's two schedule buffers (16 bytes + about
+ * 4.1 bytes per tile each).  lrt_render_rgba8 and
+ * lrt_fill_gbuffer_transparency schedule their tiles the same way.  No
  * counterpart entry point in the reference. */
 lrt_status lrt_trace_nearest_image(lrt_scene* scene, const float* rays_dev, lrt_hit* hits_dev, uint32_t width,
                                    uint32_t height, void* stream, uint32_t flags);

@@ -295,3 +295,20 @@ def test_image_tile_order_equals_linear_trace(cuda, size):
     assert bit_equal(a, b).all(), hit_summary(b, a)
     assert np.array_equal(c1, c2)
     assert (a["primId"] != MISS).sum() > 0.05 * w * h
+    # later launches follow the longest-first tile schedule the earlier ones
+    # measured (launch 3 on is reordered); natural order, a size change and a
+    # second stream in between keep every hit
+    side = torch.cuda.Stream()
+    small = torch.zeros(8 * 8 * 8, dtype=torch.float32, device="cuda")
+    for k in range(6):
+        H2.zero_()
+        if k == 3:
+            sc.trace_image(R.data_ptr(), small.data_ptr(), 8, 8)  # another size on the stream resets its schedule
+        if k == 4:
+            sc.trace_image(R.data_ptr(), H2.data_ptr(), w, h, stream=side.cuda_stream)
+            sc.sync(stream=side.cuda_stream)
+            H2.zero_()
+        sc.trace_image(R.data_ptr(), H2.data_ptr(), w, h, natural_order=(k == 5))
+        sc.sync()
+        b = H2.cpu().numpy().view(HIT_DTYPE)
+        assert bit_equal(a, b).all(), (k, hit_summary(b, a))
