@@ -28,10 +28,15 @@ constexpr int kTraceThreads = 128;
 constexpr uint32_t kImgTileW = 8, kImgTileH = 4;
 
 // Tile schedule of the image-order launches (one per stream and image size,
-// two buffers used alternately): a header {count, maxCost, 0, 0}, a bitmap
-// of the listed tiles, then the list of expensive tiles.
+// two buffers used alternately): a header {longest tile cost, count of each
+// of the kSchedClasses cost classes}, a bitmap of the listed tiles, then one
+// list of `tiles` entries per class.
 constexpr uint32_t kSchedHeader = 4;
-inline __host__ __device__ uint64_t sched_words(uint64_t tiles) { return kSchedHeader + (tiles + 31) / 32 + tiles; }
+constexpr uint32_t kSchedClasses = 3;
+inline __host__ __device__ uint64_t sched_words(uint64_t tiles)
+{
+  return kSchedHeader + (tiles + 31) / 32 + kSchedClasses * tiles;
+}
 // Per-thread shared-memory words after the traversal stack: the inputs of the
 // deferred SDF normal (sign, sample point, 8 corner values).
 constexpr uint32_t kNormalWords = 12;

@@ -715,15 +715,17 @@ __device__ void trace_one(CTX& c, uint32_t* stack, uint32_t stride, uint32_t cap
   if (hit.primId != 0xFFFFFFFFu) c.inc(kCntHits);
 }
 
-// Longest-first order of the tiles of an image-order launch.  With the
-// schedule of the previous same-size launch on its stream (rd), a launch
-// first takes the tiles that launch listed as expensive (in the order it
-// finished them), then every other tile in natural order; each tile's
-// duration is measured on lane 0 and those of at least a quarter of the
-// previous launch's longest go to the list for the next launch (wr).  Only
-// which warp traces which tile, and when, depends on it.  rd == nullptr:
-// natural order; wr == nullptr: nothing recorded.  The per-warp state lives
-// in shared memory so that the traversal keeps its registers.
+// Longest-first order of the tiles of an image-order launch.  Each launch
+// times its tiles on lane 0 and sorts the slow ones into three classes by
+// their cost against the previous launch's longest tile (at least 1/2, 1/4,
+// 1/8 of it); the next launch of the same image size on the same stream
+// (rd) hands out class 0, then 1, then 2, each in the order the tiles
+// finished, then every other tile in natural order (a bitmap skips the
+// listed ones).  Only which warp traces which tile, and when, depends on it.
+// rd == nullptr: natural order; wr == nullptr: nothing recorded.  Buffer
+// layout (sched_words): {longest cost, count of class 0, 1, 2}, the bitmap,
+// then the list of each class (`tiles` entries each).  The per-warp state
+// lives in shared memory so that the traversal keeps its registers.
 struct WarpClock {
   long long start;  // clock64 when the warp took its current tile
   uint32_t tile;    // that tile, ~0u before the first
@@ -736,31 +738,41 @@ struct WarpClock {
 __device__ __forceinline__ uint32_t sched_next(const uint32_t* __restrict__ rd, uint32_t* wr, uint32_t tiles,
                                                unsigned long long* counter, WarpClock& wc)
 {
+  const uint32_t lists = kSchedHeader + (tiles + 31) / 32;
   if (wr && wc.tile != ~0u) {
     const long long dt = (clock64() - wc.start) >> 4;
     const uint32_t cost = uint32_t(dt < 0xFFFFFFFFll ? dt : 0xFFFFFFFFll);
     if (cost > wc.longest) {
       wc.longest = cost;
-      atomicMax(wr + 1, cost);
+      atomicMax(wr, cost);
     }
-    const uint32_t thr = rd ? __ldg(rd + 1) / 4 : 0u;
-    if (thr && cost >= thr) {
-      const uint32_t slot = atomicAdd(wr, 1u);
-      if (slot < tiles) wr[kSchedHeader + (tiles + 31) / 32 + slot] = wc.tile;
-      atomicOr(wr + kSchedHeader + (wc.tile >> 5), 1u << (wc.tile & 31));
+    const uint32_t mx = rd ? __ldg(rd) : 0u;
+    if (mx) {
+      const int cls = cost >= mx / 2 ? 0 : cost >= mx / 4 ? 1 : cost >= mx / 8 ? 2 : 3;
+      if (cls < 3) {
+        const uint32_t slot = atomicAdd(wr + 1 + cls, 1u);
+        if (slot < tiles) wr[lists + cls * tiles + slot] = wc.tile;
+        atomicOr(wr + kSchedHeader + (wc.tile >> 5), 1u << (wc.tile & 31));
+      }
     }
   }
-  const uint32_t nHard = rd ? min(__ldg(rd), tiles) : 0u;
+  static_assert(kSchedClasses == 3, "three cost classes");
+  uint32_t n[3] = {0, 0, 0};
+  if (rd)
+    for (int c = 0; c < 3; c++) n[c] = min(__ldg(rd + 1 + c), tiles);
+  const uint64_t nAll = uint64_t(n[0]) + n[1] + n[2];
   for (;;) {
     const unsigned long long k = atomicAdd(counter, 1ull);
     uint32_t tile;
-    if (k < nHard) {
-      tile = __ldg(rd + kSchedHeader + (tiles + 31) / 32 + k);
-      if (tile >= tiles) continue; // a listed tile is always inside the image
+    if (k < nAll) {
+      const int cls = k < n[0] ? 0 : k < uint64_t(n[0]) + n[1] ? 1 : 2;
+      const uint64_t j = cls == 0 ? k : cls == 1 ? k - n[0] : k - n[0] - n[1];
+      tile = __ldg(rd + lists + cls * tiles + j);
+      if (tile >= tiles) continue;
     } else {
-      if (k - nHard >= tiles) return wc.tile = ~0u;
-      tile = uint32_t(k - nHard);
-      if (nHard && ((__ldg(rd + kSchedHeader + (tile >> 5)) >> (tile & 31)) & 1u)) continue; // listed: taken above
+      if (k - nAll >= tiles) return wc.tile = ~0u;
+      tile = uint32_t(k - nAll);
+      if (nAll && ((__ldg(rd + kSchedHeader + (tile >> 5)) >> (tile & 31)) & 1u)) continue;
     }
     wc.start = clock64();
     return wc.tile = tile;

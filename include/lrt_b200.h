@@ -355,11 +355,11 @@ lrt_status lrt_trace_sync(lrt_scene* scene, void* stream, int32_t read_counters)
  * (MultiRenderer.cpp:185-202); every hit equals lrt_trace_nearest's for the
  * same ray.  Tiles are scheduled longest first: each launch measures its
  * tiles' durations, and the next launch of the same image size on the same
- * stream starts with the tiles that took at least a quarter of the longest
- * (the rest follow in row order), so that a few slow tiles do not finish
- * last.  The order never changes a result; the first launch of a size on a
- * stream allocates that stream's two schedule buffers (16 bytes + about
- * 4.1 bytes per tile each).  lrt_render_rgba8 and
+ * stream starts with the tiles that took at least 1/2, then 1/4, then 1/8 of
+ * the longest (the rest follow in row order), so that a few slow tiles do
+ * not finish last.  The order never changes a result; the first launch of a
+ * size on a stream allocates that stream's two schedule buffers (16 bytes +
+ * about 12.1 bytes per tile each).  lrt_render_rgba8 and
  * lrt_fill_gbuffer_transparency schedule their tiles the same way.  No
  * counterpart entry point in the reference. */
 lrt_status lrt_trace_nearest_image(lrt_scene* scene, const float* rays_dev, lrt_hit* hits_dev, uint32_t width,
