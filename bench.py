@@ -739,9 +739,15 @@ def configs_table(args):
             R = torch.from_numpy(rays).to(dev)
             H = torch.empty(n * 8, dtype=torch.float32, device=dev)
             ms = timed(lambda: sc.trace_device(R.data_ptr(), H.data_ptr(), n, stream=sp))
+            ims = timed(lambda: sc.trace_image(R.data_ptr(), H.data_ptr(), cam.width, cam.height, stream=sp))
+            nms = timed(lambda: sc.trace_image(R.data_ptr(), H.data_ptr(), cam.width, cam.height, stream=sp,
+                                               natural_order=True))
             sc.sync(stream=sp)
             emit({"config": 1, "workload": "SBS 512^3, 1920x1080", "rays": n, "gpu_ms": ms, "gpu_mrays_s": n / ms / 1e3,
-                  "roofline": roofline(sc, R, n, ms), "cpu_reference": cpu(sc, rays)})
+                  "gpu_image_order_ms": ims, "gpu_image_order_mrays_s": n / ims / 1e3,
+                  "gpu_image_natural_tile_order_ms": nms, "gpu_image_natural_tile_order_mrays_s": n / nms / 1e3,
+                  "roofline": roofline(sc, R, n, ms), "roofline_image_order": roofline(sc, R, n, ims),
+                  "cpu_reference": cpu(sc, rays)})
 
         if 3 in only:
             # 3: 64 batched cameras on the same scene
