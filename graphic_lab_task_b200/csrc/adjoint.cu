@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <iterator>
 #include <cstring>
 
 #include "device_scene.h"
@@ -83,6 +84,50 @@ lrt_status begin(lrt_scene* s, cudaStream_t stream, StreamSlot** slot, DevScene*
   return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "cudaMemsetAsync");
 }
 
+// The renderer's material tables on the device, copied when they changed
+// since the last copy (synchronous: they change rarely).
+lrt_status upload_materials(lrt_scene* s)
+{
+  DeviceScene* d = s->dev;
+  if (d->matVersion == s->matVersion) return LRT_OK;
+  cudaFree(d->mats);
+  cudaFree(d->matIds);
+  cudaFree(d->matOffsets);
+  d->mats = nullptr;
+  d->matIds = nullptr;
+  d->matOffsets = nullptr;
+  cudaError_t e = cudaMalloc(&d->mats, std::max<size_t>(1, s->mats.size()) * sizeof(lrt_material));
+  if (e == cudaSuccess) e = cudaMalloc(&d->matIds, std::max<size_t>(1, s->matIds.size()) * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&d->matOffsets, std::max<size_t>(1, s->matOffsets.size()) * sizeof(uint32_t));
+  if (e == cudaSuccess && !s->mats.empty())
+    e = cudaMemcpy(d->mats, s->mats.data(), s->mats.size() * sizeof(lrt_material), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !s->matIds.empty())
+    e = cudaMemcpy(d->matIds, s->matIds.data(), s->matIds.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !s->matOffsets.empty())
+    e = cudaMemcpy(d->matOffsets, s->matOffsets.data(), s->matOffsets.size() * sizeof(uint32_t),
+                   cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(s, e, "material tables host->device");
+  d->matVersion = s->matVersion;
+  return LRT_OK;
+}
+
+// Every geometry whose hits read a material (all but the types in `skip`,
+// a list ending in ~0u) needs a nonempty material range.
+lrt_status check_material_ranges(lrt_scene* s, const char* who, const uint32_t* skip)
+{
+  const HostArrays& h = s->h;
+  for (size_t g = 0; g < h.geomData.size(); g++) {
+    const uint32_t type = h.geomData[g].type;
+    bool skipped = false;
+    for (const uint32_t* k = skip; *k != ~0u; k++) skipped |= type == *k;
+    if (skipped) continue;
+    if (2 * g + 1 >= s->matOffsets.size() || s->matOffsets[2 * g + 1] == 0)
+      return fail(s, LRT_ERR_INVALID_ARGUMENT, "%s: geometry %zu (type %u) has no material range (lrt_set_materials)",
+                  who, g, type);
+  }
+  return LRT_OK;
+}
+
 } // namespace
 } // namespace lrt
 
@@ -135,10 +180,35 @@ lrt_status lrt_render_rgba8(lrt_scene* s, const lrt_camera* camera, const lrt_li
     return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_render_rgba8: NULL camera, background, lights or image");
   if (light_count > LRT_MAX_LIGHTS)
     return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_render_rgba8: %u lights (at most %d)", light_count, LRT_MAX_LIGHTS);
-  if (s->preset.render_mode != LRT_RENDER_MODE_LAMBERT_NO_TEX)
-    return fail(s, LRT_ERR_UNSUPPORTED, "lrt_render_rgba8 renders the LAMBERT_NO_TEX mode (1), the preset has %u",
-                s->preset.render_mode);
+  const uint32_t mode = s->preset.render_mode;
+  static const uint32_t kModes[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 16, 17, 19, 20, 22, 24, 25};
+  if (std::find(std::begin(kModes), std::end(kModes), mode) == std::end(kModes))
+    return fail(s, LRT_ERR_UNSUPPORTED,
+                "lrt_render_rgba8: render_mode %u (textures, shadows, PBR, outlines, channels and intersection "
+                "counts are outside the ray-query path)",
+                mode);
+  if (mode == 16 || mode == 17 || mode == 22) {
+    // DIFFUSE and LAMBERT read COLORED materials; MATERIAL the material ids
+    static const uint32_t kSkipDiffuse[] = {LRT_TYPE_SDF_SBS_COL, ~0u};
+    static const uint32_t kSkipLambert[] = {LRT_TYPE_SDF_SBS_COL, LRT_TYPE_GRAPHICS_PRIM, ~0u};
+    static const uint32_t kSkipNone[] = {~0u};
+    st = check_material_ranges(s, "lrt_render_rgba8", mode == 16 ? kSkipDiffuse : mode == 17 ? kSkipLambert : kSkipNone);
+    if (st != LRT_OK) return st;
+    if (mode != 22)
+      for (const lrt_material& m : s->mats) {
+        if (m.type != LRT_MATERIAL_COLORED)
+          return fail(s, LRT_ERR_UNSUPPORTED, "lrt_render_rgba8: textured materials are not implemented");
+        // CheckForTransparency (MultiRenderer.cpp:248-258): the reference then
+        // resolves through the transparency G-buffer
+        if (m.base_color[3] < 1.0f)
+          return fail(s, LRT_ERR_UNSUPPORTED,
+                      "lrt_render_rgba8: a transparent material makes the reference resolve mode %u through "
+                      "lrt_fill_gbuffer_transparency's G-buffer",
+                      mode);
+      }
+  }
   if (camera->width == 0 || camera->height == 0) return LRT_OK;
+  if ((st = upload_materials(s)) != LRT_OK) return st;
   DevCamera cam;
   std::memcpy(cam.proj_inv, camera->proj_inv, sizeof(cam.proj_inv));
   std::memcpy(cam.world_view_inv, camera->world_view_inv, sizeof(cam.world_view_inv));
@@ -156,8 +226,12 @@ lrt_status lrt_render_rgba8(lrt_scene* s, const lrt_camera* camera, const lrt_li
   const uint32_t* rd = nullptr;
   uint32_t* wr = nullptr;
   if ((st = sched_prepare(s, stream, cam.width, cam.height, false, &rd, &wr)) != LRT_OK) return st;
+  DevMaterials M{};
+  M.mats = d->mats;
+  M.ids = d->matIds;
+  M.offsets = reinterpret_cast<const uint2*>(d->matOffsets);
   const cudaError_t e = lrt_exact::launch_render_rgba8(S, cam, L, image_dev, &slot->work, &slot->err, d->stackCap,
-                                                       grid, stream, rd, wr);
+                                                       grid, stream, rd, wr, &M, mode);
   if (e != cudaSuccess) return cuda_fail(s, e, "render launch");
   sched_commit(s, stream, false);
   return LRT_OK;
@@ -198,39 +272,11 @@ lrt_status lrt_fill_gbuffer_transparency(lrt_scene* s, const lrt_camera* camera,
   if (!camera || !background || !transparency_dev || !hits_dev)
     return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_fill_gbuffer_transparency: NULL camera, background or output");
   if ((st = check_rays(s, transparency_dev)) != LRT_OK || (st = check_rays(s, hits_dev)) != LRT_OK) return st;
-  // every geometry whose hits read a material needs a nonempty range
-  const HostArrays& h = s->h;
-  for (size_t g = 0; g < h.geomData.size(); g++) {
-    const uint32_t type = h.geomData[g].type;
-    if (type == LRT_TYPE_SDF_SBS_COL || type == LRT_TYPE_GRAPHICS_PRIM) continue;
-    if (2 * g + 1 >= s->matOffsets.size() || s->matOffsets[2 * g + 1] == 0)
-      return fail(s, LRT_ERR_INVALID_ARGUMENT,
-                  "lrt_fill_gbuffer_transparency: geometry %zu (type %u) has no material range (lrt_set_materials)", g,
-                  type);
-  }
+  static const uint32_t kSkip[] = {LRT_TYPE_SDF_SBS_COL, LRT_TYPE_GRAPHICS_PRIM, ~0u};
+  if ((st = check_material_ranges(s, "lrt_fill_gbuffer_transparency", kSkip)) != LRT_OK) return st;
   if (camera->width == 0 || camera->height == 0) return LRT_OK;
   DeviceScene* d = s->dev;
-  if (d->matVersion != s->matVersion) {
-    // copy the tables (synchronous: they change rarely)
-    cudaFree(d->mats);
-    cudaFree(d->matIds);
-    cudaFree(d->matOffsets);
-    d->mats = nullptr;
-    d->matIds = nullptr;
-    d->matOffsets = nullptr;
-    cudaError_t e = cudaMalloc(&d->mats, std::max<size_t>(1, s->mats.size()) * sizeof(lrt_material));
-    if (e == cudaSuccess) e = cudaMalloc(&d->matIds, std::max<size_t>(1, s->matIds.size()) * sizeof(uint32_t));
-    if (e == cudaSuccess) e = cudaMalloc(&d->matOffsets, std::max<size_t>(1, s->matOffsets.size()) * sizeof(uint32_t));
-    if (e == cudaSuccess && !s->mats.empty())
-      e = cudaMemcpy(d->mats, s->mats.data(), s->mats.size() * sizeof(lrt_material), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && !s->matIds.empty())
-      e = cudaMemcpy(d->matIds, s->matIds.data(), s->matIds.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && !s->matOffsets.empty())
-      e = cudaMemcpy(d->matOffsets, s->matOffsets.data(), s->matOffsets.size() * sizeof(uint32_t),
-                     cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) return cuda_fail(s, e, "material tables host->device");
-    d->matVersion = s->matVersion;
-  }
+  if ((st = upload_materials(s)) != LRT_OK) return st;
   DevCamera cam;
   std::memcpy(cam.proj_inv, camera->proj_inv, sizeof(cam.proj_inv));
   std::memcpy(cam.world_view_inv, camera->world_view_inv, sizeof(cam.world_view_inv));

@@ -908,6 +908,195 @@ __device__ __forceinline__ uint32_t resolve_rgba8(CTX& c, const DevLights& L, f3
   }
 }
 
+// MultiRenderer's colour palettes (MultiRenderer.h:269-283): objects by id
+// and LOD levels, RGBA8 words.
+__constant__ uint32_t kPalette[20] = {0xffe6194b, 0xff3cb44b, 0xffffe119, 0xff0082c8, 0xfff58231,
+                                      0xff911eb4, 0xff46f0f0, 0xfff032e6, 0xffd2f53c, 0xfffabebe,
+                                      0xff008080, 0xffe6beff, 0xffaa6e28, 0xfffffac8, 0xff800000,
+                                      0xffaaffc3, 0xff808000, 0xffffd8b1, 0xff000080, 0xff808080};
+__constant__ uint32_t kLodPalette[20] = {0xff000000, 0xff000040, 0xff000080, 0xff0000c0, 0xff0040ff,
+                                         0xff0080ff, 0xff00c0ff, 0xff00ffff, 0xff00ffc0, 0xff00ff80,
+                                         0xff00ff40, 0xff00ff00, 0xff00c000, 0xff008000, 0xff004000,
+                                         0xff000000, 0xffff0000, 0xffff0000, 0xffff0000, 0xffff0000};
+
+// decode_RGBA8 (utils/raytracing/render_common.h:250-254)
+__device__ __forceinline__ float4 decode_rgba8(uint32_t c)
+{
+  return make_float4(float(c & 0xFF) * (1.0f / 255.0f), float((c >> 8) & 0xFF) * (1.0f / 255.0f),
+                     float((c >> 16) & 0xFF) * (1.0f / 255.0f), float((c >> 24) & 0xFF) * (1.0f / 255.0f));
+}
+
+// The colour of SBS_COL and graphics-primitive hits packed in coords[0..1]
+// (MultiRenderer_resolve.cpp:629-634): round / 255, the fraction, round / 255.
+__device__ __forceinline__ f3 packed_hit_colour(const lrt_hit& h)
+{
+  return mk3(roundf(h.coords[0]) / 255.0f, h.coords[0] - floorf(h.coords[0]), roundf(h.coords[1]) / 255.0f);
+}
+
+// Sum of the lights' Lambert terms for base colour `color` (ResolveCommon,
+// MultiRenderer_resolve.cpp:638-663).
+__device__ __forceinline__ f3 lambert_lights(const DevLights& L, f3 norm, f3 color, f3 rayPos, f3 rayDir, float t)
+{
+  f3 fc = mk3(0, 0, 0);
+  for (uint32_t i = 0; i < L.count; i++) {
+    const DevLight& l = L.light[i];
+    const f3 lc = mk3(l.color[0], l.color[1], l.color[2]);
+    const f3 sp = mk3(l.space[0], l.space[1], l.space[2]);
+    if (l.type == LRT_LIGHT_DIRECT) {
+      const float q = smax(0.0f, dot(norm, sp));
+      fc = fc + (lc * color) * q;
+    } else if (l.type == LRT_LIGHT_POINT) {
+      const f3 surf = rayPos + t * rayDir;
+      f3 dir = sp - surf;
+      const float len = sqrtf(dot(dir, dir));
+      dir = mk3(dir.x / len, dir.y / len, dir.z / len);
+      const float q = smax(0.0f, dot(norm, dir));
+      fc = fc + ((lc * color) * q) / (len * len);
+    } else {
+      fc = fc + lc * color;
+    }
+  }
+  return fc;
+}
+
+// ResolveCommon / kernel1D_ResolveDebug (MultiRenderer_resolve.cpp:580-666,
+// 810-990) of one traced eye ray for the render modes without textures,
+// shadows or PBR, then Tonemap: MASK, DEPTH, LINEAR_DEPTH,
+// INVERSE_LINEAR_DEPTH, PRIMITIVE, TYPE, GEOM, NORMAL, BARYCENTRIC,
+// ST_ITERATIONS, DIFFUSE, LAMBERT, HSV_DEPTH, LOD, MATERIAL, MO_VOXEL_COUNT
+// and MO_FLAGS (colored materials only).  The normal is loadNormalTcFromGbuffer's
+// (triangles recomputed and turned to the viewer, SDF hits decoded).
+template <class CTX>
+__device__ uint32_t resolve_mode_rgba8(CTX& c, const DevLights& L, const DevMaterials& M, uint32_t mode, f3 rayPos,
+                                       f3 rayDir, const lrt_hit& h)
+{
+  const DevScene& S = c.S;
+  if (h.primId == 0xFFFFFFFFu)
+    return tonemap_rgba8(L.background[0], L.background[1], L.background[2], L.background[3]);
+  const uint32_t type = h.geomId >> 24, geomId = h.geomId & 0x00FFFFFFu;
+  f3 norm;
+  if (type == LRT_TYPE_MESH_TRIANGLE) {
+    const DevGeom& g = S.geoms[geomId];
+    const float4* tri = S.triSoup + 3 * (uint64_t(g.triBase) + c.triLocal);
+    const f3 raw = cross(ld3(__ldg(tri + 1)), ld3(__ldg(tri + 2)));
+    norm = normalize(matmul4(S.instances[h.instId].transformInvTransposed, raw, 1.0f));
+    norm = ssign(dot(-1.0f * rayDir, norm)) * norm;
+  } else {
+    norm = decode_normal(mk2(h.coords[2], h.coords[3]));
+  }
+  auto material = [&]() -> const lrt_material& {
+    const uint2 o = M.offsets[geomId];
+    return M.mats[M.ids[o.x + h.primId % o.y]];
+  };
+  const float z = h.t, z_near = 0.1f, z_far = 10.0f;
+  float4 res = make_float4(1, 0, 1, 1);
+  switch (mode) {
+  case 0: // MASK
+    res = make_float4(1, 1, 1, 1);
+    break;
+  case 2: { // DEPTH
+    const float d = (1.0f / z - 1.0f / z_near) / (1.0f / z_far - 1.0f / z_near);
+    res = make_float4(d, d, d, 1);
+  } break;
+  case 3: { // LINEAR_DEPTH
+    const float d = (z - z_near) / (z_far - z_near);
+    res = make_float4(d, d, d, 1);
+  } break;
+  case 4: { // INVERSE_LINEAR_DEPTH
+    const float d = 1 - ((z - z_near) / (z_far - z_near));
+    res = make_float4(d, d, d, 1);
+  } break;
+  case 5: // PRIMITIVE
+  case 25: // MO_FLAGS
+    res = decode_rgba8(kPalette[h.primId % 20]);
+    break;
+  case 6: // TYPE
+    res = decode_rgba8(kPalette[type % 20]);
+    break;
+  case 22: // MATERIAL
+    res = decode_rgba8(kPalette[M.ids[M.offsets[geomId].x + h.primId % M.offsets[geomId].y] % 20]);
+    break;
+  case 8: { // NORMAL
+    const f3 v = mk3(fabsf(norm.x), fabsf(norm.y), fabsf(norm.z));
+    res = make_float4(0.25f + 0.5f * powf(v.x, 1.0f / 1.5f), 0.25f + 0.5f * powf(v.y, 1.0f / 1.5f),
+                      0.25f + 0.5f * powf(v.z, 1.0f / 1.5f), 0.5f + 0.5f * 1.0f);
+  } break;
+  case 9: // BARYCENTRIC
+    res = make_float4(h.coords[0], h.coords[1], 1 - h.coords[0] - h.coords[1], 1);
+    break;
+  case 10: // ST_ITERATIONS (primId holds the sphere-tracing steps)
+    if (h.primId == 0) {
+      res = make_float4(0.5f, 0.5f, 0.5f, 1.0f);
+    } else if (h.primId <= 64) {
+      const float q = sclamp(float(h.primId) / 64, 0.0f, 1.0f);
+      res = make_float4(q * 0 + (1.0f - q) * 0, q * 0 + (1.0f - q) * 1, q * 1 + (1.0f - q) * 0, q * 1 + (1.0f - q) * 1);
+    } else {
+      const float q = sclamp(float(h.primId - 64) / (256 - 64), 0.0f, 1.0f);
+      res = make_float4(q * 1 + (1.0f - q) * 0, q * 0 + (1.0f - q) * 0, q * 0 + (1.0f - q) * 1, q * 1 + (1.0f - q) * 1);
+    }
+    break;
+  case 24: // MO_VOXEL_COUNT
+    if (h.primId == 0) res = make_float4(0.5f, 0.5f, 0.5f, 1);
+    else if (h.primId == 1) res = make_float4(0.5f, 1, 0.5f, 1);
+    else if (h.primId == 2) res = make_float4(0.5f, 0.5f, 1, 1);
+    else if (h.primId <= 64) {
+      const float q = sclamp(float(h.primId) / 64, 0.0f, 1.0f);
+      res = make_float4(q * 1 + (1 - q) * 0.5f, q * 0 + (1 - q) * 0.5f, q * 0 + (1 - q) * 1, q * 1 + (1 - q) * 1);
+    } else {
+      res = make_float4(1, 0, 0, 1);
+    }
+    break;
+  case 19: { // HSV_DEPTH
+    const f3 isect = rayPos + z * rayDir;
+    float zt = (isect.z + 1.f) * 2.f;
+    zt = zt - float(int(zt));
+    if (zt < 0.f) zt = 1.f + zt;
+    const float hx = zt, hy = 1.f, hz = 1.f;
+    float col[4] = {hz, hz, hz, 1.f};
+    const float vmin = (1.f - hy) * hz;
+    const float x6 = hx * 6.f;
+    const float Hi = truncf(x6);
+    const float a = (hz - vmin) * (x6 - Hi);
+    uint32_t H = uint32_t(Hi);
+    H = H <= 5u ? H : 5u;
+    col[(2u + (H >> 1)) % 3u] = vmin;
+    if ((H & 1u) != 0u) col[H >> 1] = hz - a;
+    else col[(1u + (H >> 1)) % 3u] = vmin + a;
+    res = make_float4(col[0], col[1], col[2], 1.f);
+  } break;
+  case 16: { // DIFFUSE (colored materials)
+    float4 col = make_float4(0, 0, 1, 1);
+    if (type == LRT_TYPE_SDF_SBS_COL) {
+      const f3 pc = packed_hit_colour(h);
+      col = make_float4(pc.x, pc.y, pc.z, col.w);
+    } else {
+      const lrt_material& m = material();
+      col = make_float4(m.base_color[0], m.base_color[1], m.base_color[2], m.base_color[3]);
+    }
+    res = make_float4(col.x, col.y, col.z, 1);
+  } break;
+  case 1:  // LAMBERT_NO_TEX
+  case 7:  // GEOM
+  case 17: // LAMBERT (colored materials)
+  case 20: { // LOD
+    f3 color = mk3(0, 0, 1);
+    if (mode == 1) color = mk3(1, 1, 1);
+    else if (mode == 20) color = ld3(decode_rgba8(kLodPalette[h.primId % 20]));
+    else if (mode == 7) color = ld3(decode_rgba8(kPalette[geomId % 20]));
+    else if (type == LRT_TYPE_SDF_SBS_COL || type == LRT_TYPE_GRAPHICS_PRIM) color = packed_hit_colour(h);
+    else {
+      const lrt_material& m = material();
+      color = mk3(m.base_color[0], m.base_color[1], m.base_color[2]);
+    }
+    const f3 fc = lambert_lights(L, norm, color, rayPos, rayDir, h.t);
+    res = make_float4(fc.x, fc.y, fc.z, 1);
+  } break;
+  default:
+    break;
+  }
+  return tonemap_rgba8(res.x, res.y, res.z, 1.0f);
+}
+
 // Batched multi-camera form: one persistent launch over the pixel tiles of
 // all cameras.  A warp takes one tile at a time from the global counter,
 // finds its camera by binary search over the tile bases, and each lane
@@ -1015,12 +1204,13 @@ __device__ __forceinline__ float lambert(const lrt_hit& h, f3 dir, f3 L)
 // triangle and turned towards the viewer as in loadNormalTcFromGbuffer :27-75,
 // SDF normals decoded from the hit) and Tonemap (:536-542) into RGBA8.  A warp
 // takes 8x4-pixel tiles from a global counter.
+template <bool MODES>
 __global__ void __launch_bounds__(kTraceThreads, 7) k_render_rgba8(DevScene S, DevCamera cam, DevLights L,
                                                                 uint32_t* __restrict__ image,
                                                                 unsigned long long* __restrict__ work_counter,
                                                                 uint32_t* __restrict__ err_word, uint32_t stack_cap,
                                                                 const uint32_t* __restrict__ sched_rd,
-                                                                uint32_t* sched_wr)
+                                                                uint32_t* sched_wr, DevMaterials M, uint32_t mode)
 {
   extern __shared__ uint32_t smem_stack[];
   uint32_t* stack = smem_stack + threadIdx.x;
@@ -1045,7 +1235,8 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_render_rgba8(DevScene S, D
       lrt_hit h;
       trace_one(c, stack, blockDim.x, stack_cap, make_float4(r[0], r[1], r[2], r[3]),
                 make_float4(r[4], r[5], r[6], r[7]), h);
-      const uint32_t px = resolve_rgba8(c, L, mk3(r[0], r[1], r[2]), mk3(r[4], r[5], r[6]), h);
+      const uint32_t px = MODES ? resolve_mode_rgba8(c, L, M, mode, mk3(r[0], r[1], r[2]), mk3(r[4], r[5], r[6]), h)
+                                : resolve_rgba8(c, L, mk3(r[0], r[1], r[2]), mk3(r[4], r[5], r[6]), h);
       image[uint64_t(y) * cam.width + x] = px;
     }
   }
@@ -1232,14 +1423,19 @@ __global__ void __launch_bounds__(kTraceThreads) k_adjoint_lambert(DevScene S, c
 
 cudaError_t launch_render_rgba8(const DevScene& S, const DevCamera& cam, const DevLights& lights, uint32_t* image,
                                 unsigned long long* work_counter, uint32_t* err_word, uint32_t stack_cap, int grid,
-                                cudaStream_t stream, const uint32_t* sched_rd, uint32_t* sched_wr)
+                                cudaStream_t stream, const uint32_t* sched_rd, uint32_t* sched_wr,
+                                const DevMaterials* materials, uint32_t mode)
 {
   const size_t smem = trace_smem_bytes(stack_cap);
-  cudaError_t e = cudaFuncSetAttribute(k_render_rgba8, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  // LAMBERT_NO_TEX keeps its own instantiation (the benchmarked render);
+  // the other modes share the general resolve
+  const bool modes = mode != LRT_RENDER_MODE_LAMBERT_NO_TEX;
+  auto kernel = modes ? k_render_rgba8<true> : k_render_rgba8<false>;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(trace_smem_bytes(kMaxStackDev + 1)));
   if (e != cudaSuccess) return e;
-  k_render_rgba8<<<grid, kTraceThreads, smem, stream>>>(S, cam, lights, image, work_counter, err_word, stack_cap,
-                                                        sched_rd, sched_wr);
+  kernel<<<grid, kTraceThreads, smem, stream>>>(S, cam, lights, image, work_counter, err_word, stack_cap, sched_rd,
+                                                sched_wr, materials ? *materials : DevMaterials{}, mode);
   return cudaGetLastError();
 }
 

@@ -456,11 +456,18 @@ typedef struct lrt_light {
 enum { LRT_LIGHT_DIRECT = 0, LRT_LIGHT_POINT = 1, LRT_LIGHT_AMBIENT = 2 };
 #define LRT_MAX_LIGHTS 16
 
-/* MultiRenderer::Render (MultiRenderer.cpp:14-60) for the
- * MULTI_RENDER_MODE_LAMBERT_NO_TEX preset, one sample per pixel, no
- * transparency, fused into one launch: initEyeRay, RayQuery_NearestHit,
- * ResolveCommon (MultiRenderer_resolve.cpp:580-666: white albedo, the given
- * lights, `background` for misses) and Tonemap (:536-542).  Writes
+/* MultiRenderer::Render (MultiRenderer.cpp:14-60), one sample per pixel,
+ * fused into one launch: initEyeRay, RayQuery_NearestHit, the resolve of
+ * the preset's render_mode and Tonemap (MultiRenderer_resolve.cpp:536-542).
+ * Render modes: LAMBERT_NO_TEX (ResolveCommon :580-666: white albedo, the
+ * given lights), GEOM, LOD, and with the scene's COLORED materials
+ * (lrt_set_materials) LAMBERT and DIFFUSE; and kernel1D_ResolveDebug's
+ * (:810-990) MASK, DEPTH, LINEAR_DEPTH, INVERSE_LINEAR_DEPTH, HSV_DEPTH,
+ * PRIMITIVE, TYPE, MATERIAL, NORMAL, BARYCENTRIC, ST_ITERATIONS,
+ * MO_VOXEL_COUNT and MO_FLAGS.  Misses take `background`.  Other modes
+ * (textures, shadows, PBR, outlines, channels), textured materials, and
+ * transparent materials in LAMBERT or DIFFUSE (which the reference resolves
+ * through the transparency G-buffer) return LRT_ERR_UNSUPPORTED.  Writes
  * width*height RGBA8 pixels (row-major) to device memory image_dev;
  * asynchronous on `stream`, lrt_trace_sync(stream) reports bounded-loop
  * limits.  No counterpart call in the reference (it renders through a

@@ -971,10 +971,38 @@ static uint32_t tonemap_rgba8(float r, float g, float b, float a)
 }
 
 /* rays: the eye rays of the image in row-major pixel order (initEyeRay). */
-void lrto_render_rgba8(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* rays, uint64_t n,
-                       const lrt_light* lights, uint32_t light_count, const float background[4], uint32_t* image,
-                       int threads)
+/* MultiRenderer's palettes (MultiRenderer.h:269-283) and decode_RGBA8
+ * (utils/raytracing/render_common.h:250-254). */
+static const uint32_t kPalette[20] = {0xffe6194b, 0xff3cb44b, 0xffffe119, 0xff0082c8, 0xfff58231,
+                                      0xff911eb4, 0xff46f0f0, 0xfff032e6, 0xffd2f53c, 0xfffabebe,
+                                      0xff008080, 0xffe6beff, 0xffaa6e28, 0xfffffac8, 0xff800000,
+                                      0xffaaffc3, 0xff808000, 0xffffd8b1, 0xff000080, 0xff808080};
+static const uint32_t kLodPalette[20] = {0xff000000, 0xff000040, 0xff000080, 0xff0000c0, 0xff0040ff,
+                                         0xff0080ff, 0xff00c0ff, 0xff00ffff, 0xff00ffc0, 0xff00ff80,
+                                         0xff00ff40, 0xff00ff00, 0xff00c000, 0xff008000, 0xff004000,
+                                         0xff000000, 0xffff0000, 0xffff0000, 0xffff0000, 0xffff0000};
+static void decode_rgba8(uint32_t c, float out[4])
 {
+  out[0] = (float)(c & 0xFF) * (1.0f / 255.0f);
+  out[1] = (float)((c >> 8) & 0xFF) * (1.0f / 255.0f);
+  out[2] = (float)((c >> 16) & 0xFF) * (1.0f / 255.0f);
+  out[3] = (float)((c >> 24) & 0xFF) * (1.0f / 255.0f);
+}
+
+/* MultiRenderer::Render for one sample of the eye rays `rays` (row-major
+ * pixels): RayQuery_NearestHit, then ResolveCommon (MultiRenderer_resolve.cpp:
+ * 580-666) or kernel1D_ResolveDebug (:810-990) for preset->render_mode, then
+ * Tonemap (:536-542).  Modes: MASK, LAMBERT_NO_TEX, DEPTH, LINEAR_DEPTH,
+ * INVERSE_LINEAR_DEPTH, PRIMITIVE, TYPE, GEOM, NORMAL, BARYCENTRIC,
+ * ST_ITERATIONS, DIFFUSE, LAMBERT, HSV_DEPTH, LOD, MATERIAL, MO_VOXEL_COUNT,
+ * MO_FLAGS; materials COLORED only (offsets {start, size} per geometry; may
+ * be NULL for the modes that read none). */
+void lrto_render_rgba8_modes(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* rays, uint64_t n,
+                             const lrt_light* lights, uint32_t light_count, const float background[4],
+                             const lrt_material* materials, const uint32_t* mat_ids, const uint32_t* mat_offsets,
+                             uint32_t* image, int threads)
+{
+  const uint32_t mode = preset->render_mode;
   (void)threads;
 #ifdef _OPENMP
 #pragma omp parallel for num_threads(threads > 0 ? threads : 1) schedule(dynamic, 256)
@@ -988,11 +1016,12 @@ void lrto_render_rgba8(const lrt_scene_arrays* arrays, const lrt_preset* preset,
       image[i] = tonemap_rgba8(background[0], background[1], background[2], background[3]);
       continue;
     }
+    const uint32_t type = h.geomId >> 24, geomId = h.geomId & 0x00FFFFFFu;
     const f3 rayPos = mk3(r[0], r[1], r[2]), rayDir = mk3(r[4], r[5], r[6]);
     f3 norm;
-    if ((h.geomId >> 24) == LRT_TYPE_MESH_TRIANGLE) {
+    if (type == LRT_TYPE_MESH_TRIANGLE) {
       /* loadNormalTcFromGbuffer, NORMAL_MODE_GEOMETRY (:33-59) */
-      const uint32_t g = h.geomId & 0x00FFFFFFu;
+      const uint32_t g = geomId;
       const uint32_t base = arrays->geomData[g].offset[0] + 3 * c.tri_local;
       const float* vA = arrays->vertPos + 4 * (uint64_t)(arrays->geomData[g].offset[1] + arrays->indices[base + 0]);
       const float* vB = arrays->vertPos + 4 * (uint64_t)(arrays->geomData[g].offset[1] + arrays->indices[base + 1]);
@@ -1004,30 +1033,138 @@ void lrto_render_rgba8(const lrt_scene_arrays* arrays, const lrt_preset* preset,
     } else {
       norm = decode_normal(h.coords[2], h.coords[3]);
     }
-    /* ResolveCommon, LAMBERT_NO_TEX (:617-666): white albedo */
-    const f3 color = mk3(1, 1, 1);
-    f3 fc = mk3(0, 0, 0);
-    for (uint32_t k = 0; k < light_count; k++) {
-      const lrt_light* l = &lights[k];
-      const f3 lc = mk3(l->color[0], l->color[1], l->color[2]);
-      const f3 sp = mk3(l->space[0], l->space[1], l->space[2]);
-      if (l->type == LRT_LIGHT_DIRECT) {
-        const float q = smax(0.0f, dot3(norm, sp));
-        fc = add3(fc, scl3(q, mul3(lc, color)));
-      } else if (l->type == LRT_LIGHT_POINT) {
-        const f3 surf = add3(rayPos, scl3(h.t, rayDir));
-        f3 dir = sub3(sp, surf);
-        const float len = sqrtf(dot3(dir, dir));
-        dir = mk3(dir.x / len, dir.y / len, dir.z / len);
-        const float q = smax(0.0f, dot3(norm, dir));
-        const f3 lq = scl3(q, mul3(lc, color));
-        fc = add3(fc, mk3(lq.x / (len * len), lq.y / (len * len), lq.z / (len * len)));
+    /* m_matIdbyPrimId[m_matIdOffsets[geomId].x + primId % m_matIdOffsets[geomId].y] */
+#define MAT_ID() (mat_ids[mat_offsets[2 * geomId] + h.primId % mat_offsets[2 * geomId + 1]])
+    const float z = h.t, z_near = 0.1f, z_far = 10.0f;
+    float res[4] = {1, 0, 1, 1};
+    switch (mode) {
+    case 0: res[0] = res[1] = res[2] = res[3] = 1; break; /* MASK */
+    case 2: { /* DEPTH */
+      const float d = (1.0f / z - 1.0f / z_near) / (1.0f / z_far - 1.0f / z_near);
+      res[0] = res[1] = res[2] = d;
+    } break;
+    case 3: { /* LINEAR_DEPTH */
+      const float d = (z - z_near) / (z_far - z_near);
+      res[0] = res[1] = res[2] = d;
+    } break;
+    case 4: { /* INVERSE_LINEAR_DEPTH */
+      const float d = 1 - ((z - z_near) / (z_far - z_near));
+      res[0] = res[1] = res[2] = d;
+    } break;
+    case 5: case 25: decode_rgba8(kPalette[h.primId % 20], res); break; /* PRIMITIVE, MO_FLAGS */
+    case 6: decode_rgba8(kPalette[type % 20], res); break;               /* TYPE */
+    case 22: decode_rgba8(kPalette[MAT_ID() % 20], res); break;          /* MATERIAL */
+    case 8: { /* NORMAL */
+      const float vx = fabsf(norm.x), vy = fabsf(norm.y), vz = fabsf(norm.z);
+      res[0] = 0.25f + 0.5f * powf(vx, 1.0f / 1.5f);
+      res[1] = 0.25f + 0.5f * powf(vy, 1.0f / 1.5f);
+      res[2] = 0.25f + 0.5f * powf(vz, 1.0f / 1.5f);
+    } break;
+    case 9: /* BARYCENTRIC */
+      res[0] = h.coords[0];
+      res[1] = h.coords[1];
+      res[2] = 1 - h.coords[0] - h.coords[1];
+      break;
+    case 10: /* ST_ITERATIONS */
+      if (h.primId == 0) {
+        res[0] = res[1] = res[2] = 0.5f;
+      } else if (h.primId <= 64) {
+        const float q = sclamp((float)h.primId / 64, 0.0f, 1.0f);
+        res[0] = q * 0 + (1.0f - q) * 0;
+        res[1] = q * 0 + (1.0f - q) * 1;
+        res[2] = q * 1 + (1.0f - q) * 0;
       } else {
-        fc = add3(fc, mul3(lc, color));
+        const float q = sclamp((float)(h.primId - 64) / (256 - 64), 0.0f, 1.0f);
+        res[0] = q * 1 + (1.0f - q) * 0;
+        res[1] = q * 0 + (1.0f - q) * 0;
+        res[2] = q * 0 + (1.0f - q) * 1;
       }
+      break;
+    case 24: /* MO_VOXEL_COUNT */
+      if (h.primId == 0) { res[0] = 0.5f; res[1] = 0.5f; res[2] = 0.5f; }
+      else if (h.primId == 1) { res[0] = 0.5f; res[1] = 1; res[2] = 0.5f; }
+      else if (h.primId == 2) { res[0] = 0.5f; res[1] = 0.5f; res[2] = 1; }
+      else if (h.primId <= 64) {
+        const float q = sclamp((float)h.primId / 64, 0.0f, 1.0f);
+        res[0] = q * 1 + (1 - q) * 0.5f;
+        res[1] = q * 0 + (1 - q) * 0.5f;
+        res[2] = q * 0 + (1 - q) * 1;
+      } else { res[0] = 1; res[1] = 0; res[2] = 0; }
+      break;
+    case 19: { /* HSV_DEPTH */
+      const f3 isect = add3(rayPos, scl3(z, rayDir));
+      float zt = (isect.z + 1.f) * 2.f;
+      zt = zt - (float)(int)zt;
+      if (zt < 0.f) zt = 1.f + zt;
+      const float hx = zt, hy = 1.f, hz = 1.f;
+      float col[4] = {hz, hz, hz, 1.f};
+      const float vmin = (1.f - hy) * hz;
+      float Hi = 0.f;
+      const float a = (hz - vmin) * modff(hx * 6.f, &Hi);
+      uint32_t H = (uint32_t)Hi;
+      H = H <= 5u ? H : 5u;
+      col[(2u + (H >> 1)) % 3u] = vmin;
+      if ((H & 1u) != 0u) col[H >> 1] = hz - a;
+      else col[(1u + (H >> 1)) % 3u] = vmin + a;
+      res[0] = col[0]; res[1] = col[1]; res[2] = col[2];
+    } break;
+    case 16: { /* DIFFUSE, COLORED materials */
+      if (type == LRT_TYPE_SDF_SBS_COL) {
+        res[0] = roundf(h.coords[0]) / 255.0f;
+        res[1] = h.coords[0] - floorf(h.coords[0]);
+        res[2] = roundf(h.coords[1]) / 255.0f;
+      } else {
+        const lrt_material* m = &materials[MAT_ID()];
+        res[0] = m->base_color[0]; res[1] = m->base_color[1]; res[2] = m->base_color[2];
+      }
+    } break;
+    case 1: case 7: case 17: case 20: { /* LAMBERT_NO_TEX, GEOM, LAMBERT (COLORED), LOD */
+      f3 color = mk3(0, 0, 1);
+      float pc[4];
+      if (mode == 1) color = mk3(1, 1, 1);
+      else if (mode == 20) { decode_rgba8(kLodPalette[h.primId % 20], pc); color = mk3(pc[0], pc[1], pc[2]); }
+      else if (mode == 7) { decode_rgba8(kPalette[geomId % 20], pc); color = mk3(pc[0], pc[1], pc[2]); }
+      else if (type == LRT_TYPE_SDF_SBS_COL || type == LRT_TYPE_GRAPHICS_PRIM)
+        color = mk3(roundf(h.coords[0]) / 255.0f, h.coords[0] - floorf(h.coords[0]), roundf(h.coords[1]) / 255.0f);
+      else {
+        const lrt_material* m = &materials[MAT_ID()];
+        color = mk3(m->base_color[0], m->base_color[1], m->base_color[2]);
+      }
+      f3 fc = mk3(0, 0, 0);
+      for (uint32_t k = 0; k < light_count; k++) {
+        const lrt_light* l = &lights[k];
+        const f3 lc = mk3(l->color[0], l->color[1], l->color[2]);
+        const f3 sp = mk3(l->space[0], l->space[1], l->space[2]);
+        if (l->type == LRT_LIGHT_DIRECT) {
+          const float q = smax(0.0f, dot3(norm, sp));
+          fc = add3(fc, scl3(q, mul3(lc, color)));
+        } else if (l->type == LRT_LIGHT_POINT) {
+          const f3 surf = add3(rayPos, scl3(h.t, rayDir));
+          f3 dir = sub3(sp, surf);
+          const float len = sqrtf(dot3(dir, dir));
+          dir = mk3(dir.x / len, dir.y / len, dir.z / len);
+          const float q = smax(0.0f, dot3(norm, dir));
+          const f3 lq = scl3(q, mul3(lc, color));
+          fc = add3(fc, mk3(lq.x / (len * len), lq.y / (len * len), lq.z / (len * len)));
+        } else {
+          fc = add3(fc, mul3(lc, color));
+        }
+      }
+      res[0] = fc.x; res[1] = fc.y; res[2] = fc.z;
+    } break;
+    default: break;
     }
-    image[i] = tonemap_rgba8(fc.x, fc.y, fc.z, 1.0f);
+#undef MAT_ID
+    image[i] = tonemap_rgba8(res[0], res[1], res[2], 1.0f);
   }
+}
+
+/* rays: the eye rays of the image in row-major pixel order (initEyeRay). */
+void lrto_render_rgba8(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* rays, uint64_t n,
+                       const lrt_light* lights, uint32_t light_count, const float background[4], uint32_t* image,
+                       int threads)
+{
+  lrto_render_rgba8_modes(arrays, preset, rays, n, lights, light_count, background, NULL, NULL, NULL, image, threads);
 }
 
 /* MultiRenderer::AnyHit (MultiRenderer.cpp:223-246) as

@@ -204,24 +204,32 @@ def port_render_lambert(arrays, rays, light, preset=None, threads=os.cpu_count()
     return img
 
 
-def port_render_rgba8(arrays, rays, lights, background, preset=None, threads=os.cpu_count()):
+def port_render_rgba8(arrays, rays, lights, background, preset=None, threads=os.cpu_count(), materials=None,
+                      mat_ids=None, mat_offsets=None):
     """RGBA8 image of the eye rays `rays` (row-major pixels): nearest hit,
-    LAMBERT_NO_TEX resolve with `lights` (LIGHT_DTYPE) and tonemap."""
-    from graphic_lab_task_b200._abi import LIGHT_DTYPE
+    the resolve of preset.render_mode with `lights` (LIGHT_DTYPE) and the
+    renderer's COLORED materials (MATERIAL_DTYPE, ids, {start, size} per
+    geometry) where the mode reads them, and tonemap."""
+    from graphic_lab_task_b200._abi import LIGHT_DTYPE, MATERIAL_DTYPE
     lib = port_lib()
-    if not hasattr(lib, "_rgba8_bound"):
-        lib.lrto_render_rgba8.restype = None
-        lib.lrto_render_rgba8.argtypes = [C.POINTER(SceneArrays), C.POINTER(Preset), C.c_void_p, C.c_uint64,
-                                          C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int]
-        lib._rgba8_bound = True
+    if not hasattr(lib, "_rgba8_modes_bound"):
+        lib.lrto_render_rgba8_modes.restype = None
+        lib.lrto_render_rgba8_modes.argtypes = [C.POINTER(SceneArrays), C.POINTER(Preset), C.c_void_p, C.c_uint64,
+                                                C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                C.c_void_p, C.c_void_p, C.c_int]
+        lib._rgba8_modes_bound = True
     s, keep = arrays_to_struct(arrays)
     p = preset if preset is not None else parity_preset()
     rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
     lt = np.ascontiguousarray(lights, dtype=LIGHT_DTYPE)
     bg = np.ascontiguousarray(background, dtype=np.float32)
+    mats = None if materials is None else np.ascontiguousarray(materials, dtype=MATERIAL_DTYPE)
+    ids = None if mat_ids is None else np.ascontiguousarray(mat_ids, dtype=np.uint32)
+    offs = None if mat_offsets is None else np.ascontiguousarray(mat_offsets, dtype=np.uint32).reshape(-1)
     img = np.zeros(len(rays), np.uint32)
-    lib.lrto_render_rgba8(C.byref(s), C.byref(p), rays.ctypes.data, len(rays), lt.ctypes.data if len(lt) else None,
-                          len(lt), bg.ctypes.data, img.ctypes.data, int(threads))
+    ptr = lambda a: a.ctypes.data if a is not None and len(a) else None  # noqa: E731
+    lib.lrto_render_rgba8_modes(C.byref(s), C.byref(p), rays.ctypes.data, len(rays), ptr(lt), len(lt),
+                                bg.ctypes.data, ptr(mats), ptr(ids), ptr(offs), img.ctypes.data, int(threads))
     del keep
     return img
 

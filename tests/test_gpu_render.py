@@ -1,7 +1,8 @@
 """Fused camera render (lrt_render_rgba8): eye rays, nearest hit, the
-LAMBERT_NO_TEX resolve with direct, point and ambient lights, and the tonemap
-in one launch, bit-identical to the oracle's restatement of MultiRenderer's
-Render on the same scene arrays."""
+resolve of the preset's render mode (LAMBERT_NO_TEX with direct, point and
+ambient lights, and the other modes without textures, shadows or PBR) and the
+tonemap in one launch, bit-identical to the oracle's restatement of
+MultiRenderer's Render on the same scene arrays; and the transparency loop."""
 import numpy as np
 import pytest
 
@@ -69,11 +70,70 @@ def test_render_rgba8_refusals(cuda):
         sc.render_rgba8(cam, many, (0, 0, 0, 1), img.data_ptr())
     assert e.value.status == 1
     p = parity_preset()
-    p.render_mode = 0
+    p.render_mode = 11  # PBR_NO_TEX
     sc.SetPreset(p)
     with pytest.raises(LrtError) as e:
         sc.render_rgba8(cam, _lights(), (0, 0, 0, 1), img.data_ptr())
-    assert e.value.status == 6 and "LAMBERT_NO_TEX" in str(e.value)
+    assert e.value.status == 6 and "render_mode 11" in str(e.value)
+    from graphic_lab_task_b200 import MATERIAL_TEXTURED
+    from test_oracle import transparency_tables
+    for mode in (16, 17, 22):  # materials needed
+        p.render_mode = mode
+        sc.SetPreset(p)
+        with pytest.raises(LrtError) as e:
+            sc.render_rgba8(cam, _lights(), (0, 0, 0, 1), img.data_ptr())
+        assert e.value.status == 1 and "material range" in str(e.value)
+    mats, ids, offs = transparency_tables(4)  # has transparent and textured materials
+    sc.set_materials(mats, ids, offs)
+    p.render_mode = 17
+    sc.SetPreset(p)
+    with pytest.raises(LrtError) as e:
+        sc.render_rgba8(cam, _lights(), (0, 0, 0, 1), img.data_ptr())
+    assert e.value.status == 6
+    mats["base_color"][:, 3] = 1.0  # opaque, but one is textured
+    sc.set_materials(mats, ids, offs)
+    with pytest.raises(LrtError) as e:
+        sc.render_rgba8(cam, _lights(), (0, 0, 0, 1), img.data_ptr())
+    assert e.value.status == 6 and "textured" in str(e.value)
+    assert (mats["type"] == MATERIAL_TEXTURED).any()
+
+
+# the render modes of ResolveCommon / kernel1D_ResolveDebug without textures,
+# shadows or PBR (core/render_settings.h:61-88)
+RENDER_MODES = [0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 16, 17, 19, 20, 22, 24, 25]
+
+
+@pytest.mark.parametrize("mode", RENDER_MODES)
+def test_render_modes_match_oracle(cuda, mode):
+    """lrt_render_rgba8 in every implemented render mode equals the oracle's
+    restatement of Render pixel for pixel (NORMAL within one 8-bit step: its
+    pow is CUDA's on the device)."""
+    torch = cuda
+    from graphic_lab_task_b200 import MATERIAL_COLORED
+    from test_oracle import transparency_tables
+    sc = _mixed_scene()
+    mats, ids, offs = transparency_tables(4, seed=11)
+    mats["type"] = MATERIAL_COLORED
+    mats["base_color"][:, 3] = 1.0
+    sc.set_materials(mats, ids, offs)
+    p = parity_preset()
+    p.render_mode = mode
+    sc.SetPreset(p)
+    cam = wl.camera((0.5, 0.7, 3.5), width=160, height=120)
+    bg = (0.1, 0.2, 0.3, 1.0)
+    img = torch.zeros(cam.width * cam.height, dtype=torch.int32, device="cuda")
+    sc.render_rgba8(cam, _lights(), bg, img.data_ptr())
+    sc.sync()
+    got = img.cpu().numpy().view(np.uint32)
+    want = po.port_render_rgba8(sc.export_arrays(), wl.eye_rays_host(cam), _lights(), bg, preset=p, materials=mats,
+                                mat_ids=ids, mat_offsets=offs)
+    if mode == 8:
+        d = np.abs(got.view(np.uint8).astype(int) - want.view(np.uint8).astype(int))
+        assert d.max() <= 1 and (d > 0).mean() < 0.01
+    else:
+        assert np.array_equal(got, want), "%d of %d pixels differ" % ((got != want).sum(), len(got))
+    bgpx = (255 << 24) | (int(255 * 0.3) << 16) | (int(255 * 0.2) << 8) | int(255 * 0.1)
+    assert 0.05 < (got != bgpx).mean()  # hits in view
 
 
 def test_batched_render_equals_per_camera_render(cuda):
