@@ -1091,6 +1091,45 @@ __device__ uint32_t resolve_mode_rgba8(CTX& c, const DevLights& L, const DevMate
     const f3 fc = lambert_lights(L, norm, color, rayPos, rayDir, h.t);
     res = make_float4(fc.x, fc.y, fc.z, 1);
   } break;
+  case 12: // PHONG_NO_TEX
+  case 18: { // PHONG (colored materials); the reference's shadow ray is commented out (shade = 1)
+    const float Kd = 0.25f, Ks = 0.25f, BIAS = 1e-6f;
+    f3 color = mk3(0, 0, 1);
+    if (mode == 12) color = mk3(1, 1, 1);
+    else if (type == LRT_TYPE_SDF_SBS_COL || type == LRT_TYPE_GRAPHICS_PRIM) color = packed_hit_colour(h);
+    else {
+      const lrt_material& m = material();
+      color = mk3(m.base_color[0], m.base_color[1], m.base_color[2]);
+    }
+    f3 fc = mk3(0, 0, 0);
+    for (uint32_t i = 0; i < L.count; i++) {
+      const DevLight& l = L.light[i];
+      const f3 lc = mk3(l.color[0], l.color[1], l.color[2]);
+      const f3 sp = mk3(l.space[0], l.space[1], l.space[2]);
+      if (l.type == LRT_LIGHT_AMBIENT) {
+        fc = fc + lc * color;
+        continue;
+      }
+      const f3 surf = rayPos + (h.t - BIAS) * rayDir;
+      f3 light_dir = mk3(1, 1, 1);
+      if (l.type == LRT_LIGHT_DIRECT) {
+        light_dir = sp;
+        const float q = smax(0.0f, dot(norm, sp));
+        fc = fc + (lc * color) * q;
+      } else if (l.type == LRT_LIGHT_POINT) {
+        const f3 dir = sp - surf;
+        const float len = sqrtf(dot(dir, dir));
+        light_dir = mk3(dir.x / len, dir.y / len, dir.z / len);
+      }
+      const f3 refl = -1.0f * light_dir + (2.0f * dot(norm, light_dir)) * norm;
+      // Kd * max(0, n.l) + Ks * pow(max(0, n.r), 32): pow(float, int) is the
+      // double overload, so the sum is formed in double and rounded once
+      const double spec = double(Ks) * pow(double(smax(0.0f, dot(norm, refl))), 32.0);
+      const float k = float(double(Kd * smax(0.0f, dot(norm, light_dir))) + spec);
+      fc = fc + ((1.0f * lc) * k) * color;
+    }
+    res = make_float4(fc.x, fc.y, fc.z, 1);
+  } break;
   default:
     break;
   }

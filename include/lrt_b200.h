@@ -460,13 +460,14 @@ enum { LRT_LIGHT_DIRECT = 0, LRT_LIGHT_POINT = 1, LRT_LIGHT_AMBIENT = 2 };
  * fused into one launch: initEyeRay, RayQuery_NearestHit, the resolve of
  * the preset's render_mode and Tonemap (MultiRenderer_resolve.cpp:536-542).
  * Render modes: LAMBERT_NO_TEX (ResolveCommon :580-666: white albedo, the
- * given lights), GEOM, LOD, and with the scene's COLORED materials
- * (lrt_set_materials) LAMBERT and DIFFUSE; and kernel1D_ResolveDebug's
+ * given lights), PHONG_NO_TEX (:668-732; its shadow ray is commented out
+ * there), GEOM, LOD, and with the scene's COLORED materials
+ * (lrt_set_materials) LAMBERT, PHONG and DIFFUSE; and kernel1D_ResolveDebug's
  * (:810-990) MASK, DEPTH, LINEAR_DEPTH, INVERSE_LINEAR_DEPTH, HSV_DEPTH,
  * PRIMITIVE, TYPE, MATERIAL, NORMAL, BARYCENTRIC, ST_ITERATIONS,
  * MO_VOXEL_COUNT and MO_FLAGS.  Misses take `background`.  Other modes
- * (textures, shadows, PBR, outlines, channels), textured materials, and
- * transparent materials in LAMBERT or DIFFUSE (which the reference resolves
+ * (textures, PBR, outlines, channels), textured materials, and transparent
+ * materials in LAMBERT, PHONG or DIFFUSE (which the reference resolves
  * through the transparency G-buffer) return LRT_ERR_UNSUPPORTED.  Writes
  * width*height RGBA8 pixels (row-major) to device memory image_dev;
  * asynchronous on `stream`, lrt_trace_sync(stream) reports bounded-loop

@@ -1152,6 +1152,44 @@ void lrto_render_rgba8_modes(const lrt_scene_arrays* arrays, const lrt_preset* p
       }
       res[0] = fc.x; res[1] = fc.y; res[2] = fc.z;
     } break;
+    case 12: case 18: { /* PHONG_NO_TEX, PHONG (COLORED); the shadow ray is commented out (shade = 1) */
+      const float Kd = 0.25f, Ks = 0.25f, BIAS = 1e-6f;
+      f3 color = mk3(0, 0, 1);
+      if (mode == 12) color = mk3(1, 1, 1);
+      else if (type == LRT_TYPE_SDF_SBS_COL || type == LRT_TYPE_GRAPHICS_PRIM)
+        color = mk3(roundf(h.coords[0]) / 255.0f, h.coords[0] - floorf(h.coords[0]), roundf(h.coords[1]) / 255.0f);
+      else {
+        const lrt_material* m = &materials[MAT_ID()];
+        color = mk3(m->base_color[0], m->base_color[1], m->base_color[2]);
+      }
+      f3 fc = mk3(0, 0, 0);
+      for (uint32_t k = 0; k < light_count; k++) {
+        const lrt_light* l = &lights[k];
+        const f3 lc = mk3(l->color[0], l->color[1], l->color[2]);
+        const f3 sp = mk3(l->space[0], l->space[1], l->space[2]);
+        if (l->type == LRT_LIGHT_AMBIENT) {
+          fc = add3(fc, mul3(lc, color));
+          continue;
+        }
+        const f3 surf = add3(rayPos, scl3(h.t - BIAS, rayDir));
+        f3 light_dir = mk3(1, 1, 1);
+        if (l->type == LRT_LIGHT_DIRECT) {
+          light_dir = sp;
+          const float q = smax(0.0f, dot3(norm, sp));
+          fc = add3(fc, scl3(q, mul3(lc, color)));
+        } else if (l->type == LRT_LIGHT_POINT) {
+          const f3 dir = sub3(sp, surf);
+          const float len = sqrtf(dot3(dir, dir));
+          light_dir = mk3(dir.x / len, dir.y / len, dir.z / len);
+        }
+        const f3 refl = add3(scl3(-1.0f, light_dir), scl3(2.0f * dot3(norm, light_dir), norm));
+        /* std::pow(float, int) is the double overload */
+        const double spec = (double)Ks * pow((double)smax(0.0f, dot3(norm, refl)), 32);
+        const float kk = (float)((double)(Kd * smax(0.0f, dot3(norm, light_dir))) + spec);
+        fc = add3(fc, mul3(scl3(kk, scl3(1.0f, lc)), color));
+      }
+      res[0] = fc.x; res[1] = fc.y; res[2] = fc.z;
+    } break;
     default: break;
     }
 #undef MAT_ID

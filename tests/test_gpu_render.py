@@ -77,7 +77,7 @@ def test_render_rgba8_refusals(cuda):
     assert e.value.status == 6 and "render_mode 11" in str(e.value)
     from graphic_lab_task_b200 import MATERIAL_TEXTURED
     from test_oracle import transparency_tables
-    for mode in (16, 17, 22):  # materials needed
+    for mode in (16, 17, 18, 22):  # materials needed
         p.render_mode = mode
         sc.SetPreset(p)
         with pytest.raises(LrtError) as e:
@@ -100,14 +100,14 @@ def test_render_rgba8_refusals(cuda):
 
 # the render modes of ResolveCommon / kernel1D_ResolveDebug without textures,
 # shadows or PBR (core/render_settings.h:61-88)
-RENDER_MODES = [0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 16, 17, 19, 20, 22, 24, 25]
+RENDER_MODES = [0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 12, 16, 17, 18, 19, 20, 22, 24, 25]
 
 
 @pytest.mark.parametrize("mode", RENDER_MODES)
 def test_render_modes_match_oracle(cuda, mode):
     """lrt_render_rgba8 in every implemented render mode equals the oracle's
-    restatement of Render pixel for pixel (NORMAL within one 8-bit step: its
-    pow is CUDA's on the device)."""
+    restatement of Render pixel for pixel (NORMAL and the Phong modes within
+    one 8-bit step: their pow is CUDA's on the device)."""
     torch = cuda
     from graphic_lab_task_b200 import MATERIAL_COLORED
     from test_oracle import transparency_tables
@@ -127,7 +127,7 @@ def test_render_modes_match_oracle(cuda, mode):
     got = img.cpu().numpy().view(np.uint32)
     want = po.port_render_rgba8(sc.export_arrays(), wl.eye_rays_host(cam), _lights(), bg, preset=p, materials=mats,
                                 mat_ids=ids, mat_offsets=offs)
-    if mode == 8:
+    if mode in (8, 12, 18):
         d = np.abs(got.view(np.uint8).astype(int) - want.view(np.uint8).astype(int))
         assert d.max() <= 1 and (d > 0).mean() < 0.01
     else:
