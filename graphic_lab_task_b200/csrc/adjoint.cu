@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <iterator>
 #include <cstring>
 
@@ -195,18 +196,27 @@ lrt_status lrt_render_rgba8(lrt_scene* s, const lrt_camera* camera, const lrt_li
     st = check_material_ranges(s, "lrt_render_rgba8", mode == 16 ? kSkipDiffuse : mode == 22 ? kSkipNone : kSkipLambert);
     if (st != LRT_OK) return st;
     if (mode != 22)
-      for (const lrt_material& m : s->mats) {
+      for (const lrt_material& m : s->mats)
         if (m.type != LRT_MATERIAL_COLORED)
           return fail(s, LRT_ERR_UNSUPPORTED, "lrt_render_rgba8: textured materials are not implemented");
-        // CheckForTransparency (MultiRenderer.cpp:248-258): the reference then
-        // resolves through the transparency G-buffer
-        if (m.base_color[3] < 1.0f)
-          return fail(s, LRT_ERR_UNSUPPORTED,
-                      "lrt_render_rgba8: a transparent material makes the reference resolve mode %u through "
-                      "lrt_fill_gbuffer_transparency's G-buffer",
-                      mode);
-      }
   }
+  const uint32_t spp = s->preset.spp;
+  if (spp == 0 || spp > 1024)
+    return fail(s, LRT_ERR_UNSUPPORTED, "lrt_render_rgba8: spp %u (1..1024)", spp);
+  DevRenderModes RM{};
+  RM.mode = mode;
+  RM.samples = spp;
+  RM.sqrtSpp = uint32_t(std::sqrt(double(spp)));
+  RM.invSqrt = 1.0f / float(RM.sqrtSpp);
+  RM.random = s->preset.ray_gen_mode == 1; // RAY_GEN_MODE_RANDOM: the first Hamilton point
+  RM.randomX = 0.5f;
+  RM.randomY = float(0.333333);
+  // CheckForTransparency (MultiRenderer.cpp:248-258): with a transparent
+  // COLORED material, DIFFUSE, LAMBERT and PHONG go through the AnyHit
+  // G-buffer and ResolveCommonWithTransparency (:33-46, :556-577)
+  if (mode == 16 || mode == 17 || mode == 18)
+    for (const lrt_material& m : s->mats)
+      if (m.type == LRT_MATERIAL_COLORED && m.base_color[3] < 1.0f) RM.transparency = 1;
   if (camera->width == 0 || camera->height == 0) return LRT_OK;
   if ((st = upload_materials(s)) != LRT_OK) return st;
   DevCamera cam;
@@ -230,8 +240,9 @@ lrt_status lrt_render_rgba8(lrt_scene* s, const lrt_camera* camera, const lrt_li
   M.mats = d->mats;
   M.ids = d->matIds;
   M.offsets = reinterpret_cast<const uint2*>(d->matOffsets);
+  std::memcpy(M.background, background, sizeof(M.background));
   const cudaError_t e = lrt_exact::launch_render_rgba8(S, cam, L, image_dev, &slot->work, &slot->err, d->stackCap,
-                                                       grid, stream, rd, wr, &M, mode);
+                                                       grid, stream, rd, wr, &M, &RM);
   if (e != cudaSuccess) return cuda_fail(s, e, "render launch");
   sched_commit(s, stream, false);
   return LRT_OK;

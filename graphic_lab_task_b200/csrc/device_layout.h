@@ -164,6 +164,19 @@ struct DevMaterials {
   float background[4];
 };
 
+// The render mode of lrt_render_rgba8's general kernel: the preset's
+// render_mode, its sample count (initEyeRay's sqrt(spp) grid, or one point
+// for RAY_GEN_MODE_RANDOM) and whether the transparency path applies.
+struct DevRenderModes {
+  uint32_t mode;
+  uint32_t samples;
+  uint32_t sqrtSpp;
+  float invSqrt;
+  uint32_t random;
+  float randomX, randomY;
+  uint32_t transparency;
+};
+
 // One camera of a batched multi-camera trace: its rays are generated in the
 // kernel, tile by tile; hits go to out[rayOffset + y*width + x].
 struct DevBatchCamera {

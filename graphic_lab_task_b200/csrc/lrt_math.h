@@ -181,10 +181,11 @@ LRT_HD float trilinear(const float* v, f3 dp)
 // cutting plane disabled: EyeRayDirNormalized + transform_ray3f
 // (utils/raytracing/render_common.h:25-55).  out = {posAndNear, dirAndFar}.
 LRT_HD void eye_ray(const float* proj_inv, const float* world_view_inv, uint32_t x, uint32_t y, uint32_t w,
-                    uint32_t h, float tnear, float tfar, float* out)
+                    uint32_t h, float tnear, float tfar, float* out, float dx = 0.5f, float dy = 0.5f)
 {
-  const float fx = ((float)x + 0.5f) / (float)w;
-  const float fy = ((float)y + 0.5f) / (float)h;
+  // (dx, dy): the sample's position in the pixel (initEyeRay's d)
+  const float fx = ((float)x + dx) / (float)w;
+  const float fy = ((float)y + dy) / (float)h;
   const float px = 2.0f * fx - 1.0f, py = -2.0f * fy + 1.0f;
   // pos = projInv * float4(px, py, 1, 1); pos /= pos.w
   float q[4];

@@ -908,6 +908,48 @@ __device__ __forceinline__ uint32_t resolve_rgba8(CTX& c, const DevLights& L, f3
   }
 }
 
+// MultiRenderer::AnyHit (MultiRenderer.cpp:223-246) for the eye ray r:
+// nearest hits composited front to back, each trace restarting at the
+// previous hit point with r's tNear and direction, until the remaining alpha
+// is at most 0.01 or, unlike the reference's loop, after
+// LRT_MAX_TRANSPARENCY_LAYERS traces (error bit).  Misses take the
+// background; SBS_COL (11) and graphics-primitive (17) hits keep the
+// previous colour.  h is the last hit; tc and alpha the composited colour
+// and the remaining alpha.
+template <class CTX>
+__device__ void anyhit_loop(CTX& c, uint32_t* stack, uint32_t stack_cap, const DevMaterials& M, const float* r,
+                            lrt_hit& h, f3& tc, float& alpha)
+{
+  f3 pos = mk3(r[0], r[1], r[2]);
+  const f3 dir = mk3(r[4], r[5], r[6]);
+  tc = mk3(0.0f, 0.0f, 0.0f);
+  alpha = 1.0f;
+  float4 color = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  for (uint32_t layer = 0;; layer++) {
+    if (layer == LRT_MAX_TRANSPARENCY_LAYERS) {
+      c.err |= kErrLayerCap;
+      break;
+    }
+    const float wa = alpha * color.w;
+    tc = mk3(tc.x + wa * color.x, tc.y + wa * color.y, tc.z + wa * color.z);
+    alpha *= (1.0f - color.w);
+    trace_one(c, stack, blockDim.x, stack_cap, make_float4(pos.x, pos.y, pos.z, r[3]),
+              make_float4(r[4], r[5], r[6], r[7]), h);
+    const uint32_t type = h.geomId >> 24, geomId = h.geomId & 0x00FFFFFFu;
+    if (h.primId == 0xFFFFFFFFu) {
+      color = make_float4(M.background[0], M.background[1], M.background[2], M.background[3]);
+    } else if (type != LRT_TYPE_SDF_SBS_COL && type != LRT_TYPE_GRAPHICS_PRIM) {
+      const uint2 o = M.offsets[geomId];
+      const lrt_material& m = M.mats[M.ids[o.x + h.primId % o.y]];
+      color = m.type == LRT_MATERIAL_COLORED
+                  ? make_float4(m.base_color[0], m.base_color[1], m.base_color[2], m.base_color[3])
+                  : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    }
+    pos = pos + h.t * dir;
+    if (!(alpha > 0.01f)) break;
+  }
+}
+
 // MultiRenderer's colour palettes (MultiRenderer.h:269-283): objects by id
 // and LOD levels, RGBA8 words.
 __constant__ uint32_t kPalette[20] = {0xffe6194b, 0xff3cb44b, 0xffffe119, 0xff0082c8, 0xfff58231,
@@ -961,18 +1003,18 @@ __device__ __forceinline__ f3 lambert_lights(const DevLights& L, f3 norm, f3 col
 
 // ResolveCommon / kernel1D_ResolveDebug (MultiRenderer_resolve.cpp:580-666,
 // 810-990) of one traced eye ray for the render modes without textures,
-// shadows or PBR, then Tonemap: MASK, DEPTH, LINEAR_DEPTH,
+// shadows or PBR, before Tonemap (alpha 1 for hits, the background's for
+// misses): MASK, DEPTH, LINEAR_DEPTH,
 // INVERSE_LINEAR_DEPTH, PRIMITIVE, TYPE, GEOM, NORMAL, BARYCENTRIC,
 // ST_ITERATIONS, DIFFUSE, LAMBERT, HSV_DEPTH, LOD, MATERIAL, MO_VOXEL_COUNT
 // and MO_FLAGS (colored materials only).  The normal is loadNormalTcFromGbuffer's
 // (triangles recomputed and turned to the viewer, SDF hits decoded).
 template <class CTX>
-__device__ uint32_t resolve_mode_rgba8(CTX& c, const DevLights& L, const DevMaterials& M, uint32_t mode, f3 rayPos,
-                                       f3 rayDir, const lrt_hit& h)
+__device__ float4 resolve_mode_colour(CTX& c, const DevLights& L, const DevMaterials& M, uint32_t mode, f3 rayPos,
+                                      f3 rayDir, const lrt_hit& h)
 {
   const DevScene& S = c.S;
-  if (h.primId == 0xFFFFFFFFu)
-    return tonemap_rgba8(L.background[0], L.background[1], L.background[2], L.background[3]);
+  if (h.primId == 0xFFFFFFFFu) return make_float4(L.background[0], L.background[1], L.background[2], L.background[3]);
   const uint32_t type = h.geomId >> 24, geomId = h.geomId & 0x00FFFFFFu;
   f3 norm;
   if (type == LRT_TYPE_MESH_TRIANGLE) {
@@ -1133,7 +1175,7 @@ __device__ uint32_t resolve_mode_rgba8(CTX& c, const DevLights& L, const DevMate
   default:
     break;
   }
-  return tonemap_rgba8(res.x, res.y, res.z, 1.0f);
+  return make_float4(res.x, res.y, res.z, 1.0f);
 }
 
 // Batched multi-camera form: one persistent launch over the pixel tiles of
@@ -1249,7 +1291,7 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_render_rgba8(DevScene S, D
                                                                 unsigned long long* __restrict__ work_counter,
                                                                 uint32_t* __restrict__ err_word, uint32_t stack_cap,
                                                                 const uint32_t* __restrict__ sched_rd,
-                                                                uint32_t* sched_wr, DevMaterials M, uint32_t mode)
+                                                                uint32_t* sched_wr, DevMaterials M, DevRenderModes RM)
 {
   extern __shared__ uint32_t smem_stack[];
   uint32_t* stack = smem_stack + threadIdx.x;
@@ -1272,29 +1314,56 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_render_rgba8(DevScene S, D
       float r[8];
       eye_ray(cam.proj_inv, cam.world_view_inv, x, y, cam.width, cam.height, cam.tnear, cam.tfar, r);
       lrt_hit h;
-      trace_one(c, stack, blockDim.x, stack_cap, make_float4(r[0], r[1], r[2], r[3]),
-                make_float4(r[4], r[5], r[6], r[7]), h);
-      const uint32_t px = MODES ? resolve_mode_rgba8(c, L, M, mode, mk3(r[0], r[1], r[2]), mk3(r[4], r[5], r[6]), h)
-                                : resolve_rgba8(c, L, mk3(r[0], r[1], r[2]), mk3(r[4], r[5], r[6]), h);
-      image[uint64_t(y) * cam.width + x] = px;
+      if (!MODES) {
+        trace_one(c, stack, blockDim.x, stack_cap, make_float4(r[0], r[1], r[2], r[3]),
+                  make_float4(r[4], r[5], r[6], r[7]), h);
+        image[uint64_t(y) * cam.width + x] = resolve_rgba8(c, L, mk3(r[0], r[1], r[2]), mk3(r[4], r[5], r[6]), h);
+      } else {
+        // Render's sample loop (MultiRenderer.cpp:21-64): sample s traces the
+        // ray through initEyeRay's point s of the pixel; the resolve takes the
+        // sample-0 ray (ResolveCommon calls initEyeRay with sample 0) and,
+        // in the transparency path, blends with the composited layers
+        // (ResolveTransparency, MultiRenderer_resolve.cpp:573-577); the
+        // colours are summed and the sum divided by the sample count.
+        float r0[8];
+        eye_ray(cam.proj_inv, cam.world_view_inv, x, y, cam.width, cam.height, cam.tnear, cam.tfar, r0,
+                RM.random ? RM.randomX : RM.invSqrt * 0.5f, RM.random ? RM.randomY : RM.invSqrt * 0.5f);
+        const f3 rp0 = mk3(r0[0], r0[1], r0[2]), rd0 = mk3(r0[4], r0[5], r0[6]);
+        float4 acc = make_float4(0, 0, 0, 0);
+        for (uint32_t smp = 0; smp < RM.samples; smp++) {
+          float rs[8];
+          float dx = RM.randomX, dy = RM.randomY;
+          if (!RM.random) {
+            dx = RM.invSqrt * float(double(smp / RM.sqrtSpp) + 0.5);
+            dy = RM.invSqrt * float(double(smp % RM.sqrtSpp) + 0.5);
+          }
+          eye_ray(cam.proj_inv, cam.world_view_inv, x, y, cam.width, cam.height, cam.tnear, cam.tfar, rs, dx, dy);
+          f3 tc = mk3(0, 0, 0);
+          float alpha = 1.0f;
+          if (RM.transparency)
+            anyhit_loop(c, stack, stack_cap, M, rs, h, tc, alpha);
+          else
+            trace_one(c, stack, blockDim.x, stack_cap, make_float4(rs[0], rs[1], rs[2], rs[3]),
+                      make_float4(rs[4], rs[5], rs[6], rs[7]), h);
+          float4 col = resolve_mode_colour(c, L, M, RM.mode, rp0, rd0, h);
+          if (RM.transparency) col = make_float4(tc.x + alpha * col.x, tc.y + alpha * col.y, tc.z + alpha * col.z, col.w);
+          acc = smp == 0 ? col : make_float4(acc.x + col.x, acc.y + col.y, acc.z + col.z, acc.w + col.w);
+        }
+        const float ns = float(RM.samples);
+        image[uint64_t(y) * cam.width + x] = tonemap_rgba8(acc.x / ns, acc.y / ns, acc.z / ns, acc.w / ns);
+      }
     }
   }
   if (c.err) atomicOr(err_word, c.err);
 }
 
-// kernel1D_FillGbufferWithTransparency + AnyHit (MultiRenderer.cpp:204-246)
-// for one sample: per pixel of the camera (8x4-pixel tiles per warp) the loop
-// of nearest hits compositing the COLORED materials front to back, each trace
-// starting at the previous hit point with the eye ray's tNear and direction.
-// Misses take the background; SBS_COL (11) and graphics-primitive (17) hits
-// keep the previous colour.  The loop ends when the remaining alpha is at
-// most 0.01 or, unlike the reference's, after kMaxLayers traces (error bit).
+// kernel1D_FillGbufferWithTransparency (MultiRenderer.cpp:204-221) for one
+// sample: anyhit_loop per pixel of the camera (8x4-pixel tiles per warp).
 __global__ void __launch_bounds__(kTraceThreads, 7) k_fill_gbuffer_transparency(
     DevScene S, DevCamera cam, DevMaterials M, float4* __restrict__ transparency, lrt_hit* __restrict__ gbuffer,
     unsigned long long* __restrict__ work_counter, uint32_t* __restrict__ err_word, uint32_t stack_cap,
     const uint32_t* __restrict__ sched_rd, uint32_t* sched_wr)
 {
-  constexpr uint32_t kMaxLayers = LRT_MAX_TRANSPARENCY_LAYERS;
   extern __shared__ uint32_t smem_stack[];
   uint32_t* stack = smem_stack + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
@@ -1315,35 +1384,10 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_fill_gbuffer_transparency(
     if (x < cam.width && y < cam.height) {
       float r[8];
       eye_ray(cam.proj_inv, cam.world_view_inv, x, y, cam.width, cam.height, cam.tnear, cam.tfar, r);
-      f3 pos = mk3(r[0], r[1], r[2]);
-      const f3 dir = mk3(r[4], r[5], r[6]);
-      f3 tc = mk3(0.0f, 0.0f, 0.0f);
-      float alpha = 1.0f;
-      float4 color = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
       lrt_hit h;
-      for (uint32_t layer = 0;; layer++) {
-        if (layer == kMaxLayers) {
-          c.err |= kErrLayerCap;
-          break;
-        }
-        const float wa = alpha * color.w;
-        tc = mk3(tc.x + wa * color.x, tc.y + wa * color.y, tc.z + wa * color.z);
-        alpha *= (1.0f - color.w);
-        trace_one(c, stack, blockDim.x, stack_cap, make_float4(pos.x, pos.y, pos.z, r[3]),
-                  make_float4(r[4], r[5], r[6], r[7]), h);
-        const uint32_t type = h.geomId >> 24, geomId = h.geomId & 0x00FFFFFFu;
-        if (h.primId == 0xFFFFFFFFu) {
-          color = make_float4(M.background[0], M.background[1], M.background[2], M.background[3]);
-        } else if (type != LRT_TYPE_SDF_SBS_COL && type != LRT_TYPE_GRAPHICS_PRIM) {
-          const uint2 o = M.offsets[geomId];
-          const lrt_material& m = M.mats[M.ids[o.x + h.primId % o.y]];
-          color = m.type == LRT_MATERIAL_COLORED
-                      ? make_float4(m.base_color[0], m.base_color[1], m.base_color[2], m.base_color[3])
-                      : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-        }
-        pos = pos + h.t * dir;
-        if (!(alpha > 0.01f)) break;
-      }
+      f3 tc;
+      float alpha;
+      anyhit_loop(c, stack, stack_cap, M, r, h, tc, alpha);
       const uint64_t i = uint64_t(y) * cam.width + x;
       transparency[i] = make_float4(tc.x, tc.y, tc.z, alpha);
       float4* out = reinterpret_cast<float4*>(gbuffer + i);
@@ -1463,18 +1507,22 @@ __global__ void __launch_bounds__(kTraceThreads) k_adjoint_lambert(DevScene S, c
 cudaError_t launch_render_rgba8(const DevScene& S, const DevCamera& cam, const DevLights& lights, uint32_t* image,
                                 unsigned long long* work_counter, uint32_t* err_word, uint32_t stack_cap, int grid,
                                 cudaStream_t stream, const uint32_t* sched_rd, uint32_t* sched_wr,
-                                const DevMaterials* materials, uint32_t mode)
+                                const DevMaterials* materials, const DevRenderModes* rm)
 {
   const size_t smem = trace_smem_bytes(stack_cap);
-  // LAMBERT_NO_TEX keeps its own instantiation (the benchmarked render);
-  // the other modes share the general resolve
-  const bool modes = mode != LRT_RENDER_MODE_LAMBERT_NO_TEX;
+  // one sample of LAMBERT_NO_TEX keeps its own instantiation (the benchmarked
+  // render); the other modes, several samples and transparency share the
+  // general one
+  const bool modes = rm && (rm->mode != LRT_RENDER_MODE_LAMBERT_NO_TEX || rm->samples != 1 || rm->transparency);
   auto kernel = modes ? k_render_rgba8<true> : k_render_rgba8<false>;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(trace_smem_bytes(kMaxStackDev + 1)));
   if (e != cudaSuccess) return e;
+  DevRenderModes one{};
+  one.mode = LRT_RENDER_MODE_LAMBERT_NO_TEX;
+  one.samples = 1;
   kernel<<<grid, kTraceThreads, smem, stream>>>(S, cam, lights, image, work_counter, err_word, stack_cap, sched_rd,
-                                                sched_wr, materials ? *materials : DevMaterials{}, mode);
+                                                sched_wr, materials ? *materials : DevMaterials{}, rm ? *rm : one);
   return cudaGetLastError();
 }
 

@@ -163,9 +163,21 @@ def camera(eye, center=(0, 0, 0), up=(0, 1, 0), fovy=60.0, width=256, height=256
     return cam
 
 
-def eye_rays_host(cam):
-    """(H*W, 8) float32 rays in row-major pixel order; the float32 evaluation
-    order matches lrt::eye_ray (csrc/lrt_math.h)."""
+def sample_offset(sample, spp, ray_gen_mode=0):
+    """initEyeRay's position of sample `sample` of `spp` in the pixel
+    (MultiRenderer.cpp:162-166, first frame): a regular sqrt(spp) grid, or
+    the first Hamilton point for RAY_GEN_MODE_RANDOM."""
+    if ray_gen_mode == 1:
+        return F(0.5), F(0.333333)
+    q = int(math.sqrt(spp))
+    inv = F(1.0) / F(q)
+    return inv * F(sample // q + 0.5), inv * F(sample % q + 0.5)
+
+
+def eye_rays_host(cam, dx=0.5, dy=0.5):
+    """(H*W, 8) float32 rays in row-major pixel order through the points
+    (x + dx, y + dy) of the pixels; the float32 evaluation order matches
+    lrt::eye_ray (csrc/lrt_math.h)."""
     W, H = cam.width, cam.height
     P = np.array(cam.proj_inv[:], np.float32)
     M = np.array(cam.world_view_inv[:], np.float32)
@@ -173,8 +185,8 @@ def eye_rays_host(cam):
     x = (idx % W).astype(np.float32)
     y = (idx // W).astype(np.float32)
     with np.errstate(all="ignore"):
-        fx = (x + F(0.5)) / F(W)
-        fy = (y + F(0.5)) / F(H)
+        fx = (x + F(dx)) / F(W)
+        fy = (y + F(dy)) / F(H)
         px = F(2.0) * fx - F(1.0)
         py = F(-2.0) * fy + F(1.0)
         q = [px * P[i] + py * P[4 + i] + F(1.0) * P[8 + i] + F(1.0) * P[12 + i] for i in range(4)]

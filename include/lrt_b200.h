@@ -465,10 +465,15 @@ enum { LRT_LIGHT_DIRECT = 0, LRT_LIGHT_POINT = 1, LRT_LIGHT_AMBIENT = 2 };
  * (lrt_set_materials) LAMBERT, PHONG and DIFFUSE; and kernel1D_ResolveDebug's
  * (:810-990) MASK, DEPTH, LINEAR_DEPTH, INVERSE_LINEAR_DEPTH, HSV_DEPTH,
  * PRIMITIVE, TYPE, MATERIAL, NORMAL, BARYCENTRIC, ST_ITERATIONS,
- * MO_VOXEL_COUNT and MO_FLAGS.  Misses take `background`.  Other modes
- * (textures, PBR, outlines, channels), textured materials, and transparent
- * materials in LAMBERT, PHONG or DIFFUSE (which the reference resolves
- * through the transparency G-buffer) return LRT_ERR_UNSUPPORTED.  Writes
+ * MO_VOXEL_COUNT and MO_FLAGS.  Misses take `background`.  The preset's
+ * spp samples per pixel are traced through initEyeRay's sqrt(spp) grid (one
+ * point for RAY_GEN_MODE_RANDOM), resolved with the sample-0 ray as
+ * ResolveCommon does, and averaged; with a transparent COLORED material,
+ * LAMBERT, PHONG and DIFFUSE take the reference's transparency path (the
+ * AnyHit G-buffer blended into the resolved colour).  Other modes (textures,
+ * PBR, outlines, channels) and textured materials return
+ * LRT_ERR_UNSUPPORTED; the pixel grid is the camera's (the reference pads
+ * widths to a multiple of 8).  Writes
  * width*height RGBA8 pixels (row-major) to device memory image_dev;
  * asynchronous on `stream`, lrt_trace_sync(stream) reports bounded-loop
  * limits.  No counterpart call in the reference (it renders through a

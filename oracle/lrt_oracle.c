@@ -989,40 +989,34 @@ static void decode_rgba8(uint32_t c, float out[4])
   out[3] = (float)((c >> 24) & 0xFF) * (1.0f / 255.0f);
 }
 
-/* MultiRenderer::Render for one sample of the eye rays `rays` (row-major
- * pixels): RayQuery_NearestHit, then ResolveCommon (MultiRenderer_resolve.cpp:
- * 580-666) or kernel1D_ResolveDebug (:810-990) for preset->render_mode, then
- * Tonemap (:536-542).  Modes: MASK, LAMBERT_NO_TEX, DEPTH, LINEAR_DEPTH,
- * INVERSE_LINEAR_DEPTH, PRIMITIVE, TYPE, GEOM, NORMAL, BARYCENTRIC,
- * ST_ITERATIONS, DIFFUSE, LAMBERT, HSV_DEPTH, LOD, MATERIAL, MO_VOXEL_COUNT,
- * MO_FLAGS; materials COLORED only (offsets {start, size} per geometry; may
- * be NULL for the modes that read none). */
-void lrto_render_rgba8_modes(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* rays, uint64_t n,
-                             const lrt_light* lights, uint32_t light_count, const float background[4],
-                             const lrt_material* materials, const uint32_t* mat_ids, const uint32_t* mat_offsets,
-                             uint32_t* image, int threads)
+/* ResolveCommon (MultiRenderer_resolve.cpp:580-666) / kernel1D_ResolveDebug
+ * (:810-990) of hit h for `mode`, with the resolve ray r (initEyeRay of
+ * sample 0) and c->tri_local of the trace that found h: the float4 colour
+ * before Tonemap (alpha 1 for hits, the background's for misses).  Modes:
+ * MASK, LAMBERT_NO_TEX, DEPTH, LINEAR_DEPTH, INVERSE_LINEAR_DEPTH, PRIMITIVE,
+ * TYPE, GEOM, NORMAL, BARYCENTRIC, ST_ITERATIONS, PHONG_NO_TEX, DIFFUSE,
+ * LAMBERT, PHONG, HSV_DEPTH, LOD, MATERIAL, MO_VOXEL_COUNT, MO_FLAGS;
+ * materials COLORED only (offsets {start, size} per geometry; may be NULL
+ * for the modes that read none). */
+static void resolve_colour(const lrt_scene_arrays* arrays, const ctx_t* cp, uint32_t mode, lrt_hit h, const float* r,
+                           const lrt_light* lights, uint32_t light_count, const float background[4],
+                           const lrt_material* materials, const uint32_t* mat_ids, const uint32_t* mat_offsets,
+                           float out[4])
 {
-  const uint32_t mode = preset->render_mode;
-  (void)threads;
-#ifdef _OPENMP
-#pragma omp parallel for num_threads(threads > 0 ? threads : 1) schedule(dynamic, 256)
-#endif
-  for (int64_t i = 0; i < (int64_t)n; i++) {
-    uint64_t cnt[LRT_COUNTER_COUNT];
-    ctx_t c = {arrays, preset, cnt, 0, NULL, 0};
-    const float* r = rays + 8 * i;
-    const lrt_hit h = nearest_hit(&c, r, r + 4);
-    if (h.primId == 0xFFFFFFFFu) {
-      image[i] = tonemap_rgba8(background[0], background[1], background[2], background[3]);
-      continue;
-    }
+  const ctx_t cc = *cp;
+  const ctx_t* c = &cc;
+  if (h.primId == 0xFFFFFFFFu) {
+    memcpy(out, background, 4 * sizeof(float));
+    return;
+  }
+  {
     const uint32_t type = h.geomId >> 24, geomId = h.geomId & 0x00FFFFFFu;
     const f3 rayPos = mk3(r[0], r[1], r[2]), rayDir = mk3(r[4], r[5], r[6]);
     f3 norm;
     if (type == LRT_TYPE_MESH_TRIANGLE) {
       /* loadNormalTcFromGbuffer, NORMAL_MODE_GEOMETRY (:33-59) */
       const uint32_t g = geomId;
-      const uint32_t base = arrays->geomData[g].offset[0] + 3 * c.tri_local;
+      const uint32_t base = arrays->geomData[g].offset[0] + 3 * c->tri_local;
       const float* vA = arrays->vertPos + 4 * (uint64_t)(arrays->geomData[g].offset[1] + arrays->indices[base + 0]);
       const float* vB = arrays->vertPos + 4 * (uint64_t)(arrays->geomData[g].offset[1] + arrays->indices[base + 1]);
       const float* vC = arrays->vertPos + 4 * (uint64_t)(arrays->geomData[g].offset[1] + arrays->indices[base + 2]);
@@ -1193,24 +1187,67 @@ void lrto_render_rgba8_modes(const lrt_scene_arrays* arrays, const lrt_preset* p
     default: break;
     }
 #undef MAT_ID
-    image[i] = tonemap_rgba8(res[0], res[1], res[2], 1.0f);
+    out[0] = res[0];
+    out[1] = res[1];
+    out[2] = res[2];
+    out[3] = 1.0f;
   }
 }
 
-/* rays: the eye rays of the image in row-major pixel order (initEyeRay). */
-void lrto_render_rgba8(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* rays, uint64_t n,
-                       const lrt_light* lights, uint32_t light_count, const float background[4], uint32_t* image,
-                       int threads)
-{
-  lrto_render_rgba8_modes(arrays, preset, rays, n, lights, light_count, background, NULL, NULL, NULL, image, threads);
-}
 
-/* MultiRenderer::AnyHit (MultiRenderer.cpp:223-246) as
- * kernel1D_FillGbufferWithTransparency (:204-221) calls it per eye ray:
+/* MultiRenderer::AnyHit (MultiRenderer.cpp:223-246) for the eye ray r:
  * nearest hits composited front to back, each trace restarting at the
  * previous hit point; offsets are {start, size} per geometry.  The loop is
- * the reference's, bounded by max_layers traces (the reference has no bound);
- * returns how many rays reached that bound. */
+ * the reference's, bounded by max_layers traces (the reference has no
+ * bound); returns 1 if it reached that bound. */
+static int anyhit(ctx_t* c, const float* r, const lrt_material* materials, const uint32_t* mat_ids,
+                  const uint32_t* mat_offsets, const float background[4], uint32_t max_layers, lrt_hit* out,
+                  f3* out_tc, float* out_alpha)
+{
+  float pn[4] = {r[0], r[1], r[2], r[3]};
+  f3 tc = mk3(0, 0, 0);
+  float alpha = 1.0f;
+  float color[4] = {0, 0, 0, 0};
+  lrt_hit h;
+  uint32_t layer = 0;
+  int capped = 0;
+  memset(&h, 0, sizeof(h));
+  do {
+    if (layer++ == max_layers) {
+      capped = 1;
+      break;
+    }
+    /* transparencyColor += alpha * color.w * to_float3(color) */
+    const float wa = alpha * color[3];
+    tc = mk3(tc.x + wa * color[0], tc.y + wa * color[1], tc.z + wa * color[2]);
+    alpha *= (1.0f - color[3]);
+    h = nearest_hit(c, pn, r + 4);
+    const uint32_t type = h.geomId >> 24, geomId = h.geomId & 0x00FFFFFFu;
+    if (h.primId == 0xFFFFFFFFu) {
+      memcpy(color, background, sizeof(color));
+    } else if (type != LRT_TYPE_SDF_SBS_COL && type != LRT_TYPE_GRAPHICS_PRIM) {
+      const uint32_t matId = mat_ids[mat_offsets[2 * geomId] + h.primId % mat_offsets[2 * geomId + 1]];
+      const lrt_material* m = &materials[matId];
+      if (m->type == LRT_MATERIAL_COLORED) {
+        memcpy(color, m->base_color, sizeof(color));
+      } else {
+        color[0] = color[1] = color[2] = 0.0f;
+        color[3] = 1.0f;
+      }
+    }
+    /* rayPos = to_float3(rayPosAndNear) + to_float3(rayDirAndFar) * hit->t */
+    pn[0] = pn[0] + r[4] * h.t;
+    pn[1] = pn[1] + r[5] * h.t;
+    pn[2] = pn[2] + r[6] * h.t;
+  } while (alpha > 0.01f);
+  *out = h;
+  *out_tc = tc;
+  *out_alpha = alpha;
+  return capped;
+}
+
+/* kernel1D_FillGbufferWithTransparency (MultiRenderer.cpp:204-221): anyhit
+ * per eye ray; returns how many rays reached the layer bound. */
 uint64_t lrto_fill_gbuffer_transparency(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* rays,
                                         uint64_t n, const lrt_material* materials, const uint32_t* mat_ids,
                                         const uint32_t* mat_offsets, const float background[4], uint32_t max_layers,
@@ -1224,46 +1261,77 @@ uint64_t lrto_fill_gbuffer_transparency(const lrt_scene_arrays* arrays, const lr
   for (int64_t i = 0; i < (int64_t)n; i++) {
     uint64_t cnt[LRT_COUNTER_COUNT];
     ctx_t c = {arrays, preset, cnt, 0, NULL, 0};
-    const float* r = rays + 8 * i;
-    float pn[4] = {r[0], r[1], r[2], r[3]};
-    f3 tc = mk3(0, 0, 0);
-    float alpha = 1.0f;
-    float color[4] = {0, 0, 0, 0};
-    lrt_hit h;
-    uint32_t layer = 0;
-    do {
-      if (layer++ == max_layers) {
-        capped++;
-        break;
-      }
-      /* transparencyColor += alpha * color.w * to_float3(color) */
-      const float wa = alpha * color[3];
-      tc = mk3(tc.x + wa * color[0], tc.y + wa * color[1], tc.z + wa * color[2]);
-      alpha *= (1.0f - color[3]);
-      h = nearest_hit(&c, pn, r + 4);
-      const uint32_t type = h.geomId >> 24, geomId = h.geomId & 0x00FFFFFFu;
-      if (h.primId == 0xFFFFFFFFu) {
-        memcpy(color, background, sizeof(color));
-      } else if (type != LRT_TYPE_SDF_SBS_COL && type != LRT_TYPE_GRAPHICS_PRIM) {
-        const uint32_t matId = mat_ids[mat_offsets[2 * geomId] + h.primId % mat_offsets[2 * geomId + 1]];
-        const lrt_material* m = &materials[matId];
-        if (m->type == LRT_MATERIAL_COLORED) {
-          memcpy(color, m->base_color, sizeof(color));
-        } else {
-          color[0] = color[1] = color[2] = 0.0f;
-          color[3] = 1.0f;
-        }
-      }
-      /* rayPos = to_float3(rayPosAndNear) + to_float3(rayDirAndFar) * hit->t */
-      pn[0] = pn[0] + r[4] * h.t;
-      pn[1] = pn[1] + r[5] * h.t;
-      pn[2] = pn[2] + r[6] * h.t;
-    } while (alpha > 0.01f);
+    f3 tc;
+    float alpha;
+    capped += (uint64_t)anyhit(&c, rays + 8 * i, materials, mat_ids, mat_offsets, background, max_layers, &hits[i],
+                               &tc, &alpha);
     transparency[4 * i + 0] = tc.x;
     transparency[4 * i + 1] = tc.y;
     transparency[4 * i + 2] = tc.z;
     transparency[4 * i + 3] = alpha;
-    hits[i] = h;
   }
   return capped;
+}
+
+/* MultiRenderer::Render (MultiRenderer.cpp:14-70) for one pass of
+ * `samples` samples: sample s traces sample_rays[s] (n row-major eye rays
+ * through initEyeRay's point s of each pixel) — through anyhit when
+ * `transparency` (DIFFUSE / LAMBERT / PHONG with a transparent material),
+ * blending as ResolveTransparency (MultiRenderer_resolve.cpp:573-577) — and
+ * resolves with resolve_rays (sample 0's, as ResolveCommon does); the
+ * colours are summed, divided by the sample count and tonemapped. */
+void lrto_render_rgba8_ex(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* sample_rays,
+                          uint32_t samples, const float* resolve_rays, uint64_t n, const lrt_light* lights,
+                          uint32_t light_count, const float background[4], const lrt_material* materials,
+                          const uint32_t* mat_ids, const uint32_t* mat_offsets, int transparency, uint32_t max_layers,
+                          uint32_t* image, int threads)
+{
+  const uint32_t mode = preset->render_mode;
+  (void)threads;
+#ifdef _OPENMP
+#pragma omp parallel for num_threads(threads > 0 ? threads : 1) schedule(dynamic, 256)
+#endif
+  for (int64_t i = 0; i < (int64_t)n; i++) {
+    uint64_t cnt[LRT_COUNTER_COUNT];
+    float acc[4] = {0, 0, 0, 0};
+    for (uint32_t smp = 0; smp < samples; smp++) {
+      ctx_t c = {arrays, preset, cnt, 0, NULL, 0};
+      const float* r = sample_rays + 8 * ((uint64_t)smp * n + (uint64_t)i);
+      lrt_hit h;
+      f3 tc = mk3(0, 0, 0);
+      float alpha = 1.0f, col[4];
+      if (transparency)
+        anyhit(&c, r, materials, mat_ids, mat_offsets, background, max_layers, &h, &tc, &alpha);
+      else
+        h = nearest_hit(&c, r, r + 4);
+      resolve_colour(arrays, &c, mode, h, resolve_rays + 8 * i, lights, light_count, background, materials, mat_ids,
+                     mat_offsets, col);
+      if (transparency) {
+        col[0] = tc.x + alpha * col[0];
+        col[1] = tc.y + alpha * col[1];
+        col[2] = tc.z + alpha * col[2];
+      }
+      for (int k = 0; k < 4; k++) acc[k] = smp == 0 ? col[k] : acc[k] + col[k];
+    }
+    const float ns = (float)samples;
+    image[i] = tonemap_rgba8(acc[0] / ns, acc[1] / ns, acc[2] / ns, acc[3] / ns);
+  }
+}
+
+void lrto_render_rgba8_modes(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* rays, uint64_t n,
+                             const lrt_light* lights, uint32_t light_count, const float background[4],
+                             const lrt_material* materials, const uint32_t* mat_ids, const uint32_t* mat_offsets,
+                             uint32_t* image, int threads)
+{
+  lrto_render_rgba8_ex(arrays, preset, rays, 1, rays, n, lights, light_count, background, materials, mat_ids,
+                       mat_offsets, 0, 256, image, threads);
+}
+
+/* rays: the eye rays of the image in row-major pixel order (initEyeRay). */
+void lrto_render_rgba8(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* rays, uint64_t n,
+                       const lrt_light* lights, uint32_t light_count, const float background[4], uint32_t* image,
+                       int threads)
+{
+  lrto_render_rgba8_ex(arrays, preset, rays, 1, rays, n, lights, light_count, background, NULL, NULL, NULL, 0, 256,
+                       image, threads);
 }

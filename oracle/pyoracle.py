@@ -234,6 +234,39 @@ def port_render_rgba8(arrays, rays, lights, background, preset=None, threads=os.
     return img
 
 
+def port_render_rgba8_samples(arrays, sample_rays, resolve_rays, lights, background, preset, materials=None,
+                              mat_ids=None, mat_offsets=None, transparency=False, max_layers=256,
+                              threads=os.cpu_count()):
+    """Render's sample loop: sample_rays is (samples, n, 8) (initEyeRay's
+    point s of each pixel), resolve_rays (n, 8) the sample-0 rays the resolve
+    uses; `transparency` takes the AnyHit path of DIFFUSE / LAMBERT / PHONG."""
+    from graphic_lab_task_b200._abi import LIGHT_DTYPE, MATERIAL_DTYPE
+    lib = port_lib()
+    if not hasattr(lib, "_rgba8_ex_bound"):
+        lib.lrto_render_rgba8_ex.restype = None
+        lib.lrto_render_rgba8_ex.argtypes = [C.POINTER(SceneArrays), C.POINTER(Preset), C.c_void_p, C.c_uint32,
+                                             C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_void_p, C.c_int]
+        lib._rgba8_ex_bound = True
+    s, keep = arrays_to_struct(arrays)
+    sr = np.ascontiguousarray(sample_rays, dtype=np.float32)
+    rr = np.ascontiguousarray(resolve_rays, dtype=np.float32).reshape(-1, 8)
+    n = len(rr)
+    assert sr.size == sr.shape[0] * n * 8
+    lt = np.ascontiguousarray(lights, dtype=LIGHT_DTYPE)
+    bg = np.ascontiguousarray(background, dtype=np.float32)
+    mats = None if materials is None else np.ascontiguousarray(materials, dtype=MATERIAL_DTYPE)
+    ids = None if mat_ids is None else np.ascontiguousarray(mat_ids, dtype=np.uint32)
+    offs = None if mat_offsets is None else np.ascontiguousarray(mat_offsets, dtype=np.uint32).reshape(-1)
+    img = np.zeros(n, np.uint32)
+    ptr = lambda a: a.ctypes.data if a is not None and len(a) else None  # noqa: E731
+    lib.lrto_render_rgba8_ex(C.byref(s), C.byref(preset), sr.ctypes.data, sr.shape[0], rr.ctypes.data, n, ptr(lt),
+                             len(lt), bg.ctypes.data, ptr(mats), ptr(ids), ptr(offs), int(bool(transparency)),
+                             int(max_layers), img.ctypes.data, int(threads))
+    del keep
+    return img
+
+
 def port_fill_gbuffer_transparency(arrays, rays, materials, mat_ids, mat_offsets, background, max_layers=256,
                                    preset=None, threads=os.cpu_count()):
     """AnyHit's transparency loop per eye ray (rays: row-major pixels).
