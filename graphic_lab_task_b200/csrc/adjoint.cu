@@ -182,18 +182,21 @@ lrt_status lrt_render_rgba8(lrt_scene* s, const lrt_camera* camera, const lrt_li
   if (light_count > LRT_MAX_LIGHTS)
     return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_render_rgba8: %u lights (at most %d)", light_count, LRT_MAX_LIGHTS);
   const uint32_t mode = s->preset.render_mode;
-  static const uint32_t kModes[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 12, 16, 17, 18, 19, 20, 22, 24, 25};
+  static const uint32_t kModes[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 16, 17, 18, 19, 20, 21, 22, 24, 25};
   if (std::find(std::begin(kModes), std::end(kModes), mode) == std::end(kModes))
     return fail(s, LRT_ERR_UNSUPPORTED,
                 "lrt_render_rgba8: render_mode %u (textures, shadows, PBR, outlines, channels and intersection "
                 "counts are outside the ray-query path)",
                 mode);
-  if (mode == 16 || mode == 17 || mode == 18 || mode == 22) {
-    // DIFFUSE, LAMBERT and PHONG read COLORED materials; MATERIAL the material ids
+  if (mode == 11 && (s->mats.empty() || s->mats[0].type != LRT_MATERIAL_COLORED))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_render_rgba8: PBR_NO_TEX shades with material 0, a COLORED one");
+  if (mode == 16 || mode == 17 || mode == 18 || mode == 21 || mode == 22) {
+    // DIFFUSE, LAMBERT, PHONG and PBR read COLORED materials; MATERIAL the material ids
     static const uint32_t kSkipDiffuse[] = {LRT_TYPE_SDF_SBS_COL, ~0u};
     static const uint32_t kSkipLambert[] = {LRT_TYPE_SDF_SBS_COL, LRT_TYPE_GRAPHICS_PRIM, ~0u};
     static const uint32_t kSkipNone[] = {~0u};
-    st = check_material_ranges(s, "lrt_render_rgba8", mode == 16 ? kSkipDiffuse : mode == 22 ? kSkipNone : kSkipLambert);
+    st = check_material_ranges(s, "lrt_render_rgba8",
+                               mode == 16 ? kSkipDiffuse : (mode == 21 || mode == 22) ? kSkipNone : kSkipLambert);
     if (st != LRT_OK) return st;
     if (mode != 22)
       for (const lrt_material& m : s->mats)
@@ -212,9 +215,9 @@ lrt_status lrt_render_rgba8(lrt_scene* s, const lrt_camera* camera, const lrt_li
   RM.randomX = 0.5f;
   RM.randomY = float(0.333333);
   // CheckForTransparency (MultiRenderer.cpp:248-258): with a transparent
-  // COLORED material, DIFFUSE, LAMBERT and PHONG go through the AnyHit
+  // COLORED material, DIFFUSE, LAMBERT, PHONG and PBR go through the AnyHit
   // G-buffer and ResolveCommonWithTransparency (:33-46, :556-577)
-  if (mode == 16 || mode == 17 || mode == 18)
+  if (mode == 16 || mode == 17 || mode == 18 || mode == 21)
     for (const lrt_material& m : s->mats)
       if (m.type == LRT_MATERIAL_COLORED && m.base_color[3] < 1.0f) RM.transparency = 1;
   if (camera->width == 0 || camera->height == 0) return LRT_OK;

@@ -1133,6 +1133,47 @@ __device__ float4 resolve_mode_colour(CTX& c, const DevLights& L, const DevMater
     const f3 fc = lambert_lights(L, norm, color, rayPos, rayDir, h.t);
     res = make_float4(fc.x, fc.y, fc.z, 1);
   } break;
+  case 11: // PBR_NO_TEX (material 0, DEFAULT_MATERIAL)
+  case 21: { // PBR (colored materials)
+    const lrt_material& m = mode == 11 ? M.mats[0] : material();
+    const f3 baseColor = mk3(m.base_color[0], m.base_color[1], m.base_color[2]);
+    const float metallic = m.metallic, roughness = m.roughness;
+    const float alpha = roughness * roughness, f0 = 0.04f, kPi = 3.14159265358979323846f; // LiteMath's M_PI, a float
+    const f3 surf = rayPos + h.t * rayDir;
+    const f3 eye_dir = -1.0f * rayDir;
+    const float NV = dot(norm, eye_dir);
+    f3 fc = mk3(0, 0, 0);
+    for (uint32_t i = 0; i < L.count; i++) {
+      const DevLight& l = L.light[i];
+      f3 light_dir = mk3(1, 1, 1);
+      if (l.type == LRT_LIGHT_DIRECT) {
+        light_dir = mk3(l.space[0], l.space[1], l.space[2]);
+      } else if (l.type == LRT_LIGHT_POINT) {
+        light_dir = mk3(l.space[0], l.space[1], l.space[2]) - surf;
+        const float len = sqrtf(dot(light_dir, light_dir));
+        light_dir = mk3(light_dir.x / len, light_dir.y / len, light_dir.z / len);
+      }
+      f3 half = eye_dir + light_dir;
+      const float hl = sqrtf(dot(half, half));
+      half = mk3(half.x / hl, half.y / hl, half.z / hl);
+      const float NH = dot(norm, half), NL = dot(norm, light_dir), HL = dot(half, light_dir), HV = dot(half, eye_dir);
+      const float D = alpha * smax(0.0f, NH) / smax(kPi * powf(NH * NH * (alpha - 1.0f) + 1.0f, 2.0f), 0.00001f);
+      float V = smax(0.0f, HL) / smax(fabsf(NL) + sqrtf(alpha + (1 - alpha) * NL * NL), 0.00001f);
+      V *= smax(0.0f, HV) / smax(fabsf(NV) + sqrtf(alpha + (1 - alpha) * NV * NV), 0.00001f);
+      const float spec = V * D;
+      const float ip = 1.0f / kPi;
+      const f3 diffuse = mk3(ip * baseColor.x, ip * baseColor.y, ip * baseColor.z);
+      const float p5 = powf(1.0f - fabsf(HV), 5.0f);
+      const f3 metal = spec * mk3(baseColor.x + (1.0f - baseColor.x) * p5, baseColor.y + (1.0f - baseColor.y) * p5,
+                                  baseColor.z + (1.0f - baseColor.z) * p5);
+      const float F = f0 + (1.0f - f0) * p5;
+      const float fs = F * spec;
+      const f3 diel = mk3((1.0f - F) * diffuse.x + fs, (1.0f - F) * diffuse.y + fs, (1.0f - F) * diffuse.z + fs);
+      const f3 brdf = (1.0f - metallic) * diel + metallic * metal;
+      fc = fc + brdf * smax(NL, 0.0f);
+    }
+    res = make_float4(fc.x, fc.y, fc.z, 1);
+  } break;
   case 12: // PHONG_NO_TEX
   case 18: { // PHONG (colored materials); the reference's shadow ray is commented out (shade = 1)
     const float Kd = 0.25f, Ks = 0.25f, BIAS = 1e-6f;

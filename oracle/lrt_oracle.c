@@ -1146,6 +1146,47 @@ static void resolve_colour(const lrt_scene_arrays* arrays, const ctx_t* cp, uint
       }
       res[0] = fc.x; res[1] = fc.y; res[2] = fc.z;
     } break;
+    case 11: case 21: { /* PBR_NO_TEX (material 0), PBR (COLORED) */
+      const lrt_material* m = mode == 11 ? &materials[0] : &materials[MAT_ID()];
+      const f3 baseColor = mk3(m->base_color[0], m->base_color[1], m->base_color[2]);
+      const float metallic = m->metallic, roughness = m->roughness;
+      const float alpha = roughness * roughness, f0 = 0.04f;
+      const f3 surf = add3(rayPos, scl3(h.t, rayDir));
+      const f3 eye_dir = scl3(-1.0f, rayDir);
+      const float NV = dot3(norm, eye_dir);
+      f3 fc = mk3(0, 0, 0);
+      for (uint32_t k = 0; k < light_count; k++) {
+        const lrt_light* l = &lights[k];
+        f3 light_dir = mk3(1, 1, 1);
+        if (l->type == LRT_LIGHT_DIRECT) {
+          light_dir = mk3(l->space[0], l->space[1], l->space[2]);
+        } else if (l->type == LRT_LIGHT_POINT) {
+          light_dir = sub3(mk3(l->space[0], l->space[1], l->space[2]), surf);
+          const float len = sqrtf(dot3(light_dir, light_dir));
+          light_dir = mk3(light_dir.x / len, light_dir.y / len, light_dir.z / len);
+        }
+        f3 half = add3(eye_dir, light_dir);
+        const float hl = sqrtf(dot3(half, half));
+        half = mk3(half.x / hl, half.y / hl, half.z / hl);
+        const float NH = dot3(norm, half), NL = dot3(norm, light_dir), HL = dot3(half, light_dir),
+                    HV = dot3(half, eye_dir);
+        const float D = alpha * smax(0.0f, NH) / smax(LRT_PI_F * powf(NH * NH * (alpha - 1.0f) + 1.0f, 2.0f), 0.00001f);
+        float V = smax(0.0f, HL) / smax(fabsf(NL) + sqrtf(alpha + (1 - alpha) * NL * NL), 0.00001f);
+        V *= smax(0.0f, HV) / smax(fabsf(NV) + sqrtf(alpha + (1 - alpha) * NV * NV), 0.00001f);
+        const float spec = V * D;
+        const float ip = 1.0f / LRT_PI_F;
+        const f3 diffuse = scl3(ip, baseColor);
+        const float p5 = powf(1.0f - fabsf(HV), 5.0f);
+        const f3 metal = scl3(spec, mk3(baseColor.x + (1.0f - baseColor.x) * p5, baseColor.y + (1.0f - baseColor.y) * p5,
+                                        baseColor.z + (1.0f - baseColor.z) * p5));
+        const float F = f0 + (1.0f - f0) * p5;
+        const float fs = F * spec;
+        const f3 diel = mk3((1.0f - F) * diffuse.x + fs, (1.0f - F) * diffuse.y + fs, (1.0f - F) * diffuse.z + fs);
+        const f3 brdf = add3(scl3(1.0f - metallic, diel), scl3(metallic, metal));
+        fc = add3(fc, scl3(smax(NL, 0.0f), brdf));
+      }
+      res[0] = fc.x; res[1] = fc.y; res[2] = fc.z;
+    } break;
     case 12: case 18: { /* PHONG_NO_TEX, PHONG (COLORED); the shadow ray is commented out (shade = 1) */
       const float Kd = 0.25f, Ks = 0.25f, BIAS = 1e-6f;
       f3 color = mk3(0, 0, 1);

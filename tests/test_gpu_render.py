@@ -70,14 +70,19 @@ def test_render_rgba8_refusals(cuda):
         sc.render_rgba8(cam, many, (0, 0, 0, 1), img.data_ptr())
     assert e.value.status == 1
     p = parity_preset()
-    p.render_mode = 11  # PBR_NO_TEX
+    p.render_mode = 13  # OUTLINE_PRIM
     sc.SetPreset(p)
     with pytest.raises(LrtError) as e:
         sc.render_rgba8(cam, _lights(), (0, 0, 0, 1), img.data_ptr())
-    assert e.value.status == 6 and "render_mode 11" in str(e.value)
+    assert e.value.status == 6 and "render_mode 13" in str(e.value)
+    p.render_mode = 11  # PBR_NO_TEX shades with material 0
+    sc.SetPreset(p)
+    with pytest.raises(LrtError) as e:
+        sc.render_rgba8(cam, _lights(), (0, 0, 0, 1), img.data_ptr())
+    assert e.value.status == 1 and "material 0" in str(e.value)
     from graphic_lab_task_b200 import MATERIAL_TEXTURED
     from test_oracle import transparency_tables
-    for mode in (16, 17, 18, 22):  # materials needed
+    for mode in (16, 17, 18, 21, 22):  # materials needed
         p.render_mode = mode
         sc.SetPreset(p)
         with pytest.raises(LrtError) as e:
@@ -100,14 +105,14 @@ def test_render_rgba8_refusals(cuda):
 
 # the render modes of ResolveCommon / kernel1D_ResolveDebug without textures,
 # shadows or PBR (core/render_settings.h:61-88)
-RENDER_MODES = [0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 12, 16, 17, 18, 19, 20, 22, 24, 25]
+RENDER_MODES = [0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 16, 17, 18, 19, 20, 21, 22, 24, 25]
 
 
 @pytest.mark.parametrize("mode", RENDER_MODES)
 def test_render_modes_match_oracle(cuda, mode):
     """lrt_render_rgba8 in every implemented render mode equals the oracle's
-    restatement of Render pixel for pixel (NORMAL and the Phong modes within
-    one 8-bit step: their pow is CUDA's on the device)."""
+    restatement of Render pixel for pixel (NORMAL, Phong and PBR within one
+    8-bit step: their pow is CUDA's on the device)."""
     torch = cuda
     from graphic_lab_task_b200 import MATERIAL_COLORED
     from test_oracle import transparency_tables
@@ -115,6 +120,8 @@ def test_render_modes_match_oracle(cuda, mode):
     mats, ids, offs = transparency_tables(4, seed=11)
     mats["type"] = MATERIAL_COLORED
     mats["base_color"][:, 3] = 1.0
+    mats["metallic"] = np.linspace(0, 1, len(mats))
+    mats["roughness"] = np.linspace(0.2, 0.9, len(mats))
     sc.set_materials(mats, ids, offs)
     p = parity_preset()
     p.render_mode = mode
@@ -127,7 +134,7 @@ def test_render_modes_match_oracle(cuda, mode):
     got = img.cpu().numpy().view(np.uint32)
     want = po.port_render_rgba8(sc.export_arrays(), wl.eye_rays_host(cam), _lights(), bg, preset=p, materials=mats,
                                 mat_ids=ids, mat_offsets=offs)
-    if mode in (8, 12, 18):
+    if mode in (8, 11, 12, 18, 21):
         d = np.abs(got.view(np.uint8).astype(int) - want.view(np.uint8).astype(int))
         assert d.max() <= 1 and (d > 0).mean() < 0.01
     else:
@@ -137,7 +144,8 @@ def test_render_modes_match_oracle(cuda, mode):
 
 
 @pytest.mark.parametrize("mode,spp,ray_gen,transparent", [(1, 4, 0, False), (17, 4, 0, False), (12, 2, 1, False),
-                                                           (17, 1, 0, True), (16, 4, 0, True), (18, 4, 0, True)])
+                                                           (17, 1, 0, True), (16, 4, 0, True), (18, 4, 0, True),
+                                                           (21, 4, 0, True)])
 def test_render_samples_and_transparency_match_oracle(cuda, mode, spp, ray_gen, transparent):
     """Several samples per pixel (initEyeRay's sqrt(spp) grid, or the first
     Hamilton point for RAY_GEN_MODE_RANDOM; the resolve uses sample 0's ray,
@@ -167,7 +175,7 @@ def test_render_samples_and_transparency_match_oracle(cuda, mode, spp, ray_gen, 
     sample_rays = np.stack([wl.eye_rays_host(cam, dx, dy) for dx, dy in offsets])
     want = po.port_render_rgba8_samples(sc.export_arrays(), sample_rays, sample_rays[0], _lights(), bg, p,
                                         materials=mats, mat_ids=ids, mat_offsets=offs, transparency=transparent)
-    if mode in (12, 18):
+    if mode in (12, 18, 21):
         d = np.abs(got.view(np.uint8).astype(int) - want.view(np.uint8).astype(int))
         assert d.max() <= 1 and (d > 0).mean() < 0.01
     else:
