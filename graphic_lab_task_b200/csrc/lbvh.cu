@@ -13,6 +13,8 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <map>
+#include <mutex>
 
 #include <cub/device/device_radix_sort.cuh>
 
@@ -195,6 +197,14 @@ __global__ void k_fit_boxes(const float* __restrict__ boxes, const uint32_t* __r
   atomicOr(err, 1u);
 }
 
+// Per-device scratch of the builds, reused while large enough.
+struct ArenaCache {
+  void* ptr = nullptr;
+  size_t size = 0;
+};
+std::map<int, ArenaCache> g_arena;
+std::mutex g_arenaMutex;
+
 // Carves 256-byte-aligned pieces out of one device allocation.
 struct Arena {
   size_t used = 0;
@@ -253,8 +263,24 @@ const char* lbvh_build(const float* boxes6, uint32_t n, std::vector<uint32_t>& o
     return p;
   };
   carve(A);
+  // the scratch of the largest build so far stays allocated per device, so
+  // that repeated builds (dynamic meshes, TLAS rebuilds) do not pay for
+  // cudaMalloc/cudaFree every time
+  std::lock_guard<std::mutex> lock(g_arenaMutex);
+  int dev = 0;
+  LBVH_TRY(cudaGetDevice(&dev), "cudaGetDevice");
   void* arena = nullptr;
-  LBVH_TRY(cudaMalloc(&arena, A.used), "device memory for the tree build");
+  if (e == cudaSuccess) {
+    ArenaCache& ac = g_arena[dev];
+    if (ac.size < A.used) {
+      cudaFree(ac.ptr);
+      ac.ptr = nullptr;
+      ac.size = 0;
+      LBVH_TRY(cudaMalloc(&ac.ptr, A.used), "device memory for the tree build");
+      if (e == cudaSuccess) ac.size = A.used;
+    }
+    arena = ac.ptr;
+  }
   A.base = static_cast<char*>(arena);
   A.used = 0;
   const auto P = carve(A);
@@ -299,7 +325,6 @@ const char* lbvh_build(const float* boxes6, uint32_t n, std::vector<uint32_t>& o
   LBVH_TRY(cudaMemcpyAsync(&herr, dErr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st), "status device->host");
   LBVH_TRY(cudaStreamSynchronize(st), "tree build");
 #undef LBVH_TRY
-  cudaFree(arena);
   if (st) cudaStreamDestroy(st);
   if (e != cudaSuccess) {
     order.clear();

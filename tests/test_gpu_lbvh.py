@@ -124,11 +124,16 @@ def test_device_aabb_blas(cuda):
 
 
 def test_device_build_is_much_faster_on_large_meshes(cuda):
+    """Best of three builds each (the first device build of a process also
+    loads the builder's kernels)."""
     v, t = wl.noisy_sphere(wl.segments_for_triangles(500000), seed=500000)
     times = {}
     for flags in (BUILD_LOW, BUILD_HIGH):
-        sc = SceneRT()
-        t0 = time.perf_counter()
-        sc.AddGeom_Triangles3f(v, t, flags=flags)
-        times[flags] = time.perf_counter() - t0
+        best = float("inf")
+        for _ in range(3):
+            sc = SceneRT()
+            t0 = time.perf_counter()
+            sc.AddGeom_Triangles3f(v, t, flags=flags)
+            best = min(best, time.perf_counter() - t0)
+        times[flags] = best
     assert times[BUILD_LOW] < 0.5 * times[BUILD_HIGH], times
