@@ -50,11 +50,6 @@ struct lrt_camera_batch {
 namespace lrt {
 namespace {
 
-lrt_status bfail(lrt_camera_batch* b, lrt_status code, const char* what)
-{
-  return fail(b ? b->scene : nullptr, code, "%s", what);
-}
-
 // Fills the pinned camera table for the current shape and returns the tile count.
 void fill_table(lrt_camera_batch* b)
 {
