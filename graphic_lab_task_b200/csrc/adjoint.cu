@@ -182,7 +182,7 @@ lrt_status lrt_render_rgba8(lrt_scene* s, const lrt_camera* camera, const lrt_li
   if (light_count > LRT_MAX_LIGHTS)
     return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_render_rgba8: %u lights (at most %d)", light_count, LRT_MAX_LIGHTS);
   const uint32_t mode = s->preset.render_mode;
-  static const uint32_t kModes[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 16, 17, 18, 19, 20, 21, 22, 24, 25};
+  static const uint32_t kModes[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 16, 17, 18, 19, 20, 21, 22, 24, 25};
   if (std::find(std::begin(kModes), std::end(kModes), mode) == std::end(kModes))
     return fail(s, LRT_ERR_UNSUPPORTED,
                 "lrt_render_rgba8: render_mode %u (textures, shadows, PBR, outlines, channels and intersection "

@@ -1118,11 +1118,12 @@ __device__ float4 resolve_mode_colour(CTX& c, const DevLights& L, const DevMater
     res = make_float4(col.x, col.y, col.z, 1);
   } break;
   case 1:  // LAMBERT_NO_TEX
+  case 13: // OUTLINE_PRIM: ResolveOutline (:1073-1121) never sets its outline flag in this mode
   case 7:  // GEOM
   case 17: // LAMBERT (colored materials)
   case 20: { // LOD
     f3 color = mk3(0, 0, 1);
-    if (mode == 1) color = mk3(1, 1, 1);
+    if (mode == 1 || mode == 13) color = mk3(1, 1, 1);
     else if (mode == 20) color = ld3(decode_rgba8(kLodPalette[h.primId % 20]));
     else if (mode == 7) color = ld3(decode_rgba8(kPalette[geomId % 20]));
     else if (type == LRT_TYPE_SDF_SBS_COL || type == LRT_TYPE_GRAPHICS_PRIM) color = packed_hit_colour(h);
@@ -1440,7 +1441,7 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_fill_gbuffer_transparency(
 }
 
 // Forward render: image[i] = Lambert shade of ray i's nearest hit.
-__global__ void __launch_bounds__(kTraceThreads) k_render_lambert(DevScene S, const float4* __restrict__ rays,
+__global__ void __launch_bounds__(kTraceThreads, 7) k_render_lambert(DevScene S, const float4* __restrict__ rays,
                                                                   uint64_t n, float3 light, float* __restrict__ image,
                                                                   unsigned long long* __restrict__ work_counter,
                                                                   uint32_t* __restrict__ err_word, uint32_t stack_cap)
@@ -1476,7 +1477,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_render_lambert(DevScene S, co
 // and dLoss/dI * dI/dtheta_i is added to grad[idx_i] for the 8 corners.
 // Rays whose dLoss/dI is 0 are skipped.  Hits off indexed SBS bricks
 // contribute nothing.
-__global__ void __launch_bounds__(kTraceThreads) k_adjoint_lambert(DevScene S, const float4* __restrict__ rays,
+__global__ void __launch_bounds__(kTraceThreads, 7) k_adjoint_lambert(DevScene S, const float4* __restrict__ rays,
                                                                    uint64_t n, float3 light,
                                                                    const float* __restrict__ dimage,
                                                                    float* __restrict__ grad,

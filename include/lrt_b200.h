@@ -461,7 +461,8 @@ enum { LRT_LIGHT_DIRECT = 0, LRT_LIGHT_POINT = 1, LRT_LIGHT_AMBIENT = 2 };
  * the preset's render_mode and Tonemap (MultiRenderer_resolve.cpp:536-542).
  * Render modes: LAMBERT_NO_TEX (ResolveCommon :580-666: white albedo, the
  * given lights), PHONG_NO_TEX (:668-732; its shadow ray is commented out
- * there), PBR_NO_TEX (:734-792, material 0), GEOM, LOD, and with the scene's
+ * there), PBR_NO_TEX (:734-792, material 0), OUTLINE_PRIM (whose outline
+ * test the reference applies only in OUTLINE_BORDER), GEOM, LOD, and with the scene's
  * COLORED materials (lrt_set_materials) LAMBERT, PHONG, PBR and DIFFUSE; and
  * kernel1D_ResolveDebug's
  * (:810-990) MASK, DEPTH, LINEAR_DEPTH, INVERSE_LINEAR_DEPTH, HSV_DEPTH,
@@ -471,8 +472,8 @@ enum { LRT_LIGHT_DIRECT = 0, LRT_LIGHT_POINT = 1, LRT_LIGHT_AMBIENT = 2 };
  * point for RAY_GEN_MODE_RANDOM), resolved with the sample-0 ray as
  * ResolveCommon does, and averaged; with a transparent COLORED material,
  * LAMBERT, PHONG, PBR and DIFFUSE take the reference's transparency path (the
- * AnyHit G-buffer blended into the resolved colour).  Other modes (outlines,
- * channels, voxel-octree counts) and textured materials return
+ * AnyHit G-buffer blended into the resolved colour).  Other modes
+ * (OUTLINE_BORDER, channels, intersection counts) and textured materials return
  * LRT_ERR_UNSUPPORTED; the pixel grid is the camera's (the reference pads
  * widths to a multiple of 8).  Writes
  * width*height RGBA8 pixels (row-major) to device memory image_dev;

@@ -1112,10 +1112,10 @@ static void resolve_colour(const lrt_scene_arrays* arrays, const ctx_t* cp, uint
         res[0] = m->base_color[0]; res[1] = m->base_color[1]; res[2] = m->base_color[2];
       }
     } break;
-    case 1: case 7: case 17: case 20: { /* LAMBERT_NO_TEX, GEOM, LAMBERT (COLORED), LOD */
+    case 1: case 7: case 13: case 17: case 20: { /* LAMBERT_NO_TEX, GEOM, OUTLINE_PRIM, LAMBERT (COLORED), LOD */
       f3 color = mk3(0, 0, 1);
       float pc[4];
-      if (mode == 1) color = mk3(1, 1, 1);
+      if (mode == 1 || mode == 13) color = mk3(1, 1, 1);
       else if (mode == 20) { decode_rgba8(kLodPalette[h.primId % 20], pc); color = mk3(pc[0], pc[1], pc[2]); }
       else if (mode == 7) { decode_rgba8(kPalette[geomId % 20], pc); color = mk3(pc[0], pc[1], pc[2]); }
       else if (type == LRT_TYPE_SDF_SBS_COL || type == LRT_TYPE_GRAPHICS_PRIM)

@@ -70,11 +70,11 @@ def test_render_rgba8_refusals(cuda):
         sc.render_rgba8(cam, many, (0, 0, 0, 1), img.data_ptr())
     assert e.value.status == 1
     p = parity_preset()
-    p.render_mode = 13  # OUTLINE_PRIM
+    p.render_mode = 14  # OUTLINE_BORDER
     sc.SetPreset(p)
     with pytest.raises(LrtError) as e:
         sc.render_rgba8(cam, _lights(), (0, 0, 0, 1), img.data_ptr())
-    assert e.value.status == 6 and "render_mode 13" in str(e.value)
+    assert e.value.status == 6 and "render_mode 14" in str(e.value)
     p.render_mode = 11  # PBR_NO_TEX shades with material 0
     sc.SetPreset(p)
     with pytest.raises(LrtError) as e:
@@ -105,7 +105,7 @@ def test_render_rgba8_refusals(cuda):
 
 # the render modes of ResolveCommon / kernel1D_ResolveDebug without textures,
 # shadows or PBR (core/render_settings.h:61-88)
-RENDER_MODES = [0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 16, 17, 18, 19, 20, 21, 22, 24, 25]
+RENDER_MODES = [0, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 16, 17, 18, 19, 20, 21, 22, 24, 25]
 
 
 @pytest.mark.parametrize("mode", RENDER_MODES)
