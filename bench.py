@@ -549,6 +549,16 @@ def adjoint_section(dev, args):
         sc.adjoint_lambert(R.data_ptr(), n, L, dimage.data_ptr(), grad.data_ptr(), stream=sp)
 
     adj_ms = timed(adj)
+    # the same passes with the rays as one image of the views stacked as rows,
+    # in 8x4-pixel tiles and the stream's tile schedule
+    shape = (512, n // 512)
+    fwd_img_ms = timed(lambda: sc.render_lambert(R.data_ptr(), n, L, img.data_ptr(), stream=sp, image_size=shape))
+
+    def adj_img():
+        grad.zero_()
+        sc.adjoint_lambert(R.data_ptr(), n, L, dimage.data_ptr(), grad.data_ptr(), stream=sp, image_size=shape)
+
+    adj_img_ms = timed(adj_img)
     upd_ms = timed(lambda: sc.update_sbs_values(V.data_ptr(), V.numel(), stream=sp))
     sc.sync(stream=sp)
     loss0 = float(((img - timg).double() ** 2).mean())
@@ -589,7 +599,11 @@ def adjoint_section(dev, args):
     out = {"grid": 256, "views": len(cams), "res": 512, "rays": n, "bricks": int(len(nodes)),
            "values": int(len(vf)), "loss": loss0, "forward_ms": fwd_ms, "adjoint_ms": adj_ms,
            "adjoint_over_forward": adj_ms / fwd_ms, "update_values_ms": upd_ms,
-           "forward_mrays_s": n / fwd_ms / 1e3, "nonzero_grad_values": int(len(cand)),
+           "forward_mrays_s": n / fwd_ms / 1e3, "image_order": {
+               "call": "lrt_render_lambert_image / lrt_adjoint_lambert_sbs_image, views stacked as a 512 x 8192 image",
+               "forward_ms": fwd_img_ms, "adjoint_ms": adj_img_ms, "forward_mrays_s": n / fwd_img_ms / 1e3,
+               "adjoint_over_forward": adj_img_ms / fwd_img_ms},
+           "nonzero_grad_values": int(len(cand)),
            "fd": {"voxels": int(len(pick)), "h": h, "smooth_voxels": int(smooth.sum()),
                   "all_h": stats(fd1, allm), "smooth_h": stats(fd1, smooth),
                   "smooth_richardson": stats(fdr, smooth), "seconds": fd_s}}
@@ -848,10 +862,22 @@ def configs_table(args):
             sc.adjoint_lambert(R.data_ptr(), n, wl.LIGHT, dimg.data_ptr(), grad.data_ptr(), stream=sp)
 
         ams = timed(adj)
+        shape = (512, n // 512)  # the 16 views stacked as one image
+        fims = timed(lambda: sc.render_lambert(R.data_ptr(), n, wl.LIGHT, img.data_ptr(), stream=sp, image_size=shape))
+
+        def adj_img():
+            grad.zero_()
+            sc.adjoint_lambert(R.data_ptr(), n, wl.LIGHT, dimg.data_ptr(), grad.data_ptr(), stream=sp,
+                               image_size=shape)
+
+        aims = timed(adj_img)
         sc.sync(stream=sp)
         emit({"config": 4, "workload": "SBS 256^3, 16 views of 512^2, Lambert forward + adjoint", "rays": n,
               "gpu_forward_ms": fms, "gpu_forward_mrays_s": n / fms / 1e3, "gpu_adjoint_ms": ams,
-              "adjoint_over_forward": ams / fms, "cpu_reference_trace": cpu(sc, rays[:: 16])})
+              "adjoint_over_forward": ams / fms,
+              "image_order": {"forward_ms": fims, "forward_mrays_s": n / fims / 1e3, "adjoint_ms": aims,
+                              "adjoint_over_forward": aims / fims},
+              "cpu_reference_trace": cpu(sc, rays[:: 16])})
         sc.close()
 
 

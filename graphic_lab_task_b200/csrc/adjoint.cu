@@ -129,6 +129,76 @@ lrt_status check_material_ranges(lrt_scene* s, const char* who, const uint32_t* 
   return LRT_OK;
 }
 
+// Shared arguments of the Lambert passes: width > 0 makes the n = width *
+// height rays an image traced in 8x4-pixel tiles in the stream's tile
+// schedule (natural tile order with LRT_TRACE_NATURAL_ORDER, the only flag).
+lrt_status lambert_begin(lrt_scene* s, const char* who, const float* rays_dev, uint64_t n, uint32_t width,
+                         uint32_t height, const float* light, uint32_t flags, cudaStream_t stream, StreamSlot** slot,
+                         DevScene* S, int* grid)
+{
+  lrt_status st = begin(s, stream, slot, S);
+  if (st != LRT_OK) return st;
+  if (!light) return fail(s, LRT_ERR_INVALID_ARGUMENT, "%s: NULL light", who);
+  if (flags & ~LRT_TRACE_NATURAL_ORDER) return fail(s, LRT_ERR_INVALID_ARGUMENT, "%s: unknown flags 0x%x", who, flags);
+  if (width && (uint64_t(width / kImgTileW + 1) * (height / kImgTileH + 1) >= 0xFFFFFFFFull))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "%s: %u x %u pixels is more tiles than a launch can count", who, width,
+                height);
+  if ((st = check_rays(s, rays_dev)) != LRT_OK) return st;
+  const uint64_t warps =
+      width ? uint64_t((width + kImgTileW - 1) / kImgTileW) * ((height + kImgTileH - 1) / kImgTileH) : (n + 31) / 32;
+  *grid = int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(s->dev->grid),
+                                                       (warps * 32 + kTraceThreads - 1) / kTraceThreads)));
+  return LRT_OK;
+}
+
+lrt_status render_lambert(lrt_scene* s, const float* rays_dev, uint64_t n, uint32_t width, uint32_t height,
+                          const float light[3], float* image_dev, cudaStream_t stream, uint32_t flags)
+{
+  StreamSlot* slot = nullptr;
+  DevScene S;
+  int grid = 1;
+  lrt_status st = lambert_begin(s, "lrt_render_lambert", rays_dev, n, width, height, light, flags, stream, &slot, &S,
+                                &grid);
+  if (st != LRT_OK) return st;
+  if ((st = check_rays(s, image_dev)) != LRT_OK) return st;
+  if (n == 0) return LRT_OK;
+  const bool natural = !width || (flags & LRT_TRACE_NATURAL_ORDER);
+  const uint32_t* rd = nullptr;
+  uint32_t* wr = nullptr;
+  if ((st = sched_prepare(s, stream, width, height, natural, &rd, &wr)) != LRT_OK) return st;
+  cudaError_t e = lrt_exact::launch_render_lambert(S, reinterpret_cast<const float4*>(rays_dev), n,
+                                                   make_float3(light[0], light[1], light[2]), image_dev, &slot->work,
+                                                   &slot->err, s->dev->stackCap, grid, stream, width, height, rd, wr);
+  if (e != cudaSuccess) return cuda_fail(s, e, "render launch");
+  sched_commit(s, stream, natural);
+  return LRT_OK;
+}
+
+lrt_status adjoint_lambert(lrt_scene* s, const float* rays_dev, uint64_t n, uint32_t width, uint32_t height,
+                           const float light[3], const float* dimage_dev, float* grad_dev, cudaStream_t stream,
+                           uint32_t flags)
+{
+  StreamSlot* slot = nullptr;
+  DevScene S;
+  int grid = 1;
+  lrt_status st = lambert_begin(s, "lrt_adjoint_lambert_sbs", rays_dev, n, width, height, light, flags, stream, &slot,
+                                &S, &grid);
+  if (st != LRT_OK) return st;
+  if (!dimage_dev || !grad_dev) return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_adjoint_lambert_sbs: NULL argument");
+  if (n == 0) return LRT_OK;
+  const bool natural = !width || (flags & LRT_TRACE_NATURAL_ORDER);
+  const uint32_t* rd = nullptr;
+  uint32_t* wr = nullptr;
+  if ((st = sched_prepare(s, stream, width, height, natural, &rd, &wr)) != LRT_OK) return st;
+  cudaError_t e = lrt_exact::launch_adjoint_lambert(S, reinterpret_cast<const float4*>(rays_dev), n,
+                                                    make_float3(light[0], light[1], light[2]), dimage_dev, grad_dev,
+                                                    &slot->work, &slot->err, s->dev->stackCap, grid, stream, width,
+                                                    height, rd, wr);
+  if (e != cudaSuccess) return cuda_fail(s, e, "adjoint launch");
+  sched_commit(s, stream, natural);
+  return LRT_OK;
+}
+
 } // namespace
 } // namespace lrt
 
@@ -319,40 +389,29 @@ lrt_status lrt_fill_gbuffer_transparency(lrt_scene* s, const lrt_camera* camera,
 lrt_status lrt_render_lambert(lrt_scene* s, const float* rays_dev, uint64_t n, const float light[3], float* image_dev,
                               void* stream_p)
 {
-  StreamSlot* slot = nullptr;
-  DevScene S;
-  cudaStream_t stream = static_cast<cudaStream_t>(stream_p);
-  lrt_status st = begin(s, stream, &slot, &S);
-  if (st != LRT_OK) return st;
-  if (!light) return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_render_lambert: NULL light");
-  if ((st = check_rays(s, rays_dev)) != LRT_OK || (st = check_rays(s, image_dev)) != LRT_OK) return st;
-  if (n == 0) return LRT_OK;
-  DeviceScene* d = s->dev;
-  const int grid = int(std::min<uint64_t>(uint64_t(d->grid), (n + kTraceThreads - 1) / kTraceThreads));
-  cudaError_t e = lrt_exact::launch_render_lambert(S, reinterpret_cast<const float4*>(rays_dev), n,
-                                                   make_float3(light[0], light[1], light[2]), image_dev, &slot->work,
-                                                   &slot->err, d->stackCap, std::max(1, grid), stream);
-  return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "render launch");
+  return lrt::render_lambert(s, rays_dev, n, 0, 0, light, image_dev, static_cast<cudaStream_t>(stream_p), 0);
+}
+
+lrt_status lrt_render_lambert_image(lrt_scene* s, const float* rays_dev, uint32_t width, uint32_t height,
+                                    const float light[3], float* image_dev, void* stream_p, uint32_t flags)
+{
+  return lrt::render_lambert(s, rays_dev, uint64_t(width) * height, width, height, light, image_dev,
+                             static_cast<cudaStream_t>(stream_p), flags);
 }
 
 lrt_status lrt_adjoint_lambert_sbs(lrt_scene* s, const float* rays_dev, uint64_t n, const float light[3],
                                    const float* dimage_dev, float* grad_dev, void* stream_p)
 {
-  StreamSlot* slot = nullptr;
-  DevScene S;
-  cudaStream_t stream = static_cast<cudaStream_t>(stream_p);
-  lrt_status st = begin(s, stream, &slot, &S);
-  if (st != LRT_OK) return st;
-  if (!light || !dimage_dev || !grad_dev)
-    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_adjoint_lambert_sbs: NULL argument");
-  if ((st = check_rays(s, rays_dev)) != LRT_OK) return st;
-  if (n == 0) return LRT_OK;
-  DeviceScene* d = s->dev;
-  const int grid = int(std::min<uint64_t>(uint64_t(d->grid), (n + kTraceThreads - 1) / kTraceThreads));
-  cudaError_t e = lrt_exact::launch_adjoint_lambert(S, reinterpret_cast<const float4*>(rays_dev), n,
-                                                    make_float3(light[0], light[1], light[2]), dimage_dev, grad_dev,
-                                                    &slot->work, &slot->err, d->stackCap, std::max(1, grid), stream);
-  return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "adjoint launch");
+  return lrt::adjoint_lambert(s, rays_dev, n, 0, 0, light, dimage_dev, grad_dev, static_cast<cudaStream_t>(stream_p),
+                              0);
+}
+
+lrt_status lrt_adjoint_lambert_sbs_image(lrt_scene* s, const float* rays_dev, uint32_t width, uint32_t height,
+                                         const float light[3], const float* dimage_dev, float* grad_dev,
+                                         void* stream_p, uint32_t flags)
+{
+  return lrt::adjoint_lambert(s, rays_dev, uint64_t(width) * height, width, height, light, dimage_dev, grad_dev,
+                              static_cast<cudaStream_t>(stream_p), flags);
 }
 
 } // extern "C"

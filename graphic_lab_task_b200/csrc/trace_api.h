@@ -34,10 +34,14 @@
                                                uint32_t* sched_wr = nullptr);                                   \
   cudaError_t launch_render_lambert(const lrt::DevScene& S, const float4* rays, uint64_t n, float3 light,       \
                                     float* image, unsigned long long* work_counter, uint32_t* err_word,         \
-                                    uint32_t stack_cap, int grid, cudaStream_t stream);                         \
+                                    uint32_t stack_cap, int grid, cudaStream_t stream, uint32_t img_w = 0,      \
+                                    uint32_t img_h = 0, const uint32_t* sched_rd = nullptr,                     \
+                                    uint32_t* sched_wr = nullptr);                                              \
   cudaError_t launch_adjoint_lambert(const lrt::DevScene& S, const float4* rays, uint64_t n, float3 light,      \
                                      const float* dimage, float* grad, unsigned long long* work_counter,        \
-                                     uint32_t* err_word, uint32_t stack_cap, int grid, cudaStream_t stream);    \
+                                     uint32_t* err_word, uint32_t stack_cap, int grid, cudaStream_t stream,     \
+                                     uint32_t img_w = 0, uint32_t img_h = 0, const uint32_t* sched_rd = nullptr, \
+                                     uint32_t* sched_wr = nullptr);                                             \
   }
 
 LRT_DECLARE_TRACE_API(lrt_exact)

@@ -1440,24 +1440,64 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_fill_gbuffer_transparency(
   if (c.err) atomicOr(err_word, c.err);
 }
 
+// The next ray of this lane for the Lambert passes; false (warp-uniform) when
+// the launch's work is done.  IMG: the rays are an img_w x img_h image in
+// row-major pixel order and the warp takes its next 8x4-pixel tile from the
+// stream's tile schedule (as k_trace does); otherwise the next 32 rays of n.
+// `valid` is false for the lanes of a tile past the image's edge or past n.
+template <bool IMG>
+__device__ __forceinline__ bool next_ray(uint64_t n, uint32_t img_w, uint32_t img_h, unsigned long long* counter,
+                                         const uint32_t* sched_rd, uint32_t* sched_wr, WarpClock* wc, uint64_t& i,
+                                         bool& valid)
+{
+  const uint32_t lane = threadIdx.x & 31;
+  if (IMG) {
+    const uint32_t tilesX = (img_w + kImgTileW - 1) / kImgTileW;
+    __syncwarp();
+    uint32_t tile = 0;
+    if (lane == 0) tile = sched_next(sched_rd, sched_wr, tilesX * ((img_h + kImgTileH - 1) / kImgTileH), counter, *wc);
+    tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
+    if (tile == ~0u) return false;
+    const uint32_t x = (tile % tilesX) * kImgTileW + lane % kImgTileW;
+    const uint32_t y = (tile / tilesX) * kImgTileH + lane / kImgTileW;
+    valid = x < img_w && y < img_h;
+    i = uint64_t(y) * img_w + x;
+    return true;
+  }
+  unsigned long long base = 0;
+  if (lane == 0) base = atomicAdd(counter, 32ull);
+  base = __shfl_sync(0xFFFFFFFFu, base, 0);
+  if (base >= n) return false;
+  i = base + lane;
+  valid = i < n;
+  return true;
+}
+
 // Forward render: image[i] = Lambert shade of ray i's nearest hit.
+template <bool IMG>
 __global__ void __launch_bounds__(kTraceThreads, 7) k_render_lambert(DevScene S, const float4* __restrict__ rays,
                                                                   uint64_t n, float3 light, float* __restrict__ image,
                                                                   unsigned long long* __restrict__ work_counter,
-                                                                  uint32_t* __restrict__ err_word, uint32_t stack_cap)
+                                                                  uint32_t* __restrict__ err_word, uint32_t stack_cap,
+                                                                  uint32_t img_w, uint32_t img_h,
+                                                                  const uint32_t* __restrict__ sched_rd,
+                                                                  uint32_t* sched_wr)
 {
   extern __shared__ uint32_t smem_stack[];
   uint32_t* stack = smem_stack + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
+  __shared__ WarpClock wclock[IMG ? kTraceThreads / 32 : 1];
+  WarpClock* wc = wclock + (IMG ? threadIdx.x >> 5 : 0);
+  if (IMG && lane == 0) {
+    wc->tile = ~0u;
+    wc->longest = 0;
+  }
   Ctx<false> c(S, normal_words(smem_stack, stack_cap));
   const f3 L = mk3(light.x, light.y, light.z);
-  for (;;) {
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(work_counter, 32ull);
-    base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    if (base >= n) break;
-    const uint64_t i = base + lane;
-    if (i < n) {
+  uint64_t i = 0;
+  bool valid = false;
+  while (next_ray<IMG>(n, img_w, img_h, work_counter, sched_rd, sched_wr, wc, i, valid)) {
+    if (valid) {
       const float4 pn = __ldg(rays + 2 * i), df = __ldg(rays + 2 * i + 1);
       lrt_hit h;
       trace_one(c, stack, blockDim.x, stack_cap, pn, df, h);
@@ -1477,25 +1517,32 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_render_lambert(DevScene S,
 // and dLoss/dI * dI/dtheta_i is added to grad[idx_i] for the 8 corners.
 // Rays whose dLoss/dI is 0 are skipped.  Hits off indexed SBS bricks
 // contribute nothing.
+template <bool IMG>
 __global__ void __launch_bounds__(kTraceThreads, 7) k_adjoint_lambert(DevScene S, const float4* __restrict__ rays,
                                                                    uint64_t n, float3 light,
                                                                    const float* __restrict__ dimage,
                                                                    float* __restrict__ grad,
                                                                    unsigned long long* __restrict__ work_counter,
-                                                                   uint32_t* __restrict__ err_word, uint32_t stack_cap)
+                                                                   uint32_t* __restrict__ err_word, uint32_t stack_cap,
+                                                                   uint32_t img_w, uint32_t img_h,
+                                                                   const uint32_t* __restrict__ sched_rd,
+                                                                   uint32_t* sched_wr)
 {
   extern __shared__ uint32_t smem_stack[];
   uint32_t* stack = smem_stack + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
+  __shared__ WarpClock wclock[IMG ? kTraceThreads / 32 : 1];
+  WarpClock* wc = wclock + (IMG ? threadIdx.x >> 5 : 0);
+  if (IMG && lane == 0) {
+    wc->tile = ~0u;
+    wc->longest = 0;
+  }
   const f3 L = mk3(light.x, light.y, light.z);
   uint32_t err = 0;
-  for (;;) {
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(work_counter, 32ull);
-    base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    if (base >= n) break;
-    const uint64_t i = base + lane;
-    if (i >= n) continue;
+  uint64_t i = 0;
+  bool valid = false;
+  while (next_ray<IMG>(n, img_w, img_h, work_counter, sched_rd, sched_wr, wc, i, valid)) {
+    if (!valid) continue;
     const float dLdI = __ldg(dimage + i);
     if (dLdI == 0.0f) continue;
     Ctx<false, true> c(S, normal_words(smem_stack, stack_cap));
@@ -1582,28 +1629,36 @@ cudaError_t launch_fill_gbuffer_transparency(const DevScene& S, const DevCamera&
   return cudaGetLastError();
 }
 
+// img_w > 0: the n = img_w * img_h rays are an image (row-major pixels)
+// traced in 8x4-pixel tiles in the order of the tile schedule (sched_rd,
+// sched_wr; nullptr for natural order).
 cudaError_t launch_render_lambert(const DevScene& S, const float4* rays, uint64_t n, float3 light, float* image,
                                   unsigned long long* work_counter, uint32_t* err_word, uint32_t stack_cap, int grid,
-                                  cudaStream_t stream)
+                                  cudaStream_t stream, uint32_t img_w, uint32_t img_h, const uint32_t* sched_rd,
+                                  uint32_t* sched_wr)
 {
   const size_t smem = trace_smem_bytes(stack_cap);
-  cudaError_t e = cudaFuncSetAttribute(k_render_lambert, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  auto kernel = img_w ? k_render_lambert<true> : k_render_lambert<false>;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(trace_smem_bytes(kMaxStackDev + 1)));
   if (e != cudaSuccess) return e;
-  k_render_lambert<<<grid, kTraceThreads, smem, stream>>>(S, rays, n, light, image, work_counter, err_word, stack_cap);
+  kernel<<<grid, kTraceThreads, smem, stream>>>(S, rays, n, light, image, work_counter, err_word, stack_cap, img_w,
+                                                img_h, sched_rd, sched_wr);
   return cudaGetLastError();
 }
 
 cudaError_t launch_adjoint_lambert(const DevScene& S, const float4* rays, uint64_t n, float3 light,
                                    const float* dimage, float* grad, unsigned long long* work_counter,
-                                   uint32_t* err_word, uint32_t stack_cap, int grid, cudaStream_t stream)
+                                   uint32_t* err_word, uint32_t stack_cap, int grid, cudaStream_t stream,
+                                   uint32_t img_w, uint32_t img_h, const uint32_t* sched_rd, uint32_t* sched_wr)
 {
   const size_t smem = trace_smem_bytes(stack_cap);
-  cudaError_t e = cudaFuncSetAttribute(k_adjoint_lambert, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  auto kernel = img_w ? k_adjoint_lambert<true> : k_adjoint_lambert<false>;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(trace_smem_bytes(kMaxStackDev + 1)));
   if (e != cudaSuccess) return e;
-  k_adjoint_lambert<<<grid, kTraceThreads, smem, stream>>>(S, rays, n, light, dimage, grad, work_counter, err_word,
-                                                           stack_cap);
+  kernel<<<grid, kTraceThreads, smem, stream>>>(S, rays, n, light, dimage, grad, work_counter, err_word, stack_cap,
+                                                img_w, img_h, sched_rd, sched_wr);
   return cudaGetLastError();
 }
 

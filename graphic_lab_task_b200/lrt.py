@@ -30,7 +30,7 @@ EXPORTED = (
     "lrt_batch_update_cameras", "lrt_batch_set_shape", "lrt_batch_get_shape", "lrt_batch_trace", "lrt_batch_sync",
     "lrt_batch_autotune", "lrt_render_lambert", "lrt_adjoint_lambert_sbs", "lrt_sbs_update_values",
     "lrt_generate_bounce_rays", "lrt_generate_bounce_rays_compact", "lrt_render_rgba8", "lrt_trace_nearest_image",
-    "lrt_set_materials", "lrt_fill_gbuffer_transparency",
+    "lrt_set_materials", "lrt_fill_gbuffer_transparency", "lrt_render_lambert_image", "lrt_adjoint_lambert_sbs_image",
     "lrt_update_instance", "lrt_add_geom_sdf_frame_octree_file", "lrt_add_geom_sdf_svs_file",
     "lrt_add_geom_sdf_sbs_file", "lrt_batch_render_rgba8",
     "lrt_wl_noisy_sphere", "lrt_wl_spheres", "lrt_wl_sphere_sdf", "lrt_wl_sbs_from_spheres",
@@ -42,6 +42,13 @@ EXPORTED = (
 # (csrc/device.cu, pipeline_chunks): sizes ramp PIPE_CHUNK_MIN -> PIPE_CHUNK
 # and back down, one trace launch per chunk.
 PIPE_MIN_RAYS, PIPE_CHUNK, PIPE_CHUNK_MIN = 262144, 262144, 32768
+
+
+def _image_size(image_size, n):
+    w, h = (int(v) for v in image_size)
+    if w * h != n:
+        raise ValueError(f"image_size {w} x {h} does not hold {n} rays")
+    return w, h
 
 
 def pipeline_chunks(n):
@@ -110,6 +117,8 @@ def lib():
         "lrt_generate_bounce_rays": [vp, vp, vp, u64, u64, C.c_float, C.c_float, vp, vp],
         "lrt_generate_bounce_rays_compact": [vp, vp, vp, u64, u64, C.c_float, C.c_float, vp, vp, vp, vp],
         "lrt_adjoint_lambert_sbs": [vp, vp, u64, vp, vp, vp, vp],
+        "lrt_render_lambert_image": [vp, vp, u32, u32, vp, vp, vp, u32],
+        "lrt_adjoint_lambert_sbs_image": [vp, vp, u32, u32, vp, vp, vp, vp, u32],
         "lrt_sbs_update_values": [vp, vp, u64, vp, u32],
         "lrt_batch_create": [vp, vp, u32, P(vp)],
         "lrt_batch_destroy": [vp],
@@ -325,10 +334,19 @@ class SceneRT:
                                                            C.c_void_p(index_ptr), C.c_void_p(count_ptr),
                                                            C.c_void_p(stream) if stream else None))
 
-    def render_lambert(self, rays_ptr, n, light, image_ptr, stream=0):
+    def render_lambert(self, rays_ptr, n, light, image_ptr, stream=0, image_size=None, natural_order=False):
+        """Lambert image of n device rays.  image_size=(width, height) with
+        width * height == n: the rays are an image (views stacked as rows),
+        traced in 8x4-pixel tiles in the stream's tile schedule unless
+        natural_order."""
         L = (C.c_float * 3)(*[float(x) for x in light])
-        self._check(lib().lrt_render_lambert(self.h, C.c_void_p(rays_ptr), n, L, C.c_void_p(image_ptr),
-                                             C.c_void_p(stream) if stream else None))
+        st = C.c_void_p(stream) if stream else None
+        if image_size is None:
+            self._check(lib().lrt_render_lambert(self.h, C.c_void_p(rays_ptr), n, L, C.c_void_p(image_ptr), st))
+            return
+        w, h = _image_size(image_size, n)
+        self._check(lib().lrt_render_lambert_image(self.h, C.c_void_p(rays_ptr), w, h, L, C.c_void_p(image_ptr), st,
+                                                   LRT_TRACE_NATURAL_ORDER if natural_order else 0))
 
     def render_rgba8(self, camera, lights, background, image_ptr, stream=0):
         """Fused Render (eye rays, nearest hit, LAMBERT_NO_TEX resolve with
@@ -356,10 +374,20 @@ class SceneRT:
         self._check(lib().lrt_fill_gbuffer_transparency(self.h, C.byref(camera), bg, C.c_void_p(transparency_ptr),
                                                         C.c_void_p(hits_ptr), C.c_void_p(stream) if stream else None))
 
-    def adjoint_lambert(self, rays_ptr, n, light, dimage_ptr, grad_ptr, stream=0):
+    def adjoint_lambert(self, rays_ptr, n, light, dimage_ptr, grad_ptr, stream=0, image_size=None,
+                        natural_order=False):
+        """Adds dLoss/d(SBS float values) of the Lambert image of n device
+        rays to grad_ptr; image_size and natural_order as render_lambert."""
         L = (C.c_float * 3)(*[float(x) for x in light])
-        self._check(lib().lrt_adjoint_lambert_sbs(self.h, C.c_void_p(rays_ptr), n, L, C.c_void_p(dimage_ptr),
-                                                  C.c_void_p(grad_ptr), C.c_void_p(stream) if stream else None))
+        st = C.c_void_p(stream) if stream else None
+        if image_size is None:
+            self._check(lib().lrt_adjoint_lambert_sbs(self.h, C.c_void_p(rays_ptr), n, L, C.c_void_p(dimage_ptr),
+                                                      C.c_void_p(grad_ptr), st))
+            return
+        w, h = _image_size(image_size, n)
+        self._check(lib().lrt_adjoint_lambert_sbs_image(self.h, C.c_void_p(rays_ptr), w, h, L, C.c_void_p(dimage_ptr),
+                                                        C.c_void_p(grad_ptr), st,
+                                                        LRT_TRACE_NATURAL_ORDER if natural_order else 0))
 
     def update_sbs_values(self, values_ptr, count, device=True, stream=0):
         self._check(lib().lrt_sbs_update_values(self.h, C.c_void_p(values_ptr), count,

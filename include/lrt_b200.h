@@ -311,8 +311,8 @@ lrt_status lrt_scene_export(const lrt_scene* scene, lrt_scene_arrays* out);
 #define LRT_TRACE_FAST_MATH 0x2u       /* FMA-contracted kernels (tolerance
                                           parity); default is the exact build */
 #define LRT_TRACE_COUNT_WORK 0x4u      /* also accumulate work counters     */
-#define LRT_TRACE_NATURAL_ORDER 0x8u   /* lrt_trace_nearest_image: tiles in
-                                          row order, no tile schedule      */
+#define LRT_TRACE_NATURAL_ORDER 0x8u   /* image-order calls: tiles in row
+                                          order, no tile schedule          */
 
 /* Batched BVHRT::RayQuery_NearestHit.  rays: n x {float4 posAndNear,
  * float4 dirAndFar} (32 bytes per ray), hits: n x lrt_hit.  A ray whose
@@ -444,6 +444,15 @@ lrt_status lrt_generate_bounce_rays_compact(lrt_scene* scene, const float* rays_
 lrt_status lrt_render_lambert(lrt_scene* scene, const float* rays_dev, uint64_t n, const float light[3],
                               float* image_dev, void* stream);
 
+/* lrt_render_lambert for rays that form a width x height image (row-major
+ * pixels; several views of one size stack as a taller image), traced in
+ * 8x4-pixel tiles per warp in the stream's longest-first tile schedule, which
+ * it shares with lrt_trace_nearest_image, lrt_render_rgba8 and
+ * lrt_adjoint_lambert_sbs_image (LRT_TRACE_NATURAL_ORDER, the only flag:
+ * tiles in row order).  Every pixel's value equals lrt_render_lambert's. */
+lrt_status lrt_render_lambert_image(lrt_scene* scene, const float* rays_dev, uint32_t width, uint32_t height,
+                                    const float light[3], float* image_dev, void* stream, uint32_t flags);
+
 /* Light, core/IRenderer.h:72-78 (32 bytes).  space is the direction of a
  * LRT_LIGHT_DIRECT light (normalised by the caller, as create_direct_light
  * does) or the position of a LRT_LIGHT_POINT one; color includes intensity. */
@@ -525,6 +534,14 @@ lrt_status lrt_fill_gbuffer_transparency(lrt_scene* scene, const lrt_camera* cam
  * grad_dev holds sdfSBSDataF_count floats and is accumulated into. */
 lrt_status lrt_adjoint_lambert_sbs(lrt_scene* scene, const float* rays_dev, uint64_t n, const float light[3],
                                    const float* dimage_dev, float* grad_dev, void* stream);
+
+/* lrt_adjoint_lambert_sbs over a width x height image of rays in 8x4-pixel
+ * tiles and the stream's tile schedule, as lrt_render_lambert_image.  The
+ * contributions are those of lrt_adjoint_lambert_sbs; only the order of the
+ * float atomic additions into grad_dev differs. */
+lrt_status lrt_adjoint_lambert_sbs_image(lrt_scene* scene, const float* rays_dev, uint32_t width, uint32_t height,
+                                         const float light[3], const float* dimage_dev, float* grad_dev, void* stream,
+                                         uint32_t flags);
 
 /* Replaces the scene's SBS float values (count must equal the uploaded
  * sdfSBSDataF count; host memory, or device memory with

@@ -45,6 +45,44 @@ def test_forward_matches_oracle_after_value_updates(small):
         assert (img > 0).sum() > 1000
 
 
+@pytest.mark.parametrize("shape", [(96, 288), (27, 1024)], ids=["views_stacked", "ragged_tiles"])
+def test_forward_image_order_matches_oracle(small, shape):
+    """lrt_render_lambert_image: the rays as a width x height image in
+    8x4-pixel tiles, the stream's tile schedule from the second launch on, a
+    second stream and natural tile order; every pixel equals the oracle's."""
+    s = small
+    torch = s["torch"]
+    n = len(s["rays"])
+    v = torch.from_numpy(s["vf"]).cuda()
+    s["sc"].update_sbs_values(v.data_ptr(), v.numel())
+    want = po.port_render_lambert(s["sc"].export_arrays(), s["rays"], LIGHT)
+    side = torch.cuda.Stream()
+    runs = [dict(), dict(), dict(), dict(stream=side.cuda_stream), dict(natural_order=True)]
+    for kw in runs:
+        img = torch.full((n,), -1.0, dtype=torch.float32, device="cuda")
+        s["sc"].render_lambert(s["R"].data_ptr(), n, LIGHT, img.data_ptr(), image_size=shape, **kw)
+        s["sc"].sync(stream=kw.get("stream", 0))
+        assert np.array_equal(img.cpu().numpy().view(np.uint32), want.view(np.uint32)), kw
+
+
+def test_image_order_arguments_are_checked(small):
+    s = small
+    torch = s["torch"]
+    img = torch.empty(len(s["rays"]), dtype=torch.float32, device="cuda")
+    with pytest.raises(ValueError):
+        s["sc"].render_lambert(s["R"].data_ptr(), len(s["rays"]), LIGHT, img.data_ptr(), image_size=(95, 288))
+    import ctypes as C
+    from graphic_lab_task_b200 import lrt
+    invalid_argument = 1
+    L = (C.c_float * 3)(*LIGHT)
+    rc = lrt.lib().lrt_render_lambert_image(s["sc"].h, C.c_void_p(s["R"].data_ptr()), 96, 288, L,
+                                            C.c_void_p(img.data_ptr()), None, lrt.LRT_TRACE_FAST_MATH)
+    assert rc == invalid_argument
+    rc = lrt.lib().lrt_adjoint_lambert_sbs_image(s["sc"].h, C.c_void_p(s["R"].data_ptr()), 96, 288, L, None,
+                                                 C.c_void_p(img.data_ptr()), None, 0)
+    assert rc == invalid_argument
+
+
 def _loss_grad(s):
     torch = s["torch"]
     target_img = _render(s, s["target"])
@@ -67,6 +105,25 @@ def test_adjoint_matches_fp64_cpu_adjoint(small):
     assert np.array_equal(g != 0, g64 != 0)
     rel = np.linalg.norm(g - g64) / np.linalg.norm(g64)
     assert rel < 1e-4, rel
+
+
+def test_adjoint_image_order_matches_row_order(small):
+    """lrt_adjoint_lambert_sbs_image adds the same contributions as the
+    row-order adjoint (only the order of the float atomics differs), over
+    repeated launches with the tile schedule and in natural tile order."""
+    s = small
+    torch = s["torch"]
+    _, dimage, grad = _loss_grad(s)
+    g0 = grad.cpu().numpy().astype(np.float64)
+    P = dimage.numel()
+    for kw in (dict(), dict(), dict(natural_order=True)):
+        gi = torch.zeros_like(grad)
+        s["sc"].adjoint_lambert(s["R"].data_ptr(), P, LIGHT, dimage.data_ptr(), gi.data_ptr(), image_size=(96, 288),
+                                **kw)
+        s["sc"].sync()
+        g = gi.cpu().numpy().astype(np.float64)
+        assert np.array_equal(g != 0, g0 != 0)
+        assert np.linalg.norm(g - g0) <= 1e-5 * np.linalg.norm(g0)
 
 
 def test_adjoint_matches_central_differences(small):
@@ -121,12 +178,13 @@ def test_adjoint_matches_fp64_model_differences(small):
     assert rel_l2 < 1e-3 and np.median(per) < 1e-3
 
 
-def test_autograd_function(small):
+@pytest.mark.parametrize("image_size", [None, (96, 288)], ids=["row_order", "image_order"])
+def test_autograd_function(small, image_size):
     s = small
     torch = s["torch"]
     target_img, dimage, grad = _loss_grad(s)
     v = torch.from_numpy(s["vf"]).cuda().requires_grad_(True)
-    img = SbsLambertRender.apply(v, s["sc"], s["R"], LIGHT)
+    img = SbsLambertRender.apply(v, s["sc"], s["R"], LIGHT, image_size)
     loss = ((img - target_img) ** 2).mean()
     loss.backward()
     rel = (v.grad - grad).norm() / grad.norm()
