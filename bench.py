@@ -831,6 +831,26 @@ def configs_table(args):
             sc.trace_device(B.data_ptr(), HB.data_ptr(), k, stream=sp)
 
         wms = timed(wave, steps=5)
+        # the same wavefront with the bounce rays in coherence order
+        sidx = torch.empty(n, dtype=torch.int32, device=dev)
+        scnt = torch.zeros(1, dtype=torch.int64, device=dev)
+        SB = torch.empty_like(R)
+        sgen = lambda: sc.generate_bounce_rays_sorted(R.data_ptr(), H.data_ptr(), n, 11, SB.data_ptr(),
+                                                      sidx.data_ptr(), scnt.data_ptr(), stream=sp)
+        sc.trace_image(R.data_ptr(), H.data_ptr(), 4096, 4096, stream=sp)
+        sgen()
+        torch.cuda.synchronize(dev)
+        assert int(scnt.item()) == nb
+        sbms = timed(lambda: sc.trace_device(SB.data_ptr(), HB.data_ptr(), nb, stream=sp), steps=5)
+        sgms = timed(sgen, steps=5)
+
+        def wave_sorted():
+            sc.trace_image(R.data_ptr(), H.data_ptr(), 4096, 4096, stream=sp)
+            sgen()
+            k = int(scnt.item())
+            sc.trace_device(SB.data_ptr(), HB.data_ptr(), k, stream=sp)
+
+        wsms = timed(wave_sorted, steps=5)
         sc.sync(stream=sp)
         prim = R.view(-1, 8)[:: 256].cpu().numpy()
         bnc = bv[:: max(1, nb // 65536)].cpu().numpy()
@@ -839,10 +859,15 @@ def configs_table(args):
               "gpu_primary_image_order_ms": pims, "gpu_primary_image_order_mrays_s": n / pims / 1e3,
               "gpu_bounce_ms": bms, "gpu_bounce_mrays_s": nb / bms / 1e3, "gpu_bounce_generate_compact_ms": cms,
               "gpu_wavefront_ms": wms,
-              "gpu_wavefront_mrays_s": (n + nb) / wms / 1e3, "roofline_primary": roofline(sc, R, n, pms),
+              "gpu_wavefront_mrays_s": (n + nb) / wms / 1e3,
+              "sorted_bounce": {"call": "lrt_generate_bounce_rays_sorted (coherence order: direction cell, origin "
+                                        "Morton code)", "generate_ms": sgms, "bounce_ms": sbms,
+                                "bounce_mrays_s": nb / sbms / 1e3, "wavefront_ms": wsms,
+                                "wavefront_mrays_s": (n + nb) / wsms / 1e3},
+              "roofline_primary": roofline(sc, R, n, pms),
               "cpu_reference_primary": cpu(sc, prim), "cpu_reference_bounce": cpu(sc, bnc)})
         sc.close()
-        del R, H, B, HB, bv
+        del R, H, B, HB, bv, SB, sidx
 
     if 4 in only:
         # 4: differentiable render, 16 views of 512^2 at a virtual 256^3 grid

@@ -56,6 +56,10 @@ struct DeviceScene {
   // per-tile hit counts of lrt_generate_bounce_rays_compact
   uint32_t* tileScratch = nullptr;
   uint64_t tileCap = 0;
+  // keys, sorted keys, ray indices and radix-sort storage of
+  // lrt_generate_bounce_rays_sorted
+  void* sortScratch = nullptr;
+  size_t sortBytes = 0;
   // the renderer's material tables (lrt_set_materials), copied at the first
   // transparency trace after they changed
   lrt_material* mats = nullptr;
@@ -84,6 +88,7 @@ struct DeviceScene {
     if (rays) cudaFree(rays);
     if (hits) cudaFree(hits);
     if (tileScratch) cudaFree(tileScratch);
+    if (sortScratch) cudaFree(sortScratch);
     if (mats) cudaFree(mats);
     if (matIds) cudaFree(matIds);
     if (matOffsets) cudaFree(matOffsets);

@@ -9,7 +9,11 @@
 // tests, and a caller can drop them (origin x != x) before tracing.
 #include <cuda_runtime.h>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include <algorithm>
+#include <cfloat>
+#include <cmath>
 #include <cstdint>
 
 #include "device_scene.h"
@@ -193,6 +197,99 @@ __global__ void __launch_bounds__(kCompactThreads)
   }
 }
 
+// Coherence key of a hit's bounce ray (lrt_generate_bounce_rays_sorted): the
+// cell of the direction in a 4x4x4 grid over [-1, 1]^3 (bits 18..23) above
+// the Morton code of the origin on a 64^3 grid over the scene box (bits
+// 0..17, x highest of each triple), at most kMissKey - 1; misses get
+// kMissKey and sort last.  24 bits: three passes of the radix sort.  Every
+// rounding is an explicit IEEE round-to-nearest operation (no contraction),
+// so a host restatement in float32 computes the same key.
+constexpr uint32_t kMissKey = 0xFFFFFFu;
+constexpr int kKeyBits = 24;
+
+__device__ __forceinline__ uint32_t spread3_6(uint32_t x)
+{
+  x &= 0x3Fu;
+  x = (x | (x << 8)) & 0x0000F00Fu;
+  x = (x | (x << 4)) & 0x000C30C3u;
+  x = (x | (x << 2)) & 0x00249249u;
+  return x;
+}
+
+__device__ __forceinline__ uint32_t dir_cell(float d)
+{
+  const float g = __fmul_rn(__fadd_rn(d, 1.0f), 2.0f);
+  return !(g > 0.0f) ? 0u : g >= 3.0f ? 3u : uint32_t(g);
+}
+
+__device__ __forceinline__ uint32_t box_cell(float o, float lo, float scale)
+{
+  const float f = __fmul_rn(__fsub_rn(o, lo), scale);
+  return !(f > 0.0f) ? 0u : f >= 63.0f ? 63u : uint32_t(f);
+}
+
+__device__ __forceinline__ uint32_t coherence_key(const float4* b, float3 lo, float3 scale)
+{
+  const uint32_t cell = (dir_cell(b[1].x) << 4) | (dir_cell(b[1].y) << 2) | dir_cell(b[1].z);
+  const uint32_t m = (spread3_6(box_cell(b[0].x, lo.x, scale.x)) << 2) |
+                     (spread3_6(box_cell(b[0].y, lo.y, scale.y)) << 1) | spread3_6(box_cell(b[0].z, lo.z, scale.z));
+  return min((cell << 18) | m, kMissKey - 1u);
+}
+
+// keys[i] = coherence key of ray i's bounce ray (kMissKey for a miss),
+// vals[i] = i; *count += the number of hits.
+__global__ void __launch_bounds__(256) k_bounce_keys(const float4* __restrict__ rays, const lrt_hit* __restrict__ hits,
+                                                     uint64_t n, uint64_t seed, float tnear, float tfar, float3 lo,
+                                                     float3 scale, uint32_t* __restrict__ keys,
+                                                     uint32_t* __restrict__ vals, unsigned long long* __restrict__ count)
+{
+  uint32_t c = 0;
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+    const float4 h0 = reinterpret_cast<const float4*>(hits + i)[0];
+    uint32_t key = kMissKey;
+    if (__float_as_uint(h0.y) != 0xFFFFFFFFu) {
+      float4 b[2];
+      bounce_ray(rays[2 * i], rays[2 * i + 1], h0, reinterpret_cast<const float4*>(hits + i)[1], i, seed, tnear, tfar,
+                 b);
+      key = coherence_key(b, lo, scale);
+      c++;
+    }
+    keys[i] = key;
+    vals[i] = uint32_t(i);
+  }
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
+}
+
+// Bounce ray j of the sorted order: ray index[j]'s, for every j before the
+// first miss key (misses sort last, so a thread stops at its first one).
+__global__ void __launch_bounds__(256) k_bounce_gather(const float4* __restrict__ rays,
+                                                       const lrt_hit* __restrict__ hits, uint64_t n, uint64_t seed,
+                                                       float tnear, float tfar, const uint32_t* __restrict__ keys,
+                                                       const uint32_t* __restrict__ index, float4* __restrict__ out)
+{
+  for (uint64_t j = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; j < n; j += uint64_t(gridDim.x) * blockDim.x) {
+    if (keys[j] == kMissKey) return;
+    const uint64_t i = index[j];
+    const float4* h = reinterpret_cast<const float4*>(hits + i);
+    bounce_ray(rays[2 * i], rays[2 * i + 1], h[0], h[1], i, seed, tnear, tfar, out + 2 * j);
+  }
+}
+
+// Arguments shared by the compacting generators.
+lrt_status check_compact_args(lrt_scene* s, const char* who, const float* rays_dev, const lrt_hit* hits_dev,
+                              const float* bounce_dev, const uint32_t* index_dev, const uint64_t* count_dev)
+{
+  if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  if (!s->dev) return fail(s, LRT_ERR_NOT_COMMITTED, "%s before CommitScene/upload", who);
+  if (!rays_dev || !hits_dev || !bounce_dev || !index_dev || !count_dev)
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "%s: NULL buffer", who);
+  if ((reinterpret_cast<uintptr_t>(rays_dev) | reinterpret_cast<uintptr_t>(hits_dev) |
+       reinterpret_cast<uintptr_t>(bounce_dev)) & 15 || (reinterpret_cast<uintptr_t>(count_dev) & 7))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "%s: misaligned buffer", who);
+  return LRT_OK;
+}
+
 } // namespace
 } // namespace lrt
 
@@ -220,13 +317,9 @@ extern "C" lrt_status lrt_generate_bounce_rays_compact(lrt_scene* s, const float
                                                        float* bounce_dev, uint32_t* index_dev, uint64_t* count_dev,
                                                        void* stream_p)
 {
-  if (!s) return LRT_ERR_INVALID_ARGUMENT;
-  if (!s->dev) return fail(s, LRT_ERR_NOT_COMMITTED, "lrt_generate_bounce_rays_compact before CommitScene/upload");
-  if (!rays_dev || !hits_dev || !bounce_dev || !index_dev || !count_dev)
-    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_generate_bounce_rays_compact: NULL buffer");
-  if ((reinterpret_cast<uintptr_t>(rays_dev) | reinterpret_cast<uintptr_t>(hits_dev) |
-       reinterpret_cast<uintptr_t>(bounce_dev)) & 15 || (reinterpret_cast<uintptr_t>(count_dev) & 7))
-    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_generate_bounce_rays_compact: misaligned buffer");
+  lrt_status st = check_compact_args(s, "lrt_generate_bounce_rays_compact", rays_dev, hits_dev, bounce_dev, index_dev,
+                                     count_dev);
+  if (st != LRT_OK) return st;
   if (n > 0xFFFFFFFFull)
     return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_generate_bounce_rays_compact: more than 2^32 - 1 rays");
   cudaStream_t stream = static_cast<cudaStream_t>(stream_p);
@@ -252,4 +345,66 @@ extern "C" lrt_status lrt_generate_bounce_rays_compact(lrt_scene* s, const float
       reinterpret_cast<float4*>(bounce_dev), index_dev);
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "bounce compaction");
+}
+
+extern "C" lrt_status lrt_generate_bounce_rays_sorted(lrt_scene* s, const float* rays_dev, const lrt_hit* hits_dev,
+                                                      uint64_t n, uint64_t seed, float tnear, float tfar,
+                                                      float* bounce_dev, uint32_t* index_dev, uint64_t* count_dev,
+                                                      void* stream_p)
+{
+  lrt_status st = check_compact_args(s, "lrt_generate_bounce_rays_sorted", rays_dev, hits_dev, bounce_dev, index_dev,
+                                     count_dev);
+  if (st != LRT_OK) return st;
+  if (n > 0x7FFFFFFFull)
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_generate_bounce_rays_sorted: more than 2^31 - 1 rays");
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_p);
+  unsigned long long* cnt = reinterpret_cast<unsigned long long*>(count_dev);
+  cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), stream);
+  if (e != cudaSuccess) return cuda_fail(s, e, "cudaMemsetAsync");
+  if (n == 0) return LRT_OK;
+  // the scene box: the union of the instances' world boxes
+  float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  for (const lrt_instance_data& in : s->h.instanceData)
+    for (int k = 0; k < 3; k++)
+      if (in.boxMin[k] <= in.boxMax[k]) {
+        lo[k] = std::min(lo[k], in.boxMin[k]);
+        hi[k] = std::max(hi[k], in.boxMax[k]);
+      }
+  float scale[3];
+  for (int k = 0; k < 3; k++) {
+    const float ext = hi[k] - lo[k];
+    scale[k] = (lo[k] <= hi[k] && ext > 0.0f && std::isfinite(ext)) ? 64.0f / ext : 0.0f;
+    if (!(lo[k] <= hi[k])) lo[k] = 0.0f;
+  }
+  DeviceScene* d = s->dev;
+  size_t tempBytes = 0;
+  e = cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, static_cast<const uint32_t*>(nullptr),
+                                      static_cast<uint32_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
+                                      static_cast<uint32_t*>(nullptr), int(n), 0, kKeyBits, stream);
+  if (e != cudaSuccess) return cuda_fail(s, e, "radix sort size");
+  const size_t words = (3 * n + 63) & ~size_t(63); // keys, sorted keys, ray indices (256-byte aligned)
+  const size_t need = words * sizeof(uint32_t) + tempBytes;
+  if (need > d->sortBytes) {
+    if (d->sortScratch) cudaFree(d->sortScratch);
+    d->sortScratch = nullptr;
+    d->sortBytes = 0;
+    if ((e = cudaMalloc(&d->sortScratch, need)) != cudaSuccess) return cuda_fail(s, e, "bounce sort scratch");
+    d->sortBytes = need;
+  }
+  uint32_t* keys = static_cast<uint32_t*>(d->sortScratch);
+  uint32_t* sorted = keys + n;
+  uint32_t* vals = keys + 2 * n;
+  void* temp = keys + words;
+  const int grid = int(std::min<uint64_t>((n + 255) / 256, 148ull * 16));
+  const float4* rays = reinterpret_cast<const float4*>(rays_dev);
+  k_bounce_keys<<<grid, 256, 0, stream>>>(rays, hits_dev, n, seed, tnear, tfar, make_float3(lo[0], lo[1], lo[2]),
+                                          make_float3(scale[0], scale[1], scale[2]), keys, vals, cnt);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(s, e, "bounce keys");
+  e = cub::DeviceRadixSort::SortPairs(temp, tempBytes, static_cast<const uint32_t*>(keys), sorted,
+                                      static_cast<const uint32_t*>(vals), index_dev, int(n), 0, kKeyBits, stream);
+  if (e != cudaSuccess) return cuda_fail(s, e, "radix sort");
+  k_bounce_gather<<<grid, 256, 0, stream>>>(rays, hits_dev, n, seed, tnear, tfar, sorted, index_dev,
+                                            reinterpret_cast<float4*>(bounce_dev));
+  e = cudaGetLastError();
+  return e == cudaSuccess ? LRT_OK : cuda_fail(s, e, "bounce gather");
 }

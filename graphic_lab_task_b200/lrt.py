@@ -31,6 +31,7 @@ EXPORTED = (
     "lrt_batch_autotune", "lrt_render_lambert", "lrt_adjoint_lambert_sbs", "lrt_sbs_update_values",
     "lrt_generate_bounce_rays", "lrt_generate_bounce_rays_compact", "lrt_render_rgba8", "lrt_trace_nearest_image",
     "lrt_set_materials", "lrt_fill_gbuffer_transparency", "lrt_render_lambert_image", "lrt_adjoint_lambert_sbs_image",
+    "lrt_generate_bounce_rays_sorted",
     "lrt_update_instance", "lrt_add_geom_sdf_frame_octree_file", "lrt_add_geom_sdf_svs_file",
     "lrt_add_geom_sdf_sbs_file", "lrt_batch_render_rgba8",
     "lrt_wl_noisy_sphere", "lrt_wl_spheres", "lrt_wl_sphere_sdf", "lrt_wl_sbs_from_spheres",
@@ -116,6 +117,7 @@ def lib():
         "lrt_trace_nearest_image": [vp, vp, vp, u32, u32, vp, u32],
         "lrt_generate_bounce_rays": [vp, vp, vp, u64, u64, C.c_float, C.c_float, vp, vp],
         "lrt_generate_bounce_rays_compact": [vp, vp, vp, u64, u64, C.c_float, C.c_float, vp, vp, vp, vp],
+        "lrt_generate_bounce_rays_sorted": [vp, vp, vp, u64, u64, C.c_float, C.c_float, vp, vp, vp, vp],
         "lrt_adjoint_lambert_sbs": [vp, vp, u64, vp, vp, vp, vp],
         "lrt_render_lambert_image": [vp, vp, u32, u32, vp, vp, vp, u32],
         "lrt_adjoint_lambert_sbs_image": [vp, vp, u32, u32, vp, vp, vp, vp, u32],
@@ -333,6 +335,16 @@ class SceneRT:
                                                            seed, tnear, tfar, C.c_void_p(out_ptr),
                                                            C.c_void_p(index_ptr), C.c_void_p(count_ptr),
                                                            C.c_void_p(stream) if stream else None))
+
+    def generate_bounce_rays_sorted(self, rays_ptr, hits_ptr, n, seed, out_ptr, index_ptr, count_ptr, tnear=1e-4,
+                                    tfar=1e9, stream=0):
+        """generate_bounce_rays_compact in coherence order (direction cell,
+        then the origin's Morton code in the scene box); index_ptr (uint32, n
+        entries) maps them to the traced rays."""
+        self._check(lib().lrt_generate_bounce_rays_sorted(self.h, C.c_void_p(rays_ptr), C.c_void_p(hits_ptr), n,
+                                                          seed, tnear, tfar, C.c_void_p(out_ptr),
+                                                          C.c_void_p(index_ptr), C.c_void_p(count_ptr),
+                                                          C.c_void_p(stream) if stream else None))
 
     def render_lambert(self, rays_ptr, n, light, image_ptr, stream=0, image_size=None, natural_order=False):
         """Lambert image of n device rays.  image_size=(width, height) with

@@ -431,6 +431,25 @@ lrt_status lrt_generate_bounce_rays_compact(lrt_scene* scene, const float* rays_
                                             uint64_t n, uint64_t seed, float tnear, float tfar, float* bounce_dev,
                                             uint32_t* index_dev, uint64_t* count_dev, void* stream);
 
+/* lrt_generate_bounce_rays_compact with the bounce rays in coherence order
+ * instead of ray order, so that a warp's 32 rays head the same way from
+ * nearby points: sorted (stably, ties in ray order) by the key
+ *   min(cell(d.x) << 22 | cell(d.y) << 20 | cell(d.z) << 18
+ *       | morton(q.x, q.y, q.z), 2^24 - 2)
+ * of the bounce direction d and origin o, with cell(v) = clamp(int((v + 1) *
+ * 2), 0, 3), q = clamp(int((o - lo) * (64 / (hi - lo))), 0, 63) per axis
+ * over the union [lo, hi] of the instances' world boxes (float32, each
+ * operation rounded to nearest), and morton() interleaving the three 6-bit
+ * values x-highest.  index_dev[k] is the traced ray of bounce ray k;
+ * index_dev must hold n entries (its entries from *count_dev on are
+ * unspecified), as must bounce_dev.  At most 2^31 - 1 rays.  Three launches
+ * plus a device radix sort, no host synchronisation; the scratch grows with
+ * n on the device and is kept with the scene.  Each bounce ray equals
+ * lrt_generate_bounce_rays's for its traced ray. */
+lrt_status lrt_generate_bounce_rays_sorted(lrt_scene* scene, const float* rays_dev, const lrt_hit* hits_dev,
+                                           uint64_t n, uint64_t seed, float tnear, float tfar, float* bounce_dev,
+                                           uint32_t* index_dev, uint64_t* count_dev, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Differentiable form (SBS distances)                                      */
 /* ------------------------------------------------------------------------ */

@@ -123,3 +123,40 @@ def check_tlas_layout(nodes, n_inst):
                     assert np.all(nodes[c]["boxMin"] >= n["boxMin"]) and np.all(nodes[c]["boxMax"] <= n["boxMax"])
                 stack.append((lo, int(n["escapeIndex"])))
     assert sorted(leaves) == list(range(n_inst))
+
+
+def _spread3_6(x):
+    x = x & 0x3F
+    x = (x | (x << 8)) & 0x0000F00F
+    x = (x | (x << 4)) & 0x000C30C3
+    x = (x | (x << 2)) & 0x00249249
+    return x
+
+
+def bounce_coherence_keys(bounce, instance_data):
+    """The sort key of lrt_generate_bounce_rays_sorted, restated in numpy
+    float32 from its definition in include/lrt_b200.h: direction cell of a
+    4x4x4 grid over [-1, 1]^3 above the 6-bit-per-axis Morton code of the
+    origin in the union of the instances' world boxes."""
+    bmin = instance_data["boxMin"][:, :3].astype(np.float32)
+    bmax = instance_data["boxMax"][:, :3].astype(np.float32)
+    lo = np.zeros(3, np.float32)
+    scale = np.zeros(3, np.float32)
+    for k in range(3):
+        ok = bmin[:, k] <= bmax[:, k]
+        if not ok.any():
+            continue
+        lo[k] = bmin[ok, k].min()
+        ext = np.float32(bmax[ok, k].max() - lo[k])
+        if ext > 0 and np.isfinite(ext):
+            scale[k] = np.float32(64) / ext
+    o = bounce[:, 0:3].astype(np.float32)
+    d = bounce[:, 4:7].astype(np.float32)
+    with np.errstate(invalid="ignore"):
+        f = (o - lo) * scale
+        q = np.where(~(f > 0), 0, np.where(f >= 63, 63, np.nan_to_num(f).astype(np.int64)))
+        g = (d + np.float32(1)) * np.float32(2)
+        c = np.where(~(g > 0), 0, np.where(g >= 3, 3, np.nan_to_num(g).astype(np.int64)))
+    cell = (c[:, 0] << 4) | (c[:, 1] << 2) | c[:, 2]
+    morton = (_spread3_6(q[:, 0]) << 2) | (_spread3_6(q[:, 1]) << 1) | _spread3_6(q[:, 2])
+    return np.minimum((cell << 18) | morton, (1 << 24) - 2).astype(np.int64)

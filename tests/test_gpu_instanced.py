@@ -6,7 +6,7 @@ import pytest
 
 import pyoracle as po
 from graphic_lab_task_b200 import HIT_DTYPE, SceneRT, workloads as wl
-from helpers import MISS, bit_equal, hit_summary
+from helpers import MISS, bit_equal, bounce_coherence_keys, hit_summary
 
 pytestmark = pytest.mark.gpu
 
@@ -97,3 +97,53 @@ def test_compacted_bounce_rays_equal_the_full_generator(cuda, n):
     c = comp.cpu().numpy().reshape(-1, 8)
     assert np.array_equal(c[:k].view(np.uint32), f[want_idx].view(np.uint32))
     assert np.all(c[k:] == -7.0)  # nothing written past the count
+
+
+@pytest.mark.parametrize("n", [0, 1, 2047, 300001])
+def test_sorted_bounce_rays_are_the_compact_ones_in_key_order(cuda, n):
+    """lrt_generate_bounce_rays_sorted returns the compacted bounce rays and
+    their index map permuted by a stable sort of the coherence key (restated
+    in numpy), the same count, and traces of the sorted rays equal the
+    oracle's."""
+    torch = cuda
+    sc = SceneRT()
+    wl.build_instanced(sc, mesh_tris=(2000, 8000, 20000), octree_depth=6, n_instances=256)
+    sc.CommitScene()
+    rays = wl.eye_rays_host(wl.camera(wl.INSTANCED_EYE, width=600, height=501))[:n]
+    m = max(n, 1)
+    R = torch.from_numpy(np.ascontiguousarray(rays)).cuda() if n else torch.zeros(8, device="cuda")
+    H = torch.empty(m * 8, dtype=torch.float32, device="cuda")
+    sc.trace_device(R.data_ptr(), H.data_ptr(), n)
+    comp = torch.full((m * 8,), -7.0, dtype=torch.float32, device="cuda")
+    idx = torch.zeros(m, dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    sc.generate_bounce_rays_compact(R.data_ptr(), H.data_ptr(), n, 5, comp.data_ptr(), idx.data_ptr(), cnt.data_ptr())
+    srt = torch.full((m * 8,), -7.0, dtype=torch.float32, device="cuda")
+    sidx = torch.zeros(m, dtype=torch.int32, device="cuda")
+    scnt = torch.full((1,), 99, dtype=torch.int64, device="cuda")
+    for _ in range(2):  # the second call reuses the scene's sort scratch
+        sc.generate_bounce_rays_sorted(R.data_ptr(), H.data_ptr(), n, 5, srt.data_ptr(), sidx.data_ptr(),
+                                       scnt.data_ptr())
+    sc.sync()
+    k = int(cnt.item())
+    assert int(scnt.item()) == k
+    c = comp.cpu().numpy().reshape(-1, 8)[:k]
+    ci = idx.cpu().numpy()[:k]
+    order = np.argsort(bounce_coherence_keys(c, sc.export_arrays()["instanceData"]), kind="stable")
+    got = srt.cpu().numpy().reshape(-1, 8)
+    assert np.array_equal(got[:k].view(np.uint32), c[order].view(np.uint32))
+    assert np.array_equal(sidx.cpu().numpy()[:k], ci[order])
+    assert np.all(got[k:] == -7.0)  # nothing written past the count
+    if k:
+        if n > 2047:
+            # consecutive sorted rays share their direction cell far more often than in ray order
+            cells = bounce_coherence_keys(got[:k], sc.export_arrays()["instanceData"]) >> 18
+            assert (cells[1:] == cells[:-1]).mean() > 0.9
+        sel = np.unique(np.linspace(0, k - 1, min(k, 4000)).astype(np.int64))
+        B = torch.from_numpy(np.ascontiguousarray(got[sel])).cuda()
+        HB = torch.empty(len(sel) * 8, dtype=torch.float32, device="cuda")
+        sc.trace_device(B.data_ptr(), HB.data_ptr(), len(sel))
+        sc.sync()
+        bh = HB.cpu().numpy().view(HIT_DTYPE)
+        want = po.port_trace(sc.export_arrays(), got[sel])
+        assert bit_equal(bh, want).all(), hit_summary(bh, want)
