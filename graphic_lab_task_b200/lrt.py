@@ -295,9 +295,9 @@ class SceneRT:
         return hits
 
     def trace_host(self, rays_ptr, hits_ptr, n, fast_math=False):
-        """Synchronous trace of host buffers.  Page-locked buffers are read and
-        written by the kernel over PCIe; pageable ones are staged through device
-        memory in a chunked copy/trace/copy pipeline."""
+        """Synchronous trace of host buffers, staged through device memory:
+        from PIPE_MIN_RAYS rays on in a chunked copy/trace/copy pipeline
+        (page-locked buffers let both copy directions overlap)."""
         flags = LRT_TRACE_FAST_MATH if fast_math else 0
         self._check(lib().lrt_trace_nearest(self.h, C.c_void_p(rays_ptr), C.c_void_p(hits_ptr), n, None, flags))
 
