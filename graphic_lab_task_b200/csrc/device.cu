@@ -132,9 +132,11 @@ namespace {
 // img_w > 0: the n = img_w * img_h rays are an image in row-major order,
 // traced in 8x4-pixel tiles, in the stream's tile schedule unless flags has
 // LRT_TRACE_NATURAL_ORDER (or LRT_TRACE_COUNT_WORK).
+// err: the error word the kernel reports into (default: the slot's).
 lrt_status launch(lrt_scene* s, const float4* rays, lrt_hit* hits, uint64_t n, cudaStream_t stream, uint32_t flags,
-                  StreamSlot* slot, uint32_t img_w = 0, uint32_t img_h = 0)
+                  StreamSlot* slot, uint32_t img_w = 0, uint32_t img_h = 0, uint32_t* err = nullptr)
 {
+  if (!err) err = &slot->err;
   DeviceScene* d = s->dev;
   DevScene S = d->S;
   S.flags = launch_flags(s);
@@ -152,14 +154,21 @@ lrt_status launch(lrt_scene* s, const float4* rays, lrt_hit* hits, uint64_t n, c
   lrt_status st = sched_prepare(s, stream, img_w, img_h, natural, &rd, &wr);
   if (st != LRT_OK) return st;
   if (flags & LRT_TRACE_FAST_MATH)
-    e = lrt_fast::launch_trace(S, rays, hits, n, &slot->work, slot->counters, &slot->err, d->stackCap, grid, stream,
-                               count, img_w, img_h, rd, wr);
+    e = lrt_fast::launch_trace(S, rays, hits, n, &slot->work, slot->counters, err, d->stackCap, grid, stream, count,
+                               img_w, img_h, rd, wr);
   else
-    e = lrt_exact::launch_trace(S, rays, hits, n, &slot->work, slot->counters, &slot->err, d->stackCap, grid,
-                                stream, count, img_w, img_h, rd, wr);
+    e = lrt_exact::launch_trace(S, rays, hits, n, &slot->work, slot->counters, err, d->stackCap, grid, stream,
+                                count, img_w, img_h, rd, wr);
   if (e != cudaSuccess) return cuda_fail(s, e, "trace launch");
   sched_commit(s, stream, natural);
   return LRT_OK;
+}
+
+lrt_status limit_fail(lrt_scene* s, uint32_t bits)
+{
+  return fail(s, LRT_ERR_DEVICE_LIMIT,
+              "trace hit a bounded-loop limit (error bits 0x%x: 1 = stack, 2 = voxel march, 4 = transparency layers)",
+              bits);
 }
 
 // Reads back (and clears) the error word and, if asked, the counters of a slot.
@@ -174,8 +183,7 @@ lrt_status finish(lrt_scene* s, cudaStream_t stream, StreamSlot* slot, bool coun
   if (hs.err) {
     cudaMemsetAsync(&slot->err, 0, sizeof(uint32_t), stream);
     cudaStreamSynchronize(stream);
-    return fail(s, LRT_ERR_DEVICE_LIMIT, "trace hit a bounded-loop limit (error bits 0x%x: 1 = stack, 2 = voxel march, 4 = transparency layers)",
-                hs.err);
+    return limit_fail(s, hs.err);
   }
   return LRT_OK;
 }
@@ -211,7 +219,9 @@ void pipeline_chunks(uint64_t n, std::vector<uint64_t>& out)
 // the traces of several chunks run at the same time.  The pipeline starts
 // after the work already queued on the caller's stream, and the caller's
 // stream waits for it.  Events are re-recorded once per chunk: a wait takes
-// the record made before it.
+// the record made before it.  Every trace reports into one error word, which
+// the copy-out stream (that has waited for every trace) reads into page-locked
+// host memory after the last hits, so one synchronisation ends the call.
 lrt_status trace_host_pipelined(lrt_scene* s, const float* rays, lrt_hit* hits, uint64_t n, cudaStream_t stream,
                                 uint32_t flags)
 {
@@ -222,6 +232,7 @@ lrt_status trace_host_pipelined(lrt_scene* s, const float* rays, lrt_hit* hits, 
       e = cudaStreamCreateWithFlags(&d->pipe[p], cudaStreamNonBlocking);
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&d->pipeEv[p], cudaEventDisableTiming);
     }
+    if (e == cudaSuccess) e = cudaHostAlloc(&d->pipeErrHost, sizeof(uint32_t), cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&d->pipeStart, cudaEventDisableTiming);
     if (e != cudaSuccess) return cuda_fail(s, e, "pipeline streams");
   }
@@ -231,6 +242,7 @@ lrt_status trace_host_pipelined(lrt_scene* s, const float* rays, lrt_hit* hits, 
     lrt_status st = slot_for(s, d->pipe[kPipeTrace + k], &slots[k]);
     if (st != LRT_OK) return st;
   }
+  uint32_t* err = &slots[0]->err;
   e = cudaEventRecord(d->pipeStart, stream);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(in, d->pipeStart, 0);
   if (e != cudaSuccess) return cuda_fail(s, e, "pipeline start");
@@ -248,7 +260,7 @@ lrt_status trace_host_pipelined(lrt_scene* s, const float* rays, lrt_hit* hits, 
       st = cuda_fail(s, e, "rays host->device");
       break;
     }
-    st = launch(s, d->rays + 2 * off, d->hits + off, m, tr, flags, slots[k]);
+    st = launch(s, d->rays + 2 * off, d->hits + off, m, tr, flags, slots[k], 0, 0, err);
     if (st != LRT_OK) break;
     e = cudaEventRecord(d->pipeEv[kPipeTrace + k], tr);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(out, d->pipeEv[kPipeTrace + k], 0);
@@ -259,17 +271,27 @@ lrt_status trace_host_pipelined(lrt_scene* s, const float* rays, lrt_hit* hits, 
       break;
     }
   }
-  // the caller's stream waits for the last copy out; every stream is drained
-  // (and each trace stream's error word read) also after a failure
+  if (st == LRT_OK) {
+    e = cudaMemcpyAsync(d->pipeErrHost, err, sizeof(uint32_t), cudaMemcpyDeviceToHost, out);
+    if (e != cudaSuccess) st = cuda_fail(s, e, "error word");
+  }
+  // the caller's stream waits for the last copy out
   if (cudaEventRecord(d->pipeEv[kPipeOut], out) == cudaSuccess) cudaStreamWaitEvent(stream, d->pipeEv[kPipeOut], 0);
-  cudaStreamSynchronize(in);
-  for (int k = 0; k < kPipeTraceStreams; k++) {
-    const lrt_status sf = finish(s, d->pipe[kPipeTrace + k], slots[k], false);
-    if (st == LRT_OK) st = sf;
+  if (st != LRT_OK) { // drain every stream after a failure
+    for (int p = 0; p < kPipeStreams; p++) cudaStreamSynchronize(d->pipe[p]);
+    cudaMemsetAsync(err, 0, sizeof(uint32_t), out);
+    cudaStreamSynchronize(out);
+    return st;
   }
   e = cudaStreamSynchronize(out);
-  if (st == LRT_OK && e != cudaSuccess) st = cuda_fail(s, e, "hits device->host");
-  return st;
+  if (e != cudaSuccess) return cuda_fail(s, e, "hits device->host");
+  const uint32_t bits = *d->pipeErrHost;
+  if (bits) {
+    cudaMemsetAsync(err, 0, sizeof(uint32_t), out);
+    cudaStreamSynchronize(out);
+    return limit_fail(s, bits);
+  }
+  return LRT_OK;
 }
 
 } // namespace

@@ -77,8 +77,10 @@ struct DeviceScene {
   cudaStream_t pipe[kPipeStreams] = {};
   cudaEvent_t pipeEv[kPipeStreams] = {};
   cudaEvent_t pipeStart = nullptr;
+  uint32_t* pipeErrHost = nullptr; // page-locked copy of the pipeline's error word
   ~DeviceScene()
   {
+    if (pipeErrHost) cudaFreeHost(pipeErrHost);
     for (int p = 0; p < kPipeStreams; p++) {
       if (pipe[p]) cudaStreamDestroy(pipe[p]);
       if (pipeEv[p]) cudaEventDestroy(pipeEv[p]);

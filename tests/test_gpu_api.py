@@ -116,6 +116,24 @@ def test_voxel_march_limit_reports_and_recovers(cuda):
     assert bit_equal(got, want).all()
 
 
+def test_pipelined_host_trace_reports_limit_and_recovers(cuda):
+    """Host buffers of 262,144 rays or more run through the chunked
+    pipeline, whose traces share one error word: a march limit in any chunk
+    is reported once, and the next call (default limit) is exact."""
+    sc, rays, want = _sbs_scene()
+    reps = -(-300000 // len(rays))
+    big = np.ascontiguousarray(np.tile(rays, (reps, 1)))
+    big_want = np.tile(want, reps)
+    sc.set_voxel_step_limit(1)
+    with pytest.raises(LrtError) as e:
+        sc.RayQuery_NearestHitBatch(big)
+    assert e.value.status == 5 and "voxel" in str(e.value)
+    sc.set_voxel_step_limit(0)
+    for _ in range(2):
+        got = sc.RayQuery_NearestHitBatch(big)
+        assert bit_equal(got, big_want).all()
+
+
 def test_recommit_and_clear(cuda):
     sc = SceneRT()
     v, t = wl.noisy_sphere(16)
