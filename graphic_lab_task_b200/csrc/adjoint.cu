@@ -199,6 +199,49 @@ lrt_status adjoint_lambert(lrt_scene* s, const float* rays_dev, uint64_t n, uint
   return LRT_OK;
 }
 
+// OUTLINE_BORDER needs every pixel's neighbours' hits of the same sample: per
+// sample a G-buffer pass (k_outline_fill, in the stream's tile schedule) and a
+// resolve pass that applies the outline test and sums the samples; the last
+// one tonemaps into the image.  The G-buffer (t and miss flag), the colours
+// and the sums (8 + 16 + 16 bytes per pixel) are kept with the scene.
+lrt_status render_outline_border(lrt_scene* s, const DevScene& S, StreamSlot* slot, const DevCamera& cam,
+                                 const DevLights& L, const DevMaterials& M, const DevRenderModes& RM,
+                                 uint32_t* image_dev, int grid, cudaStream_t stream)
+{
+  DeviceScene* d = s->dev;
+  const uint64_t n = uint64_t(cam.width) * cam.height;
+  auto up = [](uint64_t b) { return (b + 255) & ~uint64_t(255); };
+  const uint64_t tmBytes = up(n * sizeof(float2)), colBytes = up(n * sizeof(float4));
+  const uint64_t need = tmBytes + 2 * colBytes;
+  cudaError_t e = cudaSuccess;
+  if (need > d->outlineBytes) {
+    if (d->outlineScratch) cudaFree(d->outlineScratch);
+    d->outlineScratch = nullptr;
+    d->outlineBytes = 0;
+    if ((e = cudaMalloc(&d->outlineScratch, need)) != cudaSuccess) return cuda_fail(s, e, "outline G-buffer");
+    d->outlineBytes = need;
+  }
+  char* base = static_cast<char*>(d->outlineScratch);
+  float2* tm = reinterpret_cast<float2*>(base);
+  float4* col = reinterpret_cast<float4*>(base + tmBytes);
+  float4* acc = reinterpret_cast<float4*>(base + tmBytes + colBytes);
+  for (uint32_t smp = 0; smp < RM.samples; smp++) {
+    if (smp && (e = cudaMemsetAsync(&slot->work, 0, sizeof(unsigned long long), stream)) != cudaSuccess)
+      return cuda_fail(s, e, "cudaMemsetAsync");
+    const uint32_t* rd = nullptr;
+    uint32_t* wr = nullptr;
+    lrt_status st = sched_prepare(s, stream, cam.width, cam.height, false, &rd, &wr);
+    if (st != LRT_OK) return st;
+    e = lrt_exact::launch_outline_fill(S, cam, L, M, RM, smp, tm, col, &slot->work, &slot->err, d->stackCap, grid,
+                                       stream, rd, wr);
+    if (e != cudaSuccess) return cuda_fail(s, e, "outline G-buffer launch");
+    sched_commit(s, stream, false);
+    e = lrt_exact::launch_outline_resolve(tm, col, cam.width, cam.height, smp, RM.samples, acc, image_dev, stream);
+    if (e != cudaSuccess) return cuda_fail(s, e, "outline resolve launch");
+  }
+  return LRT_OK;
+}
+
 } // namespace
 } // namespace lrt
 
@@ -252,11 +295,12 @@ lrt_status lrt_render_rgba8(lrt_scene* s, const lrt_camera* camera, const lrt_li
   if (light_count > LRT_MAX_LIGHTS)
     return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_render_rgba8: %u lights (at most %d)", light_count, LRT_MAX_LIGHTS);
   const uint32_t mode = s->preset.render_mode;
-  static const uint32_t kModes[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 16, 17, 18, 19, 20, 21, 22, 24, 25};
+  static const uint32_t kModes[] = {0,  1,  2,  3,  4,  5,  6,  7,  8,  9,  10, 11,
+                                    12, 13, 14, 16, 17, 18, 19, 20, 21, 22, 24, 25};
   if (std::find(std::begin(kModes), std::end(kModes), mode) == std::end(kModes))
     return fail(s, LRT_ERR_UNSUPPORTED,
-                "lrt_render_rgba8: render_mode %u (textures, shadows, PBR, outlines, channels and intersection "
-                "counts are outside the ray-query path)",
+                "lrt_render_rgba8: render_mode %u (texture coordinates, channels and intersection counts are outside "
+                "the ray-query path)",
                 mode);
   if (mode == 11 && (s->mats.empty() || s->mats[0].type != LRT_MATERIAL_COLORED))
     return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_render_rgba8: PBR_NO_TEX shades with material 0, a COLORED one");
@@ -308,12 +352,13 @@ lrt_status lrt_render_rgba8(lrt_scene* s, const lrt_camera* camera, const lrt_li
   const int grid = int(std::min<uint64_t>(uint64_t(d->grid), (tiles * 32 + kTraceThreads - 1) / kTraceThreads));
   const uint32_t* rd = nullptr;
   uint32_t* wr = nullptr;
-  if ((st = sched_prepare(s, stream, cam.width, cam.height, false, &rd, &wr)) != LRT_OK) return st;
   DevMaterials M{};
   M.mats = d->mats;
   M.ids = d->matIds;
   M.offsets = reinterpret_cast<const uint2*>(d->matOffsets);
   std::memcpy(M.background, background, sizeof(M.background));
+  if (mode == LRT_RENDER_MODE_OUTLINE_BORDER) return render_outline_border(s, S, slot, cam, L, M, RM, image_dev, grid, stream);
+  if ((st = sched_prepare(s, stream, cam.width, cam.height, false, &rd, &wr)) != LRT_OK) return st;
   const cudaError_t e = lrt_exact::launch_render_rgba8(S, cam, L, image_dev, &slot->work, &slot->err, d->stackCap,
                                                        grid, stream, rd, wr, &M, &RM);
   if (e != cudaSuccess) return cuda_fail(s, e, "render launch");

@@ -60,6 +60,9 @@ struct DeviceScene {
   // lrt_generate_bounce_rays_sorted
   void* sortScratch = nullptr;
   size_t sortBytes = 0;
+  // G-buffer, colours and sums of the OUTLINE_BORDER render
+  void* outlineScratch = nullptr;
+  size_t outlineBytes = 0;
   // the renderer's material tables (lrt_set_materials), copied at the first
   // transparency trace after they changed
   lrt_material* mats = nullptr;
@@ -91,6 +94,7 @@ struct DeviceScene {
     if (hits) cudaFree(hits);
     if (tileScratch) cudaFree(tileScratch);
     if (sortScratch) cudaFree(sortScratch);
+    if (outlineScratch) cudaFree(outlineScratch);
     if (mats) cudaFree(mats);
     if (matIds) cudaFree(matIds);
     if (matOffsets) cudaFree(matOffsets);

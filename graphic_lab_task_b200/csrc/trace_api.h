@@ -32,6 +32,13 @@
                                                uint32_t stack_cap, int grid, cudaStream_t stream,               \
                                                const uint32_t* sched_rd = nullptr,                              \
                                                uint32_t* sched_wr = nullptr);                                   \
+  cudaError_t launch_outline_fill(const lrt::DevScene& S, const lrt::DevCamera& cam, const lrt::DevLights& lights, \
+                                 const lrt::DevMaterials& M, const lrt::DevRenderModes& RM, uint32_t smp,       \
+                                 float2* tm, float4* col, unsigned long long* work_counter, uint32_t* err_word, \
+                                 uint32_t stack_cap, int grid, cudaStream_t stream, const uint32_t* sched_rd,   \
+                                 uint32_t* sched_wr);                                                           \
+  cudaError_t launch_outline_resolve(const float2* tm, const float4* col, uint32_t w, uint32_t h, uint32_t smp,  \
+                                     uint32_t samples, float4* acc, uint32_t* image, cudaStream_t stream);     \
   cudaError_t launch_render_lambert(const lrt::DevScene& S, const float4* rays, uint64_t n, float3 light,       \
                                     float* image, unsigned long long* work_counter, uint32_t* err_word,         \
                                     uint32_t stack_cap, int grid, cudaStream_t stream, uint32_t img_w = 0,      \

@@ -1399,6 +1399,96 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_render_rgba8(DevScene S, D
   if (c.err) atomicOr(err_word, c.err);
 }
 
+// OUTLINE_BORDER (MultiRenderer.cpp:55-58: FillGbuffer, then ResolveOutline,
+// MultiRenderer_resolve.cpp:1073-1128), the G-buffer pass of sample smp: per
+// pixel the nearest hit of the sample's ray — its t and whether it missed
+// (tm) — and the pixel's colour before the outline test (col): white Lambert
+// of the hit under the lights, shaded with the sample-0 ray as ResolveOutline
+// does (the OUTLINE_PRIM colour), or the background for a miss.  The colour
+// is resolved here, with the trace's context, because a triangle's normal
+// needs the triangle record the traversal found.
+__global__ void __launch_bounds__(kTraceThreads, 7) k_outline_fill(DevScene S, DevCamera cam, DevLights L,
+                                                                DevMaterials M, DevRenderModes RM, uint32_t smp,
+                                                                float2* __restrict__ tm, float4* __restrict__ col,
+                                                                unsigned long long* __restrict__ work_counter,
+                                                                uint32_t* __restrict__ err_word, uint32_t stack_cap,
+                                                                const uint32_t* __restrict__ sched_rd,
+                                                                uint32_t* sched_wr)
+{
+  extern __shared__ uint32_t smem_stack[];
+  uint32_t* stack = smem_stack + threadIdx.x;
+  const uint32_t lane = threadIdx.x & 31;
+  Ctx<false> c(S, normal_words(smem_stack, stack_cap));
+  const uint32_t tilesX = (cam.width + 7) / 8, ntiles = tilesX * ((cam.height + 3) / 4);
+  __shared__ WarpClock wclock[kTraceThreads / 32];
+  if (lane == 0) {
+    wclock[threadIdx.x >> 5].tile = ~0u;
+    wclock[threadIdx.x >> 5].longest = 0;
+  }
+  for (;;) {
+    uint32_t tile = 0;
+    __syncwarp();
+    if (lane == 0) tile = sched_next(sched_rd, sched_wr, ntiles, work_counter, wclock[threadIdx.x >> 5]);
+    tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
+    if (tile == ~0u) break;
+    const uint32_t x = (tile % tilesX) * 8 + (lane & 7), y = (tile / tilesX) * 4 + (lane >> 3);
+    if (x < cam.width && y < cam.height) {
+      float r0[8], rs[8];
+      eye_ray(cam.proj_inv, cam.world_view_inv, x, y, cam.width, cam.height, cam.tnear, cam.tfar, r0,
+              RM.random ? RM.randomX : RM.invSqrt * 0.5f, RM.random ? RM.randomY : RM.invSqrt * 0.5f);
+      float dx = RM.randomX, dy = RM.randomY;
+      if (!RM.random) {
+        dx = RM.invSqrt * float(double(smp / RM.sqrtSpp) + 0.5);
+        dy = RM.invSqrt * float(double(smp % RM.sqrtSpp) + 0.5);
+      }
+      eye_ray(cam.proj_inv, cam.world_view_inv, x, y, cam.width, cam.height, cam.tnear, cam.tfar, rs, dx, dy);
+      lrt_hit h;
+      trace_one(c, stack, blockDim.x, stack_cap, make_float4(rs[0], rs[1], rs[2], rs[3]),
+                make_float4(rs[4], rs[5], rs[6], rs[7]), h);
+      const uint64_t p = uint64_t(y) * cam.width + x;
+      tm[p] = make_float2(h.t, h.primId == 0xFFFFFFFFu ? 1.0f : 0.0f);
+      col[p] = resolve_mode_colour(c, L, M, LRT_RENDER_MODE_OUTLINE_PRIM, mk3(r0[0], r0[1], r0[2]),
+                                   mk3(r0[4], r0[5], r0[6]), h);
+    }
+  }
+  if (c.err) atomicOr(err_word, c.err);
+}
+
+// ResolveOutline's test (MultiRenderer_resolve.cpp:1112-1127) and the sum over
+// samples: a hit pixel whose t differs from the t of one of its four
+// neighbours (the pixel itself at the image's edges) by more than
+// 10 t / width takes (0.2, 0.2, 0.2, 1); misses keep the background.  The
+// last sample's pass divides the sum by the sample count and tonemaps.
+__global__ void __launch_bounds__(256) k_outline_resolve(const float2* __restrict__ tm, const float4* __restrict__ col,
+                                                         uint32_t w, uint32_t h, uint32_t smp, uint32_t samples,
+                                                         float4* __restrict__ acc, uint32_t* __restrict__ image)
+{
+  const uint64_t n = uint64_t(w) * h;
+  for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < n; p += uint64_t(gridDim.x) * blockDim.x) {
+    const uint32_t x = uint32_t(p % w), y = uint32_t(p / w);
+    const float2 me = tm[p];
+    float4 c = col[p];
+    if (me.y == 0.0f) {
+      const float t = me.x;
+      const float tol = 10.0f * t / float(w);
+      const float tl = tm[x == 0 ? p : p - 1].x, tu = tm[y == 0 ? p : p - w].x;
+      const float tr = tm[x == w - 1 ? p : p + 1].x, td = tm[y == h - 1 ? p : p + w].x;
+      if (fabsf(tl - t) > tol || fabsf(tu - t) > tol || fabsf(tr - t) > tol || fabsf(td - t) > tol)
+        c = make_float4(0.2f, 0.2f, 0.2f, 1.0f);
+    }
+    if (smp) {
+      const float4 a = acc[p];
+      c = make_float4(a.x + c.x, a.y + c.y, a.z + c.z, a.w + c.w);
+    }
+    if (smp + 1 < samples) {
+      acc[p] = c;
+    } else {
+      const float ns = float(samples);
+      image[p] = tonemap_rgba8(c.x / ns, c.y / ns, c.z / ns, c.w / ns);
+    }
+  }
+}
+
 // kernel1D_FillGbufferWithTransparency (MultiRenderer.cpp:204-221) for one
 // sample: anyhit_loop per pixel of the camera (8x4-pixel tiles per warp).
 __global__ void __launch_bounds__(kTraceThreads, 7) k_fill_gbuffer_transparency(
@@ -1612,6 +1702,28 @@ cudaError_t launch_render_rgba8(const DevScene& S, const DevCamera& cam, const D
   one.samples = 1;
   kernel<<<grid, kTraceThreads, smem, stream>>>(S, cam, lights, image, work_counter, err_word, stack_cap, sched_rd,
                                                 sched_wr, materials ? *materials : DevMaterials{}, rm ? *rm : one);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_outline_fill(const DevScene& S, const DevCamera& cam, const DevLights& lights,
+                               const DevMaterials& M, const DevRenderModes& RM, uint32_t smp, float2* tm, float4* col,
+                               unsigned long long* work_counter, uint32_t* err_word, uint32_t stack_cap, int grid,
+                               cudaStream_t stream, const uint32_t* sched_rd, uint32_t* sched_wr)
+{
+  cudaError_t e = cudaFuncSetAttribute(k_outline_fill, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(trace_smem_bytes(kMaxStackDev + 1)));
+  if (e != cudaSuccess) return e;
+  k_outline_fill<<<grid, kTraceThreads, trace_smem_bytes(stack_cap), stream>>>(
+      S, cam, lights, M, RM, smp, tm, col, work_counter, err_word, stack_cap, sched_rd, sched_wr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_outline_resolve(const float2* tm, const float4* col, uint32_t w, uint32_t h, uint32_t smp,
+                                   uint32_t samples, float4* acc, uint32_t* image, cudaStream_t stream)
+{
+  const uint64_t n = uint64_t(w) * h;
+  const int grid = int(std::min<uint64_t>((n + 255) / 256, 148ull * 16));
+  k_outline_resolve<<<grid, 256, 0, stream>>>(tm, col, w, h, smp, samples, acc, image);
   return cudaGetLastError();
 }
 

@@ -163,6 +163,8 @@ typedef struct lrt_preset {
 #define LRT_SBS_LAYOUT_MASK 0xFF000000u
 #define LRT_RENDER_MODE_LAMBERT_NO_TEX 1u
 #define LRT_RENDER_MODE_ST_ITERATIONS 10u
+#define LRT_RENDER_MODE_OUTLINE_PRIM 13u   /* MULTI_RENDER_MODE_*, core/render_settings.h */
+#define LRT_RENDER_MODE_OUTLINE_BORDER 14u
 #define LRT_SDF_INTERSECT_ST 0u
 #define LRT_NORMAL_MODE_GEOMETRY 0u
 #define LRT_INTERPOLATION_TRILINEAR 0u
@@ -500,10 +502,14 @@ enum { LRT_LIGHT_DIRECT = 0, LRT_LIGHT_POINT = 1, LRT_LIGHT_AMBIENT = 2 };
  * point for RAY_GEN_MODE_RANDOM), resolved with the sample-0 ray as
  * ResolveCommon does, and averaged; with a transparent COLORED material,
  * LAMBERT, PHONG, PBR and DIFFUSE take the reference's transparency path (the
- * AnyHit G-buffer blended into the resolved colour).  Other modes
- * (OUTLINE_BORDER, channels, intersection counts) and textured materials return
- * LRT_ERR_UNSUPPORTED; the pixel grid is the camera's (the reference pads
- * widths to a multiple of 8).  Writes
+ * AnyHit G-buffer blended into the resolved colour).  OUTLINE_BORDER
+ * (ResolveOutline, :1073-1128) runs two launches per sample: a G-buffer pass
+ * and the outline test against the four neighbours' t (more than 10 t / width
+ * apart: colour (0.2, 0.2, 0.2)); it keeps 40 bytes per pixel of device
+ * scratch with the scene.  Other modes (texture coordinates, channels,
+ * intersection counts) and textured materials return LRT_ERR_UNSUPPORTED; the
+ * pixel grid is the camera's (the reference pads widths to a multiple of 8,
+ * and its outline test reads the padded grid).  Writes
  * width*height RGBA8 pixels (row-major) to device memory image_dev;
  * asynchronous on `stream`, lrt_trace_sync(stream) reports bounded-loop
  * limits.  No counterpart call in the reference (it renders through a

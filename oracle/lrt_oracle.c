@@ -27,6 +27,7 @@
  */
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include "../include/lrt_b200.h"
@@ -1357,6 +1358,65 @@ void lrto_render_rgba8_ex(const lrt_scene_arrays* arrays, const lrt_preset* pres
     const float ns = (float)samples;
     image[i] = tonemap_rgba8(acc[0] / ns, acc[1] / ns, acc[2] / ns, acc[3] / ns);
   }
+}
+
+/* MultiRenderer::Render for OUTLINE_BORDER (MultiRenderer.cpp:55-58) over a
+ * width x height image: per sample the G-buffer of that sample's rays
+ * (kernel1D_FillGbuffer) and ResolveOutline (MultiRenderer_resolve.cpp:
+ * 1073-1128) per pixel: the background for a miss, else white Lambert of the
+ * hit shaded with the sample-0 ray, replaced by (0.2, 0.2, 0.2, 1) when the t
+ * of one of the four neighbours (the pixel itself at the image's edges)
+ * differs from the pixel's by more than 10 t / width; the colours are summed
+ * over the samples, divided by their count and tonemapped. */
+void lrto_render_outline_border(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* sample_rays,
+                                uint32_t samples, const float* resolve_rays, uint32_t width, uint32_t height,
+                                const lrt_light* lights, uint32_t light_count, const float background[4],
+                                uint32_t* image, int threads)
+{
+  const uint64_t n = (uint64_t)width * height;
+  lrt_hit* g = (lrt_hit*)malloc((n ? n : 1) * sizeof(lrt_hit));
+  float* col = (float*)malloc((n ? n : 1) * 4 * sizeof(float));
+  float* acc = (float*)calloc((n ? n : 1) * 4, sizeof(float));
+  (void)threads;
+  for (uint32_t smp = 0; smp < samples; smp++) {
+#ifdef _OPENMP
+#pragma omp parallel for num_threads(threads > 0 ? threads : 1) schedule(dynamic, 256)
+#endif
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+      uint64_t cnt[LRT_COUNTER_COUNT];
+      ctx_t c = {arrays, preset, cnt, 0, NULL, 0};
+      const float* r = sample_rays + 8 * ((uint64_t)smp * n + (uint64_t)i);
+      g[i] = nearest_hit(&c, r, r + 4);
+      /* the Lambert colour of ResolveOutline is OUTLINE_PRIM's; resolved with
+         the trace's context (a triangle's normal needs its record) */
+      resolve_colour(arrays, &c, 13u, g[i], resolve_rays + 8 * i, lights, light_count, background, NULL, NULL, NULL,
+                     col + 4 * i);
+    }
+    for (uint64_t i = 0; i < n; i++) {
+      float c4[4];
+      memcpy(c4, col + 4 * i, sizeof(c4));
+      if (g[i].primId != 0xFFFFFFFFu) {
+        const uint32_t x = (uint32_t)(i % width), y = (uint32_t)(i / width);
+        const float t = g[i].t;
+        const float tol = 10.0f * t / (float)width;
+        const float tl = g[x == 0 ? i : i - 1].t, tu = g[y == 0 ? i : i - width].t;
+        const float tr = g[x == width - 1 ? i : i + 1].t, td = g[y == height - 1 ? i : i + width].t;
+        if (fabsf(tl - t) > tol || fabsf(tu - t) > tol || fabsf(tr - t) > tol || fabsf(td - t) > tol) {
+          c4[0] = 0.2f;
+          c4[1] = 0.2f;
+          c4[2] = 0.2f;
+          c4[3] = 1.0f;
+        }
+      }
+      for (int k = 0; k < 4; k++) acc[4 * i + k] = smp == 0 ? c4[k] : acc[4 * i + k] + c4[k];
+    }
+  }
+  const float ns = (float)samples;
+  for (uint64_t i = 0; i < n; i++)
+    image[i] = tonemap_rgba8(acc[4 * i] / ns, acc[4 * i + 1] / ns, acc[4 * i + 2] / ns, acc[4 * i + 3] / ns);
+  free(g);
+  free(col);
+  free(acc);
 }
 
 void lrto_render_rgba8_modes(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* rays, uint64_t n,

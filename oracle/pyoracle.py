@@ -267,6 +267,33 @@ def port_render_rgba8_samples(arrays, sample_rays, resolve_rays, lights, backgro
     return img
 
 
+def port_render_outline_border(arrays, sample_rays, resolve_rays, width, height, lights, background, preset,
+                               threads=os.cpu_count()):
+    """Render for OUTLINE_BORDER over a width x height image (row-major):
+    sample_rays (samples, n, 8), resolve_rays (n, 8) the sample-0 rays."""
+    from graphic_lab_task_b200._abi import LIGHT_DTYPE
+    lib = port_lib()
+    if not hasattr(lib, "_outline_bound"):
+        lib.lrto_render_outline_border.restype = None
+        lib.lrto_render_outline_border.argtypes = [C.POINTER(SceneArrays), C.POINTER(Preset), C.c_void_p, C.c_uint32,
+                                                   C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32,
+                                                   C.c_void_p, C.c_void_p, C.c_int]
+        lib._outline_bound = True
+    s, keep = arrays_to_struct(arrays)
+    sr = np.ascontiguousarray(sample_rays, dtype=np.float32)
+    rr = np.ascontiguousarray(resolve_rays, dtype=np.float32).reshape(-1, 8)
+    n = width * height
+    assert len(rr) == n and sr.size == sr.shape[0] * n * 8
+    lt = np.ascontiguousarray(lights, dtype=LIGHT_DTYPE)
+    bg = np.ascontiguousarray(background, dtype=np.float32)
+    img = np.zeros(n, np.uint32)
+    lib.lrto_render_outline_border(C.byref(s), C.byref(preset), sr.ctypes.data, sr.shape[0], rr.ctypes.data, width,
+                                   height, lt.ctypes.data if len(lt) else None, len(lt), bg.ctypes.data,
+                                   img.ctypes.data, int(threads))
+    del keep
+    return img
+
+
 def port_fill_gbuffer_transparency(arrays, rays, materials, mat_ids, mat_offsets, background, max_layers=256,
                                    preset=None, threads=os.cpu_count()):
     """AnyHit's transparency loop per eye ray (rays: row-major pixels).

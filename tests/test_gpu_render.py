@@ -70,11 +70,11 @@ def test_render_rgba8_refusals(cuda):
         sc.render_rgba8(cam, many, (0, 0, 0, 1), img.data_ptr())
     assert e.value.status == 1
     p = parity_preset()
-    p.render_mode = 14  # OUTLINE_BORDER
+    p.render_mode = 23  # CHANNEL
     sc.SetPreset(p)
     with pytest.raises(LrtError) as e:
         sc.render_rgba8(cam, _lights(), (0, 0, 0, 1), img.data_ptr())
-    assert e.value.status == 6 and "render_mode 14" in str(e.value)
+    assert e.value.status == 6 and "render_mode 23" in str(e.value)
     p.render_mode = 11  # PBR_NO_TEX shades with material 0
     sc.SetPreset(p)
     with pytest.raises(LrtError) as e:
@@ -186,6 +186,38 @@ def test_render_samples_and_transparency_match_oracle(cuda, mode, spp, ray_gen, 
         assert (one != want).sum() > 10
 
 
+@pytest.mark.parametrize("spp,size", [(1, (96, 64)), (4, (96, 64)), (1, (61, 37))],
+                         ids=["spp1", "spp4", "ragged"])
+def test_render_outline_border_matches_oracle(cuda, spp, size):
+    """OUTLINE_BORDER: per sample a G-buffer pass and ResolveOutline's test
+    against the four neighbours' t (more than 10 t / width apart: the
+    (0.2, 0.2, 0.2) outline colour), summed over the samples; bit-identical to
+    the oracle, repeated on the stream's tile schedule."""
+    torch = cuda
+    sc = _mixed_scene()
+    p = parity_preset()
+    p.render_mode, p.spp = 14, spp
+    sc.SetPreset(p)
+    cam = wl.camera((0.5, 0.7, 3.5), width=size[0], height=size[1])
+    bg = (0.1, 0.2, 0.3, 1.0)
+    offsets = [wl.sample_offset(k, spp, 0) for k in range(spp)]
+    sample_rays = np.stack([wl.eye_rays_host(cam, dx, dy) for dx, dy in offsets])
+    want = po.port_render_outline_border(sc.export_arrays(), sample_rays, sample_rays[0], cam.width, cam.height,
+                                         _lights(), bg, p)
+    for _ in range(3):
+        img = torch.zeros(cam.width * cam.height, dtype=torch.int32, device="cuda")
+        sc.render_rgba8(cam, _lights(), bg, img.data_ptr())
+        sc.sync()
+        got = img.cpu().numpy().view(np.uint32)
+        assert np.array_equal(got, want), "%d of %d pixels differ" % ((got != want).sum(), len(got))
+    outline = (255 << 24) | (51 << 16) | (51 << 8) | 51  # tonemap of (0.2, 0.2, 0.2, 1)
+    if spp == 1:
+        assert (got == outline).sum() > 20
+    prim = po.port_render_rgba8_samples(sc.export_arrays(), sample_rays, sample_rays[0], _lights(), bg,
+                                        _preset_mode(p, 13))
+    assert (prim != want).sum() > 20  # the outlines are what OUTLINE_PRIM does not draw
+
+
 def test_batched_render_equals_per_camera_render(cuda):
     """lrt_batch_render_rgba8 renders every camera of a batch in one launch;
     each image equals lrt_render_rgba8's for that camera."""
@@ -274,3 +306,9 @@ def test_fill_gbuffer_transparency_refusals_and_layer_bound(cuda):
     assert e.value.status == 5 and "transparency" in str(e.value)
     sc.fill_gbuffer_transparency(cam, bg, tr.data_ptr(), hits.data_ptr())
     sc.sync()
+
+
+def _preset_mode(p, mode):
+    q = parity_preset()
+    q.render_mode, q.spp, q.ray_gen_mode = mode, p.spp, p.ray_gen_mode
+    return q
