@@ -736,9 +736,11 @@ def configs_table(args):
         R = torch.from_numpy(rays).to(dev)
         H = torch.empty(n * 8, dtype=torch.float32, device=dev)
         ms = timed(lambda: sc.trace_device(R.data_ptr(), H.data_ptr(), n, stream=sp))
+        ims = timed(lambda: sc.trace_image(R.data_ptr(), H.data_ptr(), 256, 256, stream=sp))
         sc.sync(stream=sp)
         emit({"config": 0, "workload": "mesh 200k triangles, 256x256", "rays": n, "gpu_ms": ms,
-              "gpu_mrays_s": n / ms / 1e3, "roofline": roofline(sc, R, n, ms), "cpu_reference": cpu(sc, rays)})
+              "gpu_mrays_s": n / ms / 1e3, "gpu_image_order_ms": ims, "gpu_image_order_mrays_s": n / ims / 1e3,
+              "roofline": roofline(sc, R, n, ms), "cpu_reference": cpu(sc, rays)})
         sc.close()
 
     if 1 in only or 3 in only:
