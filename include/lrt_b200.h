@@ -428,7 +428,9 @@ lrt_status lrt_generate_bounce_rays(lrt_scene* scene, const float* rays_dev, con
  * bounce ray k (each bounce ray equals lrt_generate_bounce_rays's for that
  * ray).  count_dev: one uint64 in device memory, written on `stream` (read it
  * back, or size the next trace by it).  At most 2^32 - 1 rays.  Three
- * launches (count per tile, scan, write), no host synchronisation. */
+ * launches (count per tile, scan, write), no host synchronisation.  The
+ * per-tile counts live in scratch kept with the scene: calls that overlap on
+ * different streams race. */
 lrt_status lrt_generate_bounce_rays_compact(lrt_scene* scene, const float* rays_dev, const lrt_hit* hits_dev,
                                             uint64_t n, uint64_t seed, float tnear, float tfar, float* bounce_dev,
                                             uint32_t* index_dev, uint64_t* count_dev, void* stream);
@@ -446,7 +448,8 @@ lrt_status lrt_generate_bounce_rays_compact(lrt_scene* scene, const float* rays_
  * index_dev must hold n entries (its entries from *count_dev on are
  * unspecified), as must bounce_dev.  At most 2^31 - 1 rays.  Three launches
  * plus a device radix sort, no host synchronisation; the scratch grows with
- * n on the device and is kept with the scene.  Each bounce ray equals
+ * n on the device and is kept with the scene, so calls that overlap on
+ * different streams race.  Each bounce ray equals
  * lrt_generate_bounce_rays's for its traced ray. */
 lrt_status lrt_generate_bounce_rays_sorted(lrt_scene* scene, const float* rays_dev, const lrt_hit* hits_dev,
                                            uint64_t n, uint64_t seed, float tnear, float tfar, float* bounce_dev,
