@@ -411,32 +411,72 @@ Aabb lod_box(uint32_t pos_xy, uint32_t pos_z_lod_size)
   return b;
 }
 
-// inverse of a column-major 4x4 (Gauss-Jordan in double, rounded to float).
+// Inverse of a column-major 4x4 in float, by cofactors, rounding exactly like
+// LiteMath's inverse4x4 (dependencies/1st-party/LiteMath/LiteMath.h:2070-2153),
+// which BVHRT::AddInstance and UpdateInstance use for transformInv
+// (BVH2Common_host.cpp:1295-1296, 1333): the instance matrices must be the
+// reference's floats, or rays enter the BLAS at other points and hits drift.
+//
+// 2x2 products p[k] = a(i, u_k) * a(j, v_k) are formed for the row pairs
+// (i, j) = (2, 3) (output columns 0, 1) and (0, 1) (columns 2, 3).  Each
+// cofactor is (three products) - (three products), each triple summed left to
+// right, with the terms in the order of kCof; the result is scaled by
+// 1 / (row 0 of the input . column 0 of the cofactors).  Returns false for a
+// matrix whose determinant is zero or not finite (the reference would return
+// infinities and NaNs).
 bool invert4(const float* m, float* out)
 {
-  double a[4][8];
-  for (int r = 0; r < 4; r++)
-    for (int c = 0; c < 4; c++) {
-      a[r][c] = m[c * 4 + r];
-      a[r][4 + c] = (r == c) ? 1.0 : 0.0;
-    }
+  auto a = [m](int r, int c) { return m[c * 4 + r]; };
+  // the column pairs (u_k, v_k) of the 12 products of one row pair
+  static const uint8_t kPairCols[12][2] = {{2, 3}, {3, 2}, {1, 3}, {3, 1}, {1, 2}, {2, 1},
+                                           {0, 3}, {3, 0}, {0, 2}, {2, 0}, {0, 1}, {1, 0}};
+  // cofactor (r, c): six {product index, column of the multiplying row} terms,
+  // three added then three subtracted; the multiplying row of output column
+  // c is kRowOf[c]
+  static const uint8_t kRowOf[4] = {1, 0, 3, 2};
+  static const uint8_t kCof[4][4][6][2] = {
+      // output column 0
+      {{{0, 1}, {3, 2}, {4, 3}, {1, 1}, {2, 2}, {5, 3}},
+       {{1, 0}, {6, 2}, {9, 3}, {0, 0}, {7, 2}, {8, 3}},
+       {{2, 0}, {7, 1}, {10, 3}, {3, 0}, {6, 1}, {11, 3}},
+       {{5, 0}, {8, 1}, {11, 2}, {4, 0}, {9, 1}, {10, 2}}},
+      // output column 1
+      {{{1, 1}, {2, 2}, {5, 3}, {0, 1}, {3, 2}, {4, 3}},
+       {{0, 0}, {7, 2}, {8, 3}, {1, 0}, {6, 2}, {9, 3}},
+       {{3, 0}, {6, 1}, {11, 3}, {2, 0}, {7, 1}, {10, 3}},
+       {{4, 0}, {9, 1}, {10, 2}, {5, 0}, {8, 1}, {11, 2}}},
+      // output column 2
+      {{{0, 1}, {3, 2}, {4, 3}, {1, 1}, {2, 2}, {5, 3}},
+       {{1, 0}, {6, 2}, {9, 3}, {0, 0}, {7, 2}, {8, 3}},
+       {{2, 0}, {7, 1}, {10, 3}, {3, 0}, {6, 1}, {11, 3}},
+       {{5, 0}, {8, 1}, {11, 2}, {4, 0}, {9, 1}, {10, 2}}},
+      // output column 3
+      {{{2, 2}, {5, 3}, {1, 1}, {4, 3}, {0, 1}, {3, 2}},
+       {{8, 3}, {0, 0}, {7, 2}, {6, 2}, {9, 3}, {1, 0}},
+       {{6, 1}, {11, 3}, {3, 0}, {10, 3}, {2, 0}, {7, 1}},
+       {{10, 2}, {4, 0}, {9, 1}, {8, 1}, {11, 2}, {5, 0}}},
+  };
+  float p[2][12];
+  for (int half = 0; half < 2; half++) {
+    const int i = half ? 0 : 2, j = i + 1;
+    for (int k = 0; k < 12; k++) p[half][k] = a(i, kPairCols[k][0]) * a(j, kPairCols[k][1]);
+  }
+  float cof[4][4]; // cof[r][c]
   for (int c = 0; c < 4; c++) {
-    int piv = c;
-    for (int r = c + 1; r < 4; r++)
-      if (std::fabs(a[r][c]) > std::fabs(a[piv][c])) piv = r;
-    if (std::fabs(a[piv][c]) < 1e-300) return false;
-    if (piv != c)
-      for (int k = 0; k < 8; k++) std::swap(a[c][k], a[piv][k]);
-    const double inv = 1.0 / a[c][c];
-    for (int k = 0; k < 8; k++) a[c][k] *= inv;
+    const float* t = p[c >> 1];
+    const int row = kRowOf[c];
     for (int r = 0; r < 4; r++) {
-      if (r == c) continue;
-      const double f = a[r][c];
-      for (int k = 0; k < 8; k++) a[r][k] -= f * a[c][k];
+      const uint8_t(*q)[2] = kCof[c][r];
+      float v = t[q[0][0]] * a(row, q[0][1]) + t[q[1][0]] * a(row, q[1][1]) + t[q[2][0]] * a(row, q[2][1]);
+      v -= t[q[3][0]] * a(row, q[3][1]) + t[q[4][0]] * a(row, q[4][1]) + t[q[5][0]] * a(row, q[5][1]);
+      cof[r][c] = v;
     }
   }
+  const float det = a(0, 0) * cof[0][0] + a(0, 1) * cof[1][0] + a(0, 2) * cof[2][0] + a(0, 3) * cof[3][0];
+  if (det == 0.0f || !std::isfinite(det)) return false;
+  const float k = 1.0f / det;
   for (int r = 0; r < 4; r++)
-    for (int c = 0; c < 4; c++) out[c * 4 + r] = float(a[r][4 + c]);
+    for (int c = 0; c < 4; c++) out[c * 4 + r] = cof[r][c] * k;
   return true;
 }
 

@@ -78,6 +78,8 @@ def ref_lib(fast=False):
         lib.lrtr_add_sbs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64,
                                      C.c_void_p, C.c_uint64]
         lib.lrtr_add_instance.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+        lib.lrtr_update_instance.restype = None
+        lib.lrtr_update_instance.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
         lib.lrtr_commit.argtypes = [C.c_void_p]
         lib.lrtr_export.argtypes = [C.c_void_p, C.POINTER(SceneArrays)]
         lib.lrtr_import.argtypes = [C.c_void_p, C.POINTER(SceneArrays)]
@@ -161,6 +163,10 @@ class RefScene:
     def add_instance(self, geom_id, matrix_col_major):
         m = np.ascontiguousarray(matrix_col_major, dtype=np.float32).reshape(16)
         return self.lib.lrtr_add_instance(self.h, geom_id, m.ctypes.data)
+
+    def update_instance(self, inst_id, matrix_col_major):
+        m = np.ascontiguousarray(matrix_col_major, dtype=np.float32).reshape(16)
+        self.lib.lrtr_update_instance(self.h, inst_id, m.ctypes.data)
 
     def commit(self):
         self.lib.lrtr_commit(self.h)

@@ -110,6 +110,16 @@ uint32_t lrtr_add_instance(void* p, uint32_t geom_id, const float* m_col_major16
   return static_cast<Holder*>(p)->rt->AddInstance(geom_id, m);
 }
 
+// BVHRT::UpdateInstance (BVH2Common_host.cpp:1303-1335) with the same matrix
+// convention as lrtr_add_instance.
+void lrtr_update_instance(void* p, uint32_t inst_id, const float* m_col_major16)
+{
+  LiteMath::float4x4 m;
+  for (int c = 0; c < 4; c++)
+    for (int r = 0; r < 4; r++) m(r, c) = m_col_major16[c * 4 + r];
+  static_cast<Holder*>(p)->rt->UpdateInstance(inst_id, m);
+}
+
 void lrtr_commit(void* p) { static_cast<Holder*>(p)->rt->CommitScene(BUILD_HIGH); }
 
 // View of the BVHRT members the traversal reads (BVH2Common.h:262-365).

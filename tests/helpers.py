@@ -71,6 +71,61 @@ def tolerance_report(got, want, rays=None):
             "n_fail": int((dn > 1e-4).sum()), "mismatch_idx": np.nonzero(~ids)[0]}
 
 
+def assert_within_spec(got, want, max_tie_frac=1e-4, what=""):
+    """The hot path's acceptance rule against the reference's own build:
+    ids (primId, instId, geomId) bit-exact except on rays whose two nearest
+    hits lie within 1e-5 relative t (here: the two answers name different
+    primitives at t values within 1e-5 of each other, so the ray has two hits
+    that close), t within 1e-5 relative on every hit ray, decoded normals
+    within 1e-4 where the ids agree.  Hit/miss disagreements are failures.
+    At most `max_tie_frac` of the rays may be near ties.  Returns the report."""
+    hg, hw = got["primId"] != MISS, want["primId"] != MISS
+    assert np.array_equal(hg, hw), "%s: %d rays hit in one and miss in the other" % (what, int((hg != hw).sum()))
+    ids = (got["primId"] == want["primId"]) & (got["instId"] == want["instId"]) & (got["geomId"] == want["geomId"])
+    both = hg & hw
+    rel_t = np.abs(got["t"][both].astype(np.float64) - want["t"][both]) / np.maximum(np.abs(want["t"][both]), 1e-30)
+    assert (rel_t <= 1e-5).all(), "%s: %d hits outside 1e-5 relative t (max %.3g)" % (
+        what, int((rel_t > 1e-5).sum()), rel_t.max())
+    rep = tolerance_report(got, want)
+    ties = int((~ids).sum())
+    assert ties <= max(1, max_tie_frac * len(got)), "%s: %d id mismatches (near ties) of %d rays" % (
+        what, ties, len(got))
+    assert rep["n_fail"] == 0, "%s: %d normals outside 1e-4 (max %.3g)" % (what, rep["n_fail"], rep["max_normal_err"])
+    rep["ties"] = ties
+    rep["bit_identical"] = int(bit_equal(got, want).sum())
+    return rep
+
+
+class RefBuilder:
+    """The reference's own scene assembly (pyoracle.RefScene: BVHRT
+    AddGeom_* / AddInstance / CommitScene compiled from its sources) behind
+    the method names of SceneRT, so that one workload generator builds the
+    same scene through both."""
+
+    def __init__(self, fast=False):
+        import pyoracle
+        self.ref = pyoracle.RefScene(fast=fast)
+
+    def AddGeom_Triangles3f(self, verts, tris):
+        return self.ref.add_triangles(verts, tris)
+
+    def AddGeom_SdfFrameOctree(self, nodes):
+        return self.ref.add_frame_octree(nodes)
+
+    def AddGeom_SdfSVS(self, nodes):
+        return self.ref.add_svs(nodes)
+
+    def AddGeom_SdfSBS(self, header, nodes, values, values_f=None):
+        return self.ref.add_sbs(header, nodes, values, values_f)
+
+    def AddInstance(self, geom, matrix):
+        return self.ref.add_instance(geom, matrix)
+
+    def CommitScene(self):
+        self.ref.commit()
+        return self.ref
+
+
 LEAF = 0x80000000
 
 

@@ -1,17 +1,23 @@
 """The product's scene assembly (csrc/scene.cpp): flattened arrays with the
 reference's layouts, traced identically by the reference and the oracle, and
 upload validation of malformed arrays (no GPU needed)."""
+import os
+
 import numpy as np
 import pytest
 
 import pyoracle as po
 from graphic_lab_task_b200 import LrtError, SceneRT, workloads as wl
-from helpers import LEAF, MISS, bit_equal, check_blas_layout, check_tlas_layout, hit_summary
+from helpers import (LEAF, MISS, RefBuilder, assert_within_spec, bit_equal, check_blas_layout, check_tlas_layout,
+                     hit_summary)
 
 
-def build_mixed(seed=0, n_inst=8):
+def build_mixed(seed=0, n_inst=8, sc=None):
+    """A mesh, an SBS, a frame octree and an SVS under `n_inst` random
+    instances, assembled through `sc` (a SceneRT by default; a RefBuilder
+    gives the same scene through the reference's own host code)."""
     sph = wl.spheres(12, seed=200 + seed)
-    sc = SceneRT()
+    sc = SceneRT() if sc is None else sc
     v, t = wl.noisy_sphere(20, seed=seed)
     gm = sc.AddGeom_Triangles3f(v, t)
     hdr, nodes, vals, vf = wl.sbs_from_spheres(sph, grid_res=32, brick_size=4, brick_pad=1)
@@ -20,6 +26,8 @@ def build_mixed(seed=0, n_inst=8):
     gs = sc.AddGeom_SdfSVS(wl.svs_from_spheres(sph, 4))
     for i, m in enumerate(wl.random_instances(n_inst, seed=seed, scale=(0.3, 0.8), trans=1.2)):
         sc.AddInstance([gm, gb, go, gs][i % 4], m)
+    if isinstance(sc, RefBuilder):
+        return sc.CommitScene(), (v, t)
     sc.CommitScene(host_only=True)
     return sc, (v, t)
 
@@ -65,7 +73,97 @@ def test_product_arrays_trace_like_reference(seed):
         assert bit_equal(got, want).all(), hit_summary(got, want)
 
 
-@pytest.mark.skipif(not po.ref_available(), reason="reference build absent (make -C oracle ref)")
+needs_ref = pytest.mark.skipif(not po.ref_available(), reason="reference build absent (make -C oracle ref)")
+
+
+def _instance_fields_equal(a, b):
+    """Bitwise equality of every instance field the traversal reads."""
+    for f in ("boxMin", "boxMax", "geomId", "transform", "transformInv", "transformInvTransposed"):
+        assert a[f].tobytes() == b[f].tobytes(), f
+
+
+@needs_ref
+def test_instance_matrices_equal_reference_add_and_update_instance():
+    """AddInstance / UpdateInstance store the reference's floats
+    (BVH2Common_host.cpp:1264-1335, LiteMath inverse4x4): box, transform,
+    inverse and normal matrix bit-equal to the reference's own host code for
+    rotations with scales from 1e-3 to 50 and translations up to 1e4."""
+    v, t = wl.noisy_sphere(12, seed=9)
+    mats = (wl.random_instances(600, seed=5) + wl.random_instances(200, seed=6, scale=(1e-3, 50), trans=1e4)
+            + [wl.IDENTITY, wl.similarity(0.5, (1, 2, 3))])
+    ref = po.RefScene()
+    gr = ref.add_triangles(v, t)
+    sc = SceneRT()
+    gs = sc.AddGeom_Triangles3f(v, t)
+    for m in mats:
+        ref.add_instance(gr, m)
+        sc.AddInstance(gs, m)
+    # UpdateInstance: new transform and inverse; the normal matrix stays in both
+    new = wl.random_instances(len(mats), seed=8, scale=(0.01, 10), trans=100)
+    for i in range(0, len(mats), 7):
+        ref.update_instance(i, new[i])
+        sc.UpdateInstance(i, new[i])
+    ref.commit()
+    sc.CommitScene(host_only=True)
+    _instance_fields_equal(sc.export_arrays()["instanceData"], ref.export()["instanceData"])
+
+
+def _interior_rays(n, seed, lo=-5.0, hi=5.0):
+    """Seeded rays from points inside the instance cloud in uniform directions."""
+    rng = np.random.default_rng(seed)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r = np.zeros((n, 8), np.float32)
+    r[:, 0:3] = rng.uniform(lo, hi, size=(n, 3))
+    r[:, 3] = 1e-4
+    r[:, 4:7] = d
+    r[:, 7] = 1e9
+    return r
+
+
+@needs_ref
+def test_instanced_scene_built_through_product_matches_reference_build():
+    """The two-level workload (three noisy-sphere meshes, two frame octrees,
+    256 random instances; reduced sizes) assembled through the product's API
+    and through the reference's own AddGeom_* / AddInstance / CommitScene:
+    every eye ray and every ray from inside the instance cloud gets the same
+    hit, bit for bit (the product's SAH tree and the reference's tree differ;
+    nearest hits do not depend on them here)."""
+    kw = dict(mesh_tris=(2000, 8000, 20000), octree_depth=6, n_instances=256)
+    sc = SceneRT()
+    wl.build_instanced(sc, **kw)
+    sc.CommitScene(host_only=True)
+    rb = RefBuilder()
+    wl.build_instanced(rb, **kw)
+    ref = rb.CommitScene()
+    _instance_fields_equal(sc.export_arrays()["instanceData"], ref.export()["instanceData"])
+    rays = np.concatenate([wl.eye_rays_host(wl.camera(wl.INSTANCED_EYE, width=256, height=256)),
+                           _interior_rays(65536, seed=21)])
+    got = po.port_trace(sc.export_arrays(), rays)
+    want = ref.trace(rays, threads=os.cpu_count())
+    assert (got["primId"] != MISS).sum() > 8000
+    assert bit_equal(got, want).all(), hit_summary(got, want)
+
+
+@needs_ref
+@pytest.mark.parametrize("seed", [0, 1])
+def test_mixed_scene_built_through_product_matches_reference_build(seed):
+    """A mesh, an SBS, a frame octree and an SVS under random instances,
+    assembled by both hosts: hits within the specification's tolerance of the
+    reference's build (bit-identical apart from near ties)."""
+    sc, _ = build_mixed(seed, n_inst=12)
+    ref, _ = build_mixed(seed, n_inst=12, sc=RefBuilder())
+    _instance_fields_equal(sc.export_arrays()["instanceData"], ref.export()["instanceData"])
+    rays = np.concatenate([wl.eye_rays_host(wl.camera((0.3, 0.9, 3.2), width=96, height=72)),
+                           _interior_rays(20000, seed=30 + seed, lo=-1.5, hi=1.5)])
+    got = po.port_trace(sc.export_arrays(), rays)
+    want = ref.trace(rays, threads=os.cpu_count())
+    assert (got["primId"] != MISS).sum() > 5000
+    rep = assert_within_spec(got, want, what="mixed scene")
+    assert rep["bit_identical"] >= len(rays) - rep["ties"]
+
+
+@needs_ref
 def test_triangle_hits_independent_of_builder():
     """Nearest triangle hits do not depend on the tree: the product builder
     and the reference builder give the same answers on a mesh."""
