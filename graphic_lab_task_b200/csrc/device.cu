@@ -296,6 +296,10 @@ lrt_status trace_host_pipelined(lrt_scene* s, const float* rays, lrt_hit* hits, 
 
 } // namespace
 
+// Device address of the static scratch array of lrt_trace_nearest_noalloc
+// (defined with it at the end of this file), for the current device.
+cudaError_t noalloc_scratch_address(void** p);
+
 lrt_status device_upload(lrt_scene* s)
 {
   device_release(s);
@@ -377,6 +381,15 @@ lrt_status device_upload(lrt_scene* s)
     return st;
   }
   d->grid = std::max(1, perSm) * sms;
+  // The allocation-free trace's static array is looked up here, with the
+  // scene's device current, not in the trace call: under lazy module loading
+  // the first lookup loads this file's module and places the array in device
+  // memory, which an upload may do and lrt_trace_nearest_noalloc must not.
+  // A failed lookup fails only that entry point.
+  void* base = nullptr;
+  d->noallocErr = noalloc_scratch_address(&base);
+  if (d->noallocErr != cudaSuccess) cudaGetLastError(); // not sticky: clear it
+  d->noallocBase = static_cast<unsigned char*>(base);
   return LRT_OK;
 }
 
@@ -566,8 +579,9 @@ lrt_status lrt_generate_eye_rays(lrt_scene* s, const lrt_camera* cam, float* ray
 // bounded-loop error word — and, for host buffers, the staging copies of the
 // rays and hits live in one file-scope __device__ array instead of memory
 // from cudaMalloc.  Its size is fixed: 256 bytes of launch state plus room for
-// kNoAllocMaxRays rays and hits (1 MiB + 256 B in all), held by every GPU that
-// loads this library until the process exits.
+// kNoAllocMaxRays rays and hits (1 MiB + 256 B in all).  A device holds it
+// from the first scene upload on that device (which looks its address up)
+// until the process exits.
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -578,34 +592,11 @@ static_assert(sizeof(lrt::StreamSlot) <= kNoAllocStateBytes, "launch state fits 
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
-// Device address of g_noalloc_scratch on each device, looked up once per
-// device with that device current (the symbol name is only a host-side
-// stand-in and must never be handed to a kernel).
-constexpr int kNoAllocMaxDevices = 64;
-void* g_noalloc_addr[kNoAllocMaxDevices] = {};
-
-lrt_status noalloc_scratch(lrt_scene* s, unsigned char** out)
-{
-  int dev = -1;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return lrt::fail(s, LRT_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
-  if (dev != s->device)
-    return lrt::fail(s, LRT_ERR_INVALID_ARGUMENT,
-                     "lrt_trace_nearest_noalloc: make the scene's device (%d) current, not %d", s->device, dev);
-  if (dev < 0 || dev >= kNoAllocMaxDevices)
-    return lrt::fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_trace_nearest_noalloc: device %d out of range", dev);
-  if (!g_noalloc_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess)
-      return lrt::fail(s, LRT_ERR_CUDA, "cudaGetSymbolAddress(static scratch): %s", cudaGetErrorString(e));
-    g_noalloc_addr[dev] = p;
-  }
-  *out = static_cast<unsigned char*>(g_noalloc_addr[dev]);
-  return LRT_OK;
-}
-
 } // namespace
+
+// The array's device address for the current device.  The symbol's name is
+// only a host-side stand-in for the array and must never reach a kernel.
+cudaError_t lrt::noalloc_scratch_address(void** p) { return cudaGetSymbolAddress(p, g_noalloc_scratch); }
 
 extern "C" lrt_status lrt_trace_nearest_noalloc(lrt_scene* s, const float* rays, lrt_hit* hits, uint64_t n,
                                                 void* stream_p, uint32_t flags)
@@ -626,9 +617,16 @@ extern "C" lrt_status lrt_trace_nearest_noalloc(lrt_scene* s, const float* rays,
     return fail(s, LRT_ERR_INVALID_ARGUMENT, "device rays/hits must be 16-byte aligned");
   lrt_status st = check_preset(s);
   if (st != LRT_OK) return st;
-  unsigned char* base = nullptr;
-  st = noalloc_scratch(s, &base);
-  if (st != LRT_OK) return st;
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(s, e, "cudaGetDevice");
+  if (dev != s->device)
+    return fail(s, LRT_ERR_INVALID_ARGUMENT,
+                "lrt_trace_nearest_noalloc: make the scene's device (%d) current, not %d", s->device, dev);
+  if (!s->dev->noallocBase)
+    return fail(s, LRT_ERR_CUDA, "lrt_trace_nearest_noalloc: the static scratch array was not found at upload: %s",
+                cudaGetErrorString(s->dev->noallocErr));
+  unsigned char* base = s->dev->noallocBase;
   StreamSlot* slot = reinterpret_cast<StreamSlot*>(base);
   float4* srays = reinterpret_cast<float4*>(base + kNoAllocStateBytes);
   lrt_hit* shits = reinterpret_cast<lrt_hit*>(base + kNoAllocStateBytes + kNoAllocMaxRays * 32);
@@ -639,7 +637,7 @@ extern "C" lrt_status lrt_trace_nearest_noalloc(lrt_scene* s, const float* rays,
   S.voxelStepCap = s->voxelStepCap ? s->voxelStepCap : kMaxVoxelSteps;
   // the array keeps the previous call's contents: the ray counter and the
   // error word must start at zero
-  cudaError_t e = cudaMemsetAsync(slot, 0, sizeof(StreamSlot), stream);
+  e = cudaMemsetAsync(slot, 0, sizeof(StreamSlot), stream);
   if (e != cudaSuccess) return cuda_fail(s, e, "cudaMemsetAsync(static scratch)");
   const float4* krays = onDevice ? reinterpret_cast<const float4*>(rays) : srays;
   lrt_hit* khits = onDevice ? hits : shits;

@@ -81,6 +81,10 @@ struct DeviceScene {
   cudaEvent_t pipeEv[kPipeStreams] = {};
   cudaEvent_t pipeStart = nullptr;
   uint32_t* pipeErrHost = nullptr; // page-locked copy of the pipeline's error word
+  // device address of lrt_trace_nearest_noalloc's static scratch array on
+  // this scene's device, looked up at upload (and the lookup's result)
+  unsigned char* noallocBase = nullptr;
+  cudaError_t noallocErr = cudaSuccess;
   ~DeviceScene()
   {
     if (pipeErrHost) cudaFreeHost(pipeErrHost);

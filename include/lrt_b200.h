@@ -330,16 +330,18 @@ lrt_status lrt_trace_nearest(lrt_scene* scene, const float* rays, lrt_hit* hits,
  * own pool, or forbids device allocation inside its frame loop).  The trace
  * kernel's scratch (ray counter, error word) and, for host buffers, the
  * staging copies of rays and hits live in a fixed file-scope device array of
- * 1 MiB + 256 B that every GPU loading the library keeps until exit.  With
- * host pointers at most 16384 rays per call are accepted (larger n returns
+ * 1 MiB + 256 B, which a GPU holds from the first scene upload on it until
+ * the process exits: the upload (lrt_commit_scene, lrt_scene_upload) looks
+ * the array's device address up with the scene's device current, so this
+ * call loads no module and allocates no device memory.  With host pointers at
+ * most 16384 rays per call are accepted (larger n returns
  * LRT_ERR_INVALID_ARGUMENT); with LRT_TRACE_DEVICE_POINTERS any n.  The call
- * calls no cudaMalloc/cudaFree and returns after `stream` has drained, with
- * LRT_ERR_DEVICE_LIMIT if the kernel hit a bounded-loop limit.  The first call
- * on a device looks up the array's device address (cudaGetSymbolAddress) with
- * the scene's device current; make that first call before any stream capture.
- * All calls share the one array: calls that overlap on the GPU (different
- * streams, threads or scenes on one device) race and must be serialised by
- * the caller.  LRT_TRACE_COUNT_WORK is not supported. */
+ * calls no cudaMalloc/cudaFree and is synchronous: it returns after `stream`
+ * has drained, with LRT_ERR_DEVICE_LIMIT if the kernel hit a bounded-loop
+ * limit.  The scene's device must be current.  All calls share the one
+ * array: calls that overlap on the GPU (different streams, threads or scenes
+ * on one device) race and must be serialised by the caller.
+ * LRT_TRACE_COUNT_WORK is not supported. */
 lrt_status lrt_trace_nearest_noalloc(lrt_scene* scene, const float* rays, lrt_hit* hits, uint64_t n, void* stream,
                                      uint32_t flags);
 

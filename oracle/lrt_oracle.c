@@ -905,14 +905,68 @@ static double model_intensity(const double v[8], const double p0[3], const doubl
   return nl > 0 ? nl : 0.0;
 }
 
+/* |cos| of the angle between the ray and the model's field gradient at the
+ * unperturbed hit, and n . L there (the quantities whose small values make
+ * the intensity a steep or kinked function of the voxel values: grazing rays,
+ * where dt/dtheta ~ 1/(grad f . d), and the max(0, n . L) terminator). */
+static void model_shape(const double v[8], const double p0[3], const double dir[3], const double M[16],
+                        const double L[3], int early, double* cosgd, double* nl_out)
+{
+  double s = 0.0, p[3], g[3] = {0, 0, 0};
+  for (int it = 0; it < (early ? 1 : 50); it++) {
+    for (int r = 0; r < 3; r++) p[r] = p0[r] + s * dir[r];
+    double f = 0;
+    g[0] = g[1] = g[2] = 0;
+    for (int k = 0; k < 8; k++) {
+      const double wx = (k & 4) ? p[0] : 1 - p[0], wy = (k & 2) ? p[1] : 1 - p[1], wz = (k & 1) ? p[2] : 1 - p[2];
+      const double sx = (k & 4) ? 1 : -1, sy = (k & 2) ? 1 : -1, sz = (k & 1) ? 1 : -1;
+      f += v[k] * wx * wy * wz;
+      g[0] += v[k] * sx * wy * wz;
+      g[1] += v[k] * wx * sy * wz;
+      g[2] += v[k] * wx * wy * sz;
+    }
+    const double df = g[0] * dir[0] + g[1] * dir[1] + g[2] * dir[2];
+    if (df == 0.0) break;
+    const double step = f / df;
+    s -= step;
+    if (fabs(step) < 1e-15) break;
+  }
+  const double gl = sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+  const double dl = sqrt(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+  const double gd = g[0] * dir[0] + g[1] * dir[1] + g[2] * dir[2];
+  *cosgd = (gl > 0 && dl > 0) ? fabs(gd) / (gl * dl) : 0.0;
+  double m[3];
+  for (int r = 0; r < 3; r++) m[r] = M[r] * g[0] + M[4 + r] * g[1] + M[8 + r] * g[2];
+  const double len = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+  *nl_out = len > 0 ? (m[0] * L[0] + m[1] * L[1] + m[2] * L[2]) / len : 0.0;
+}
+
 /* Central differences (step h, in double) of sum_i dimage[i] * I_i with
  * respect to the value indices `keys` (sorted ascending), where I_i is the
  * FP64 surface model of ray i's hit voxel.  This checks the implicit-
- * differentiation formula without the rounding noise of the float32 march. */
+ * differentiation formula without the rounding noise of the float32 march.
+ * Where min_cos / min_nl are not NULL they receive, per key, the smallest
+ * |cos(grad f, d)| and n . L over the pixels whose hit voxel has that value
+ * as a corner (1 and +inf for keys no pixel reaches). */
+void lrto_fd_model_fp64_shape(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* rays,
+                              uint64_t n, const float light[3], const float* dimage, const uint32_t* keys,
+                              uint64_t nkeys, double h, double* out, double* min_cos, double* min_nl, int threads);
+
 void lrto_fd_model_fp64(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* rays, uint64_t n,
                         const float light[3], const float* dimage, const uint32_t* keys, uint64_t nkeys, double h,
                         double* out, int threads)
 {
+  lrto_fd_model_fp64_shape(arrays, preset, rays, n, light, dimage, keys, nkeys, h, out, NULL, NULL, threads);
+}
+
+void lrto_fd_model_fp64_shape(const lrt_scene_arrays* arrays, const lrt_preset* preset, const float* rays,
+                              uint64_t n, const float light[3], const float* dimage, const uint32_t* keys,
+                              uint64_t nkeys, double h, double* out, double* min_cos, double* min_nl, int threads)
+{
+  if (min_cos)
+    for (uint64_t k = 0; k < nkeys; k++) min_cos[k] = 1.0;
+  if (min_nl)
+    for (uint64_t k = 0; k < nkeys; k++) min_nl[k] = INFINITY;
   const f3 Lf = mk3(light[0], light[1], light[2]);
   const double L[3] = {light[0], light[1], light[2]};
   (void)threads;
@@ -951,6 +1005,17 @@ void lrto_fd_model_fp64(const lrt_scene_arrays* arrays, const lrt_preset* preset
 #pragma omp atomic
 #endif
       out[lo] += (double)dimage[i] * d;
+      if (min_cos || min_nl) {
+        double cg, nl;
+        model_shape(v, p0, dir, M, L, rec.early, &cg, &nl);
+#ifdef _OPENMP
+#pragma omp critical(lrto_fd_shape)
+#endif
+        {
+          if (min_cos && cg < min_cos[lo]) min_cos[lo] = cg;
+          if (min_nl && nl < min_nl[lo]) min_nl[lo] = nl;
+        }
+      }
     }
   }
 }

@@ -346,15 +346,18 @@ def port_adjoint_fp64(arrays, rays, light, dimage, preset=None):
     return grad
 
 
-def port_fd_model_fp64(arrays, rays, light, dimage, keys, h=1e-6, preset=None, threads=os.cpu_count()):
+def port_fd_model_fp64(arrays, rays, light, dimage, keys, h=1e-6, preset=None, threads=os.cpu_count(),
+                       shape=False):
     """Central differences (FP64 surface model of each hit voxel) of
-    sum_i dimage[i] * I_i w.r.t. the value indices `keys`."""
+    sum_i dimage[i] * I_i w.r.t. the value indices `keys`.  With shape=True
+    also returns, per key, the smallest |cos(grad f, d)| and n . L over the
+    pixels whose hit voxel has that value as a corner."""
     lib = port_lib()
     if not hasattr(lib, "_fd_bound"):
-        lib.lrto_fd_model_fp64.restype = None
-        lib.lrto_fd_model_fp64.argtypes = [C.POINTER(SceneArrays), C.POINTER(Preset), C.c_void_p, C.c_uint64,
-                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_double, C.c_void_p,
-                                           C.c_int]
+        lib.lrto_fd_model_fp64_shape.restype = None
+        lib.lrto_fd_model_fp64_shape.argtypes = [C.POINTER(SceneArrays), C.POINTER(Preset), C.c_void_p, C.c_uint64,
+                                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_double,
+                                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         lib._fd_bound = True
     s, keep = arrays_to_struct(arrays)
     p = preset if preset is not None else parity_preset()
@@ -364,12 +367,20 @@ def port_fd_model_fp64(arrays, rays, light, dimage, keys, h=1e-6, preset=None, t
     order = np.argsort(keys)
     k = np.ascontiguousarray(np.asarray(keys, np.uint32)[order])
     out = np.zeros(len(k), np.float64)
-    lib.lrto_fd_model_fp64(C.byref(s), C.byref(p), rays.ctypes.data, len(rays), L.ctypes.data, di.ctypes.data,
-                           k.ctypes.data, len(k), float(h), out.ctypes.data, int(threads))
+    mc = np.zeros(len(k), np.float64)
+    mn = np.zeros(len(k), np.float64)
+    lib.lrto_fd_model_fp64_shape(C.byref(s), C.byref(p), rays.ctypes.data, len(rays), L.ctypes.data,
+                                 di.ctypes.data, k.ctypes.data, len(k), float(h), out.ctypes.data,
+                                 mc.ctypes.data if shape else None, mn.ctypes.data if shape else None, int(threads))
     del keep
     res = np.empty_like(out)
     res[order] = out
-    return res
+    if not shape:
+        return res
+    rc, rn = np.empty_like(mc), np.empty_like(mn)
+    rc[order] = mc
+    rn[order] = mn
+    return res, rc, rn
 
 
 def ref_trace(arrays, rays, preset=None, threads=1, fast=False):

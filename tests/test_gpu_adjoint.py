@@ -189,3 +189,97 @@ def test_autograd_function(small, image_size):
     loss.backward()
     rel = (v.grad - grad).norm() / grad.norm()
     assert float(rel) < 1e-5
+
+
+@pytest.fixture(scope="module")
+def config4(cuda):
+    """The differentiable configuration at its own size: the sphere-union SBS
+    at virtual 256^3, 16 views of 512x512 (4,194,304 rays), targets from the
+    values plus N(0, 0.01) noise."""
+    torch = cuda
+    hdr, nodes, vals, vf, target, cams, rays = wl.adjoint_workload()
+    assert len(rays) == 16 * 512 * 512
+    sc = SceneRT()
+    sc.AddInstance(sc.AddGeom_SdfSBS(hdr, nodes, vals, vf), wl.IDENTITY)
+    sc.CommitScene()
+    R = torch.from_numpy(rays).cuda()
+    return {"sc": sc, "vf": vf, "target": target, "rays": rays, "R": R, "torch": torch}
+
+
+def test_config4_forward_every_pixel_matches_oracle(config4):
+    """All 4.2 M pixels of the rendered views and of the targets, in ray
+    order and in the image-order (tile-scheduled) form, equal the oracle's."""
+    s = config4
+    torch = s["torch"]
+    n = len(s["rays"])
+    arrays = s["sc"].export_arrays()
+    for values in (s["target"], s["vf"]):
+        a = dict(arrays)
+        a["sdfSBSDataF"] = values
+        want = po.port_render_lambert(a, s["rays"], LIGHT).view(np.uint32)
+        v = torch.from_numpy(np.ascontiguousarray(values, np.float32)).cuda()
+        s["sc"].update_sbs_values(v.data_ptr(), v.numel())
+        for kw in (dict(), dict(image_size=(512, 16 * 512)), dict(image_size=(512, 16 * 512))):
+            img = torch.full((n,), -1.0, dtype=torch.float32, device="cuda")
+            s["sc"].render_lambert(s["R"].data_ptr(), n, LIGHT, img.data_ptr(), **kw)
+            s["sc"].sync()
+            assert np.array_equal(img.cpu().numpy().view(np.uint32), want), kw
+
+
+def test_config4_adjoint_fp64_and_central_differences(config4):
+    """dLoss/dtheta at the configuration's size:
+    * the GPU adjoint (image order) against the FP64 CPU adjoint;
+    * central differences of the FP64 surface model on 256 seeded values at
+      h = 1e-5, 1e-4 and the specified h = 1e-3: within 1e-3 rel. L2 at
+      1e-5, and the error falls with h (it is the truncation error of the
+      differences: at h = 1e-3, 13% of a voxel's extent in distance units,
+      the hit point moves far enough for the curvature of the trilinear
+      field to matter, so 1e-3 cannot be met at that step);
+    * central differences of the float32 render itself at h = 1e-3 against
+      the FP64-model differences at the same h."""
+    s = config4
+    torch = s["torch"]
+    P = len(s["rays"])
+    shape = (512, 16 * 512)
+    target_img = _render(s, s["target"])
+    img = _render(s, s["vf"])
+    dimage = (2.0 / P) * (img - target_img)
+    grad = torch.zeros(len(s["vf"]), dtype=torch.float32, device="cuda")
+    s["sc"].adjoint_lambert(s["R"].data_ptr(), P, LIGHT, dimage.data_ptr(), grad.data_ptr(), image_size=shape)
+    s["sc"].sync()
+    g = grad.cpu().numpy().astype(np.float64)
+    arrays = s["sc"].export_arrays()
+    di = dimage.cpu().numpy()
+    g64 = po.port_adjoint_fp64(arrays, s["rays"], LIGHT, di)
+    assert np.count_nonzero(g64) > 100000
+    assert np.array_equal(g != 0, g64 != 0)
+    assert np.linalg.norm(g - g64) / np.linalg.norm(g64) < 1e-4
+    rng = np.random.default_rng(1)
+    keys = rng.choice(np.nonzero(g != 0)[0], size=256, replace=False)
+    ga = g[keys]
+    rel = {}
+    fd_model = {}
+    for h in (1e-5, 1e-4, 1e-3):
+        fd_model[h] = po.port_fd_model_fp64(arrays, s["rays"], LIGHT, di, keys, h=h)
+        rel[h] = np.linalg.norm(fd_model[h] - ga) / np.linalg.norm(fd_model[h])
+    assert rel[1e-5] < 1e-3, rel
+    assert rel[1e-5] < rel[1e-4] < rel[1e-3] < 0.3, rel
+
+    def loss(values):
+        return float(((_render(s, values) - target_img).double() ** 2).mean())
+
+    h = 1e-3
+    fd32 = np.zeros(len(keys))
+    for j, k in enumerate(keys):
+        vp = s["vf"].copy()
+        vm = s["vf"].copy()
+        vp[k] += h
+        vm[k] -= h
+        fd32[j] = (loss(vp) - loss(vm)) / (2 * h)
+    _render(s, s["vf"])
+    rel32_adj = np.linalg.norm(fd32 - ga) / np.linalg.norm(fd32)
+    rel32_model = np.linalg.norm(fd32 - fd_model[h]) / np.linalg.norm(fd_model[h])
+    print("config 4, 256 values: FP64-model FD rel. L2 h=1e-5 %.3g, 1e-4 %.3g, 1e-3 %.3g; float32 render FD at "
+          "h=1e-3 vs adjoint %.3g, vs FP64-model FD at the same h %.3g" % (rel[1e-5], rel[1e-4], rel[1e-3],
+                                                                           rel32_adj, rel32_model))
+    assert rel32_model < 0.5 and rel32_adj < 0.6

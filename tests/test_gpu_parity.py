@@ -10,12 +10,15 @@ central differences with h = 0.001 voxel (BVH2Common.cpp:659-673), which
 magnify a one-ulp change of the contracted trilinear sums about 500-fold, and
 on 8-bit quantised SVS voxels that reaches a few 1e-2.
 """
+import os
+
 import numpy as np
 import pytest
 
 import pyoracle as po
 from graphic_lab_task_b200 import SceneRT, workloads as wl
-from helpers import MISS, bit_equal, golden_names, hit_summary, load_golden, tolerance_report
+from helpers import (MISS, RefBuilder, assert_within_spec, bit_equal, golden_names, hit_summary, load_golden,
+                     tolerance_report)
 
 pytestmark = pytest.mark.gpu
 
@@ -53,13 +56,12 @@ def test_single_ray_api_matches_batch(cuda):
         assert sc.RayQuery_AnyHit(rays[i, :4], rays[i, 4:]) == (want[i]["geomId"] != MISS)
 
 
-def _oracle_check(sc, rays, sample=None):
+def _oracle_check(sc, rays):
+    """Every ray's hit equals the oracle's on the product's uploaded arrays."""
     arrays = sc.export_arrays()
     got = sc.RayQuery_NearestHitBatch(rays)
-    idx = np.arange(len(rays)) if sample is None else np.unique(
-        np.linspace(0, len(rays) - 1, sample).astype(np.int64))
-    want = po.port_trace(arrays, rays[idx])
-    assert bit_equal(got[idx], want).all(), hit_summary(got[idx], want)
+    want = po.port_trace(arrays, rays)
+    assert bit_equal(got, want).all(), hit_summary(got, want)
     return got
 
 
@@ -72,6 +74,13 @@ def test_mesh_200k_triangles_256x256(cuda):
     got = _oracle_check(sc, rays)
     assert (got["primId"] != MISS).sum() > 15000
     assert np.all((got["geomId"][got["primId"] != MISS] >> 24) == 0)
+    if po.ref_available():
+        # the reference's own stock build of the same mesh (its tree differs;
+        # nearest triangle hits agree apart from exact ties on shared edges)
+        rb = RefBuilder()
+        rb.AddInstance(rb.AddGeom_Triangles3f(v, t), wl.IDENTITY)
+        want = rb.CommitScene().trace(rays, threads=os.cpu_count())
+        assert_within_spec(got, want, what="200k-triangle mesh 256x256")
 
 
 def test_sbs_reduced_grid(cuda):
@@ -86,16 +95,27 @@ def test_sbs_reduced_grid(cuda):
     assert hit.sum() > 5000 and np.all((got["geomId"][hit] >> 24) == 11)  # TYPE_SDF_SBS_COL
 
 
-def test_sbs_full_size_sample_and_properties(cuda):
-    """The benchmark workload itself: 512^3 virtual grid, 1920x1080 rays;
-    exact parity on a 16k-ray strided sample, properties on every ray."""
+def test_sbs_full_size_every_ray(cuda):
+    """The benchmark workload itself: 512^3 virtual grid, all 2,073,600 rays of
+    the 1920x1080 camera.  Every hit equals the oracle's on the product's
+    arrays, and the reference's own stock build (its AddGeom_SdfSBS,
+    CommitScene and RayQuery_NearestHit compiled from its sources, run on all
+    host cores) within the specification's tolerance (bit-identical apart
+    from near ties); properties on every ray."""
     sph = wl.spheres(64, seed=1)
     hdr, nodes, vals, vf = wl.sbs_from_spheres(sph, grid_res=512)
     sc = SceneRT()
     sc.AddInstance(sc.AddGeom_SdfSBS(hdr, nodes, vals, vf), wl.IDENTITY)
     sc.CommitScene()
     rays = wl.eye_rays_host(wl.camera((0, 0, 3), width=1920, height=1080))
-    got = _oracle_check(sc, rays, sample=16384)
+    assert len(rays) == 2073600
+    got = _oracle_check(sc, rays)
+    if po.ref_available():
+        rb = RefBuilder()
+        rb.AddInstance(rb.AddGeom_SdfSBS(hdr, nodes, vals, vf), wl.IDENTITY)
+        want = rb.CommitScene().trace(rays, threads=os.cpu_count())
+        rep = assert_within_spec(got, want, what="SBS 1920x1080")
+        assert rep["bit_identical"] == len(rays), rep
     hit = got["primId"] != MISS
     assert hit.mean() > 0.1
     t = got["t"][hit]
