@@ -84,6 +84,21 @@ def ref_lib(fast=False):
         lib.lrtr_export.argtypes = [C.c_void_p, C.POINTER(SceneArrays)]
         lib.lrtr_import.argtypes = [C.c_void_p, C.POINTER(SceneArrays)]
         lib.lrtr_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_int]
+        vp, u32, u64 = C.c_void_p, C.c_uint32, C.c_uint64
+        lib.lrtr_renderer_create.restype = vp
+        for fn, args in (("lrtr_renderer_create", [vp]), ("lrtr_renderer_destroy", [vp]),
+                         ("lrtr_renderer_add_mesh", [vp, u32, vp, u64, vp, u64]),
+                         ("lrtr_renderer_set_preset", [vp, C.POINTER(Preset)]),
+                         ("lrtr_renderer_set_camera_inverse", [vp, vp, vp]),
+                         ("lrtr_renderer_look_at", [vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float]),
+                         ("lrtr_renderer_set_lights", [vp, vp, u32]), ("lrtr_renderer_set_background", [vp, vp]),
+                         ("lrtr_renderer_set_materials", [vp, vp, u32, vp, u64, vp, u32]),
+                         ("lrtr_renderer_set_frame", [vp, u32]), ("lrtr_renderer_eye_rays", [vp, u32, u32, u32, vp]),
+                         ("lrtr_renderer_render", [vp, u32, u32, vp]),
+                         ("lrtr_renderer_fill_transparency", [vp, u32, u32, u32, vp, vp])):
+            getattr(lib, fn).argtypes = args
+            if fn != "lrtr_renderer_create":
+                getattr(lib, fn).restype = None
         _refs[key] = lib
     return _refs[key]
 
@@ -186,6 +201,86 @@ class RefScene:
         hits = np.zeros(len(rays), dtype=HIT_DTYPE)
         self.lib.lrtr_trace(self.h, rays.ctypes.data, hits.ctypes.data, len(rays), int(threads))
         return hits
+
+
+class RefRenderer:
+    """The reference's own MultiRenderer (MultiRenderer/MultiRenderer*.cpp,
+    compiled in oracle/_ref) tracing a RefScene: initEyeRay, Render (fill
+    G-buffer, resolve, tonemap) and the transparency AnyHit loop.  Image
+    sizes must be multiples of 8 (the renderer's tile padding)."""
+
+    def __init__(self, scene):
+        self.scene = scene  # keeps the BVHRT alive
+        self.lib = scene.lib
+        self.h = self.lib.lrtr_renderer_create(scene.h)
+
+    def close(self):
+        if self.h:
+            self.lib.lrtr_renderer_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_mesh(self, geom_id, verts, tris):
+        """MultiRenderer::add_mesh_internal: the mesh copy the resolve reads
+        triangle normals from (positions only; no normals or texture coords)."""
+        v = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(tris, np.uint32).reshape(-1)
+        self.lib.lrtr_renderer_add_mesh(self.h, geom_id, v.ctypes.data, len(v), t.ctypes.data, len(t))
+
+    def set_preset(self, preset):
+        self.lib.lrtr_renderer_set_preset(self.h, C.byref(preset))
+
+    def set_camera(self, cam):
+        """The camera's inverse matrices (lrt_camera.proj_inv, world_view_inv)."""
+        p = np.array(cam.proj_inv[:], np.float32)
+        w = np.array(cam.world_view_inv[:], np.float32)
+        self.lib.lrtr_renderer_set_camera_inverse(self.h, p.ctypes.data, w.ctypes.data)
+
+    def look_at(self, eye, center, up, fovy, aspect, znear=0.01, zfar=100.0):
+        """LiteMath lookAt / perspectiveMatrix + MultiRenderer::UpdateCamera."""
+        e, c, u = (np.ascontiguousarray(x, np.float32) for x in (eye, center, up))
+        self.lib.lrtr_renderer_look_at(self.h, e.ctypes.data, c.ctypes.data, u.ctypes.data, fovy, aspect, znear, zfar)
+
+    def set_lights(self, lights):
+        from graphic_lab_task_b200._abi import LIGHT_DTYPE
+        lt = np.ascontiguousarray(lights, dtype=LIGHT_DTYPE)
+        self.lib.lrtr_renderer_set_lights(self.h, lt.ctypes.data if len(lt) else None, len(lt))
+
+    def set_background(self, rgba):
+        bg = np.ascontiguousarray(rgba, np.float32)
+        self.lib.lrtr_renderer_set_background(self.h, bg.ctypes.data)
+
+    def set_materials(self, materials, mat_ids, mat_offsets):
+        from graphic_lab_task_b200._abi import MATERIAL_DTYPE
+        m = np.ascontiguousarray(materials, dtype=MATERIAL_DTYPE)
+        ids = np.ascontiguousarray(mat_ids, np.uint32)
+        offs = np.ascontiguousarray(mat_offsets, np.uint32).reshape(-1)
+        self.lib.lrtr_renderer_set_materials(self.h, m.ctypes.data, len(m), ids.ctypes.data, len(ids),
+                                             offs.ctypes.data, len(offs) // 2)
+
+    def set_frame(self, frame):
+        self.lib.lrtr_renderer_set_frame(self.h, frame)
+
+    def eye_rays(self, width, height, sample=0):
+        out = np.zeros((width * height, 8), np.float32)
+        self.lib.lrtr_renderer_eye_rays(self.h, width, height, sample, out.ctypes.data)
+        return out
+
+    def render(self, width, height):
+        img = np.zeros(width * height, np.uint32)
+        self.lib.lrtr_renderer_render(self.h, width, height, img.ctypes.data)
+        return img
+
+    def fill_transparency(self, width, height, sample=0):
+        transp = np.zeros((width * height, 4), np.float32)
+        gb = np.zeros(width * height, HIT_DTYPE)
+        self.lib.lrtr_renderer_fill_transparency(self.h, width, height, sample, transp.ctypes.data, gb.ctypes.data)
+        return transp, gb
 
 
 def port_render_lambert(arrays, rays, light, preset=None, threads=os.cpu_count()):

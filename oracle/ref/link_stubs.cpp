@@ -1,11 +1,14 @@
 // link_stubs.cpp — definitions that let the reference's BVHRT host code
-// (MultiRenderer/BVH2Common_host.cpp) link without its scene-file I/O,
-// compression and scene-graph libraries.
+// (MultiRenderer/BVH2Common_host.cpp) and MultiRenderer
+// (MultiRenderer/MultiRenderer*.cpp) link without their scene-file I/O,
+// mesh-file, compression and scene-graph libraries.
 //
 // TEST INFRASTRUCTURE ONLY (part of the oracle/_ref checker build).  The ray
-// query path never reaches any of these: they back AddCustomGeom_FromFile,
-// the compressed-octree adders and LiteScene XML nodes.  Each one aborts with
-// a message if it is ever called, so a silent wrong result is impossible.
+// query and render paths never reach any of these: they back
+// AddCustomGeom_FromFile, the compressed-octree adders, LiteScene XML nodes,
+// MultiRenderer::LoadScene and the data-channel (CAE) modes.  Each one aborts
+// with a message if it is ever called, so a silent wrong result is
+// impossible.
 #include <cstdio>
 #include <cstdlib>
 #include <string>
@@ -18,6 +21,11 @@
 #include "sdf/scom2/clustering/symmetric_groups.h"
 #include "sdf/scom2/scom.h"
 #include "sdf/simple/sdf_simple.h"
+#include "utils/common/data_channel.h"
+#include "utils/common/strings.h"
+#include "utils/mesh/augmented_mesh.h"
+#include "utils/mesh/mesh.h"
+#include "utils/mesh/mesh_internal.h"
 
 [[noreturn]] static void off_path(const char* what)
 {
@@ -34,7 +42,24 @@ bool CustomGeometry::load_data(const SceneMetadata&) { off_path("CustomGeometry:
 bool CustomGeometry::save_data(const SceneMetadata&) { off_path("CustomGeometry::save_data"); }
 std::wstring s2ws(const std::string&) { off_path("LiteScene::s2ws"); }
 std::string ws2s(const std::wstring&) { off_path("LiteScene::ws2s"); }
+bool MeshGeometry::load_node(pugi::xml_node) { off_path("MeshGeometry::load_node"); }
+bool MeshGeometry::save_node(pugi::xml_node&) const { off_path("MeshGeometry::save_node"); }
+bool MeshGeometry::load_data(const SceneMetadata&) { off_path("MeshGeometry::load_data"); }
+bool MeshGeometry::save_data(const SceneMetadata&) { off_path("MeshGeometry::save_data"); }
+bool HydraScene::load(const std::string&) { off_path("HydraScene::load"); }
+void HydraScene::initialize_empty_scene() { off_path("HydraScene::initialize_empty_scene"); }
+void HydraScene::clear() { off_path("HydraScene::clear"); }
 } // namespace LiteScene
+
+DataChannelInfo get_info(const DataChannel&) { off_path("get_info(DataChannel)"); }
+std::vector<std::string> split(const std::string&, char) { off_path("split"); }
+
+namespace cmesh4 {
+void save_augmented_mesh(const AugmentedMesh&, const char*) { off_path("cmesh4::save_augmented_mesh"); }
+void recalculate_vertex_normals(SimpleMesh&) { off_path("cmesh4::recalculate_vertex_normals"); }
+void load_augmented_mesh(AugmentedMesh&, const char*) { off_path("cmesh4::load_augmented_mesh"); }
+void fix_missing(SimpleMesh&, int) { off_path("cmesh4::fix_missing"); }
+} // namespace cmesh4
 
 void save_coctree_v3(const COctreeV3View&, const std::string&) { off_path("save_coctree_v3"); }
 void load_coctree_v3(COctreeV3&, const std::string&) { off_path("load_coctree_v3"); }

@@ -15,6 +15,7 @@
 #include "sdf/simple/sdf_simple.h"
 
 #include "../../include/lrt_b200.h"
+#include "ref_holder.h"
 
 static_assert(sizeof(CRT_Hit) == sizeof(lrt_hit), "CRT_Hit layout");
 static_assert(sizeof(BVHNode) == sizeof(lrt_bvh_node), "BVHNode layout");
@@ -30,10 +31,7 @@ static_assert(sizeof(MultiRenderPreset) == sizeof(lrt_preset), "MultiRenderPrese
 std::shared_ptr<ISceneObject> CreateSceneRT(const char* a_implName, const char* a_buildName, const char* a_layoutName);
 
 namespace {
-struct Holder {
-  std::shared_ptr<ISceneObject> obj;
-  BVHRT* rt;
-};
+using Holder = LrtrHolder;
 
 template <class T, class S>
 void assign(std::vector<T>& dst, const S* src, uint64_t n)

@@ -71,27 +71,46 @@ def tolerance_report(got, want, rays=None):
             "n_fail": int((dn > 1e-4).sum()), "mismatch_idx": np.nonzero(~ids)[0]}
 
 
-def assert_within_spec(got, want, max_tie_frac=1e-4, what=""):
+def assert_within_spec(got, want, max_tie_frac=1e-4, what="", tree_ref=None, max_tree_frac=1e-6):
     """The hot path's acceptance rule against the reference's own build:
     ids (primId, instId, geomId) bit-exact except on rays whose two nearest
     hits lie within 1e-5 relative t (here: the two answers name different
     primitives at t values within 1e-5 of each other, so the ray has two hits
-    that close), t within 1e-5 relative on every hit ray, decoded normals
+    that close), t within 1e-5 relative where the ids agree, decoded normals
     within 1e-4 where the ids agree.  Hit/miss disagreements are failures.
-    At most `max_tie_frac` of the rays may be near ties.  Returns the report."""
+    At most `max_tie_frac` of the rays may be near ties.
+
+    Different trees (the product's builder against the reference's) can also
+    change an SDF answer by more than 1e-5: the first SDF leaf hit ends a
+    BLAS traversal (BVH2Common.cpp:3234-3237, 3310), so which leaf of an
+    octree answers depends on the traversal order.  With `tree_ref` (a
+    function of ray indices returning the reference code's hits on the
+    product's own arrays) such rays pass if the reference, given the
+    product's tree, returns the product's hit bit for bit; at most
+    `max_tree_frac` of the rays (at least one) may be of this kind."""
     hg, hw = got["primId"] != MISS, want["primId"] != MISS
     assert np.array_equal(hg, hw), "%s: %d rays hit in one and miss in the other" % (what, int((hg != hw).sum()))
     ids = (got["primId"] == want["primId"]) & (got["instId"] == want["instId"]) & (got["geomId"] == want["geomId"])
-    both = hg & hw
-    rel_t = np.abs(got["t"][both].astype(np.float64) - want["t"][both]) / np.maximum(np.abs(want["t"][both]), 1e-30)
-    assert (rel_t <= 1e-5).all(), "%s: %d hits outside 1e-5 relative t (max %.3g)" % (
-        what, int((rel_t > 1e-5).sum()), rel_t.max())
+    rel = np.zeros(len(got))
+    rel[hg] = np.abs(got["t"][hg].astype(np.float64) - want["t"][hg]) / np.maximum(np.abs(want["t"][hg]), 1e-30)
+    same = hg & ids
+    assert (rel[same] <= 1e-5).all(), "%s: %d hits with equal ids outside 1e-5 relative t (max %.3g)" % (
+        what, int((rel[same] > 1e-5).sum()), rel[same].max())
+    ties = hg & ~ids & (rel <= 1e-5)
+    tree = np.nonzero(hg & ~ids & (rel > 1e-5))[0]
+    assert ties.sum() <= max(1, max_tie_frac * len(got)), "%s: %d id mismatches (near ties) of %d rays" % (
+        what, int(ties.sum()), len(got))
+    if len(tree):
+        assert tree_ref is not None, "%s: %d rays with other hits more than 1e-5 apart in t (max %.3g)" % (
+            what, len(tree), rel[tree].max())
+        assert len(tree) <= max(1, max_tree_frac * len(got)), "%s: %d tree-order differences" % (what, len(tree))
+        again = tree_ref(tree)
+        assert bit_equal(again, got[tree]).all(), "%s: the reference on the product's arrays disagrees on %s" % (
+            what, tree[~bit_equal(again, got[tree])][:5])
     rep = tolerance_report(got, want)
-    ties = int((~ids).sum())
-    assert ties <= max(1, max_tie_frac * len(got)), "%s: %d id mismatches (near ties) of %d rays" % (
-        what, ties, len(got))
     assert rep["n_fail"] == 0, "%s: %d normals outside 1e-4 (max %.3g)" % (what, rep["n_fail"], rep["max_normal_err"])
-    rep["ties"] = ties
+    rep["ties"] = int(ties.sum())
+    rep["tree_order"] = int(len(tree))
     rep["bit_identical"] = int(bit_equal(got, want).sum())
     return rep
 

@@ -64,10 +64,14 @@ def test_instanced_primary_and_bounce(cuda, scale):
         wl.build_instanced(rb, **kw)
         ref = rb.CommitScene()
         assert ref.export()["instanceData"]["transformInv"].tobytes() == arrays["instanceData"]["transformInv"].tobytes()
-        rep_p = assert_within_spec(prim, ref.trace(rays, threads=os.cpu_count()), what="primary %dx%d" % (w, h))
-        rep_b = assert_within_spec(bh, ref.trace(bv, threads=os.cpu_count()), what="bounce")
-        print("reference build: primary %d/%d bit-identical (%d near ties), bounce %d/%d (%d near ties)" % (
-            rep_p["bit_identical"], len(rays), rep_p["ties"], rep_b["bit_identical"], len(bv), rep_b["ties"]))
+        rep_p = assert_within_spec(prim, ref.trace(rays, threads=os.cpu_count()), what="primary %dx%d" % (w, h),
+                                   tree_ref=lambda idx: po.ref_trace(arrays, rays[idx]))
+        rep_b = assert_within_spec(bh, ref.trace(bv, threads=os.cpu_count()), what="bounce",
+                                   tree_ref=lambda idx: po.ref_trace(arrays, bv[idx]))
+        print("reference build: primary %d/%d bit-identical (%d near ties, %d tree-order), bounce %d/%d "
+              "(%d near ties, %d tree-order)" % (rep_p["bit_identical"], len(rays), rep_p["ties"],
+                                                 rep_p["tree_order"], rep_b["bit_identical"], len(bv), rep_b["ties"],
+                                                 rep_b["tree_order"]))
     # the NaN rays of the misses miss
     nan_rays = bounce[~valid][:256]
     if len(nan_rays):
