@@ -61,8 +61,9 @@ def workload_scene_camera_only():
     return None, wl.camera((0, 0, 3), width=WIDTH, height=HEIGHT, tnear=TMIN, tfar=TMAX)
 
 
-def config_dict(extra=None):
-    d = {"workload": WORKLOAD, "rays_per_step": WIDTH * HEIGHT, "image": [WIDTH, HEIGHT], "virtual_grid": GRID,
+def config_dict(world, extra=None):
+    """The workload both arms report (identical dicts for the same run)."""
+    d = {"workload": WORKLOAD, "parallelism": "replicas" if world > 1 else "single", "rays_per_step": WIDTH * HEIGHT, "image": [WIDTH, HEIGHT], "virtual_grid": GRID,
          "brick_size": BRICK, "brick_pad": PAD, "spheres": N_SPHERES, "sbs_layout": "ID32F_IRGB32F (fp32)",
          "preset": "LAMBERT_NO_TEX, ST, GEOMETRY normals, TRILINEAR, VOLUME", "l2": "flushed before every step (256 MiB)",
          "call": "lrt_trace_nearest_image (the camera's rays in row-major order, 8x4-pixel tiles per warp)"}
@@ -160,46 +161,26 @@ def cpu_reference_rate(ref_scene, rays, seconds=12.0, threads=None):
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the reference's own host build (AddGeom_SdfSBS,
-    CommitScene) and CPU ray query on all host cores, rank 0 only."""
+    """--impl reference: the reference's own host build, camera, eye rays and
+    CPU ray query on all host cores (oracle/refbench.py), rank 0 only.  This
+    arm loads no product library and imports nothing from the package."""
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(HERE, "oracle"))
-    import pyoracle as po
-    from graphic_lab_task_b200 import workloads as wl
-    if not po.ref_available(fast=True):
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/liblrt_ref_fast.so not built (make -C oracle ref)"}))
+    import refbench
+    why = refbench.available()
+    if why:
+        print(json.dumps({"impl": "reference", "unavailable": why}))
         return
-    (hdr, nodes, vals, vf), cam = workload_scene()
-    rays = wl.eye_rays_host(cam)
-    ref = po.RefScene(fast=True)
-    g = ref.add_sbs(hdr, nodes, vals, vf)
-    ref.add_instance(g, wl.IDENTITY)
-    ref.commit()
-    threads = os.cpu_count()
-    n = len(rays)
-    probe = rays[:: max(1, n // 32768)]
-    t0 = time.perf_counter()
-    ref.trace(probe, threads=threads)
-    rate = len(probe) / max(time.perf_counter() - t0, 1e-6)
-    # each step is a strided sample sized so that all steps take ~60 s
-    per_step = max(len(probe), min(n, int(rate * 60.0 / max(1, args.steps + args.warmup))))
-    sample = rays[np.linspace(0, n - 1, per_step).astype(np.int64)]
-    for _ in range(args.warmup):
-        ref.trace(sample[: max(1, per_step // 8)], threads=threads)
-    times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        ref.trace(sample, threads=threads)
-        times.append(time.perf_counter() - t0)
-    ms = 1e3 * sum(times) / len(times)
-    value = per_step / (ms * 1e-3) / 1e6
-    desc = "%d of %d rays (strided) per step, OpenMP over rays" % (per_step, n)
+    m = refbench.run(WIDTH, HEIGHT, GRID, BRICK, PAD, N_SPHERES, SPHERE_SEED, TMIN, TMAX, args.steps, args.warmup)
+    value = m["value"]
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "config": config_dict(),
-        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": "reference", "sample": desc},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": config_dict(world),
+        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": m["threads"], "kind": "reference",
+                         "sample": m["sample"]},
         "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -207,18 +188,22 @@ def run_reference(args, rank, world):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def read_traffic():
-    """dram bytes per trace launch from the committed ncu summary, if any."""
+def read_profile():
+    """Per-launch figures of the trace kernel from the committed ncu summary
+    (profiles/k_trace_sbs_1920x1080.txt): DRAM bytes, issue-active fraction
+    and threads per executed warp instruction; None where absent."""
     p = os.path.join(HERE, "profiles", "k_trace_sbs_1920x1080.txt")
+    out = {"traffic_bytes_per_launch": None, "issue_active_frac": None, "threads_per_warp_inst": None}
     if not os.path.exists(p):
-        return None
+        return out
     for ln in open(p):
-        if ln.startswith("traffic_bytes_per_launch:"):
+        key = ln.split(":", 1)[0].strip()
+        if key in out:
             try:
-                return float(ln.split(":", 1)[1].split()[0])
-            except ValueError:
-                return None
-    return None
+                out[key] = float(ln.split(":", 1)[1].split()[0])
+            except (ValueError, IndexError):
+                pass
+    return out
 
 
 def run_ours(args, rank, world, local_rank):
@@ -294,6 +279,26 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize(dev)
     sc.sync(stream=sp)
     nat_ms = [starts[i].elapsed_time(ends[i]) for i in range(min(args.steps, 50))]
+    # the timed call with the camera moving a little before every launch (the
+    # tile schedule then comes from a slightly different frame): eye rays of
+    # the new camera generated before the L2 flush, outside the timed region
+    moving = torch.empty(n * 8, dtype=torch.float32, device=dev)
+    mov_ms = []
+    for i in range(min(args.steps, 50) + 3):
+        a = 0.25 * i
+        mcam = wl.camera((0.02 * np.sin(a), 0.02 * np.cos(a) - 0.02, 3.0), width=WIDTH, height=HEIGHT, tnear=TMIN,
+                         tfar=TMAX)
+        sc.generate_eye_rays(mcam, moving.data_ptr(), sp)
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sc.trace_image(moving.data_ptr(), hits.data_ptr(), WIDTH, HEIGHT, stream=sp)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        if i >= 3:
+            mov_ms.append(e0.elapsed_time(e1))
+    sc.sync(stream=sp)
+    del moving
     # end to end through the public API with pinned host buffers
     host_rays = torch.empty(n * 8, dtype=torch.float32, pin_memory=True)
     host_rays.copy_(rays.cpu())
@@ -329,23 +334,31 @@ def run_ours(args, rank, world, local_rank):
     peak_src = "measured" if peak else "fallback"
     peak = peak or 6650.0
     achieved = bytes_per_launch / (ms * 1e-3) / 1e9
-    traffic = read_traffic()
+    prof = read_profile()
+    traffic = prof["traffic_bytes_per_launch"]
     out = {
         "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded 64-sphere SDF union, no dataset)",
-        "config": config_dict({"parallelism": "replicas" if world > 1 else "single"}),
+        "config": config_dict(world),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": bytes_per_launch,
                      "bytes_per_ray": bytes_per_launch / n,
-                     "kernel": "k_trace (exact build) via lrt_trace_nearest_image"},
+                     "kernel": "k_trace (exact build) via lrt_trace_nearest_image",
+                     # the bound that applies: instruction issue (from the ncu summary of this launch)
+                     "issue_frac": prof["issue_active_frac"], "threads_per_inst": prof["threads_per_warp_inst"],
+                     "profile": "profiles/k_trace_sbs_1920x1080.txt"},
         "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * 32,
                 "ms_per_step": total_e2e_ms / args.steps,
                 "gpu_launches": args.steps * len(pipeline_chunks(n)),
                 "call": "lrt_trace_nearest, pinned host buffers (chunked copy/trace/copy pipeline)"},
         "row_order": {"ms_per_step": sum(row_ms) / len(row_ms), "value": n / (sum(row_ms) / len(row_ms)) / 1e3,
                       "unit": "Mrays/s", "call": "lrt_trace_nearest (same rays, 32 consecutive rays per warp)"},
+        "moving_camera": {"ms_per_step": sum(mov_ms) / len(mov_ms), "value": n / (sum(mov_ms) / len(mov_ms)) / 1e3,
+                          "unit": "Mrays/s",
+                          "call": "lrt_trace_nearest_image, camera moved by up to 0.04 before every launch (the "
+                                  "tile schedule comes from the previous, different frame)"},
         "natural_tile_order": {"ms_per_step": sum(nat_ms) / len(nat_ms),
                                "value": n / (sum(nat_ms) / len(nat_ms)) / 1e3, "unit": "Mrays/s",
                                "call": "lrt_trace_nearest_image with LRT_TRACE_NATURAL_ORDER (tiles in row order, "
@@ -629,6 +642,15 @@ def adjoint_section(dev, args):
                                    "median_rel": float(np.median(per)), "max_rel": float(per.max()),
                                    "frac_within_1e-3": float((per <= 1e-3).mean()),
                                    "seconds": time.perf_counter() - t0}
+        # the same differences at the specified h = 1e-3 and between: the
+        # error is the differences' truncation error, falling with h
+        by_h = {}
+        for hh in (1e-5, 1e-4, 1e-3):
+            fdh = po.port_fd_model_fp64(sc.export_arrays(), rays, L, dimage.cpu().numpy(), pick, h=hh)
+            perh = np.abs(fdh - ga) / np.maximum(np.maximum(np.abs(fdh), np.abs(ga)), 1e-30)
+            by_h["%g" % hh] = {"rel_l2": float(np.linalg.norm(fdh - ga) / np.linalg.norm(fdh)),
+                               "median_rel": float(np.median(perh)), "frac_within_1e-3": float((perh <= 1e-3).mean())}
+        out["fd"]["fp64_model_by_h"] = by_h
     except Exception as e:  # the checker is optional on a box without the oracle build
         out["fp64_cpu"] = {"unavailable": str(e)}
     sc.close()

@@ -22,14 +22,23 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "_build", "liblrt_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "liblrt_ref.so")
 REF_FAST_SO = os.path.join(HERE, "_ref", "liblrt_ref_fast.so")
-REFERENCE_SRC = "/root/reference"
+WL_SO = os.path.join(HERE, "_build", "liblrt_workloads.so")
+
+
+def reference_src():
+    """The reference checkout the checker build compiles from: the
+    LRT_REFERENCE environment variable, else oracle/Makefile's default."""
+    r = subprocess.run(["make", "-s", "-C", HERE, "ref-path"], capture_output=True, text=True)
+    return r.stdout.strip() if r.returncode == 0 else ""
 
 
 def build(with_reference=True):
-    """Compile the C restatement and, where the reference sources exist, the
-    reference build (oracle/Makefile)."""
-    targets = ["port"]
-    if with_reference and os.path.isdir(REFERENCE_SRC):
+    """Compile the C restatement, the seeded-workload library of the bench's
+    reference arm and, where the reference sources exist, the reference
+    build (oracle/Makefile)."""
+    targets = ["port", "wl"]
+    src = reference_src() if with_reference else ""
+    if src and os.path.isdir(src):
         targets.append("ref")
     subprocess.run(["make", "-s", "-C", HERE, "-j8"] + targets, check=True)
 

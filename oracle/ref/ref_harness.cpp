@@ -62,6 +62,16 @@ void lrtr_set_preset(void* p, const lrt_preset* preset)
   static_cast<Holder*>(p)->rt->SetPreset(mp);
 }
 
+// getDefaultPreset() (core/render_settings.h:138-160) with sphere tracing and
+// geometric normals: the preset the ray-query hot path is specified for.
+void lrtr_set_parity_preset(void* p)
+{
+  MultiRenderPreset mp = getDefaultPreset();
+  mp.sdf_node_intersect = SDF_OCTREE_NODE_INTERSECT_ST;
+  mp.normal_mode = NORMAL_MODE_GEOMETRY;
+  static_cast<Holder*>(p)->rt->SetPreset(mp);
+}
+
 uint32_t lrtr_add_triangles(void* p, const float* vpos3f, uint64_t nvert, const uint32_t* idx, uint64_t nidx)
 {
   return static_cast<Holder*>(p)->rt->AddGeom_Triangles3f(vpos3f, nvert, idx, nidx, BUILD_HIGH, 12);

@@ -36,7 +36,7 @@ from graphic_lab_task_b200 import workloads as wl  # noqa: E402
 from graphic_lab_task_b200._abi import (FRAME_OCTREE_NODE_DTYPE, SBS_HEADER_DTYPE, SBS_NODE_DTYPE,  # noqa: E402
                                         SVS_NODE_DTYPE, parity_preset)
 
-REF = "/root/reference"
+REF = po.reference_src()
 
 
 def preset_array(p):
