@@ -22,6 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "_build", "liblrt_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "liblrt_ref.so")
 REF_FAST_SO = os.path.join(HERE, "_ref", "liblrt_ref_fast.so")
+DROPIN_SO = os.path.join(HERE, "_ref", "liblrt_b200_dropin.so")
 WL_SO = os.path.join(HERE, "_build", "liblrt_workloads.so")
 
 
@@ -39,7 +40,7 @@ def build(with_reference=True):
     targets = ["port", "wl"]
     src = reference_src() if with_reference else ""
     if src and os.path.isdir(src):
-        targets.append("ref")
+        targets += ["ref", "dropin"]
     subprocess.run(["make", "-s", "-C", HERE, "-j8"] + targets, check=True)
 
 
@@ -67,10 +68,14 @@ def ref_available(fast=False):
     return os.path.exists(REF_FAST_SO if fast else REF_SO)
 
 
-def ref_lib(fast=False):
-    key = bool(fast)
+def dropin_available():
+    return os.path.exists(DROPIN_SO)
+
+
+def ref_lib(fast=False, dropin=False):
+    key = "dropin" if dropin else bool(fast)
     if key not in _refs:
-        path = REF_FAST_SO if fast else REF_SO
+        path = DROPIN_SO if dropin else (REF_FAST_SO if fast else REF_SO)
         if not os.path.exists(path):
             raise RuntimeError("reference build %s is missing (make -C oracle ref)" % path)
         lib = C.CDLL(path)
@@ -94,6 +99,13 @@ def ref_lib(fast=False):
         lib.lrtr_import.argtypes = [C.c_void_p, C.POINTER(SceneArrays)]
         lib.lrtr_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_int]
         vp, u32, u64 = C.c_void_p, C.c_uint32, C.c_uint64
+        if dropin:
+            lib.lrtd_create.restype = vp
+            lib.lrtd_create.argtypes = [C.c_char_p, C.c_char_p]
+            lib.lrtd_commit_status.restype = C.c_int32
+            lib.lrtd_commit_status.argtypes = [vp, C.c_char_p, u64]
+            lib.lrtd_trace_batch.restype = C.c_int32
+            lib.lrtd_trace_batch.argtypes = [vp, vp, vp, u64]
         lib.lrtr_renderer_create.restype = vp
         for fn, args in (("lrtr_renderer_create", [vp]), ("lrtr_renderer_destroy", [vp]),
                          ("lrtr_renderer_add_mesh", [vp, u32, vp, u64, vp, u64]),
@@ -290,6 +302,37 @@ class RefRenderer:
         gb = np.zeros(width * height, HIT_DTYPE)
         self.lib.lrtr_renderer_fill_transparency(self.h, width, height, sample, transp.ctypes.data, gb.ctypes.data)
         return transp, gb
+
+
+class DropInScene(RefScene):
+    """The reference's BVHRT with the BVHRT_B200 subclass of INTEGRATION.md
+    (oracle/ref/bvhrt_b200.cpp, linked against liblrt_b200.so): the
+    reference's own adders and CommitScene build the scene, the override
+    uploads it, and ray queries run on the GPU.  `trace` goes through the
+    virtual RayQuery_NearestHit one ray at a time (threads=1); `trace_batch`
+    through RayQuery_NearestHitBatch."""
+
+    def __init__(self, build_name="cbvh_embree2", layout_name="SuperTreeletAlignedMerged4", preset=None):
+        self.lib = ref_lib(dropin=True)
+        self.h = self.lib.lrtd_create(build_name.encode(), layout_name.encode())
+        if not self.h:
+            raise RuntimeError("BVHRT_B200: lrt_scene_create failed")
+        self.set_preset(preset if preset is not None else parity_preset())
+
+    def commit(self):
+        self.lib.lrtr_commit(self.h)
+        msg = C.create_string_buffer(512)
+        st = self.lib.lrtd_commit_status(self.h, msg, len(msg))
+        if st != 0:
+            raise RuntimeError("BVHRT_B200::CommitScene upload failed (%d): %s" % (st, msg.value.decode()))
+
+    def trace_batch(self, rays):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        hits = np.zeros(len(rays), dtype=HIT_DTYPE)
+        st = self.lib.lrtd_trace_batch(self.h, rays.ctypes.data, hits.ctypes.data, len(rays))
+        if st != 0:
+            raise RuntimeError("RayQuery_NearestHitBatch failed with status %d" % st)
+        return hits
 
 
 def port_render_lambert(arrays, rays, light, preset=None, threads=os.cpu_count()):

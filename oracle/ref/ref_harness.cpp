@@ -15,18 +15,8 @@
 #include "sdf/simple/sdf_simple.h"
 
 #include "../../include/lrt_b200.h"
+#include "abi_layout.h"
 #include "ref_holder.h"
-
-static_assert(sizeof(CRT_Hit) == sizeof(lrt_hit), "CRT_Hit layout");
-static_assert(sizeof(BVHNode) == sizeof(lrt_bvh_node), "BVHNode layout");
-static_assert(sizeof(BVHNodePair) == sizeof(lrt_bvh_node_pair), "BVHNodePair layout");
-static_assert(sizeof(GeomData) == sizeof(lrt_geom_data), "GeomData layout");
-static_assert(sizeof(InstanceData) == sizeof(lrt_instance_data), "InstanceData layout");
-static_assert(sizeof(SdfFrameOctreeNode) == sizeof(lrt_sdf_frame_octree_node), "SdfFrameOctreeNode layout");
-static_assert(sizeof(SdfSVSNode) == sizeof(lrt_sdf_svs_node), "SdfSVSNode layout");
-static_assert(sizeof(SdfSBSNode) == sizeof(lrt_sdf_sbs_node), "SdfSBSNode layout");
-static_assert(sizeof(SdfSBSHeader) == sizeof(lrt_sdf_sbs_header), "SdfSBSHeader layout");
-static_assert(sizeof(MultiRenderPreset) == sizeof(lrt_preset), "MultiRenderPreset layout");
 
 std::shared_ptr<ISceneObject> CreateSceneRT(const char* a_implName, const char* a_buildName, const char* a_layoutName);
 

@@ -25,10 +25,8 @@
 #include "utils/mesh/mesh.h"
 
 #include "../../include/lrt_b200.h"
+#include "abi_layout.h"
 #include "ref_holder.h"
-
-static_assert(sizeof(Light) == sizeof(lrt_light), "Light layout");
-static_assert(sizeof(MultiRendererMaterial) == sizeof(lrt_material), "MultiRendererMaterial layout");
 
 namespace {
 
