@@ -930,6 +930,105 @@ def configs_table(args):
         sc.close()
 
 
+def profile_case(args):
+    """--case NAME: a small instance of one kernel, launched `--steps` times
+    after `--warmup` launches, for ncu captures (inputs above the 126 MB L2,
+    a few hundred MB on the device):
+      render   lrt_render_rgba8, LAMBERT_NO_TEX, the benchmark's SBS and camera
+      batched  lrt_batch_trace, 8 cameras of 512^2 on the benchmark's SBS
+      adjoint  lrt_adjoint_lambert_sbs_image + forward, 4 views of 512^2, SBS 256^3
+      bounce   lrt_generate_bounce_rays_sorted + the bounce trace, the
+               1024-instance scene at 2048^2
+    Prints one JSON line with the mean device time per launch (CUDA events)."""
+    import torch
+    from graphic_lab_task_b200 import LIGHT_AMBIENT, LIGHT_DIRECT, LIGHT_DTYPE, SceneRT, workloads as wl
+    from graphic_lab_task_b200.lrt import CameraBatch
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        tot = 0.0
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            tot += e0.elapsed_time(e1)
+        return tot / args.steps
+
+    out = {"case": args.case}
+    if args.case in ("render", "batched"):
+        (hdr, nodes, vals, vf), cam = workload_scene()
+        sc = SceneRT()
+        sc.AddInstance(sc.AddGeom_SdfSBS(hdr, nodes, vals, vf), wl.IDENTITY)
+        sc.CommitScene()
+        if args.case == "render":
+            lights = np.zeros(2, LIGHT_DTYPE)
+            lights[0] = ((0.577, 0.577, 0.577), LIGHT_DIRECT, (1.0, 1.0, 1.0), 0)
+            lights[1] = ((0, 0, 0), LIGHT_AMBIENT, (0.1, 0.1, 0.1), 0)
+            img = torch.zeros(WIDTH * HEIGHT, dtype=torch.int32, device=dev)
+            out["ms"] = timed(lambda: sc.render_rgba8(cam, lights, (0, 0, 0, 1), img.data_ptr(), stream=sp))
+            out["pixels"] = WIDTH * HEIGHT
+        else:
+            cams = wl.sphere_cameras(8, radius=3.0, seed=3, fixed_res=512)
+            b = CameraBatch(sc, cams)
+            hb = torch.zeros(b.total_rays * 8, dtype=torch.float32, device=dev)
+            out["ms"] = timed(lambda: b.trace(hb.data_ptr(), stream=sp))
+            out["rays"] = b.total_rays
+            out["shape"] = list(b.shape)
+            b.close()
+        sc.sync(stream=sp)
+    elif args.case == "adjoint":
+        hdr, nodes, vals, vf, target, cams, rays = wl.adjoint_workload(grid_res=256, views=4, res=512)
+        sc = SceneRT()
+        sc.AddInstance(sc.AddGeom_SdfSBS(hdr, nodes, vals, vf), wl.IDENTITY)
+        sc.CommitScene()
+        n = len(rays)
+        R = torch.from_numpy(rays).to(dev)
+        img = torch.empty(n, dtype=torch.float32, device=dev)
+        dimg = torch.full((n,), 1.0 / n, dtype=torch.float32, device=dev)
+        grad = torch.zeros(len(vf), dtype=torch.float32, device=dev)
+        shape = (512, n // 512)
+        out["forward_ms"] = timed(lambda: sc.render_lambert(R.data_ptr(), n, wl.LIGHT, img.data_ptr(), stream=sp,
+                                                            image_size=shape))
+        out["ms"] = timed(lambda: sc.adjoint_lambert(R.data_ptr(), n, wl.LIGHT, dimg.data_ptr(), grad.data_ptr(),
+                                                     stream=sp, image_size=shape))
+        out["rays"] = n
+        sc.sync(stream=sp)
+    elif args.case == "bounce":
+        sc = SceneRT()
+        wl.build_instanced(sc)
+        sc.CommitScene()
+        w = 2048
+        n = w * w
+        R = torch.empty(n * 8, dtype=torch.float32, device=dev)
+        H = torch.empty_like(R)
+        B = torch.empty_like(R)
+        HB = torch.empty_like(R)
+        idx = torch.empty(n, dtype=torch.int32, device=dev)
+        cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+        sc.generate_eye_rays(wl.camera(wl.INSTANCED_EYE, width=w, height=w), R.data_ptr(), sp)
+        sc.trace_image(R.data_ptr(), H.data_ptr(), w, w, stream=sp)
+        gen = lambda: sc.generate_bounce_rays_sorted(R.data_ptr(), H.data_ptr(), n, 11, B.data_ptr(),  # noqa: E731
+                                                     idx.data_ptr(), cnt.data_ptr(), stream=sp)
+        out["generate_ms"] = timed(gen)
+        nb = int(cnt.item())
+        out["ms"] = timed(lambda: sc.trace_device(B.data_ptr(), HB.data_ptr(), nb, stream=sp))
+        out["rays"], out["bounce_rays"] = n, nb
+        sc.sync(stream=sp)
+    else:
+        raise SystemExit("unknown --case %s" % args.case)
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -941,7 +1040,12 @@ def main():
     ap.add_argument("--configs", action="store_true",
                     help="measure every benchmark configuration (GPU and reference CPU), one JSON line each")
     ap.add_argument("--only", default="0,1,2,3,4", help="with --configs: the configurations to measure")
+    ap.add_argument("--case", default=None, help="render | batched | adjoint | bounce: one small kernel case "
+                                                  "for profiling (see profile_case)")
     args = ap.parse_args()
+    if args.case:
+        profile_case(args)
+        return
     if args.configs:
         configs_table(args)
         return
