@@ -112,6 +112,69 @@ lrt_status upload_materials(lrt_scene* s)
   return LRT_OK;
 }
 
+// Triangle slots of geometry g (its records in the triangle soup): one past
+// the largest leaf range of its leaf table, as build_tri_soup counts them.
+uint64_t triangle_slots(const HostArrays& h, size_t g)
+{
+  uint64_t ntri = 0;
+  for (uint32_t a = h.startEnd[2 * g]; a < h.startEnd[2 * g + 1]; a++) {
+    const uint32_t pk = h.primIdCount[a];
+    ntri = std::max<uint64_t>(ntri, uint64_t(pk & 0x0FFFFFFFu) + ((pk & 0x70000000u) >> 28));
+  }
+  return ntri;
+}
+
+// Copies the textures and the triangles' texture coordinates to the device
+// after they changed: the coordinates as 3 float2 per triangle slot (the
+// triangle soup's indexing), zeros for geometries without coordinates.
+lrt_status upload_textures(lrt_scene* s)
+{
+  DeviceScene* d = s->dev;
+  if (d->texVersion == s->texVersion) return LRT_OK;
+  cudaFree(d->texels);
+  cudaFree(d->texTable);
+  cudaFree(d->triTc);
+  d->texels = nullptr;
+  d->texTable = nullptr;
+  d->triTc = nullptr;
+  cudaError_t e = cudaSuccess;
+  const size_t ntex = s->texDims.size() / 2;
+  if (ntex) {
+    std::vector<uint4> table(ntex);
+    for (size_t k = 0; k < ntex; k++)
+      table[k] = make_uint4(uint32_t(s->texOffsets[k]), s->texDims[2 * k], s->texDims[2 * k + 1], 0u);
+    e = cudaMalloc(&d->texels, s->texels.size() * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&d->texTable, ntex * sizeof(uint4));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(d->texels, s->texels.data(), s->texels.size() * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d->texTable, table.data(), ntex * sizeof(uint4), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess && !s->texcoords.empty()) {
+    const HostArrays& h = s->h;
+    const size_t nslots = h.indices.size() / 3;
+    std::vector<float> tc(std::max<size_t>(1, nslots) * 6, 0.0f);
+    for (const auto& kv : s->texcoords) {
+      const size_t g = kv.first;
+      if (g >= h.geomData.size() || h.geomTags[g] != LRT_TAG_TRIANGLE) continue;
+      const lrt_geom_data& gd = h.geomData[g];
+      const uint64_t base = gd.offset[0] / 3, ntri = triangle_slots(h, g);
+      for (uint64_t t = 0; t < ntri && base + t < nslots; t++)
+        for (int c = 0; c < 3; c++) {
+          const uint64_t vi = h.indices[gd.offset[0] + 3 * t + c];
+          if (2 * vi + 1 < kv.second.size()) {
+            tc[6 * (base + t) + 2 * c] = kv.second[2 * vi];
+            tc[6 * (base + t) + 2 * c + 1] = kv.second[2 * vi + 1];
+          }
+        }
+    }
+    e = cudaMalloc(&d->triTc, tc.size() * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemcpy(d->triTc, tc.data(), tc.size() * sizeof(float), cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) return cuda_fail(s, e, "textures host->device");
+  d->texVersion = s->texVersion;
+  return LRT_OK;
+}
+
 // Every geometry whose hits read a material (all but the types in `skip`,
 // a list ending in ~0u) needs a nonempty material range.
 lrt_status check_material_ranges(lrt_scene* s, const char* who, const uint32_t* skip)
@@ -295,17 +358,22 @@ lrt_status lrt_render_rgba8(lrt_scene* s, const lrt_camera* camera, const lrt_li
   if (light_count > LRT_MAX_LIGHTS)
     return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_render_rgba8: %u lights (at most %d)", light_count, LRT_MAX_LIGHTS);
   const uint32_t mode = s->preset.render_mode;
-  static const uint32_t kModes[] = {0,  1,  2,  3,  4,  5,  6,  7,  8,  9,  10, 11,
-                                    12, 13, 14, 16, 17, 18, 19, 20, 21, 22, 24, 25};
+  static const uint32_t kModes[] = {0,  1,  2,  3,  4,  5,  6,  7,  8,  9,  10, 11, 12,
+                                    13, 14, 15, 16, 17, 18, 19, 20, 21, 22, 24, 25};
   if (std::find(std::begin(kModes), std::end(kModes), mode) == std::end(kModes))
     return fail(s, LRT_ERR_UNSUPPORTED,
-                "lrt_render_rgba8: render_mode %u (texture coordinates, channels and intersection counts are outside "
-                "the ray-query path)",
+                "lrt_render_rgba8: render_mode %u (channels and intersection counts are outside the ray-query path)",
                 mode);
-  if (mode == 11 && (s->mats.empty() || s->mats[0].type != LRT_MATERIAL_COLORED))
-    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_render_rgba8: PBR_NO_TEX shades with material 0, a COLORED one");
+  // a TEXTURED material samples texture texId (lrt_set_textures)
+  auto material_ok = [&](const lrt_material& m) {
+    return m.type == LRT_MATERIAL_COLORED || (m.type == LRT_MATERIAL_TEXTURED && m.texId < s->texDims.size() / 2);
+  };
+  if (mode == 11 && (s->mats.empty() || !material_ok(s->mats[0])))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT,
+                "lrt_render_rgba8: PBR_NO_TEX shades with material 0, a COLORED one or a TEXTURED one whose texture "
+                "is set");
   if (mode == 16 || mode == 17 || mode == 18 || mode == 21 || mode == 22) {
-    // DIFFUSE, LAMBERT, PHONG and PBR read COLORED materials; MATERIAL the material ids
+    // DIFFUSE, LAMBERT, PHONG and PBR read the materials; MATERIAL the material ids
     static const uint32_t kSkipDiffuse[] = {LRT_TYPE_SDF_SBS_COL, ~0u};
     static const uint32_t kSkipLambert[] = {LRT_TYPE_SDF_SBS_COL, LRT_TYPE_GRAPHICS_PRIM, ~0u};
     static const uint32_t kSkipNone[] = {~0u};
@@ -313,9 +381,11 @@ lrt_status lrt_render_rgba8(lrt_scene* s, const lrt_camera* camera, const lrt_li
                                mode == 16 ? kSkipDiffuse : (mode == 21 || mode == 22) ? kSkipNone : kSkipLambert);
     if (st != LRT_OK) return st;
     if (mode != 22)
-      for (const lrt_material& m : s->mats)
-        if (m.type != LRT_MATERIAL_COLORED)
-          return fail(s, LRT_ERR_UNSUPPORTED, "lrt_render_rgba8: textured materials are not implemented");
+      for (size_t k = 0; k < s->mats.size(); k++)
+        if (!material_ok(s->mats[k]))
+          return fail(s, LRT_ERR_INVALID_ARGUMENT,
+                      "lrt_render_rgba8: material %zu (type %u, texture %u of %zu set with lrt_set_textures)", k,
+                      s->mats[k].type, s->mats[k].texId, s->texDims.size() / 2);
   }
   const uint32_t spp = s->preset.spp;
   if (spp == 0 || spp > 1024)
@@ -336,6 +406,7 @@ lrt_status lrt_render_rgba8(lrt_scene* s, const lrt_camera* camera, const lrt_li
       if (m.type == LRT_MATERIAL_COLORED && m.base_color[3] < 1.0f) RM.transparency = 1;
   if (camera->width == 0 || camera->height == 0) return LRT_OK;
   if ((st = upload_materials(s)) != LRT_OK) return st;
+  if ((st = upload_textures(s)) != LRT_OK) return st;
   DevCamera cam;
   std::memcpy(cam.proj_inv, camera->proj_inv, sizeof(cam.proj_inv));
   std::memcpy(cam.world_view_inv, camera->world_view_inv, sizeof(cam.world_view_inv));
@@ -357,6 +428,10 @@ lrt_status lrt_render_rgba8(lrt_scene* s, const lrt_camera* camera, const lrt_li
   M.ids = d->matIds;
   M.offsets = reinterpret_cast<const uint2*>(d->matOffsets);
   std::memcpy(M.background, background, sizeof(M.background));
+  M.texels = d->texels;
+  M.texs = d->texTable;
+  M.texCount = d->texTable ? uint32_t(s->texDims.size() / 2) : 0u;
+  M.triTc = d->triTc;
   if (mode == LRT_RENDER_MODE_OUTLINE_BORDER) return render_outline_border(s, S, slot, cam, L, M, RM, image_dev, grid, stream);
   if ((st = sched_prepare(s, stream, cam.width, cam.height, false, &rd, &wr)) != LRT_OK) return st;
   const cudaError_t e = lrt_exact::launch_render_rgba8(S, cam, L, image_dev, &slot->work, &slot->err, d->stackCap,
@@ -387,6 +462,57 @@ lrt_status lrt_set_materials(lrt_scene* s, const lrt_material* materials, uint32
   s->matIds.assign(mat_id_by_prim_id, mat_id_by_prim_id + mat_id_count);
   s->matOffsets.assign(mat_id_offsets, mat_id_offsets + 2 * size_t(offset_count));
   s->matVersion++;
+  return LRT_OK;
+}
+
+lrt_status lrt_set_textures(lrt_scene* s, const float* texels_rgba, const uint32_t* dims, uint32_t count)
+{
+  if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  if (count && (!texels_rgba || !dims))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_set_textures: NULL texels or sizes with %u textures", count);
+  std::vector<uint64_t> offs(count);
+  uint64_t total = 0;
+  for (uint32_t k = 0; k < count; k++) {
+    const uint64_t w = dims[2 * k], hgt = dims[2 * k + 1];
+    if (w == 0 || hgt == 0 || w > (1u << 16) || hgt > (1u << 16))
+      return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_set_textures: texture %u is %llu x %llu (1..65536 each way)", k,
+                  (unsigned long long)w, (unsigned long long)hgt);
+    offs[k] = total;
+    total += w * hgt;
+  }
+  if (total >= (uint64_t(1) << 32))
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_set_textures: %llu texels (fewer than 2^32)",
+                (unsigned long long)total);
+  s->texels.assign(texels_rgba, texels_rgba + 4 * total);
+  s->texDims.assign(dims, dims + 2 * size_t(count));
+  s->texOffsets = offs;
+  s->texVersion++;
+  return LRT_OK;
+}
+
+lrt_status lrt_set_texcoords(lrt_scene* s, uint32_t geom_id, const float* texcoords, uint64_t vertex_count)
+{
+  if (!s) return LRT_ERR_INVALID_ARGUMENT;
+  const HostArrays& h = s->h;
+  if (geom_id >= h.geomData.size() || h.geomTags[geom_id] != LRT_TAG_TRIANGLE)
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_set_texcoords: geometry %u is not a triangle mesh", geom_id);
+  if (vertex_count == 0) {
+    s->texcoords.erase(geom_id);
+    s->texVersion++;
+    return LRT_OK;
+  }
+  if (!texcoords) return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_set_texcoords: NULL coordinates");
+  // the geometry's vertices: from its vertex offset to the next mesh's (or the end)
+  uint64_t end = h.vertPos.size() / 4;
+  for (size_t g = 0; g < h.geomData.size(); g++)
+    if (h.geomTags[g] == LRT_TAG_TRIANGLE && h.geomData[g].offset[1] > h.geomData[geom_id].offset[1])
+      end = std::min<uint64_t>(end, h.geomData[g].offset[1]);
+  const uint64_t nv = end - h.geomData[geom_id].offset[1];
+  if (vertex_count != nv)
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_set_texcoords: %llu coordinates for the %llu vertices of geometry %u",
+                (unsigned long long)vertex_count, (unsigned long long)nv, geom_id);
+  s->texcoords[geom_id].assign(texcoords, texcoords + 2 * vertex_count);
+  s->texVersion++;
   return LRT_OK;
 }
 

@@ -162,6 +162,13 @@ struct DevMaterials {
   const uint32_t* ids;
   const uint2* offsets;
   float background[4];
+  // the renderer's textures (MultiRenderer::m_textures): texels, and per
+  // texture {first texel, width, height, 0}; the texture coordinates of each
+  // triangle slot's 3 vertices (the triangle soup's indexing), or NULL
+  const float4* texels;
+  const uint4* texs;
+  uint32_t texCount;
+  const float2* triTc;
 };
 
 // The render mode of lrt_render_rgba8's general kernel: the preset's

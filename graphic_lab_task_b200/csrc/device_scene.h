@@ -69,6 +69,12 @@ struct DeviceScene {
   uint32_t* matIds = nullptr;
   uint2* matOffsets = nullptr;
   uint64_t matVersion = 0;
+  // the renderer's textures and the triangles' texture coordinates
+  // (lrt_set_textures / lrt_set_texcoords), copied at the next render after they changed
+  float4* texels = nullptr;
+  uint4* texTable = nullptr;
+  float2* triTc = nullptr;
+  uint64_t texVersion = 0;
   std::map<cudaStream_t, ImageSchedule> sched; // per stream of image-order launches
   // staging buffers for host-pointer calls
   float4* rays = nullptr;
@@ -102,6 +108,9 @@ struct DeviceScene {
     if (mats) cudaFree(mats);
     if (matIds) cudaFree(matIds);
     if (matOffsets) cudaFree(matOffsets);
+    if (texels) cudaFree(texels);
+    if (texTable) cudaFree(texTable);
+    if (triTc) cudaFree(triTc);
     for (auto& kv : sched)
       for (uint32_t* b : kv.second.buf) cudaFree(b);
   }

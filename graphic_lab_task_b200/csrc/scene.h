@@ -8,6 +8,7 @@
 #pragma once
 #include <cstdint>
 #include <string>
+#include <map>
 #include <vector>
 
 #include "../../include/lrt_b200.h"
@@ -82,6 +83,14 @@ struct lrt_scene {
   std::vector<lrt_material> mats;
   std::vector<uint32_t> matIds, matOffsets;
   uint64_t matVersion = 0;
+  // renderer textures (lrt_set_textures: float4 texels of all images, width
+  // and height of each, its first texel) and the triangle geometries' texture
+  // coordinates (lrt_set_texcoords: 2 floats per vertex); texVersion counts changes
+  std::vector<float> texels;
+  std::vector<uint32_t> texDims;
+  std::vector<uint64_t> texOffsets;
+  std::map<uint32_t, std::vector<float>> texcoords;
+  uint64_t texVersion = 0;
 };
 
 namespace lrt {

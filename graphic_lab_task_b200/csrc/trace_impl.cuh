@@ -1009,6 +1009,36 @@ __device__ __forceinline__ f3 lambert_lights(const DevLights& L, f3 norm, f3 col
 // ST_ITERATIONS, DIFFUSE, LAMBERT, HSV_DEPTH, LOD, MATERIAL, MO_VOXEL_COUNT
 // and MO_FLAGS (colored materials only).  The normal is loadNormalTcFromGbuffer's
 // (triangles recomputed and turned to the viewer, SDF hits decoded).
+// Image2D<float4>::sample (dependencies/1st-party/LiteMath/Image2d.cpp:
+// 105-183) with the sampler every MultiRenderer texture has (AddTexture,
+// MultiRenderer_host.cpp:827-839): LINEAR filter, CLAMP addressing
+// (bilinearOffsets, Image2d.cpp:50-102), in its operation order.
+__device__ __forceinline__ float4 sample_texture(const DevMaterials& M, uint32_t tex, float u, float v)
+{
+  if (tex >= M.texCount) return make_float4(0, 0, 0, 0);
+  const uint4 t = __ldg(M.texs + tex);
+  const int w = int(t.y), hgt = int(t.z);
+  const float4* data = M.texels + t.x;
+  float ffx = u * float(w) - 0.5f;
+  float ffy = v * float(hgt) - 0.5f;
+  if (ffx < 0) ffx = 0.0f;
+  if (ffy < 0) ffy = 0.0f;
+  const int px = int(ffx), py = int(ffy);
+  const float fx = fabsf(ffx - float(px)), fy = fabsf(ffy - float(py));
+  const float fx1 = 1.0f - fx, fy1 = 1.0f - fy;
+  const float w1 = fx1 * fy1, w2 = fx * fy1, w3 = fx1 * fy, w4 = fx * fy;
+  int px0 = px >= w ? w - 1 : px, px1 = px + 1 >= w ? w - 1 : px + 1;
+  int py0 = py >= hgt ? hgt - 1 : py, py1 = py + 1 >= hgt ? hgt - 1 : py + 1;
+  px0 = px0 < 0 ? 0 : px0;
+  px1 = px1 < 0 ? 0 : px1;
+  py0 = py0 < 0 ? 0 : py0;
+  py1 = py1 < 0 ? 0 : py1;
+  const float4 f1 = __ldg(data + int64_t(py0) * w + px0), f2 = __ldg(data + int64_t(py0) * w + px1);
+  const float4 f3 = __ldg(data + int64_t(py1) * w + px0), f4 = __ldg(data + int64_t(py1) * w + px1);
+  return make_float4(f1.x * w1 + f2.x * w2 + f3.x * w3 + f4.x * w4, f1.y * w1 + f2.y * w2 + f3.y * w3 + f4.y * w4,
+                     f1.z * w1 + f2.z * w2 + f3.z * w3 + f4.z * w4, f1.w * w1 + f2.w * w2 + f3.w * w3 + f4.w * w4);
+}
+
 template <class CTX>
 __device__ float4 resolve_mode_colour(CTX& c, const DevLights& L, const DevMaterials& M, uint32_t mode, f3 rayPos,
                                       f3 rayDir, const lrt_hit& h)
@@ -1017,18 +1047,37 @@ __device__ float4 resolve_mode_colour(CTX& c, const DevLights& L, const DevMater
   if (h.primId == 0xFFFFFFFFu) return make_float4(L.background[0], L.background[1], L.background[2], L.background[3]);
   const uint32_t type = h.geomId >> 24, geomId = h.geomId & 0x00FFFFFFu;
   f3 norm;
+  // loadNormalTcFromGbuffer's texture coordinates (:27-76): SDF hits' coords[0..1]
+  float tcu = h.coords[0], tcv = h.coords[1];
   if (type == LRT_TYPE_MESH_TRIANGLE) {
     const DevGeom& g = S.geoms[geomId];
-    const float4* tri = S.triSoup + 3 * (uint64_t(g.triBase) + c.triLocal);
+    const uint64_t slot = uint64_t(g.triBase) + c.triLocal;
+    const float4* tri = S.triSoup + 3 * slot;
     const f3 raw = cross(ld3(__ldg(tri + 1)), ld3(__ldg(tri + 2)));
     norm = normalize(matmul4(S.instances[h.instId].transformInvTransposed, raw, 1.0f));
     norm = ssign(dot(-1.0f * rayDir, norm)) * norm;
+    // (1 - c0 - c1) * A_tc + c1 * B_tc + c0 * C_tc of the vertices' coordinates
+    float2 A = make_float2(0, 0), B = A, C = A;
+    if (M.triTc) {
+      A = __ldg(M.triTc + 3 * slot);
+      B = __ldg(M.triTc + 3 * slot + 1);
+      C = __ldg(M.triTc + 3 * slot + 2);
+    }
+    const float wa = 1.0f - h.coords[0] - h.coords[1];
+    tcu = wa * A.x + h.coords[1] * B.x + h.coords[0] * C.x;
+    tcv = wa * A.y + h.coords[1] * B.y + h.coords[0] * C.y;
   } else {
     norm = decode_normal(mk2(h.coords[2], h.coords[3]));
   }
   auto material = [&]() -> const lrt_material& {
     const uint2 o = M.offsets[geomId];
     return M.mats[M.ids[o.x + h.primId % o.y]];
+  };
+  // a material's colour: base_color if COLORED, else its texture at the hit's coordinates
+  auto material_colour = [&](const lrt_material& m) -> float4 {
+    if (m.type == LRT_MATERIAL_COLORED) return make_float4(m.base_color[0], m.base_color[1], m.base_color[2],
+                                                           m.base_color[3]);
+    return sample_texture(M, m.texId, tcu, tcv);
   };
   const float z = h.t, z_near = 0.1f, z_far = 10.0f;
   float4 res = make_float4(1, 0, 1, 1);
@@ -1112,11 +1161,13 @@ __device__ float4 resolve_mode_colour(CTX& c, const DevLights& L, const DevMater
       const f3 pc = packed_hit_colour(h);
       col = make_float4(pc.x, pc.y, pc.z, col.w);
     } else {
-      const lrt_material& m = material();
-      col = make_float4(m.base_color[0], m.base_color[1], m.base_color[2], m.base_color[3]);
+      col = material_colour(material());
     }
     res = make_float4(col.x, col.y, col.z, 1);
   } break;
+  case 15: // TEX_COORDS
+    res = make_float4(tcu, tcv, 0, 1);
+    break;
   case 1:  // LAMBERT_NO_TEX
   case 13: // OUTLINE_PRIM: ResolveOutline (:1073-1121) never sets its outline flag in this mode
   case 7:  // GEOM
@@ -1127,17 +1178,14 @@ __device__ float4 resolve_mode_colour(CTX& c, const DevLights& L, const DevMater
     else if (mode == 20) color = ld3(decode_rgba8(kLodPalette[h.primId % 20]));
     else if (mode == 7) color = ld3(decode_rgba8(kPalette[geomId % 20]));
     else if (type == LRT_TYPE_SDF_SBS_COL || type == LRT_TYPE_GRAPHICS_PRIM) color = packed_hit_colour(h);
-    else {
-      const lrt_material& m = material();
-      color = mk3(m.base_color[0], m.base_color[1], m.base_color[2]);
-    }
+    else color = ld3(material_colour(material()));
     const f3 fc = lambert_lights(L, norm, color, rayPos, rayDir, h.t);
     res = make_float4(fc.x, fc.y, fc.z, 1);
   } break;
   case 11: // PBR_NO_TEX (material 0, DEFAULT_MATERIAL)
   case 21: { // PBR (colored materials)
     const lrt_material& m = mode == 11 ? M.mats[0] : material();
-    const f3 baseColor = mk3(m.base_color[0], m.base_color[1], m.base_color[2]);
+    const f3 baseColor = ld3(material_colour(m));
     const float metallic = m.metallic, roughness = m.roughness;
     const float alpha = roughness * roughness, f0 = 0.04f, kPi = 3.14159265358979323846f; // LiteMath's M_PI, a float
     const f3 surf = rayPos + h.t * rayDir;
@@ -1181,10 +1229,7 @@ __device__ float4 resolve_mode_colour(CTX& c, const DevLights& L, const DevMater
     f3 color = mk3(0, 0, 1);
     if (mode == 12) color = mk3(1, 1, 1);
     else if (type == LRT_TYPE_SDF_SBS_COL || type == LRT_TYPE_GRAPHICS_PRIM) color = packed_hit_colour(h);
-    else {
-      const lrt_material& m = material();
-      color = mk3(m.base_color[0], m.base_color[1], m.base_color[2]);
-    }
+    else color = ld3(material_colour(material()));
     f3 fc = mk3(0, 0, 0);
     for (uint32_t i = 0; i < L.count; i++) {
       const DevLight& l = L.light[i];

@@ -30,7 +30,7 @@ EXPORTED = (
     "lrt_batch_update_cameras", "lrt_batch_set_shape", "lrt_batch_get_shape", "lrt_batch_trace", "lrt_batch_sync",
     "lrt_batch_autotune", "lrt_render_lambert", "lrt_adjoint_lambert_sbs", "lrt_sbs_update_values",
     "lrt_generate_bounce_rays", "lrt_generate_bounce_rays_compact", "lrt_render_rgba8", "lrt_trace_nearest_image",
-    "lrt_set_materials", "lrt_fill_gbuffer_transparency", "lrt_render_lambert_image", "lrt_adjoint_lambert_sbs_image",
+    "lrt_set_materials", "lrt_set_textures", "lrt_set_texcoords", "lrt_fill_gbuffer_transparency", "lrt_render_lambert_image", "lrt_adjoint_lambert_sbs_image",
     "lrt_generate_bounce_rays_sorted",
     "lrt_update_instance", "lrt_add_geom_sdf_frame_octree_file", "lrt_add_geom_sdf_svs_file",
     "lrt_add_geom_sdf_sbs_file", "lrt_batch_render_rgba8",
@@ -113,6 +113,8 @@ def lib():
         "lrt_render_lambert": [vp, vp, u64, vp, vp, vp],
         "lrt_render_rgba8": [vp, vp, vp, u32, vp, vp, vp],
         "lrt_set_materials": [vp, vp, u32, vp, u64, vp, u32],
+        "lrt_set_textures": [vp, vp, vp, u32],
+        "lrt_set_texcoords": [vp, u32, vp, u64],
         "lrt_fill_gbuffer_transparency": [vp, vp, vp, vp, vp, vp],
         "lrt_trace_nearest_image": [vp, vp, vp, u32, u32, vp, u32],
         "lrt_generate_bounce_rays": [vp, vp, vp, u64, u64, C.c_float, C.c_float, vp, vp],
@@ -378,6 +380,23 @@ class SceneRT:
         self._check(lib().lrt_set_materials(self.h, m.ctypes.data if len(m) else None, len(m),
                                             ids.ctypes.data if len(ids) else None, len(ids),
                                             offs.ctypes.data if len(offs) else None, len(offs) // 2))
+
+    def set_textures(self, images):
+        """MultiRenderer's m_textures: a list of (h, w, 4) float32 images
+        (slot k = images[k]), sampled bilinear with clamped addressing."""
+        imgs = [np.ascontiguousarray(i, np.float32) for i in (images or [])]
+        dims = np.array([[i.shape[1], i.shape[0]] for i in imgs], np.uint32).reshape(-1)
+        texels = np.concatenate([i.reshape(-1) for i in imgs]) if imgs else np.zeros(0, np.float32)
+        self._check(lib().lrt_set_textures(self.h, texels.ctypes.data if len(texels) else None,
+                                           dims.ctypes.data if len(dims) else None, len(imgs)))
+
+    def set_texcoords(self, geom_id, texcoords):
+        """Per-vertex texture coordinates (nverts, 2) of triangle geometry geom_id (None clears them)."""
+        if texcoords is None:
+            self._check(lib().lrt_set_texcoords(self.h, geom_id, None, 0))
+            return
+        tc = np.ascontiguousarray(texcoords, np.float32).reshape(-1, 2)
+        self._check(lib().lrt_set_texcoords(self.h, geom_id, tc.ctypes.data, len(tc)))
 
     def fill_gbuffer_transparency(self, camera, background, transparency_ptr, hits_ptr, stream=0):
         """kernel1D_FillGbufferWithTransparency for `camera`: float4

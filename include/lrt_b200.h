@@ -511,10 +511,14 @@ enum { LRT_LIGHT_DIRECT = 0, LRT_LIGHT_POINT = 1, LRT_LIGHT_AMBIENT = 2 };
  * (ResolveOutline, :1073-1128) runs two launches per sample: a G-buffer pass
  * and the outline test against the four neighbours' t (more than 10 t / width
  * apart: colour (0.2, 0.2, 0.2)); it keeps 40 bytes per pixel of device
- * scratch with the scene.  Other modes (texture coordinates, channels,
- * intersection counts) and textured materials return LRT_ERR_UNSUPPORTED; the
- * pixel grid is the camera's (the reference pads widths to a multiple of 8,
- * and its outline test reads the padded grid).  Writes
+ * scratch with the scene.  TEXTURED materials (LAMBERT, PHONG, PBR, DIFFUSE;
+ * PBR_NO_TEX's material 0) sample texture texId of lrt_set_textures at the
+ * hit's texture coordinates, and TEX_COORDS shows those coordinates
+ * (loadNormalTcFromGbuffer, :27-76: for triangles the barycentric blend of
+ * the per-vertex coordinates of lrt_set_texcoords, zeros where none were set;
+ * for SDF hits coords[0..1]).  Channel and intersection-count modes return
+ * LRT_ERR_UNSUPPORTED; the pixel grid is the camera's (the reference pads
+ * widths to a multiple of 8, and its outline test reads the padded grid).  Writes
  * width*height RGBA8 pixels (row-major) to device memory image_dev;
  * asynchronous on `stream`, lrt_trace_sync(stream) reports bounded-loop
  * limits.  No counterpart call in the reference (it renders through a
@@ -541,6 +545,31 @@ enum { LRT_MATERIAL_COLORED = 0, LRT_MATERIAL_TEXTURED = 1 };
 lrt_status lrt_set_materials(lrt_scene* scene, const lrt_material* materials, uint32_t material_count,
                              const uint32_t* mat_id_by_prim_id, uint64_t mat_id_count, const uint32_t* mat_id_offsets,
                              uint32_t offset_count);
+
+/* The renderer's textures (MultiRenderer::m_textures, MultiRenderer.h:256;
+ * MultiRenderer::AddTexture, MultiRenderer_host.cpp:827-839): `count` float4
+ * (RGBA) images, texture k of dims[2k] x dims[2k+1] texels (1..65536 each),
+ * row-major, stored one after another in texels_rgba; every one is sampled
+ * as the reference samples its textures, bilinear with clamped addressing
+ * (Image2D<float4>::sample with Filter::LINEAR and AddressMode::CLAMP,
+ * dependencies/1st-party/LiteMath/Image2d.cpp:50-183).  Texture k is what a
+ * TEXTURED material with texId k samples (the reference renderer starts with
+ * a 16x16 image of (0, 1, 1, 1) in every slot and AddTexture fills slots 1,
+ * 2, ...: pass its slots as they are).  Copied to the device at the next
+ * lrt_render_rgba8; a count of 0 clears them.  Texture coordinates beyond
+ * +-2^31 / size convert differently (the reference's float-to-int
+ * conversion of them is undefined). */
+lrt_status lrt_set_textures(lrt_scene* scene, const float* texels_rgba, const uint32_t* dims, uint32_t count);
+
+/* The per-vertex texture coordinates of triangle geometry geom_id (two
+ * floats per vertex of its vertex array, in the order AddGeom_Triangles3f
+ * received the vertices): what MultiRenderer::add_mesh_internal keeps in
+ * m_vertices[].w / m_normals[].w (MultiRenderer_host.cpp:499-520) and the
+ * resolve blends at a hit (loadNormalTcFromGbuffer, MultiRenderer_resolve.cpp:
+ * 27-76).  vertex_count must equal the geometry's vertex count; 0 clears the
+ * geometry's coordinates (they are then zero, as for a mesh loaded without
+ * any). */
+lrt_status lrt_set_texcoords(lrt_scene* scene, uint32_t geom_id, const float* texcoords, uint64_t vertex_count);
 
 /* MultiRenderer::kernel1D_FillGbufferWithTransparency with AnyHit
  * (MultiRenderer.cpp:204-246), one sample of `camera`: per pixel the loop of

@@ -1055,6 +1055,64 @@ static void decode_rgba8(uint32_t c, float out[4])
   out[3] = (float)((c >> 24) & 0xFF) * (1.0f / 255.0f);
 }
 
+/* The renderer's textures and the meshes' texture coordinates for the
+ * resolve (MultiRenderer::m_textures, MultiRenderer.h:256; the per-vertex
+ * coordinates add_mesh_internal keeps in m_vertices[].w / m_normals[].w,
+ * MultiRenderer_host.cpp:499-520).  Texture k: dims[2k] x dims[2k+1] float4
+ * texels, row-major, from texel offset tex_off[k] of texels; vert_tc: two
+ * floats per vertex of the scene's vertex array (NULL: all zero).  Set with
+ * lrto_set_textures before a render call (test infrastructure: one set per
+ * process, not thread-safe). */
+static struct {
+  const float* texels;
+  const uint32_t* dims;
+  const uint64_t* tex_off;
+  uint32_t count;
+  const float* vert_tc;
+  uint64_t nverts;
+} g_tex;
+
+void lrto_set_textures(const float* texels, const uint32_t* dims, const uint64_t* tex_off, uint32_t count,
+                       const float* vert_tc, uint64_t nverts)
+{
+  g_tex.texels = texels;
+  g_tex.dims = dims;
+  g_tex.tex_off = tex_off;
+  g_tex.count = count;
+  g_tex.vert_tc = vert_tc;
+  g_tex.nverts = nverts;
+}
+
+/* Image2D<float4>::sample (dependencies/1st-party/LiteMath/Image2d.cpp:105-183)
+ * with the sampler every MultiRenderer texture has (AddTexture,
+ * MultiRenderer_host.cpp:827-839): LINEAR filter, CLAMP in both directions
+ * (bilinearOffsets, Image2d.cpp:50-102). */
+static void sample_texture(uint32_t tex, float u, float v, float out[4])
+{
+  if (tex >= g_tex.count) { out[0] = out[1] = out[2] = out[3] = 0.0f; return; }
+  const int w = (int)g_tex.dims[2 * tex], hgt = (int)g_tex.dims[2 * tex + 1];
+  const float* data = g_tex.texels + 4 * g_tex.tex_off[tex];
+  float ffx = u * (float)w - 0.5f;
+  float ffy = v * (float)hgt - 0.5f;
+  if (ffx < 0) ffx = 0.0f;
+  if (ffy < 0) ffy = 0.0f;
+  const int px = (int)ffx, py = (int)ffy;
+  const float fx = fabsf(ffx - (float)px), fy = fabsf(ffy - (float)py);
+  const float fx1 = 1.0f - fx, fy1 = 1.0f - fy;
+  const float w1 = fx1 * fy1, w2 = fx * fy1, w3 = fx1 * fy, w4 = fx * fy;
+  int px0 = px >= w ? w - 1 : px, px1 = px + 1 >= w ? w - 1 : px + 1;
+  int py0 = py >= hgt ? hgt - 1 : py, py1 = py + 1 >= hgt ? hgt - 1 : py + 1;
+  px0 = px0 < 0 ? 0 : px0;
+  px1 = px1 < 0 ? 0 : px1;
+  py0 = py0 < 0 ? 0 : py0;
+  py1 = py1 < 0 ? 0 : py1;
+  const float* f1 = data + 4 * ((int64_t)py0 * w + px0);
+  const float* f2 = data + 4 * ((int64_t)py0 * w + px1);
+  const float* f3 = data + 4 * ((int64_t)py1 * w + px0);
+  const float* f4 = data + 4 * ((int64_t)py1 * w + px1);
+  for (int k = 0; k < 4; k++) out[k] = f1[k] * w1 + f2[k] * w2 + f3[k] * w3 + f4[k] * w4;
+}
+
 /* ResolveCommon (MultiRenderer_resolve.cpp:580-666) / kernel1D_ResolveDebug
  * (:810-990) of hit h for `mode`, with the resolve ray r (initEyeRay of
  * sample 0) and c->tri_local of the trace that found h: the float4 colour
@@ -1079,10 +1137,23 @@ static void resolve_colour(const lrt_scene_arrays* arrays, const ctx_t* cp, uint
     const uint32_t type = h.geomId >> 24, geomId = h.geomId & 0x00FFFFFFu;
     const f3 rayPos = mk3(r[0], r[1], r[2]), rayDir = mk3(r[4], r[5], r[6]);
     f3 norm;
+    float tcu = h.coords[0], tcv = h.coords[1]; /* loadNormalTcFromGbuffer's tc (:27-76) */
     if (type == LRT_TYPE_MESH_TRIANGLE) {
       /* loadNormalTcFromGbuffer, NORMAL_MODE_GEOMETRY (:33-59) */
       const uint32_t g = geomId;
       const uint32_t base = arrays->geomData[g].offset[0] + 3 * c->tri_local;
+      float tcs[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+      for (int k = 0; k < 3; k++) {
+        const uint64_t vi = (uint64_t)arrays->geomData[g].offset[1] + arrays->indices[base + k];
+        if (g_tex.vert_tc && vi < g_tex.nverts) {
+          tcs[k][0] = g_tex.vert_tc[2 * vi];
+          tcs[k][1] = g_tex.vert_tc[2 * vi + 1];
+        }
+      }
+      /* (1 - c0 - c1) * A_tc + c1 * B_tc + c0 * C_tc */
+      const float wa = 1.0f - h.coords[0] - h.coords[1];
+      tcu = wa * tcs[0][0] + h.coords[1] * tcs[1][0] + h.coords[0] * tcs[2][0];
+      tcv = wa * tcs[0][1] + h.coords[1] * tcs[1][1] + h.coords[0] * tcs[2][1];
       const float* vA = arrays->vertPos + 4 * (uint64_t)(arrays->geomData[g].offset[1] + arrays->indices[base + 0]);
       const float* vB = arrays->vertPos + 4 * (uint64_t)(arrays->geomData[g].offset[1] + arrays->indices[base + 1]);
       const float* vC = arrays->vertPos + 4 * (uint64_t)(arrays->geomData[g].offset[1] + arrays->indices[base + 2]);
@@ -1095,6 +1166,13 @@ static void resolve_colour(const lrt_scene_arrays* arrays, const ctx_t* cp, uint
     }
     /* m_matIdbyPrimId[m_matIdOffsets[geomId].x + primId % m_matIdOffsets[geomId].y] */
 #define MAT_ID() (mat_ids[mat_offsets[2 * geomId] + h.primId % mat_offsets[2 * geomId + 1]])
+    /* a material's colour: base_color if COLORED, else its texture at tc */
+    float mc[4];
+#define MAT_COLOUR(m)                                                            \
+  do {                                                                           \
+    if ((m)->type == LRT_MATERIAL_COLORED) memcpy(mc, (m)->base_color, sizeof(mc)); \
+    else sample_texture((m)->texId, tcu, tcv, mc);                                 \
+  } while (0)
     const float z = h.t, z_near = 0.1f, z_far = 10.0f;
     float res[4] = {1, 0, 1, 1};
     switch (mode) {
@@ -1175,9 +1253,15 @@ static void resolve_colour(const lrt_scene_arrays* arrays, const ctx_t* cp, uint
         res[2] = roundf(h.coords[1]) / 255.0f;
       } else {
         const lrt_material* m = &materials[MAT_ID()];
-        res[0] = m->base_color[0]; res[1] = m->base_color[1]; res[2] = m->base_color[2];
+        MAT_COLOUR(m);
+        res[0] = mc[0]; res[1] = mc[1]; res[2] = mc[2];
       }
     } break;
+    case 15: /* TEX_COORDS */
+      res[0] = tcu;
+      res[1] = tcv;
+      res[2] = 0;
+      break;
     case 1: case 7: case 13: case 17: case 20: { /* LAMBERT_NO_TEX, GEOM, OUTLINE_PRIM, LAMBERT (COLORED), LOD */
       f3 color = mk3(0, 0, 1);
       float pc[4];
@@ -1188,7 +1272,8 @@ static void resolve_colour(const lrt_scene_arrays* arrays, const ctx_t* cp, uint
         color = mk3(roundf(h.coords[0]) / 255.0f, h.coords[0] - floorf(h.coords[0]), roundf(h.coords[1]) / 255.0f);
       else {
         const lrt_material* m = &materials[MAT_ID()];
-        color = mk3(m->base_color[0], m->base_color[1], m->base_color[2]);
+        MAT_COLOUR(m);
+        color = mk3(mc[0], mc[1], mc[2]);
       }
       f3 fc = mk3(0, 0, 0);
       for (uint32_t k = 0; k < light_count; k++) {
@@ -1214,7 +1299,8 @@ static void resolve_colour(const lrt_scene_arrays* arrays, const ctx_t* cp, uint
     } break;
     case 11: case 21: { /* PBR_NO_TEX (material 0), PBR (COLORED) */
       const lrt_material* m = mode == 11 ? &materials[0] : &materials[MAT_ID()];
-      const f3 baseColor = mk3(m->base_color[0], m->base_color[1], m->base_color[2]);
+      MAT_COLOUR(m);
+      const f3 baseColor = mk3(mc[0], mc[1], mc[2]);
       const float metallic = m->metallic, roughness = m->roughness;
       const float alpha = roughness * roughness, f0 = 0.04f;
       const f3 surf = add3(rayPos, scl3(h.t, rayDir));
@@ -1261,7 +1347,8 @@ static void resolve_colour(const lrt_scene_arrays* arrays, const ctx_t* cp, uint
         color = mk3(roundf(h.coords[0]) / 255.0f, h.coords[0] - floorf(h.coords[0]), roundf(h.coords[1]) / 255.0f);
       else {
         const lrt_material* m = &materials[MAT_ID()];
-        color = mk3(m->base_color[0], m->base_color[1], m->base_color[2]);
+        MAT_COLOUR(m);
+        color = mk3(mc[0], mc[1], mc[2]);
       }
       f3 fc = mk3(0, 0, 0);
       for (uint32_t k = 0; k < light_count; k++) {
@@ -1294,6 +1381,7 @@ static void resolve_colour(const lrt_scene_arrays* arrays, const ctx_t* cp, uint
     default: break;
     }
 #undef MAT_ID
+#undef MAT_COLOUR
     out[0] = res[0];
     out[1] = res[1];
     out[2] = res[2];

@@ -108,7 +108,8 @@ def ref_lib(fast=False, dropin=False):
             lib.lrtd_trace_batch.argtypes = [vp, vp, vp, u64]
         lib.lrtr_renderer_create.restype = vp
         for fn, args in (("lrtr_renderer_create", [vp]), ("lrtr_renderer_destroy", [vp]),
-                         ("lrtr_renderer_add_mesh", [vp, u32, vp, u64, vp, u64]),
+                         ("lrtr_renderer_add_mesh", [vp, u32, vp, u64, vp, u64, vp]),
+                         ("lrtr_renderer_add_texture", [vp, u32, u32, vp]),
                          ("lrtr_renderer_set_preset", [vp, C.POINTER(Preset)]),
                          ("lrtr_renderer_set_camera_inverse", [vp, vp, vp]),
                          ("lrtr_renderer_look_at", [vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float]),
@@ -117,9 +118,13 @@ def ref_lib(fast=False, dropin=False):
                          ("lrtr_renderer_set_frame", [vp, u32]), ("lrtr_renderer_eye_rays", [vp, u32, u32, u32, vp]),
                          ("lrtr_renderer_render", [vp, u32, u32, vp]),
                          ("lrtr_renderer_fill_transparency", [vp, u32, u32, u32, vp, vp])):
+            if not hasattr(lib, fn):  # a checker library built before the entry point existed
+                continue
             getattr(lib, fn).argtypes = args
-            if fn != "lrtr_renderer_create":
+            if fn not in ("lrtr_renderer_create", "lrtr_renderer_add_texture"):
                 getattr(lib, fn).restype = None
+        if hasattr(lib, "lrtr_renderer_add_texture"):
+            lib.lrtr_renderer_add_texture.restype = u32
         _refs[key] = lib
     return _refs[key]
 
@@ -246,12 +251,21 @@ class RefRenderer:
         except Exception:
             pass
 
-    def add_mesh(self, geom_id, verts, tris):
+    def add_mesh(self, geom_id, verts, tris, texcoords=None):
         """MultiRenderer::add_mesh_internal: the mesh copy the resolve reads
-        triangle normals from (positions only; no normals or texture coords)."""
+        triangle normals and texture coordinates from (no vertex normals)."""
         v = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
         t = np.ascontiguousarray(tris, np.uint32).reshape(-1)
-        self.lib.lrtr_renderer_add_mesh(self.h, geom_id, v.ctypes.data, len(v), t.ctypes.data, len(t))
+        tc = None if texcoords is None else np.ascontiguousarray(texcoords, np.float32).reshape(-1, 2)
+        assert tc is None or len(tc) == len(v)
+        self.lib.lrtr_renderer_add_mesh(self.h, geom_id, v.ctypes.data, len(v), t.ctypes.data, len(t),
+                                        tc.ctypes.data if tc is not None else None)
+
+    def add_texture(self, image):
+        """MultiRenderer::AddTexture of an (h, w, 4) float32 image; returns its slot (1, 2, ...: every
+        slot of a new renderer holds a 16x16 (0, 1, 1, 1) image, slot 0 keeps it)."""
+        img = np.ascontiguousarray(image, np.float32)
+        return self.lib.lrtr_renderer_add_texture(self.h, img.shape[1], img.shape[0], img.ctypes.data)
 
     def set_preset(self, preset):
         self.lib.lrtr_renderer_set_preset(self.h, C.byref(preset))
@@ -333,6 +347,30 @@ class DropInScene(RefScene):
         if st != 0:
             raise RuntimeError("RayQuery_NearestHitBatch failed with status %d" % st)
         return hits
+
+
+_port_textures = None
+
+
+def port_set_textures(images, vert_tc=None):
+    """The textures (a list of (h, w, 4) float32 images, slot k = images[k])
+    and the per-vertex texture coordinates ((nverts, 2), parallel to the
+    scene's vertPos; None: zeros) of the restated renderer's next calls."""
+    global _port_textures
+    lib = port_lib()
+    if not hasattr(lib, "_tex_bound"):
+        lib.lrto_set_textures.restype = None
+        lib.lrto_set_textures.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64]
+        lib._tex_bound = True
+    imgs = [np.ascontiguousarray(i, np.float32) for i in (images or [])]
+    dims = np.array([[i.shape[1], i.shape[0]] for i in imgs], np.uint32).reshape(-1)
+    offs = np.cumsum([0] + [i.shape[0] * i.shape[1] for i in imgs])[:-1].astype(np.uint64)
+    texels = np.concatenate([i.reshape(-1) for i in imgs]) if imgs else np.zeros(4, np.float32)
+    tc = None if vert_tc is None else np.ascontiguousarray(vert_tc, np.float32).reshape(-1, 2)
+    _port_textures = (texels, dims, offs, tc)  # kept alive for the C side
+    lib.lrto_set_textures(texels.ctypes.data, dims.ctypes.data if len(dims) else None,
+                          offs.ctypes.data if len(offs) else None, len(imgs),
+                          tc.ctypes.data if tc is not None else None, 0 if tc is None else len(tc))
 
 
 def port_render_lambert(arrays, rays, light, preset=None, threads=os.cpu_count()):

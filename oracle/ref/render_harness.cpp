@@ -38,13 +38,13 @@ public:
     m_preset = m_rt->m_preset;
   }
 
-  void add_mesh(uint32_t geom_id, const float* v3, uint64_t nv, const uint32_t* idx, uint64_t ni)
+  void add_mesh(uint32_t geom_id, const float* v3, uint64_t nv, const uint32_t* idx, uint64_t ni, const float* tc2)
   {
     cmesh4::SimpleMesh m(nv, ni);
     for (uint64_t i = 0; i < nv; i++) {
       m.vPos4f[i] = LiteMath::float4(v3[3 * i], v3[3 * i + 1], v3[3 * i + 2], 1.0f);
       m.vNorm4f[i] = LiteMath::float4(0, 0, 0, 0);
-      m.vTexCoord2f[i] = LiteMath::float2(0, 0);
+      m.vTexCoord2f[i] = tc2 ? LiteMath::float2(tc2[2 * i], tc2[2 * i + 1]) : LiteMath::float2(0, 0);
     }
     for (uint64_t i = 0; i < ni; i++) m.indices[i] = idx[i];
     m.matIndices.clear();
@@ -132,9 +132,18 @@ void* lrtr_renderer_create(void* scene)
 
 void lrtr_renderer_destroy(void* r) { delete static_cast<HarnessRenderer*>(r); }
 
-void lrtr_renderer_add_mesh(void* r, uint32_t geom_id, const float* v3, uint64_t nv, const uint32_t* idx, uint64_t ni)
+// add_mesh_internal's copy of a mesh; tc2: 2 texture coordinates per vertex (NULL: zeros)
+void lrtr_renderer_add_mesh(void* r, uint32_t geom_id, const float* v3, uint64_t nv, const uint32_t* idx, uint64_t ni,
+                            const float* tc2)
 {
-  static_cast<HarnessRenderer*>(r)->add_mesh(geom_id, v3, nv, idx, ni);
+  static_cast<HarnessRenderer*>(r)->add_mesh(geom_id, v3, nv, idx, ni, tc2);
+}
+
+// MultiRenderer::AddTexture of a w x h float4 image (row-major); returns its slot
+uint32_t lrtr_renderer_add_texture(void* r, uint32_t w, uint32_t h, const float* rgba)
+{
+  LiteImage::Image2D<LiteMath::float4> img(w, h, reinterpret_cast<const LiteMath::float4*>(rgba));
+  return static_cast<HarnessRenderer*>(r)->AddTexture(img);
 }
 
 void lrtr_renderer_set_preset(void* r, const lrt_preset* p)

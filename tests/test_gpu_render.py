@@ -88,18 +88,18 @@ def test_render_rgba8_refusals(cuda):
         with pytest.raises(LrtError) as e:
             sc.render_rgba8(cam, _lights(), (0, 0, 0, 1), img.data_ptr())
         assert e.value.status == 1 and "material range" in str(e.value)
-    mats, ids, offs = transparency_tables(4)  # has transparent and textured materials
+    mats, ids, offs = transparency_tables(4)  # has transparent and textured materials, no texture is set
     sc.set_materials(mats, ids, offs)
     p.render_mode = 17
     sc.SetPreset(p)
     with pytest.raises(LrtError) as e:
         sc.render_rgba8(cam, _lights(), (0, 0, 0, 1), img.data_ptr())
-    assert e.value.status == 6
-    mats["base_color"][:, 3] = 1.0  # opaque, but one is textured
+    assert e.value.status == 1 and "texture" in str(e.value)
+    mats["base_color"][:, 3] = 1.0  # opaque, but one is textured and no texture is set
     sc.set_materials(mats, ids, offs)
     with pytest.raises(LrtError) as e:
         sc.render_rgba8(cam, _lights(), (0, 0, 0, 1), img.data_ptr())
-    assert e.value.status == 6 and "textured" in str(e.value)
+    assert e.value.status == 1 and "texture" in str(e.value)
     assert (mats["type"] == MATERIAL_TEXTURED).any()
 
 
@@ -312,3 +312,116 @@ def _preset_mode(p, mode):
     q = parity_preset()
     q.render_mode, q.spp, q.ray_gen_mode = mode, p.spp, p.ray_gen_mode
     return q
+
+
+def _textured_scene():
+    """The mixed scene with spherical texture coordinates on its mesh, the
+    textures of tests/test_ref_renderer.py and half the materials TEXTURED."""
+    from test_ref_renderer import _textured_materials, _textures, mesh_texcoords
+    sph = wl.spheres(32, seed=4)
+    sc = SceneRT()
+    v, t = wl.noisy_sphere(60, seed=2)
+    gm = sc.AddGeom_Triangles3f(v, t)
+    go = sc.AddGeom_SdfFrameOctree(wl.frame_octree_from_spheres(sph, 6))
+    gs = sc.AddGeom_SdfSVS(wl.svs_from_spheres(sph, 6))
+    hdr, nodes, vals, vf = wl.sbs_from_spheres(sph, grid_res=64)
+    gb = sc.AddGeom_SdfSBS(hdr, nodes, vals, vf)
+    for i, m in enumerate(wl.random_instances(40, seed=7, scale=(0.1, 0.4), trans=1.5)):
+        sc.AddInstance([gm, go, gs, gb][i % 4], m)
+    sc.CommitScene()
+    tc = mesh_texcoords(v)
+    sc.set_texcoords(gm, tc)
+    texs = _textures()
+    sc.set_textures(texs)
+    a = sc.export_arrays()
+    vert_tc = np.zeros((len(a["vertPos"]), 2), np.float32)
+    off = int(a["geomData"]["offset"][gm][1])
+    vert_tc[off:off + len(v)] = tc
+    mats, ids, offs = _textured_materials()
+    return sc, a, texs, vert_tc, (mats, ids, offs)
+
+
+@pytest.mark.parametrize("mode", [15, 16, 17, 18, 21, 11])
+def test_render_textured_materials_match_oracle(cuda, mode):
+    """TEXTURED materials (bilinear, clamped sampling at the hit's texture
+    coordinates) in DIFFUSE, LAMBERT, PHONG, PBR and PBR_NO_TEX, and the
+    TEX_COORDS mode: the images equal the oracle's restatement, which
+    equals the reference's own renderer (tests/test_ref_renderer.py); Phong
+    and PBR within one 8-bit step (CUDA's pow)."""
+    torch = cuda
+    from graphic_lab_task_b200 import MATERIAL_TEXTURED
+    sc, a, texs, vert_tc, (mats, ids, offs) = _textured_scene()
+    if mode == 11:
+        mats["type"][0] = MATERIAL_TEXTURED
+        mats["texId"][0] = 2
+    sc.set_materials(mats, ids, offs)
+    p = parity_preset()
+    p.render_mode = mode
+    sc.SetPreset(p)
+    cam = wl.camera((0.5, 0.7, 3.5), width=160, height=120)
+    bg = (0.1, 0.2, 0.3, 1.0)
+    img = torch.zeros(cam.width * cam.height, dtype=torch.int32, device="cuda")
+    sc.render_rgba8(cam, _lights(), bg, img.data_ptr())
+    sc.sync()
+    got = img.cpu().numpy().view(np.uint32)
+    po.port_set_textures(texs, vert_tc)
+    want = po.port_render_rgba8(a, wl.eye_rays_host(cam), _lights(), bg, preset=p, materials=mats, mat_ids=ids,
+                                mat_offsets=offs)
+    po.port_set_textures(None)
+    if mode in (11, 18, 21):
+        d = np.abs(got.view(np.uint8).astype(int) - want.view(np.uint8).astype(int))
+        assert d.max() <= 1 and (d > 0).mean() < 0.01
+    else:
+        assert np.array_equal(got, want), "%d of %d pixels differ" % ((got != want).sum(), len(got))
+    assert len(np.unique(got)) > 50
+
+
+def test_render_textured_samples_and_transparency_match_oracle(cuda):
+    """Four samples per pixel with a transparent COLORED material beside the
+    TEXTURED ones (LAMBERT takes the AnyHit path; the resolve samples the
+    textures of the last hit's material)."""
+    torch = cuda
+    sc, a, texs, vert_tc, (mats, ids, offs) = _textured_scene()
+    mats["base_color"][0, 3] = 0.4
+    sc.set_materials(mats, ids, offs)
+    p = parity_preset()
+    p.render_mode, p.spp = 17, 4
+    sc.SetPreset(p)
+    cam = wl.camera((0.5, 0.7, 3.5), width=96, height=64)
+    bg = (0.1, 0.2, 0.3, 1.0)
+    img = torch.zeros(cam.width * cam.height, dtype=torch.int32, device="cuda")
+    sc.render_rgba8(cam, _lights(), bg, img.data_ptr())
+    sc.sync()
+    got = img.cpu().numpy().view(np.uint32)
+    sample_rays = np.stack([wl.eye_rays_host(cam, *wl.sample_offset(k, 4, 0)) for k in range(4)])
+    po.port_set_textures(texs, vert_tc)
+    want = po.port_render_rgba8_samples(a, sample_rays, sample_rays[0], _lights(), bg, p, materials=mats,
+                                        mat_ids=ids, mat_offsets=offs, transparency=True)
+    po.port_set_textures(None)
+    assert np.array_equal(got, want), "%d of %d pixels differ" % ((got != want).sum(), len(got))
+
+
+def test_texture_api_refusals(cuda):
+    from graphic_lab_task_b200 import MATERIAL_TEXTURED
+    sc, a, texs, vert_tc, (mats, ids, offs) = _textured_scene()
+    bad = mats.copy()
+    bad["type"][0] = MATERIAL_TEXTURED
+    bad["texId"][0] = 3  # three textures are set
+    sc.set_materials(bad, ids, offs)
+    p = parity_preset()
+    p.render_mode = 17
+    sc.SetPreset(p)
+    torch = cuda
+    img = torch.zeros(64, dtype=torch.int32, device="cuda")
+    with pytest.raises(LrtError) as e:
+        sc.render_rgba8(wl.camera((0.5, 0.7, 3.5), width=8, height=8), _lights(), (0, 0, 0, 1), img.data_ptr())
+    assert e.value.status == 1 and "texture 3 of 3" in str(e.value)
+    with pytest.raises(LrtError) as e:
+        sc.set_texcoords(0, np.zeros((5, 2), np.float32))  # not the mesh's vertex count
+    assert e.value.status == 1 and "vertices" in str(e.value)
+    with pytest.raises(LrtError) as e:
+        sc.set_texcoords(1, np.zeros((5, 2), np.float32))  # the frame octree
+    assert e.value.status == 1 and "not a triangle mesh" in str(e.value)
+    with pytest.raises(LrtError) as e:
+        sc.set_textures([np.zeros((0, 4, 4), np.float32)])
+    assert e.value.status == 1

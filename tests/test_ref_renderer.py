@@ -168,3 +168,111 @@ def test_fill_gbuffer_transparency_equals_reference_any_hit(mixed):
     assert same.all(), "%d of %d pixels differ" % ((~same).sum(), len(same))
     assert (want_t[:, 3] < 0.99).sum() > 500
     r.close()
+
+
+def _textures(seed=5):
+    """Slot 0 as a new MultiRenderer holds it (16x16 of (0, 1, 1, 1)), then a
+    seeded random 37x23 image and a 64x64 checker."""
+    rng = np.random.default_rng(seed)
+    default = np.zeros((16, 16, 4), np.float32)
+    default[:] = (0, 1, 1, 1)
+    noise = rng.uniform(0, 1, size=(23, 37, 4)).astype(np.float32)
+    yy, xx = np.mgrid[0:64, 0:64]
+    checker = np.zeros((64, 64, 4), np.float32)
+    checker[..., 0] = ((xx // 8 + yy // 8) % 2).astype(np.float32)
+    checker[..., 1] = 0.3
+    checker[..., 2] = xx / 63.0
+    checker[..., 3] = 1
+    return [default, noise, checker]
+
+
+def mesh_texcoords(verts):
+    """Seeded-free spherical texture coordinates of a mesh around the origin,
+    beyond [0, 1] in places (the sampler clamps)."""
+    v = np.asarray(verts, np.float64)
+    u = np.arctan2(v[:, 2], v[:, 0]) / (2 * np.pi) + 0.5
+    w = np.arccos(np.clip(v[:, 1] / np.linalg.norm(v, axis=1), -1, 1)) / np.pi
+    return np.stack([1.3 * u - 0.15, w], axis=1).astype(np.float32)
+
+
+def _textured_materials():
+    from graphic_lab_task_b200 import MATERIAL_TEXTURED
+    mats, ids, offs = _materials(13)
+    mats["type"][1::2] = MATERIAL_TEXTURED
+    mats["texId"] = np.arange(len(mats)) % 3
+    return mats, ids, offs
+
+
+@pytest.mark.parametrize("mode", [15, 16, 17, 18, 21, 11])
+def test_textured_materials_equal_reference_render(mixed, mode):
+    """TEXTURED materials in DIFFUSE, LAMBERT, PHONG and PBR (PBR_NO_TEX with
+    a textured material 0) and the TEX_COORDS mode: the reference's
+    bilinear / clamp sampling at loadNormalTcFromGbuffer's coordinates
+    (barycentric blend of the mesh's per-vertex coordinates, the hit's coords
+    for SDF leaves), restated bit for bit."""
+    from graphic_lab_task_b200 import MATERIAL_TEXTURED
+    cam = _camera(160, 120)
+    p = parity_preset()
+    p.render_mode = mode
+    mats, ids, offs = _textured_materials()
+    if mode == 11:
+        mats["type"][0] = MATERIAL_TEXTURED
+        mats["texId"][0] = 2
+    gm, v, t = mixed["mesh"]
+    tc = mesh_texcoords(v)
+    r = po.RefRenderer(mixed["ref"])
+    r.add_mesh(gm, v, t, tc)
+    texs = _textures()
+    assert [r.add_texture(x) for x in texs[1:]] == [1, 2]
+    r.set_camera(cam)
+    r.set_lights(_lights())
+    r.set_background(BG)
+    r.set_preset(p)
+    r.set_materials(mats, ids, offs)
+    want = r.render(cam.width, cam.height)
+    a = mixed["arrays"]
+    vert_tc = np.zeros((len(a["vertPos"]), 2), np.float32)
+    off = int(a["geomData"]["offset"][gm][1])
+    vert_tc[off:off + len(v)] = tc
+    po.port_set_textures(texs, vert_tc)
+    got = po.port_render_rgba8(a, wl.eye_rays_host(cam), _lights(), BG, preset=p, materials=mats, mat_ids=ids,
+                               mat_offsets=offs)
+    po.port_set_textures(None)
+    assert np.array_equal(got, want), "%d of %d pixels differ" % ((got != want).sum(), len(got))
+    assert len(np.unique(want)) > 50
+    r.close()
+
+
+def test_textured_samples_and_transparency_equal_reference_render(mixed):
+    """Four samples per pixel, LAMBERT, a transparent COLORED material beside
+    the TEXTURED ones: the AnyHit G-buffer (textured layers opaque black) and
+    the resolve's texture samples, blended as ResolveTransparency does."""
+    cam = _camera(96, 64)
+    p = parity_preset()
+    p.render_mode, p.spp = 17, 4
+    mats, ids, offs = _textured_materials()
+    mats["base_color"][0, 3] = 0.4
+    gm, v, t = mixed["mesh"]
+    tc = mesh_texcoords(v)
+    r = po.RefRenderer(mixed["ref"])
+    r.add_mesh(gm, v, t, tc)
+    texs = _textures()
+    for x in texs[1:]:
+        r.add_texture(x)
+    r.set_camera(cam)
+    r.set_lights(_lights())
+    r.set_background(BG)
+    r.set_preset(p)
+    r.set_materials(mats, ids, offs)
+    want = r.render(cam.width, cam.height)
+    a = mixed["arrays"]
+    vert_tc = np.zeros((len(a["vertPos"]), 2), np.float32)
+    off = int(a["geomData"]["offset"][gm][1])
+    vert_tc[off:off + len(v)] = tc
+    po.port_set_textures(texs, vert_tc)
+    sample_rays = np.stack([wl.eye_rays_host(cam, *wl.sample_offset(k, 4, 0)) for k in range(4)])
+    got = po.port_render_rgba8_samples(a, sample_rays, sample_rays[0], _lights(), BG, p, materials=mats, mat_ids=ids,
+                                       mat_offsets=offs, transparency=True)
+    po.port_set_textures(None)
+    assert np.array_equal(got, want), "%d of %d pixels differ" % ((got != want).sum(), len(got))
+    r.close()
