@@ -342,6 +342,8 @@ lrt_status lrt_sbs_update_values(lrt_scene* s, const float* values_f, uint64_t c
   // the pruned node pairs were derived from the old masks: trace the
   // unpruned pairs from now on
   d->S.pairs = d->pairsOrig;
+  d->pfCand[1] = {d->pairsOrig, d->pairsOrigBytes}; // the node-pair entry of the prefetch ranges
+  set_prefetch(d);
   return LRT_OK;
 }
 

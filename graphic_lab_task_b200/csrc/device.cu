@@ -141,6 +141,8 @@ lrt_status launch(lrt_scene* s, const float4* rays, lrt_hit* hits, uint64_t n, c
   DevScene S = d->S;
   S.flags = launch_flags(s);
   S.voxelStepCap = s->voxelStepCap ? s->voxelStepCap : kMaxVoxelSteps;
+  if (n < kPrefetchMinRays)
+    for (int r = 0; r < kPrefetchRanges; r++) S.pfBytes[r] = 0;
   const bool count = (flags & LRT_TRACE_COUNT_WORK) != 0;
   cudaError_t e = cudaMemsetAsync(&slot->work, 0, count ? offsetof(StreamSlot, err) : sizeof(unsigned long long),
                                   stream);
@@ -352,6 +354,19 @@ lrt_status device_upload(lrt_scene* s)
     }
   }
   d->sbsHost = sbs;
+  d->pairsOrigBytes = (h.sdfSBSNodes.empty() ? pairs.size() : h.allNodePairs.size()) * sizeof(lrt_bvh_node_pair);
+  // what a traversal reads per node, leaf, brick and voxel, most shared first
+  d->pfCand = {{S.tlas, h.nodesTLAS.size() * sizeof(lrt_bvh_node)},
+               {S.pairs, pairs.size() * sizeof(lrt_bvh_node_pair)},
+               {S.primIdCount, h.primIdCount.size() * sizeof(uint32_t)},
+               {S.sbsNodes, h.sdfSBSNodes.size() * sizeof(lrt_sdf_sbs_node)},
+               {S.sbsMask, mask.size() * sizeof(uint32_t)},
+               {S.triSoup, soup.size() * sizeof(float)},
+               {S.origNodes, h.origNodes.size() * sizeof(lrt_bvh_node)},
+               {S.frameOctreeNodes, h.sdfFrameOctreeNodes.size() * sizeof(lrt_sdf_frame_octree_node)},
+               {S.svsNodes, h.sdfSVSNodes.size() * sizeof(lrt_sdf_svs_node)},
+               {S.sbsDense, dense.size() * sizeof(float)}};
+  set_prefetch(d);
   d->pairsClean = boxes_clean(reinterpret_cast<const lrt_bvh_node*>(pairs.data()), 2 * pairs.size()) &&
                   boxes_clean(reinterpret_cast<const lrt_bvh_node*>(h.allNodePairs.data()), 2 * h.allNodePairs.size());
   d->cleanBoxes = d->pairsClean && boxes_clean(h.nodesTLAS.data(), h.nodesTLAS.size());
@@ -429,6 +444,25 @@ lrt_status device_update_instances(lrt_scene* s)
   if (st != LRT_OK) return st;
   d->cleanBoxes = d->pairsClean && boxes_clean(h.nodesTLAS.data(), h.nodesTLAS.size());
   return LRT_OK;
+}
+
+void set_prefetch(DeviceScene* d)
+{
+  DevScene& S = d->S;
+  uint64_t total = 0;
+  int k = 0;
+  for (int r = 0; r < kPrefetchRanges; r++) {
+    S.pfPtr[r] = nullptr;
+    S.pfBytes[r] = 0;
+  }
+  for (const auto& c : d->pfCand) {
+    const uint64_t bytes = c.second & ~uint64_t(15); // whole 16-byte granules (cudaMalloc bases are aligned)
+    if (!c.first || bytes == 0 || k == kPrefetchRanges || total + bytes > kPrefetchMaxBytes) continue;
+    S.pfPtr[k] = static_cast<const char*>(c.first);
+    S.pfBytes[k] = bytes;
+    total += bytes;
+    k++;
+  }
 }
 
 void device_release(lrt_scene* s)

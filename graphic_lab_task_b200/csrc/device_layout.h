@@ -117,6 +117,20 @@ struct DevSbs {
 
 typedef lrt_instance_data DevInstance;
 
+// L2 prefetch of small scenes.  A launch whose rays are few takes as long as
+// its slowest warp, a chain of dependent node, leaf and triangle loads; after
+// an L2 flush (another job, a large previous launch) each of those is a DRAM
+// round trip.  The trace kernel therefore streams the scene's node and leaf
+// arrays into L2 first (cp.async.bulk.prefetch.L2, spread over its CTAs, one
+// warp each), so that those chains run at L2 latency.  Ranges are taken in
+// order while their sum stays within kPrefetchMaxBytes (well inside the
+// 126 MB L2, leaving room for rays and hits); launches of fewer than
+// kPrefetchMinRays rays skip it.
+constexpr int kPrefetchRanges = 10;
+constexpr uint64_t kPrefetchMaxBytes = 48ull << 20;
+constexpr uint64_t kPrefetchMinRays = 4096;
+constexpr uint32_t kPrefetchChunk = 4096; // bytes per prefetch instruction
+
 struct DevScene {
   const lrt_bvh_node* tlas;
   const lrt_bvh_node_pair* pairs;
@@ -136,6 +150,10 @@ struct DevScene {
   const DevSbs* sbs;
   uint32_t flags;
   uint32_t voxelStepCap; // bounded SBS voxel march (kMaxVoxelSteps unless set)
+  // byte ranges streamed into L2 at the start of a trace launch (16-byte
+  // aligned bases, sizes multiples of 16; 0 bytes: none)
+  const char* pfPtr[kPrefetchRanges];
+  uint64_t pfBytes[kPrefetchRanges];
 };
 
 struct DevCamera {

@@ -49,6 +49,10 @@ struct DeviceScene {
   StreamSlot* slots = nullptr; // device, kMaxStreams
   std::map<cudaStream_t, int> slotOf;
   const lrt_bvh_node_pair* pairsOrig = nullptr; // unpruned node pairs (used once SBS values change)
+  uint64_t pairsOrigBytes = 0;
+  // the arrays a trace may stream into L2 (DevScene::pfPtr), in priority
+  // order, with their sizes; set_prefetch picks those that fit
+  std::vector<std::pair<const void*, uint64_t>> pfCand;
   std::vector<DevSbs> sbsHost;                  // host copy of the SBS model table
   bool cleanBoxes = false;                      // every node box has 0 or 6 NaN coordinates
   bool pairsClean = false;                      // the BLAS part of cleanBoxes
@@ -126,6 +130,9 @@ lrt_status sched_prepare(lrt_scene* s, cudaStream_t stream, uint32_t width, uint
                          const uint32_t** rd, uint32_t** wr);
 void sched_commit(lrt_scene* s, cudaStream_t stream, bool natural);
 uint32_t launch_flags(const lrt_scene* s); // preset flags + the uploaded scene's own
+// DevScene::pfPtr/pfBytes from d->pfCand: the candidates in order while
+// their sum stays within kPrefetchMaxBytes
+void set_prefetch(DeviceScene* d);
 lrt_status cuda_fail(lrt_scene* s, cudaError_t e, const char* what);
 
 } // namespace lrt

@@ -787,6 +787,28 @@ __device__ __forceinline__ uint32_t sched_next(const uint32_t* __restrict__ rd, 
 // order and a warp's 32 rays are an 8x4-pixel tile instead of 32 pixels of a
 // row (the reference's kernel1D_FillGbuffer also walks pixels in packed
 // tiles, MultiRenderer.cpp:185-202); each ray's hit is unchanged.
+// The L2 prefetch of a small scene (DevScene::pfPtr): CTA b of the grid
+// takes the b-th share of each range, in whole kPrefetchChunk pieces, and
+// its first warp issues one cp.async.bulk.prefetch.L2 per piece (no result,
+// no completion to wait for).  Bases are 16-byte aligned and sizes multiples
+// of 16, so every piece is too.
+__device__ __forceinline__ void l2_prefetch_scene(const DevScene& S)
+{
+  if (threadIdx.x >= 32) return;
+#pragma unroll 1
+  for (int r = 0; r < kPrefetchRanges; r++) {
+    const uint64_t bytes = S.pfBytes[r];
+    if (bytes == 0) continue;
+    const uint64_t per = (bytes + gridDim.x - 1) / gridDim.x;
+    const uint64_t share = (per + kPrefetchChunk - 1) / kPrefetchChunk * kPrefetchChunk;
+    const uint64_t lo = min(bytes, share * blockIdx.x), hi = min(bytes, lo + share);
+    for (uint64_t off = lo + uint64_t(threadIdx.x) * kPrefetchChunk; off < hi; off += 32ull * kPrefetchChunk) {
+      const uint32_t size = uint32_t(min(uint64_t(kPrefetchChunk), hi - off));
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(S.pfPtr[r] + off), "r"(size) : "memory");
+    }
+  }
+}
+
 template <bool COUNT, bool SOLVERS, bool IMG>
 __global__ void __launch_bounds__(kTraceThreads, 7) k_trace(DevScene S, const float4* __restrict__ rays,
                                                          lrt_hit* __restrict__ hits, uint64_t n,
@@ -806,6 +828,7 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_trace(DevScene S, const fl
     wclock[threadIdx.x >> 5].tile = ~0u;
     wclock[threadIdx.x >> 5].longest = 0;
   }
+  l2_prefetch_scene(S);
   for (;;) {
     unsigned long long base = 0;
     if (IMG) { // work counter in tiles
@@ -1282,6 +1305,7 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_trace_cameras(DevScene S, 
                                                                  uint32_t* __restrict__ image)
 {
   extern __shared__ uint32_t smem_stack[];
+  l2_prefetch_scene(S);
   uint32_t* stack = smem_stack + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
   Ctx<false> c(S, normal_words(smem_stack, shape.stackCap));
@@ -1381,6 +1405,7 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_render_rgba8(DevScene S, D
                                                                 uint32_t* sched_wr, DevMaterials M, DevRenderModes RM)
 {
   extern __shared__ uint32_t smem_stack[];
+  l2_prefetch_scene(S);
   uint32_t* stack = smem_stack + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
   Ctx<false> c(S, normal_words(smem_stack, stack_cap));
@@ -1461,6 +1486,7 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_outline_fill(DevScene S, D
                                                                 uint32_t* sched_wr)
 {
   extern __shared__ uint32_t smem_stack[];
+  l2_prefetch_scene(S);
   uint32_t* stack = smem_stack + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
   Ctx<false> c(S, normal_words(smem_stack, stack_cap));
@@ -1542,6 +1568,7 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_fill_gbuffer_transparency(
     const uint32_t* __restrict__ sched_rd, uint32_t* sched_wr)
 {
   extern __shared__ uint32_t smem_stack[];
+  l2_prefetch_scene(S);
   uint32_t* stack = smem_stack + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
   Ctx<false> c(S, normal_words(smem_stack, stack_cap));
@@ -1619,6 +1646,7 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_render_lambert(DevScene S,
                                                                   uint32_t* sched_wr)
 {
   extern __shared__ uint32_t smem_stack[];
+  l2_prefetch_scene(S);
   uint32_t* stack = smem_stack + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
   __shared__ WarpClock wclock[IMG ? kTraceThreads / 32 : 1];
@@ -1664,6 +1692,7 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_adjoint_lambert(DevScene S
                                                                    uint32_t* sched_wr)
 {
   extern __shared__ uint32_t smem_stack[];
+  l2_prefetch_scene(S);
   uint32_t* stack = smem_stack + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31;
   __shared__ WarpClock wclock[IMG ? kTraceThreads / 32 : 1];
