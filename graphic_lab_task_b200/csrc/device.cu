@@ -147,8 +147,17 @@ lrt_status launch(lrt_scene* s, const float4* rays, lrt_hit* hits, uint64_t n, c
   cudaError_t e = cudaMemsetAsync(&slot->work, 0, count ? offsetof(StreamSlot, err) : sizeof(unsigned long long),
                                   stream);
   if (e != cudaSuccess) return cuda_fail(s, e, "cudaMemsetAsync");
+  // Row order: rays to a warp.  A launch of fewer rays than one wave of the
+  // kernel's warps can hold takes as long as its slowest warp, and a warp's
+  // time grows with the number of slow rays among its lanes, so such a launch
+  // gives each warp 16 or 8 rays while the warps still fit in one wave.
+  uint32_t group = 32;
+  if (!img_w) {
+    const uint64_t slots = uint64_t(d->grid) * (kTraceThreads / 32);
+    while (group > 8 && (n + group / 2 - 1) / (group / 2) <= slots) group /= 2;
+  }
   const uint64_t warps = img_w ? uint64_t((img_w + kImgTileW - 1) / kImgTileW) * ((img_h + kImgTileH - 1) / kImgTileH)
-                               : (n + 31) / 32;
+                               : (n + group - 1) / group;
   const int grid = int(std::min<uint64_t>(uint64_t(d->grid), (warps * 32 + kTraceThreads - 1) / kTraceThreads));
   const bool natural = !img_w || count || (flags & LRT_TRACE_NATURAL_ORDER);
   const uint32_t* rd = nullptr;
@@ -157,10 +166,10 @@ lrt_status launch(lrt_scene* s, const float4* rays, lrt_hit* hits, uint64_t n, c
   if (st != LRT_OK) return st;
   if (flags & LRT_TRACE_FAST_MATH)
     e = lrt_fast::launch_trace(S, rays, hits, n, &slot->work, slot->counters, err, d->stackCap, grid, stream, count,
-                               img_w, img_h, rd, wr);
+                               img_w, img_h, rd, wr, group);
   else
     e = lrt_exact::launch_trace(S, rays, hits, n, &slot->work, slot->counters, err, d->stackCap, grid, stream,
-                                count, img_w, img_h, rd, wr);
+                                count, img_w, img_h, rd, wr, group);
   if (e != cudaSuccess) return cuda_fail(s, e, "trace launch");
   sched_commit(s, stream, natural);
   return LRT_OK;

@@ -816,7 +816,8 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_trace(DevScene S, const fl
                                                          unsigned long long* __restrict__ counters,
                                                          uint32_t* __restrict__ err_word, uint32_t stack_cap,
                                                          uint32_t img_w, uint32_t img_h,
-                                                         const uint32_t* __restrict__ sched_rd, uint32_t* sched_wr)
+                                                         const uint32_t* __restrict__ sched_rd, uint32_t* sched_wr,
+                                                         uint32_t group)
 {
   extern __shared__ uint32_t smem_stack[];
   uint32_t* stack = smem_stack + threadIdx.x;
@@ -840,13 +841,13 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_trace(DevScene S, const fl
       tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
       if (tile == ~0u) break;
       base = uint64_t(tile) * 32;
-    } else { // in rays
-      if (lane == 0) base = atomicAdd(work_counter, 32ull);
+    } else { // in rays, `group` (32, 16 or 8) to a warp
+      if (lane == 0) base = atomicAdd(work_counter, (unsigned long long)group);
       base = __shfl_sync(0xFFFFFFFFu, base, 0);
       if (base >= n) break;
     }
     uint64_t i = base + lane;
-    bool valid = i < n;
+    bool valid = i < n && (IMG || lane < group);
     if (IMG) {
       const uint64_t b = base >> 5;
       const uint32_t x = uint32_t(b % tilesX) * kImgTileW + (lane % kImgTileW);
@@ -1865,7 +1866,7 @@ __global__ void k_eye_rays(DevCamera cam, float4* __restrict__ rays)
 cudaError_t launch_trace(const DevScene& S, const float4* rays, lrt_hit* hits, uint64_t n,
                                 unsigned long long* work_counter, unsigned long long* counters, uint32_t* err_word,
                                 uint32_t stack_cap, int grid, cudaStream_t stream, bool count, uint32_t img_w,
-                                uint32_t img_h, const uint32_t* sched_rd, uint32_t* sched_wr)
+                                uint32_t img_h, const uint32_t* sched_rd, uint32_t* sched_wr, uint32_t group)
 {
   const size_t smem = trace_smem_bytes(stack_cap);
   // the ANALYTIC / NEWTON / IT node solvers live in their own instantiation,
@@ -1876,7 +1877,7 @@ cudaError_t launch_trace(const DevScene& S, const float4* rays, lrt_hit* hits, u
   // costs the row-order kernel nothing
   auto go = [&](auto kernel) {
     kernel<<<grid, kTraceThreads, smem, stream>>>(S, rays, hits, n, work_counter, counters, err_word, stack_cap, img_w,
-                                                  img_h, sched_rd, sched_wr);
+                                                  img_h, sched_rd, sched_wr, group);
   };
   if (img_w) {
     if (count && solvers) go(k_trace<true, true, true>);
