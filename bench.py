@@ -939,6 +939,9 @@ def profile_case(args):
       adjoint  lrt_adjoint_lambert_sbs_image + forward, 4 views of 512^2, SBS 256^3
       bounce   lrt_generate_bounce_rays_sorted + the bounce trace, the
                1024-instance scene at 2048^2
+      mesh     lrt_trace_nearest on the 200k-triangle mesh at 256^2 (the
+               workload of config 0, whole: 16 MB of scene, 2 + 2 MB of rays
+               and hits)
     Prints one JSON line with the mean device time per launch (CUDA events)."""
     import torch
     from graphic_lab_task_b200 import LIGHT_AMBIENT, LIGHT_DIRECT, LIGHT_DTYPE, SceneRT, workloads as wl
@@ -1024,6 +1027,18 @@ def profile_case(args):
         out["ms"] = timed(lambda: sc.trace_device(B.data_ptr(), HB.data_ptr(), nb, stream=sp))
         out["rays"], out["bounce_rays"] = n, nb
         sc.sync(stream=sp)
+    elif args.case == "mesh":
+        v, t = wl.noisy_sphere(317, seed=0)
+        sc = SceneRT()
+        sc.AddInstance(sc.AddGeom_Triangles3f(v, t), wl.IDENTITY)
+        sc.CommitScene()
+        rays = wl.eye_rays_host(wl.camera((0, 0, 3), width=256, height=256))
+        n = len(rays)
+        R = torch.from_numpy(rays).to(dev)
+        H = torch.empty(n * 8, dtype=torch.float32, device=dev)
+        out["ms"] = timed(lambda: sc.trace_device(R.data_ptr(), H.data_ptr(), n, stream=sp))
+        out["rays"] = n
+        sc.sync(stream=sp)
     else:
         raise SystemExit("unknown --case %s" % args.case)
     print(json.dumps(out))
@@ -1040,7 +1055,7 @@ def main():
     ap.add_argument("--configs", action="store_true",
                     help="measure every benchmark configuration (GPU and reference CPU), one JSON line each")
     ap.add_argument("--only", default="0,1,2,3,4", help="with --configs: the configurations to measure")
-    ap.add_argument("--case", default=None, help="render | batched | adjoint | bounce: one small kernel case "
+    ap.add_argument("--case", default=None, help="render | batched | adjoint | bounce | mesh: one small kernel case "
                                                   "for profiling (see profile_case)")
     args = ap.parse_args()
     if args.case:
