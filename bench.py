@@ -942,6 +942,9 @@ def profile_case(args):
       mesh     lrt_trace_nearest on the 200k-triangle mesh at 256^2 (the
                workload of config 0, whole: 16 MB of scene, 2 + 2 MB of rays
                and hits)
+      lbvh     AddGeom_Triangles3f(BUILD_LOW) of a 501k-triangle mesh: the
+               device tree build and pair emission (host-timed per build,
+               "ms"; the SAH build of the same mesh beside it, "sah_ms")
     Prints one JSON line with the mean device time per launch (CUDA events)."""
     import torch
     from graphic_lab_task_b200 import LIGHT_AMBIENT, LIGHT_DIRECT, LIGHT_DTYPE, SceneRT, workloads as wl
@@ -1027,6 +1030,25 @@ def profile_case(args):
         out["ms"] = timed(lambda: sc.trace_device(B.data_ptr(), HB.data_ptr(), nb, stream=sp))
         out["rays"], out["bounce_rays"] = n, nb
         sc.sync(stream=sp)
+    elif args.case == "lbvh":
+        import time as _time
+        from graphic_lab_task_b200 import BUILD_HIGH, BUILD_LOW
+        v, t = wl.noisy_sphere(wl.segments_for_triangles(500000), seed=500000)
+
+        def build(flags, reps):
+            best = float("inf")
+            for _ in range(reps):
+                sc = SceneRT()
+                t0 = _time.perf_counter()
+                sc.AddGeom_Triangles3f(v, t, flags=flags)
+                best = min(best, _time.perf_counter() - t0)
+                sc.close()
+            return 1e3 * best
+
+        build(BUILD_LOW, args.warmup)
+        out["ms"] = build(BUILD_LOW, args.steps)
+        out["sah_ms"] = build(BUILD_HIGH, 1)
+        out["triangles"] = len(t)
     elif args.case == "mesh":
         v, t = wl.noisy_sphere(317, seed=0)
         sc = SceneRT()
@@ -1055,7 +1077,7 @@ def main():
     ap.add_argument("--configs", action="store_true",
                     help="measure every benchmark configuration (GPU and reference CPU), one JSON line each")
     ap.add_argument("--only", default="0,1,2,3,4", help="with --configs: the configurations to measure")
-    ap.add_argument("--case", default=None, help="render | batched | adjoint | bounce | mesh: one small kernel case "
+    ap.add_argument("--case", default=None, help="render | batched | adjoint | bounce | mesh | lbvh: one small kernel case "
                                                   "for profiling (see profile_case)")
     args = ap.parse_args()
     if args.case:

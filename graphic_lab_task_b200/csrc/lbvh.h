@@ -22,4 +22,20 @@ struct LbvhInner {
 // n == 1).  Returns nullptr on success, else a message.
 const char* lbvh_build(const float* boxes6, uint32_t n, std::vector<uint32_t>& order, std::vector<LbvhInner>& inner);
 
+// One BLAS node pair as the reference stores it (BVHNodePair, cbvh.h:21-33):
+// per child {boxMin.xyz, leftOffset, boxMax.xyz, escapeIndex}.
+struct LbvhPairOut {
+  float node[2][8];
+};
+
+// Builds the tree as lbvh_build does and emits a triangle BLAS from it on the
+// device, exactly as the host emitter would from the same tree with inner
+// nodes of at most maxLeaf boxes collapsed into leaves: `pairs` (relative
+// child indices), the leaf table entries Pack(start, count) in leaf-id order
+// (`startCount`) and the box order of the leaves (`order`: position ->
+// box).  Needs n > maxLeaf (a root that is one leaf has no pairs to emit).
+// Returns nullptr on success, else a message.
+const char* lbvh_build_blas(const float* boxes6, uint32_t n, uint32_t maxLeaf, std::vector<LbvhPairOut>& pairs,
+                            std::vector<uint32_t>& startCount, std::vector<uint32_t>& order);
+
 } // namespace lrt

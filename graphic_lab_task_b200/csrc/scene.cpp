@@ -883,14 +883,31 @@ lrt_status lrt_add_geom_triangles3f(lrt_scene* s, const float* vpos, size_t nver
     });
   };
   if (flags & LRT_BUILD_LOW) {
-    RadixTree R;
-    if (const char* err = R.build(boxes, s->primsInLeaf)) {
+    // the device builds the tree and, when the root is not a single leaf,
+    // also emits the pairs, leaf table and triangle order (lbvh_build_blas:
+    // the arrays the host emitter makes from the same tree)
+    const char* err = nullptr;
+    if (nt > s->primsInLeaf) {
+      std::vector<LbvhPairOut> dp;
+      err = lbvh_build_blas(reinterpret_cast<const float*>(boxes.data()), uint32_t(nt), s->primsInLeaf, dp,
+                            startCount, reordered);
+      if (!err) {
+        static_assert(sizeof(LbvhPairOut) == sizeof(lrt_bvh_node_pair), "a pair is 64 bytes");
+        const size_t base = h.allNodePairs.size();
+        h.allNodePairs.resize(base + dp.size());
+        std::memcpy(h.allNodePairs.data() + base, dp.data(), dp.size() * sizeof(lrt_bvh_node_pair));
+      }
+    } else {
+      RadixTree R;
+      err = R.build(boxes, s->primsInLeaf);
+      if (!err) emit(R);
+    }
+    if (err) {
       h.vertPos.resize(4 * oldV);
       h.geomData.pop_back();
       h.geomTags.pop_back();
       return fail(s, LRT_ERR_CUDA, "AddGeom_Triangles3f (BUILD_LOW): %s", err);
     }
-    emit(R);
   } else {
     SahBuilder B(boxes, s->primsInLeaf);
     B.build(0, uint32_t(nt));

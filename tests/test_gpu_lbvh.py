@@ -40,6 +40,39 @@ def test_device_blas_layout_and_oracle_parity(cuda, build_name):
     assert (got["primId"] != MISS).mean() > 0.2
 
 
+def _coincident_mesh():
+    """A small sphere plus 600 copies of one triangle and 300 of another:
+    long runs of equal Morton codes, told apart by their sorted positions."""
+    v, t = wl.noisy_sphere(24, seed=3)
+    n = len(v)
+    extra_v = np.array([[0.1, 0.1, 0.1], [0.2, 0.1, 0.1], [0.1, 0.2, 0.1], [-0.5, 0.3, 0.0], [-0.4, 0.3, 0.0],
+                        [-0.5, 0.4, 0.0]], np.float32)
+    extra_t = np.array([[n, n + 1, n + 2]] * 600 + [[n + 3, n + 4, n + 5]] * 300, np.uint32)
+    return np.concatenate([v, extra_v]), np.concatenate([t, extra_t])
+
+
+@pytest.mark.parametrize("build_name,cap", [(None, 2), ("cbvh_embree1", 1), ("cbvh_embree4", 4), ("cbvh_embree7", 7)])
+@pytest.mark.parametrize("mesh", ["sphere", "coincident"])
+def test_device_emission_equals_the_host_emitter(cuda, build_name, cap, mesh):
+    """The triangle BLAS the device emits (pairs with their boxes, child and
+    escape words; the leaf table; the triangle order) equals, bit for bit,
+    the host emitter's layout of the same tree, modelled on the CPU from the
+    same float32 Morton codes (tests/lbvh_model.py)."""
+    import lbvh_model
+    v, t = wl.noisy_sphere(40, seed=11) if mesh == "sphere" else _coincident_mesh()
+    sc = _mesh_scene(v, t, BUILD_LOW, build_name)
+    a = sc.export_arrays()
+    pairs, table, order = lbvh_model.blas(v, t, cap)
+    base = int(a["geomData"]["bvhOffset"][0])
+    got = np.frombuffer(a["allNodePairs"].tobytes(), np.uint32).reshape(-1, 16)
+    assert len(got) - base == len(pairs)
+    assert np.array_equal(got[base:], pairs.view(np.uint32).reshape(-1, 16))
+    a0, a1 = int(a["startEnd"][0][0]), int(a["startEnd"][0][1])
+    assert np.array_equal(np.asarray(a["primIdCount"][a0:a1], np.uint32), table)
+    assert np.array_equal(np.asarray(a["primIndices"][:len(order)], np.uint32), order)
+    check_blas_layout(a, 0)
+
+
 def test_device_and_sah_trees_give_the_same_triangle_hits(cuda):
     """Nearest triangle hits are a property of the mesh, not of the tree:
     every ray gets the same t from both builders; ids and coordinates differ

@@ -65,6 +65,27 @@ def _oracle_check(sc, rays):
     return got
 
 
+@pytest.mark.parametrize("n", [20000, 40000, 140000])
+def test_row_order_ray_groups_match_oracle(cuda, n):
+    """lrt_trace_nearest gives each warp 32, 16 or 8 rays depending on how
+    many rays the launch has against one wave of the GPU's warp slots (on a
+    148-SM B200: 8 rays for 20,000, 16 for 40,000, 32 for 140,000); every
+    ray's hit equals the oracle's in each case, the last partial group too."""
+    v, t = wl.noisy_sphere(160, seed=5)
+    sc = SceneRT()
+    sc.AddInstance(sc.AddGeom_Triangles3f(v, t), wl.IDENTITY)
+    sc.CommitScene()
+    rng = np.random.default_rng(n)
+    org = rng.normal(size=(n, 3))
+    org = 3.0 * org / np.linalg.norm(org, axis=1, keepdims=True)
+    d = rng.uniform(-0.9, 0.9, size=(n, 3)) - org
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, :3], rays[:, 3], rays[:, 4:7], rays[:, 7] = org, 1e-4, d, 1e9
+    got = _oracle_check(sc, rays)
+    assert (got["primId"] != MISS).sum() > n // 10
+
+
 def test_mesh_200k_triangles_256x256(cuda):
     v, t = wl.noisy_sphere(317, seed=0)
     sc = SceneRT()
