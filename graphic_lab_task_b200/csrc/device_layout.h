@@ -38,8 +38,10 @@ inline __host__ __device__ uint64_t sched_words(uint64_t tiles)
   return kSchedHeader + (tiles + 31) / 32 + kSchedClasses * tiles;
 }
 // Per-thread shared-memory words after the traversal stack: the inputs of the
-// deferred SDF normal (sign, sample point, 8 corner values).
-constexpr uint32_t kNormalWords = 12;
+// deferred SDF normal (sign, sample point, 8 corner values), then those of the
+// deferred SBS hit colour (object-space hit point, brick node index).
+constexpr uint32_t kNormalWords = 16;
+constexpr uint32_t kColourWord = 12;
 // Dynamic shared memory of a trace kernel with stack_cap stack entries per thread.
 constexpr size_t trace_smem_bytes(uint32_t stack_cap)
 {

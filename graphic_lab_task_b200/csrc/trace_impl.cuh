@@ -474,26 +474,53 @@ __device__ void octree_brick(CTX& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, f
     bnf.x += smax(0.0f, vfar - bnf.x) + 1e-6f;
   }
   if (hit.t < old_t && sb.colorLayout) {
-    // colour of the hit for the indexed layouts (BVH2Common.cpp:1081-1110)
+    // The colour of the hit (indexed layouts) is evaluated once the traversal
+    // has ended (trace_one, sbs_hit_colour) from the hit point and the brick,
+    // kept here, so that lanes whose hits come in different iterations of the
+    // traversal compute their colours together.
     const f3 pos = ray_pos + hit.t * ray_dir;
-    const f3 dp = (pos - brick_min_pos) * (0.5f * sz);
-    const uint32_t* tofs = S.sbsData + node.z + sb.v3;
-    f3 col = mk3(0, 0, 0);
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      const uint32_t b = __ldg(tofs + k);
-      const float wx = (k & 4) ? dp.x : (1 - dp.x);
-      const float wy = (k & 2) ? dp.y : (1 - dp.y);
-      const float wz = (k & 1) ? dp.z : (1 - dp.z);
-      const float w = wx * wy * wz;
-      const f3 cc = w * mk3(__ldg(S.sbsDataF + b), __ldg(S.sbsDataF + b + 1), __ldg(S.sbsDataF + b + 2));
-      col = (k == 0) ? cc : col + cc;
-    }
-    col = mk3(sclamp(floorf(255.0f * col.x + 0.5f), 0.0f, 255.0f), sclamp(floorf(255.0f * col.y + 0.5f), 0.0f, 255.0f),
-              sclamp(floorf(255.0f * col.z + 0.5f), 0.0f, 255.0f));
-    hit.coords[0] = col.x + col.y / 256.0f;
-    hit.coords[1] = col.z;
+    const uint32_t st = blockDim.x;
+    float* w = c.nrec + kColourWord * st;
+    w[0] = pos.x;
+    w[st] = pos.y;
+    w[2 * st] = pos.z;
+    w[3 * st] = __uint_as_float(nodeId);
   }
+}
+
+// The hit colour of OctreeBrickIntersect for the indexed layouts
+// (BVH2Common.cpp:1081-1110) from the object-space hit point and the brick's
+// node, with the brick box computed as octree_brick computes it.
+template <class CTX>
+__device__ __forceinline__ void sbs_hit_colour(CTX& c, const DevSbs& sb, lrt_hit& hit)
+{
+  const DevScene& S = c.S;
+  const uint32_t st = blockDim.x;
+  const float* w = c.nrec + kColourWord * st;
+  const f3 pos = mk3(w[0], w[st], w[2 * st]);
+  const uint32_t nodeId = __float_as_uint(w[3 * st]);
+  const uint4 node = __ldg(reinterpret_cast<const uint4*>(S.sbsNodes) + nodeId);
+  const float px = float(node.x >> 16), py = float(node.x & 0x0000FFFF);
+  const float pz = float(node.y >> 16), sz = float(node.y & 0x0000FFFF);
+  const float sz_inv = 2.0f / sz;
+  const f3 brick_min_pos = mk3(-1, -1, -1) + sz_inv * mk3(px, py, pz);
+  const f3 dp = (pos - brick_min_pos) * (0.5f * sz);
+  const uint32_t* tofs = S.sbsData + node.z + sb.v3;
+  f3 col = mk3(0, 0, 0);
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const uint32_t b = __ldg(tofs + k);
+    const float wx = (k & 4) ? dp.x : (1 - dp.x);
+    const float wy = (k & 2) ? dp.y : (1 - dp.y);
+    const float wz = (k & 1) ? dp.z : (1 - dp.z);
+    const float wt = wx * wy * wz;
+    const f3 cc = wt * mk3(__ldg(S.sbsDataF + b), __ldg(S.sbsDataF + b + 1), __ldg(S.sbsDataF + b + 2));
+    col = (k == 0) ? cc : col + cc;
+  }
+  col = mk3(sclamp(floorf(255.0f * col.x + 0.5f), 0.0f, 255.0f), sclamp(floorf(255.0f * col.y + 0.5f), 0.0f, 255.0f),
+            sclamp(floorf(255.0f * col.z + 0.5f), 0.0f, 255.0f));
+  hit.coords[0] = col.x + col.y / 256.0f;
+  hit.coords[1] = col.z;
 }
 
 template <class CTX>
@@ -520,18 +547,22 @@ __device__ void triangles(CTX& c, const DevGeom& g, f3 ray_pos, f3 ray_dir, floa
       hit.geomId = geomId | (LRT_TYPE_MESH_TRIANGLE << 24);
       hit.coords[0] = u;
       hit.coords[1] = v;
-      if (S.flags & kFlagNeedNormal) {
-        f3 n = cross(edge1, edge2);
-        n = normalize(matmul4(S.instances[instId].transformInvTransposed, n, 1.0f));
-        const f2 en = encode_normal(n);
-        hit.coords[2] = en.x;
-        hit.coords[3] = en.y;
-      } else {
-        hit.coords[2] = 0;
-        hit.coords[3] = 0;
-      }
+      // the geometric normal is computed once the traversal has ended
+      // (trace_one, triangle_normal), from the triangle the hit names
+      hit.coords[2] = 0;
+      hit.coords[3] = 0;
     }
   }
+}
+
+// The normal IntersectAllTrianglesInLeaf writes (BVH2Common.cpp:1609-1625):
+// cross(edge1, edge2) of the hit triangle (its triSoup record), through the
+// instance's transformInvTransposed, normalised and octahedrally encoded.
+__device__ __forceinline__ f2 triangle_normal(const DevScene& S, const DevGeom& g, uint32_t localPrim, uint32_t instId)
+{
+  const float4* tri = S.triSoup + 3 * (uint64_t(g.triBase) + localPrim);
+  const f3 n = cross(ld3(__ldg(tri + 1)), ld3(__ldg(tri + 2)));
+  return encode_normal(normalize(matmul4(S.instances[instId].transformInvTransposed, n, 1.0f)));
 }
 
 // IntersectAllPrimitivesInLeaf: returns the tag if the hit moved closer.
@@ -701,16 +732,29 @@ __device__ void trace_one(CTX& c, uint32_t* stack, uint32_t stride, uint32_t cap
       if (c.err & kErrStackOverflow) break;
     }
   } while (nodeIdx < 0xFFFFFFFEu && !(stopOnFirstHit && hit.primId != 0xFFFFFFFFu));
-  // the normal of a sphere-traced final hit (all other hits carry theirs)
-  if ((S.flags & kFlagNeedNormal) && hit.geomId < 0xFFFFFFFFu && ((hit.geomId >> 24) != LRT_TYPE_MESH_TRIANGLE)) {
-    const f2 en = deferred_normal(c, hit.instId);
-    hit.coords[2] = en.x;
-    hit.coords[3] = en.y;
-  }
-  if (hit.geomId < 0xFFFFFFFFu && ((hit.geomId >> 24) == LRT_TYPE_MESH_TRIANGLE)) {
+  // What the leaf tests left for the end of the traversal: the final hit's
+  // normal, an SBS hit's colour and the triangle primId remap.
+  if (hit.geomId < 0xFFFFFFFFu) {
     const DevGeom& g = S.geoms[hit.geomId & 0x00FFFFFFu];
-    c.triLocal = hit.primId;
-    hit.primId = __ldg(S.primIndices + g.triBase + hit.primId);
+    if ((hit.geomId >> 24) == LRT_TYPE_MESH_TRIANGLE) {
+      if (S.flags & kFlagNeedNormal) {
+        const f2 en = triangle_normal(S, g, hit.primId, hit.instId);
+        hit.coords[2] = en.x;
+        hit.coords[3] = en.y;
+      }
+      c.triLocal = hit.primId;
+      hit.primId = __ldg(S.primIndices + g.triBase + hit.primId);
+    } else {
+      if (S.flags & kFlagNeedNormal) {
+        const f2 en = deferred_normal(c, hit.instId);
+        hit.coords[2] = en.x;
+        hit.coords[3] = en.y;
+      }
+      if (g.tag == LRT_TAG_SDF_BRICK) {
+        const DevSbs& sb = S.sbs[g.sdfId];
+        if (sb.colorLayout) sbs_hit_colour(c, sb, hit);
+      }
+    }
   }
   if (hit.primId != 0xFFFFFFFFu) c.inc(kCntHits);
 }
