@@ -96,7 +96,7 @@ lrt_status sched_prepare(lrt_scene* s, cudaStream_t stream, uint32_t width, uint
   DeviceScene* d = s->dev;
   ImageSchedule& q = d->sched[stream];
   const uint64_t tiles = uint64_t((width + kImgTileW - 1) / kImgTileW) * ((height + kImgTileH - 1) / kImgTileH);
-  const size_t clear = (kSchedHeader + (tiles + 31) / 32) * sizeof(uint32_t); // header + bitmap
+  const size_t clear = sched_lists_offset(tiles) * sizeof(uint32_t); // header, bitmap, cost accumulators
   cudaError_t e = cudaSuccess;
   if (q.w != width || q.h != height) {
     for (uint32_t*& b : q.buf) {

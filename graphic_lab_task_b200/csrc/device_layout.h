@@ -29,13 +29,32 @@ constexpr uint32_t kImgTileW = 8, kImgTileH = 4;
 
 // Tile schedule of the image-order launches (one per stream and image size,
 // two buffers used alternately): a header {longest tile cost, count of each
-// of the kSchedClasses cost classes}, a bitmap of the listed tiles, then one
-// list of `tiles` entries per class.
-constexpr uint32_t kSchedHeader = 4;
+// of the kSchedClasses cost classes, warps of the launch, unused, 64-bit sum
+// of the warps' busy times}, a bitmap of the listed tiles, one 64-bit cost
+// accumulator per listed tile (the parts of a split tile add up there), then
+// one list of `tiles` entries per class.  Everything before the lists is
+// cleared before the launch that writes the buffer.  Costs are clock64 / 16.
+constexpr uint32_t kSchedHeader = 8;
+constexpr uint32_t kSchedWarps = 4;  // header word: warps that reported their busy time
+constexpr uint32_t kSchedBusy = 6;   // header words 6-7: the sum of those busy times
 constexpr uint32_t kSchedClasses = 3;
+// When the previous launch was tail-bound (its longest tile took longer than
+// its warps were busy on average), each tile of cost class 0 goes out as
+// kSplitParts work items, each traced by one warp on 32 / kSplitParts of the
+// tile's lanes (rows of the 8x4 tile): those tiles are the ones whose rays
+// diverge most, and a warp serialises its lanes' divergent paths.
+constexpr uint32_t kSplitParts = 2;
+inline __host__ __device__ uint64_t sched_acc_offset(uint64_t tiles) // in words, 8-byte aligned
+{
+  return (kSchedHeader + (tiles + 31) / 32 + 1) & ~1ull;
+}
+inline __host__ __device__ uint64_t sched_lists_offset(uint64_t tiles)
+{
+  return sched_acc_offset(tiles) + 2 * tiles;
+}
 inline __host__ __device__ uint64_t sched_words(uint64_t tiles)
 {
-  return kSchedHeader + (tiles + 31) / 32 + kSchedClasses * tiles;
+  return sched_lists_offset(tiles) + kSchedClasses * tiles;
 }
 // Per-thread shared-memory words after the traversal stack: the inputs of the
 // deferred SDF normal (sign, sample point, 8 corner values), then those of the

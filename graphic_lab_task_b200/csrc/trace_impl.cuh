@@ -765,61 +765,117 @@ __device__ void trace_one(CTX& c, uint32_t* stack, uint32_t stride, uint32_t cap
 // 1/8 of it); the next launch of the same image size on the same stream
 // (rd) hands out class 0, then 1, then 2, each in the order the tiles
 // finished, then every other tile in natural order (a bitmap skips the
-// listed ones).  Only which warp traces which tile, and when, depends on it.
+// listed ones).  If the previous launch was tail-bound (its longest tile
+// took longer than its warps' mean busy time), a class-0 tile goes out as
+// kSplitParts work items, each traced by one warp on its own rows of the
+// tile; the parts' costs add up in the tile's accumulator and the last part
+// to finish records the tile.  Only which warp traces which ray, and when,
+// depends on it.
 // rd == nullptr: natural order; wr == nullptr: nothing recorded.  Buffer
-// layout (sched_words): {longest cost, count of class 0, 1, 2}, the bitmap,
-// then the list of each class (`tiles` entries each).  The per-warp state
-// lives in shared memory so that the traversal keeps its registers.
+// layout: sched_words and the offsets beside it (device_layout.h).  The
+// per-warp state lives in shared memory so that the traversal keeps its
+// registers.
+//
+// A work item is a tile index with, for the part of a split tile, bit 31 set
+// and the part in bits 24..30 (tile counts stay below 2^24).
 struct WarpClock {
-  long long start;  // clock64 when the warp took its current tile
-  uint32_t tile;    // that tile, ~0u before the first
+  long long start;  // clock64 when the warp took its current item
+  uint32_t item;    // that item, ~0u before the first
   uint32_t longest; // longest tile this warp has reported
+  uint32_t pos;     // a split item's position in the concatenated class lists
+  unsigned long long busy; // sum of the costs of the items this warp traced
 };
+constexpr uint32_t kItemSplit = 0x80000000u;
+constexpr uint32_t kItemTileMask = 0x00FFFFFFu;
 
-// lane 0, after the warp has finished its current tile (if any): records
-// that tile's duration and returns the next tile of `tiles`, ~0u when none
+__device__ __forceinline__ uint32_t item_tile(uint32_t item) { return item & kItemTileMask; }
+
+// Whether `lane` traces its pixel of the item's tile: every lane for a whole
+// tile, rows part * (32 / kSplitParts) ... of it for a part.
+__device__ __forceinline__ bool item_has_lane(uint32_t item, uint32_t lane)
+{
+  return !(item & kItemSplit) || lane / (32u / kSplitParts) == ((item >> 24) & 0x7Fu);
+}
+
+// lane 0: records that a tile took `cost` (longest, class list, bitmap).
+__device__ __forceinline__ void sched_record(const uint32_t* __restrict__ rd, uint32_t* wr, uint32_t tiles,
+                                             uint32_t tile, uint32_t cost, WarpClock& wc)
+{
+  const uint64_t lists = sched_lists_offset(tiles);
+  if (cost > wc.longest) {
+    wc.longest = cost;
+    atomicMax(wr, cost);
+  }
+  const uint32_t mx = rd ? __ldg(rd) : 0u;
+  if (mx) {
+    const int cls = cost >= mx / 2 ? 0 : cost >= mx / 4 ? 1 : cost >= mx / 8 ? 2 : 3;
+    if (cls < 3) {
+      const uint32_t slot = atomicAdd(wr + 1 + cls, 1u);
+      if (slot < tiles) wr[lists + cls * tiles + slot] = tile;
+      atomicOr(wr + kSchedHeader + (tile >> 5), 1u << (tile & 31));
+    }
+  }
+}
+
+// lane 0, after the warp has finished its current item (if any): records
+// that item's duration and returns the next item of `tiles`, ~0u when none
 // is left.
 __device__ __forceinline__ uint32_t sched_next(const uint32_t* __restrict__ rd, uint32_t* wr, uint32_t tiles,
                                                unsigned long long* counter, WarpClock& wc)
 {
-  const uint32_t lists = kSchedHeader + (tiles + 31) / 32;
-  if (wr && wc.tile != ~0u) {
+  const uint64_t lists = sched_lists_offset(tiles);
+  if (wr && wc.item != ~0u) {
     const long long dt = (clock64() - wc.start) >> 4;
-    const uint32_t cost = uint32_t(dt < 0xFFFFFFFFll ? dt : 0xFFFFFFFFll);
-    if (cost > wc.longest) {
-      wc.longest = cost;
-      atomicMax(wr, cost);
+    uint32_t cost = uint32_t(dt < 0xFFFFFFFFll ? dt : 0xFFFFFFFFll);
+    bool record = true;
+    if (wc.item & kItemSplit) { // parts add up; the last one records the tile
+      unsigned long long* acc = reinterpret_cast<unsigned long long*>(wr + sched_acc_offset(tiles));
+      const unsigned long long prev = atomicAdd(acc + wc.pos, (1ull << 40) | cost);
+      record = (prev >> 40) + 1 == kSplitParts;
+      const unsigned long long sum = (prev & ((1ull << 40) - 1)) + cost;
+      cost = uint32_t(sum < 0xFFFFFFFFull ? sum : 0xFFFFFFFFull);
     }
-    const uint32_t mx = rd ? __ldg(rd) : 0u;
-    if (mx) {
-      const int cls = cost >= mx / 2 ? 0 : cost >= mx / 4 ? 1 : cost >= mx / 8 ? 2 : 3;
-      if (cls < 3) {
-        const uint32_t slot = atomicAdd(wr + 1 + cls, 1u);
-        if (slot < tiles) wr[lists + cls * tiles + slot] = wc.tile;
-        atomicOr(wr + kSchedHeader + (wc.tile >> 5), 1u << (wc.tile & 31));
-      }
-    }
+    wc.busy += cost;
+    if (record) sched_record(rd, wr, tiles, item_tile(wc.item), cost, wc);
   }
   static_assert(kSchedClasses == 3, "three cost classes");
+  static_assert(kSplitParts >= 1 && kSplitParts <= 32 && (32 % kSplitParts) == 0, "parts of a 32-lane tile");
   uint32_t n[3] = {0, 0, 0};
   if (rd)
     for (int c = 0; c < 3; c++) n[c] = min(__ldg(rd + 1 + c), tiles);
   const uint64_t nAll = uint64_t(n[0]) + n[1] + n[2];
+  // class-0 tiles go out in kSplitParts parts if the previous launch was
+  // tail-bound: longest * warps > sum of the warps' busy times
+  const bool tailBound =
+      rd && uint64_t(__ldg(rd)) * __ldg(rd + kSchedWarps) >
+                __ldg(reinterpret_cast<const unsigned long long*>(rd + kSchedBusy));
+  const uint64_t nSplit = tailBound ? n[0] : 0;
+  const uint64_t nItems = nSplit * kSplitParts + (nAll - nSplit);
   for (;;) {
     const unsigned long long k = atomicAdd(counter, 1ull);
-    uint32_t tile;
-    if (k < nAll) {
-      const int cls = k < n[0] ? 0 : k < uint64_t(n[0]) + n[1] ? 1 : 2;
-      const uint64_t j = cls == 0 ? k : cls == 1 ? k - n[0] : k - n[0] - n[1];
-      tile = __ldg(rd + lists + cls * tiles + j);
+    uint32_t item;
+    if (k < nItems) {
+      const bool split = k < nSplit * kSplitParts;
+      const uint64_t j = split ? k / kSplitParts : k - nSplit * (kSplitParts - 1);
+      const int cls = j < n[0] ? 0 : j < uint64_t(n[0]) + n[1] ? 1 : 2;
+      const uint64_t jj = cls == 0 ? j : cls == 1 ? j - n[0] : j - n[0] - n[1];
+      const uint32_t tile = __ldg(rd + lists + cls * tiles + jj);
       if (tile >= tiles) continue;
+      item = (split && kSplitParts > 1) ? tile | kItemSplit | (uint32_t(k % kSplitParts) << 24) : tile;
+      wc.pos = uint32_t(j);
     } else {
-      if (k - nAll >= tiles) return wc.tile = ~0u;
-      tile = uint32_t(k - nAll);
-      if (nAll && ((__ldg(rd + kSchedHeader + (tile >> 5)) >> (tile & 31)) & 1u)) continue;
+      if (k - nItems >= tiles) { // none left: report this warp's busy time
+        if (wr) {
+          atomicAdd(reinterpret_cast<unsigned long long*>(wr + kSchedBusy), wc.busy);
+          atomicAdd(wr + kSchedWarps, 1u);
+        }
+        return wc.item = ~0u;
+      }
+      item = uint32_t(k - nItems);
+      if (nAll && ((__ldg(rd + kSchedHeader + (item >> 5)) >> (item & 31)) & 1u)) continue;
     }
     wc.start = clock64();
-    return wc.tile = tile;
+    return wc.item = item;
   }
 }
 
@@ -870,21 +926,24 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_trace(DevScene S, const fl
   __shared__ WarpClock wclock[IMG ? kTraceThreads / 32 : 1];
   const uint64_t tilesX = (uint64_t(img_w) + kImgTileW - 1) / kImgTileW;
   if (IMG && lane == 0) {
-    wclock[threadIdx.x >> 5].tile = ~0u;
+    wclock[threadIdx.x >> 5].item = ~0u;
     wclock[threadIdx.x >> 5].longest = 0;
+    wclock[threadIdx.x >> 5].busy = 0;
   }
   l2_prefetch_scene(S);
   for (;;) {
     unsigned long long base = 0;
+    bool mine = true; // this lane's pixel belongs to the work item
     if (IMG) { // work counter in tiles
       __syncwarp();
-      uint32_t tile = 0;
+      uint32_t item = 0;
       if (lane == 0)
-        tile = sched_next(sched_rd, sched_wr, uint32_t(tilesX * ((img_h + kImgTileH - 1) / kImgTileH)), work_counter,
+        item = sched_next(sched_rd, sched_wr, uint32_t(tilesX * ((img_h + kImgTileH - 1) / kImgTileH)), work_counter,
                           wclock[threadIdx.x >> 5]);
-      tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
-      if (tile == ~0u) break;
-      base = uint64_t(tile) * 32;
+      item = __shfl_sync(0xFFFFFFFFu, item, 0);
+      if (item == ~0u) break;
+      base = uint64_t(item_tile(item)) * 32;
+      mine = item_has_lane(item, lane);
     } else { // in rays, `group` (32, 16 or 8) to a warp
       if (lane == 0) base = atomicAdd(work_counter, (unsigned long long)group);
       base = __shfl_sync(0xFFFFFFFFu, base, 0);
@@ -896,7 +955,7 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_trace(DevScene S, const fl
       const uint64_t b = base >> 5;
       const uint32_t x = uint32_t(b % tilesX) * kImgTileW + (lane % kImgTileW);
       const uint32_t y = uint32_t(b / tilesX) * kImgTileH + (lane / kImgTileW);
-      valid = x < img_w && y < img_h;
+      valid = x < img_w && y < img_h && mine;
       i = uint64_t(y) * img_w + x;
     }
     if (valid) {
@@ -1457,17 +1516,19 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_render_rgba8(DevScene S, D
   const uint32_t tilesX = (cam.width + 7) / 8, ntiles = tilesX * ((cam.height + 3) / 4);
   __shared__ WarpClock wclock[kTraceThreads / 32];
   if (lane == 0) {
-    wclock[threadIdx.x >> 5].tile = ~0u;
+    wclock[threadIdx.x >> 5].item = ~0u;
     wclock[threadIdx.x >> 5].longest = 0;
+    wclock[threadIdx.x >> 5].busy = 0;
   }
   for (;;) {
-    uint32_t tile = 0;
+    uint32_t item = 0;
     __syncwarp();
-    if (lane == 0) tile = sched_next(sched_rd, sched_wr, ntiles, work_counter, wclock[threadIdx.x >> 5]);
-    tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
-    if (tile == ~0u) break;
+    if (lane == 0) item = sched_next(sched_rd, sched_wr, ntiles, work_counter, wclock[threadIdx.x >> 5]);
+    item = __shfl_sync(0xFFFFFFFFu, item, 0);
+    if (item == ~0u) break;
+    const uint32_t tile = item_tile(item);
     const uint32_t x = (tile % tilesX) * 8 + (lane & 7), y = (tile / tilesX) * 4 + (lane >> 3);
-    if (x < cam.width && y < cam.height) {
+    if (x < cam.width && y < cam.height && item_has_lane(item, lane)) {
       float r[8];
       eye_ray(cam.proj_inv, cam.world_view_inv, x, y, cam.width, cam.height, cam.tnear, cam.tfar, r);
       lrt_hit h;
@@ -1538,17 +1599,19 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_outline_fill(DevScene S, D
   const uint32_t tilesX = (cam.width + 7) / 8, ntiles = tilesX * ((cam.height + 3) / 4);
   __shared__ WarpClock wclock[kTraceThreads / 32];
   if (lane == 0) {
-    wclock[threadIdx.x >> 5].tile = ~0u;
+    wclock[threadIdx.x >> 5].item = ~0u;
     wclock[threadIdx.x >> 5].longest = 0;
+    wclock[threadIdx.x >> 5].busy = 0;
   }
   for (;;) {
-    uint32_t tile = 0;
+    uint32_t item = 0;
     __syncwarp();
-    if (lane == 0) tile = sched_next(sched_rd, sched_wr, ntiles, work_counter, wclock[threadIdx.x >> 5]);
-    tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
-    if (tile == ~0u) break;
+    if (lane == 0) item = sched_next(sched_rd, sched_wr, ntiles, work_counter, wclock[threadIdx.x >> 5]);
+    item = __shfl_sync(0xFFFFFFFFu, item, 0);
+    if (item == ~0u) break;
+    const uint32_t tile = item_tile(item);
     const uint32_t x = (tile % tilesX) * 8 + (lane & 7), y = (tile / tilesX) * 4 + (lane >> 3);
-    if (x < cam.width && y < cam.height) {
+    if (x < cam.width && y < cam.height && item_has_lane(item, lane)) {
       float r0[8], rs[8];
       eye_ray(cam.proj_inv, cam.world_view_inv, x, y, cam.width, cam.height, cam.tnear, cam.tfar, r0,
               RM.random ? RM.randomX : RM.invSqrt * 0.5f, RM.random ? RM.randomY : RM.invSqrt * 0.5f);
@@ -1620,17 +1683,19 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_fill_gbuffer_transparency(
   const uint32_t tilesX = (cam.width + 7) / 8, ntiles = tilesX * ((cam.height + 3) / 4);
   __shared__ WarpClock wclock[kTraceThreads / 32];
   if (lane == 0) {
-    wclock[threadIdx.x >> 5].tile = ~0u;
+    wclock[threadIdx.x >> 5].item = ~0u;
     wclock[threadIdx.x >> 5].longest = 0;
+    wclock[threadIdx.x >> 5].busy = 0;
   }
   for (;;) {
-    uint32_t tile = 0;
+    uint32_t item = 0;
     __syncwarp();
-    if (lane == 0) tile = sched_next(sched_rd, sched_wr, ntiles, work_counter, wclock[threadIdx.x >> 5]);
-    tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
-    if (tile == ~0u) break;
+    if (lane == 0) item = sched_next(sched_rd, sched_wr, ntiles, work_counter, wclock[threadIdx.x >> 5]);
+    item = __shfl_sync(0xFFFFFFFFu, item, 0);
+    if (item == ~0u) break;
+    const uint32_t tile = item_tile(item);
     const uint32_t x = (tile % tilesX) * 8 + (lane & 7), y = (tile / tilesX) * 4 + (lane >> 3);
-    if (x < cam.width && y < cam.height) {
+    if (x < cam.width && y < cam.height && item_has_lane(item, lane)) {
       float r[8];
       eye_ray(cam.proj_inv, cam.world_view_inv, x, y, cam.width, cam.height, cam.tnear, cam.tfar, r);
       lrt_hit h;
@@ -1661,13 +1726,14 @@ __device__ __forceinline__ bool next_ray(uint64_t n, uint32_t img_w, uint32_t im
   if (IMG) {
     const uint32_t tilesX = (img_w + kImgTileW - 1) / kImgTileW;
     __syncwarp();
-    uint32_t tile = 0;
-    if (lane == 0) tile = sched_next(sched_rd, sched_wr, tilesX * ((img_h + kImgTileH - 1) / kImgTileH), counter, *wc);
-    tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
-    if (tile == ~0u) return false;
+    uint32_t item = 0;
+    if (lane == 0) item = sched_next(sched_rd, sched_wr, tilesX * ((img_h + kImgTileH - 1) / kImgTileH), counter, *wc);
+    item = __shfl_sync(0xFFFFFFFFu, item, 0);
+    if (item == ~0u) return false;
+    const uint32_t tile = item_tile(item);
     const uint32_t x = (tile % tilesX) * kImgTileW + lane % kImgTileW;
     const uint32_t y = (tile / tilesX) * kImgTileH + lane / kImgTileW;
-    valid = x < img_w && y < img_h;
+    valid = x < img_w && y < img_h && item_has_lane(item, lane);
     i = uint64_t(y) * img_w + x;
     return true;
   }
@@ -1697,8 +1763,9 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_render_lambert(DevScene S,
   __shared__ WarpClock wclock[IMG ? kTraceThreads / 32 : 1];
   WarpClock* wc = wclock + (IMG ? threadIdx.x >> 5 : 0);
   if (IMG && lane == 0) {
-    wc->tile = ~0u;
+    wc->item = ~0u;
     wc->longest = 0;
+    wc->busy = 0;
   }
   Ctx<false> c(S, normal_words(smem_stack, stack_cap));
   const f3 L = mk3(light.x, light.y, light.z);
@@ -1743,8 +1810,9 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_adjoint_lambert(DevScene S
   __shared__ WarpClock wclock[IMG ? kTraceThreads / 32 : 1];
   WarpClock* wc = wclock + (IMG ? threadIdx.x >> 5 : 0);
   if (IMG && lane == 0) {
-    wc->tile = ~0u;
+    wc->item = ~0u;
     wc->longest = 0;
+    wc->busy = 0;
   }
   const f3 L = mk3(light.x, light.y, light.z);
   uint32_t err = 0;

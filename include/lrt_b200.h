@@ -361,11 +361,14 @@ lrt_status lrt_trace_sync(lrt_scene* scene, void* stream, int32_t read_counters)
  * tiles' durations, and the next launch of the same image size on the same
  * stream starts with the tiles that took at least 1/2, then 1/4, then 1/8 of
  * the longest (the rest follow in row order), so that a few slow tiles do
- * not finish last.  The order never changes a result; the first launch of a
- * size on a stream allocates that stream's two schedule buffers (16 bytes +
- * about 12.1 bytes per tile each).  lrt_render_rgba8 and
- * lrt_fill_gbuffer_transparency schedule their tiles the same way.  No
- * counterpart entry point in the reference. */
+ * not finish last; when the longest tile took longer than the warps were
+ * busy on average, the tiles of the first group are each traced by two warps
+ * (two rows of the tile each).  The order never changes a result; the first
+ * launch of a size on a stream allocates that stream's two schedule buffers
+ * (about 36 bytes + 20.1 bytes per tile each).  lrt_render_rgba8,
+ * lrt_fill_gbuffer_transparency and the _image forms of the Lambert passes
+ * schedule their tiles the same way.  No counterpart entry point in the
+ * reference. */
 lrt_status lrt_trace_nearest_image(lrt_scene* scene, const float* rays_dev, lrt_hit* hits_dev, uint32_t width,
                                    uint32_t height, void* stream, uint32_t flags);
 
