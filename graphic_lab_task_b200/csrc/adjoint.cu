@@ -233,7 +233,7 @@ lrt_status render_lambert(lrt_scene* s, const float* rays_dev, uint64_t n, uint3
                                                    make_float3(light[0], light[1], light[2]), image_dev, &slot->work,
                                                    &slot->err, s->dev->stackCap, grid, stream, width, height, rd, wr);
   if (e != cudaSuccess) return cuda_fail(s, e, "render launch");
-  sched_commit(s, stream, natural);
+  sched_commit(s, stream, width, height, natural);
   return LRT_OK;
 }
 
@@ -258,7 +258,7 @@ lrt_status adjoint_lambert(lrt_scene* s, const float* rays_dev, uint64_t n, uint
                                                     &slot->work, &slot->err, s->dev->stackCap, grid, stream, width,
                                                     height, rd, wr);
   if (e != cudaSuccess) return cuda_fail(s, e, "adjoint launch");
-  sched_commit(s, stream, natural);
+  sched_commit(s, stream, width, height, natural);
   return LRT_OK;
 }
 
@@ -298,7 +298,7 @@ lrt_status render_outline_border(lrt_scene* s, const DevScene& S, StreamSlot* sl
     e = lrt_exact::launch_outline_fill(S, cam, L, M, RM, smp, tm, col, &slot->work, &slot->err, d->stackCap, grid,
                                        stream, rd, wr);
     if (e != cudaSuccess) return cuda_fail(s, e, "outline G-buffer launch");
-    sched_commit(s, stream, false);
+    sched_commit(s, stream, cam.width, cam.height, false);
     e = lrt_exact::launch_outline_resolve(tm, col, cam.width, cam.height, smp, RM.samples, acc, image_dev, stream);
     if (e != cudaSuccess) return cuda_fail(s, e, "outline resolve launch");
   }
@@ -439,7 +439,7 @@ lrt_status lrt_render_rgba8(lrt_scene* s, const lrt_camera* camera, const lrt_li
   const cudaError_t e = lrt_exact::launch_render_rgba8(S, cam, L, image_dev, &slot->work, &slot->err, d->stackCap,
                                                        grid, stream, rd, wr, &M, &RM);
   if (e != cudaSuccess) return cuda_fail(s, e, "render launch");
-  sched_commit(s, stream, false);
+  sched_commit(s, stream, cam.width, cam.height, false);
   return LRT_OK;
 }
 
@@ -555,7 +555,7 @@ lrt_status lrt_fill_gbuffer_transparency(lrt_scene* s, const lrt_camera* camera,
       S, cam, M, reinterpret_cast<float4*>(transparency_dev), hits_dev, &slot->work, &slot->err, d->stackCap, grid,
       stream, rd, wr);
   if (e != cudaSuccess) return cuda_fail(s, e, "transparency launch");
-  sched_commit(s, stream, false);
+  sched_commit(s, stream, cam.width, cam.height, false);
   return LRT_OK;
 }
 

@@ -94,25 +94,32 @@ lrt_status sched_prepare(lrt_scene* s, cudaStream_t stream, uint32_t width, uint
   *wr = nullptr;
   if (natural) return LRT_OK;
   DeviceScene* d = s->dev;
-  ImageSchedule& q = d->sched[stream];
   const uint64_t tiles = uint64_t((width + kImgTileW - 1) / kImgTileW) * ((height + kImgTileH - 1) / kImgTileH);
   const size_t clear = sched_lists_offset(tiles) * sizeof(uint32_t); // header, bitmap, cost accumulators
   cudaError_t e = cudaSuccess;
-  if (q.w != width || q.h != height) {
-    for (uint32_t*& b : q.buf) {
-      cudaFree(b);
-      b = nullptr;
+  const SchedKey key(stream, width, height);
+  auto it = d->sched.find(key);
+  if (it == d->sched.end()) {
+    if (d->sched.size() >= kMaxSchedules) { // free the least recently used schedule
+      auto old = d->sched.begin();
+      for (auto jt = d->sched.begin(); jt != d->sched.end(); ++jt)
+        if (jt->second.lastUse < old->second.lastUse) old = jt;
+      for (uint32_t* b : old->second.buf) cudaFree(b);
+      d->sched.erase(old);
     }
-    q.w = q.h = 0;
-    for (uint32_t*& b : q.buf) {
+    ImageSchedule fresh;
+    for (uint32_t*& b : fresh.buf) {
       if (e == cudaSuccess) e = cudaMalloc(&b, sched_words(tiles) * sizeof(uint32_t));
       if (e == cudaSuccess) e = cudaMemsetAsync(b, 0, clear, stream);
     }
-    if (e != cudaSuccess) return cuda_fail(s, e, "tile schedule buffers");
-    q.w = width;
-    q.h = height;
-    q.rd = 0;
+    if (e != cudaSuccess) {
+      for (uint32_t* b : fresh.buf) cudaFree(b);
+      return cuda_fail(s, e, "tile schedule buffers");
+    }
+    it = d->sched.emplace(key, fresh).first;
   }
+  ImageSchedule& q = it->second;
+  q.lastUse = ++d->schedUses;
   e = cudaMemsetAsync(q.buf[1 - q.rd], 0, clear, stream);
   if (e != cudaSuccess) return cuda_fail(s, e, "cudaMemsetAsync");
   *rd = q.buf[q.rd];
@@ -120,11 +127,11 @@ lrt_status sched_prepare(lrt_scene* s, cudaStream_t stream, uint32_t width, uint
   return LRT_OK;
 }
 
-void sched_commit(lrt_scene* s, cudaStream_t stream, bool natural)
+void sched_commit(lrt_scene* s, cudaStream_t stream, uint32_t width, uint32_t height, bool natural)
 {
   if (natural) return;
-  ImageSchedule& q = s->dev->sched[stream];
-  q.rd = 1 - q.rd;
+  auto it = s->dev->sched.find(SchedKey(stream, width, height));
+  if (it != s->dev->sched.end()) it->second.rd = 1 - it->second.rd;
 }
 
 namespace {
@@ -171,7 +178,7 @@ lrt_status launch(lrt_scene* s, const float4* rays, lrt_hit* hits, uint64_t n, c
     e = lrt_exact::launch_trace(S, rays, hits, n, &slot->work, slot->counters, err, d->stackCap, grid, stream,
                                 count, img_w, img_h, rd, wr, group);
   if (e != cudaSuccess) return cuda_fail(s, e, "trace launch");
-  sched_commit(s, stream, natural);
+  sched_commit(s, stream, img_w, img_h, natural);
   return LRT_OK;
 }
 

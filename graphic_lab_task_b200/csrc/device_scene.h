@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <map>
+#include <tuple>
 #include <vector>
 
 #include "device_layout.h"
@@ -31,15 +32,20 @@ constexpr uint64_t kPipeChunk = 262144;   // 8 MiB of rays in, 8 MiB of hits out
 constexpr uint64_t kPipeChunkMin = 32768; // first and last chunks
 constexpr uint64_t kPipeMinRays = 262144;
 
-// Tile schedule of the image-order launches on one stream (sched_next in
-// trace_impl.cuh): two device buffers of sched_words(tiles) words for a
-// width x height image, the one the next launch reads being buf[rd]; the
-// other is cleared and written by that launch.
+// Tile schedule of the image-order launches of one image size on one stream
+// (sched_next in trace_impl.cuh): two device buffers of sched_words(tiles)
+// words, the one the next launch reads being buf[rd]; the other is cleared
+// and written by that launch.  A scene keeps up to kMaxSchedules of them, so
+// that launches alternating between image sizes on one stream keep their
+// schedules (and allocate nothing after their first launch); beyond that
+// the least recently used one is freed.
 struct ImageSchedule {
-  uint32_t w = 0, h = 0;
   uint32_t* buf[2] = {nullptr, nullptr};
   int rd = 0;
+  uint64_t lastUse = 0;
 };
+using SchedKey = std::tuple<cudaStream_t, uint32_t, uint32_t>; // stream, width, height
+constexpr size_t kMaxSchedules = 32;
 
 struct DeviceScene {
   std::vector<void*> allocs;
@@ -79,7 +85,8 @@ struct DeviceScene {
   uint4* texTable = nullptr;
   float2* triTc = nullptr;
   uint64_t texVersion = 0;
-  std::map<cudaStream_t, ImageSchedule> sched; // per stream of image-order launches
+  std::map<SchedKey, ImageSchedule> sched; // per stream and image size of image-order launches
+  uint64_t schedUses = 0;
   // staging buffers for host-pointer calls
   float4* rays = nullptr;
   lrt_hit* hits = nullptr;
@@ -123,12 +130,12 @@ struct DeviceScene {
 // device.cu
 uint32_t preset_flags(const lrt_preset& p);
 // The schedule buffers of the next image-order launch of a width x height
-// image on `stream` (allocated, or reset when the size changed, on first
-// use); *rd = *wr = nullptr when `natural` asks for plain tile order.  The
-// caller launches, then calls sched_commit.
+// image on `stream` (allocated on the first launch of that size on that
+// stream); *rd = *wr = nullptr when `natural` asks for plain tile order.
+// The caller launches, then calls sched_commit with the same arguments.
 lrt_status sched_prepare(lrt_scene* s, cudaStream_t stream, uint32_t width, uint32_t height, bool natural,
                          const uint32_t** rd, uint32_t** wr);
-void sched_commit(lrt_scene* s, cudaStream_t stream, bool natural);
+void sched_commit(lrt_scene* s, cudaStream_t stream, uint32_t width, uint32_t height, bool natural);
 uint32_t launch_flags(const lrt_scene* s); // preset flags + the uploaded scene's own
 // DevScene::pfPtr/pfBytes from d->pfCand: the candidates in order while
 // their sum stays within kPrefetchMaxBytes

@@ -344,7 +344,7 @@ def test_image_tile_order_equals_linear_trace(cuda, size):
     for k in range(6):
         H2.zero_()
         if k == 3:
-            sc.trace_image(R.data_ptr(), small.data_ptr(), 8, 8)  # another size on the stream resets its schedule
+            sc.trace_image(R.data_ptr(), small.data_ptr(), 8, 8)  # another size on the stream has a schedule of its own
         if k == 4:
             sc.trace_image(R.data_ptr(), H2.data_ptr(), w, h, stream=side.cuda_stream)
             sc.sync(stream=side.cuda_stream)
@@ -353,3 +353,30 @@ def test_image_tile_order_equals_linear_trace(cuda, size):
         sc.sync()
         b = H2.cpu().numpy().view(HIT_DTYPE)
         assert bit_equal(a, b).all(), (k, hit_summary(b, a))
+
+
+def test_image_sizes_alternating_on_one_stream(cuda):
+    """Two image sizes traced in turn on one stream each keep their own tile
+    schedule (the slowest tiles first and, once a launch was tail-bound,
+    those split over two warps); every launch of either size returns the
+    linear trace's hits."""
+    torch = cuda
+    from graphic_lab_task_b200 import HIT_DTYPE
+    hdr, nodes, vals, vf = wl.sbs_from_spheres(wl.spheres(64, seed=1), grid_res=128)
+    sc = SceneRT()
+    sc.AddInstance(sc.AddGeom_SdfSBS(hdr, nodes, vals, vf), wl.IDENTITY)
+    sc.CommitScene()
+    views = []
+    for (w, h), eye in (((203, 97), (0, 0, 3)), ((96, 64), (2.2, 1.2, 1.6))):
+        R = torch.from_numpy(wl.eye_rays_host(wl.camera(eye, width=w, height=h))).cuda()
+        ref = torch.zeros(w * h * 8, dtype=torch.float32, device="cuda")
+        sc.trace_device(R.data_ptr(), ref.data_ptr(), w * h)
+        sc.sync()
+        views.append((w, h, R, ref.cpu().numpy().view(HIT_DTYPE)))
+    for k in range(6):
+        for w, h, R, want in views:
+            out = torch.zeros(w * h * 8, dtype=torch.float32, device="cuda")
+            sc.trace_image(R.data_ptr(), out.data_ptr(), w, h)
+            sc.sync()
+            got = out.cpu().numpy().view(HIT_DTYPE)
+            assert bit_equal(got, want).all(), (k, w, h, hit_summary(got, want))
