@@ -414,12 +414,11 @@ namespace {
 // BLAS emission too.  Outputs: order and, without emission, the inner nodes;
 // with it, the pairs and leaf table (order then being the leaves' box order).
 const char* run(const float* boxes6, uint32_t n, uint32_t maxLeaf, bool emit, std::vector<uint32_t>& order,
-                std::vector<LbvhInner>* innerOut, std::vector<LbvhPairOut>* pairsOut,
+                std::vector<LbvhInner>* innerOut, const std::function<LbvhPairOut*(size_t)>* pairsAt,
                 std::vector<uint32_t>* startCountOut)
 {
   order.clear();
   if (innerOut) innerOut->clear();
-  if (pairsOut) pairsOut->clear();
   if (startCountOut) startCountOut->clear();
   if (n == 0) return "no boxes";
   if (emit && n <= maxLeaf) return "device emission of a single-leaf tree";
@@ -564,14 +563,15 @@ const char* run(const float* boxes6, uint32_t n, uint32_t maxLeaf, bool emit, st
     LBVH_TRY(cudaMemcpyAsync(&herr, P.err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st), "status device->host");
     LBVH_TRY(cudaStreamSynchronize(st), "tree emission");
     if (e == cudaSuccess && !herr && (totals[0] == 0 || totals[0] > m || totals[1] > n)) herr = 4;
+    LbvhPairOut* pairsDst = nullptr;
     if (e == cudaSuccess && !herr) {
-      pairsOut->resize(totals[0]);
+      pairsDst = (*pairsAt)(totals[0]);
       startCountOut->resize(totals[1]);
       order.resize(n);
     }
     if (!herr) {
-      LBVH_TRY(cudaMemcpyAsync(pairsOut->data(), P.pairs, sizeof(LbvhPairOut) * size_t(totals[0]),
-                               cudaMemcpyDeviceToHost, st),
+      LBVH_TRY(cudaMemcpyAsync(pairsDst, P.pairs, sizeof(LbvhPairOut) * size_t(totals[0]), cudaMemcpyDeviceToHost,
+                               st),
                "pairs device->host");
       LBVH_TRY(cudaMemcpyAsync(startCountOut->data(), P.startCount, sizeof(uint32_t) * size_t(totals[1]),
                                cudaMemcpyDeviceToHost, st),
@@ -595,10 +595,9 @@ const char* run(const float* boxes6, uint32_t n, uint32_t maxLeaf, bool emit, st
   LBVH_TRY(cudaStreamSynchronize(st), "tree build");
 #undef LBVH_TRY
   if (st) cudaStreamDestroy(st);
-  auto clear = [&]() {
+  auto clear = [&]() { // (pairs the caller made room for are the caller's to drop)
     order.clear();
     if (innerOut) innerOut->clear();
-    if (pairsOut) pairsOut->clear();
     if (startCountOut) startCountOut->clear();
   };
   if (e != cudaSuccess) {
@@ -622,10 +621,11 @@ const char* lbvh_build(const float* boxes6, uint32_t n, std::vector<uint32_t>& o
   return run(boxes6, n, 0, false, order, &inner, nullptr, nullptr);
 }
 
-const char* lbvh_build_blas(const float* boxes6, uint32_t n, uint32_t maxLeaf, std::vector<LbvhPairOut>& pairs,
-                            std::vector<uint32_t>& startCount, std::vector<uint32_t>& order)
+const char* lbvh_build_blas(const float* boxes6, uint32_t n, uint32_t maxLeaf,
+                            const std::function<LbvhPairOut*(size_t)>& pairsAt, std::vector<uint32_t>& startCount,
+                            std::vector<uint32_t>& order)
 {
-  return run(boxes6, n, std::max(1u, maxLeaf), true, order, nullptr, &pairs, &startCount);
+  return run(boxes6, n, std::max(1u, maxLeaf), true, order, nullptr, &pairsAt, &startCount);
 }
 
 } // namespace lrt

@@ -2,6 +2,7 @@
 #pragma once
 #include <stdint.h>
 
+#include <functional>
 #include <vector>
 
 namespace lrt {
@@ -30,12 +31,14 @@ struct LbvhPairOut {
 
 // Builds the tree as lbvh_build does and emits a triangle BLAS from it on the
 // device, exactly as the host emitter would from the same tree with inner
-// nodes of at most maxLeaf boxes collapsed into leaves: `pairs` (relative
-// child indices), the leaf table entries Pack(start, count) in leaf-id order
-// (`startCount`) and the box order of the leaves (`order`: position ->
-// box).  Needs n > maxLeaf (a root that is one leaf has no pairs to emit).
-// Returns nullptr on success, else a message.
-const char* lbvh_build_blas(const float* boxes6, uint32_t n, uint32_t maxLeaf, std::vector<LbvhPairOut>& pairs,
-                            std::vector<uint32_t>& startCount, std::vector<uint32_t>& order);
+// nodes of at most maxLeaf boxes collapsed into leaves: the pairs (relative
+// child indices; copied to pairsAt(count), which the caller makes room for),
+// the leaf table entries Pack(start, count) in leaf-id order (`startCount`)
+// and the box order of the leaves (`order`: position -> box).  Needs
+// n > maxLeaf (a root that is one leaf has no pairs to emit).  Returns nullptr
+// on success, else a message.
+const char* lbvh_build_blas(const float* boxes6, uint32_t n, uint32_t maxLeaf,
+                            const std::function<LbvhPairOut*(size_t)>& pairsAt, std::vector<uint32_t>& startCount,
+                            std::vector<uint32_t>& order);
 
 } // namespace lrt

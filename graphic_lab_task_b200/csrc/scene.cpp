@@ -828,9 +828,17 @@ lrt_status lrt_add_geom_triangles3f(lrt_scene* s, const float* vpos, size_t nver
   if (stride == 0) stride = 12;
   if (stride % 4 != 0 || stride < 12)
     return fail(s, LRT_ERR_INVALID_ARGUMENT, "AddGeom_Triangles3f: vertex byte stride %zu", stride);
+  // The per-element loops below run on the host's cores (OpenMP); each
+  // element's result is what the sequential loop computes, and the geometry
+  // box combines the chunks' boxes in chunk order (std::min/max keep the
+  // first of equal values, so signed zeros come out as in one pass).
+  size_t firstBad = nidx;
+#pragma omp parallel for reduction(min : firstBad) schedule(static)
   for (size_t i = 0; i < nidx; i++)
-    if (tri[i] >= nvert)
-      return fail(s, LRT_ERR_INVALID_ARGUMENT, "AddGeom_Triangles3f: index %u >= vertex count %zu", tri[i], nvert);
+    if (tri[i] >= nvert && i < firstBad) firstBad = i;
+  if (firstBad < nidx)
+    return fail(s, LRT_ERR_INVALID_ARGUMENT, "AddGeom_Triangles3f: index %u >= vertex count %zu", tri[firstBad],
+                nvert);
   HostArrays& h = s->h;
   const size_t vs = stride / 4;
   const uint32_t geomId = uint32_t(h.geomData.size());
@@ -838,14 +846,29 @@ lrt_status lrt_add_geom_triangles3f(lrt_scene* s, const float* vpos, size_t nver
   lrt_geom_data g;
   std::memset(&g, 0, sizeof(g));
   for (int k = 0; k < 4; k++) { g.boxMin[k] = FLT_MAX; g.boxMax[k] = -FLT_MAX; }
-  h.vertPos.reserve(h.vertPos.size() + 4 * nvert);
-  for (size_t i = 0; i < nvert; i++) {
-    const float v[4] = {vpos[i * vs + 0], vpos[i * vs + 1], vpos[i * vs + 2], 1.0f};
-    for (int k = 0; k < 4; k++) {
-      h.vertPos.push_back(v[k]);
-      g.boxMin[k] = std::min(g.boxMin[k], v[k]);
-      g.boxMax[k] = std::max(g.boxMax[k], v[k]);
+  h.vertPos.resize(4 * (oldV + nvert));
+  {
+    float* dst = h.vertPos.data() + 4 * oldV;
+    constexpr size_t kChunks = 64;
+    float cmin[kChunks][4], cmax[kChunks][4];
+#pragma omp parallel for schedule(static)
+    for (size_t c = 0; c < kChunks; c++) {
+      for (int k = 0; k < 4; k++) { cmin[c][k] = FLT_MAX; cmax[c][k] = -FLT_MAX; }
+      const size_t lo = nvert * c / kChunks, hi = nvert * (c + 1) / kChunks;
+      for (size_t i = lo; i < hi; i++) {
+        const float v[4] = {vpos[i * vs + 0], vpos[i * vs + 1], vpos[i * vs + 2], 1.0f};
+        for (int k = 0; k < 4; k++) {
+          dst[4 * i + k] = v[k];
+          cmin[c][k] = std::min(cmin[c][k], v[k]);
+          cmax[c][k] = std::max(cmax[c][k], v[k]);
+        }
+      }
     }
+    for (size_t c = 0; c < kChunks; c++)
+      for (int k = 0; k < 4; k++) {
+        g.boxMin[k] = std::min(g.boxMin[k], cmin[c][k]);
+        g.boxMax[k] = std::max(g.boxMax[k], cmax[c][k]);
+      }
   }
   g.offset[0] = uint32_t(oldI);
   g.offset[1] = uint32_t(oldV);
@@ -857,6 +880,7 @@ lrt_status lrt_add_geom_triangles3f(lrt_scene* s, const float* vpos, size_t nver
   const size_t nt = nidx / 3;
   std::vector<Aabb> boxes(nt);
   const float* V = h.vertPos.data() + 4 * oldV;
+#pragma omp parallel for schedule(static)
   for (size_t t = 0; t < nt; t++) {
     boxes[t].reset();
     for (int c = 0; c < 3; c++) {
@@ -888,15 +912,16 @@ lrt_status lrt_add_geom_triangles3f(lrt_scene* s, const float* vpos, size_t nver
     // the arrays the host emitter makes from the same tree)
     const char* err = nullptr;
     if (nt > s->primsInLeaf) {
-      std::vector<LbvhPairOut> dp;
-      err = lbvh_build_blas(reinterpret_cast<const float*>(boxes.data()), uint32_t(nt), s->primsInLeaf, dp,
-                            startCount, reordered);
-      if (!err) {
-        static_assert(sizeof(LbvhPairOut) == sizeof(lrt_bvh_node_pair), "a pair is 64 bytes");
-        const size_t base = h.allNodePairs.size();
-        h.allNodePairs.resize(base + dp.size());
-        std::memcpy(h.allNodePairs.data() + base, dp.data(), dp.size() * sizeof(lrt_bvh_node_pair));
-      }
+      static_assert(sizeof(LbvhPairOut) == sizeof(lrt_bvh_node_pair), "a pair is 64 bytes");
+      const size_t base = h.allNodePairs.size();
+      err = lbvh_build_blas(
+          reinterpret_cast<const float*>(boxes.data()), uint32_t(nt), s->primsInLeaf,
+          [&](size_t count) {
+            h.allNodePairs.resize(base + count);
+            return reinterpret_cast<LbvhPairOut*>(h.allNodePairs.data() + base);
+          },
+          startCount, reordered);
+      if (err) h.allNodePairs.resize(base);
     } else {
       RadixTree R;
       err = R.build(boxes, s->primsInLeaf);
@@ -915,8 +940,10 @@ lrt_status lrt_add_geom_triangles3f(lrt_scene* s, const float* vpos, size_t nver
   }
   h.primIndices.insert(h.primIndices.end(), reordered.begin(), reordered.end());
   h.indices.resize(oldI + 3 * reordered.size());
+  uint32_t* idx = h.indices.data() + oldI;
+#pragma omp parallel for schedule(static)
   for (size_t i = 0; i < reordered.size(); i++)
-    for (int c = 0; c < 3; c++) h.indices[oldI + 3 * i + c] = tri[3 * size_t(reordered[i]) + c];
+    for (int c = 0; c < 3; c++) idx[3 * i + c] = tri[3 * size_t(reordered[i]) + c];
   const uint32_t old = uint32_t(h.primIdCount.size());
   h.primIdCount.insert(h.primIdCount.end(), startCount.begin(), startCount.end());
   h.startEnd.push_back(old);
