@@ -165,7 +165,10 @@ lrt_status launch(lrt_scene* s, const float4* rays, lrt_hit* hits, uint64_t n, c
   }
   const uint64_t warps = img_w ? uint64_t((img_w + kImgTileW - 1) / kImgTileW) * ((img_h + kImgTileH - 1) / kImgTileH)
                                : (n + group - 1) / group;
-  const int grid = int(std::min<uint64_t>(uint64_t(d->grid), (warps * 32 + kTraceThreads - 1) / kTraceThreads));
+  // image-order traces of brick-only scenes use the 80-register kernel (its own grid)
+  const bool bricks = img_w && !count && d->bricksOnly;
+  const int grid = int(std::min<uint64_t>(uint64_t(bricks ? d->gridBricks : d->grid),
+                                          (warps * 32 + kTraceThreads - 1) / kTraceThreads));
   const bool natural = !img_w || count || (flags & LRT_TRACE_NATURAL_ORDER);
   const uint32_t* rd = nullptr;
   uint32_t* wr = nullptr;
@@ -173,10 +176,10 @@ lrt_status launch(lrt_scene* s, const float4* rays, lrt_hit* hits, uint64_t n, c
   if (st != LRT_OK) return st;
   if (flags & LRT_TRACE_FAST_MATH)
     e = lrt_fast::launch_trace(S, rays, hits, n, &slot->work, slot->counters, err, d->stackCap, grid, stream, count,
-                               img_w, img_h, rd, wr, group);
+                               img_w, img_h, rd, wr, group, bricks);
   else
     e = lrt_exact::launch_trace(S, rays, hits, n, &slot->work, slot->counters, err, d->stackCap, grid, stream,
-                                count, img_w, img_h, rd, wr, group);
+                                count, img_w, img_h, rd, wr, group, bricks);
   if (e != cudaSuccess) return cuda_fail(s, e, "trace launch");
   sched_commit(s, stream, img_w, img_h, natural);
   return LRT_OK;
@@ -398,8 +401,11 @@ lrt_status device_upload(lrt_scene* s)
   // scenes: raise it once to the largest stack any scene may use.
   e = lrt_exact::set_trace_smem(kMaxStack + 1);
   if (e == cudaSuccess) e = lrt_fast::set_trace_smem(kMaxStack + 1);
-  int perSm = 0, sms = 0;
+  int perSm = 0, perSmBricks = 0, sms = 0;
+  d->bricksOnly = !h.geomTags.empty() &&
+                  std::all_of(h.geomTags.begin(), h.geomTags.end(), [](uint32_t t) { return t == LRT_TAG_SDF_BRICK; });
   if (e == cudaSuccess) e = lrt_exact::trace_occupancy(d->stackCap, &perSm);
+  if (e == cudaSuccess) e = lrt_exact::trace_occupancy(d->stackCap, &perSmBricks, true);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
   if (e == cudaSuccess) e = cudaMalloc(&d->slots, sizeof(StreamSlot) * kMaxStreams);
   if (e == cudaSuccess) {
@@ -412,6 +418,7 @@ lrt_status device_upload(lrt_scene* s)
     return st;
   }
   d->grid = std::max(1, perSm) * sms;
+  d->gridBricks = std::max(1, perSmBricks) * sms;
   // The allocation-free trace's static array is looked up here, with the
   // scene's device current, not in the trace call: under lazy module loading
   // the first lookup loads this file's module and places the array in device

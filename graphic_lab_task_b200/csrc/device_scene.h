@@ -52,6 +52,10 @@ struct DeviceScene {
   DevScene S{};
   uint32_t stackCap = 0;
   int grid = 0;
+  // every geometry is a sparse-brick set: image-order traces use the
+  // 80-register kernel and its grid
+  bool bricksOnly = false;
+  int gridBricks = 0;
   StreamSlot* slots = nullptr; // device, kMaxStreams
   std::map<cudaStream_t, int> slotOf;
   const lrt_bvh_node_pair* pairsOrig = nullptr; // unpruned node pairs (used once SBS values change)

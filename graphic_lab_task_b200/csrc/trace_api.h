@@ -10,9 +10,9 @@
                            unsigned long long* work_counter, unsigned long long* counters, uint32_t* err_word,  \
                            uint32_t stack_cap, int grid, cudaStream_t stream, bool count, uint32_t img_w = 0,   \
                            uint32_t img_h = 0, const uint32_t* sched_rd = nullptr,                              \
-                           uint32_t* sched_wr = nullptr, uint32_t group = 32);                                            \
+                           uint32_t* sched_wr = nullptr, uint32_t group = 32, bool bricks_only = false);                 \
   cudaError_t set_trace_smem(uint32_t stack_cap);                                                               \
-  cudaError_t trace_occupancy(uint32_t stack_cap, int* blocks_per_sm);                                          \
+  cudaError_t trace_occupancy(uint32_t stack_cap, int* blocks_per_sm, bool bricks_only = false);                \
   cudaError_t launch_eye_rays(const lrt::DevCamera& cam, float4* rays, cudaStream_t stream);                    \
   cudaError_t launch_trace_cameras(const lrt::DevScene& S, const lrt::DevBatchCamera* cams, uint32_t ncams,     \
                                    uint32_t ntiles, const lrt::DevBatchShape& shape, lrt_hit* hits,             \

@@ -909,8 +909,13 @@ __device__ __forceinline__ void l2_prefetch_scene(const DevScene& S)
   }
 }
 
-template <bool COUNT, bool SOLVERS, bool IMG>
-__global__ void __launch_bounds__(kTraceThreads, 7) k_trace(DevScene S, const float4* __restrict__ rays,
+//
+// MINB: blocks per SM the register allocation is bounded for (7: 72
+// registers; 6: 80 registers, used for the image-order launches of scenes
+// whose geometries are all sparse-brick sets, where the brick march and the
+// sphere trace spill at 72).
+template <bool COUNT, bool SOLVERS, bool IMG, int MINB = 7>
+__global__ void __launch_bounds__(kTraceThreads, MINB) k_trace(DevScene S, const float4* __restrict__ rays,
                                                          lrt_hit* __restrict__ hits, uint64_t n,
                                                          unsigned long long* __restrict__ work_counter,
                                                          unsigned long long* __restrict__ counters,
@@ -1978,7 +1983,8 @@ __global__ void k_eye_rays(DevCamera cam, float4* __restrict__ rays)
 cudaError_t launch_trace(const DevScene& S, const float4* rays, lrt_hit* hits, uint64_t n,
                                 unsigned long long* work_counter, unsigned long long* counters, uint32_t* err_word,
                                 uint32_t stack_cap, int grid, cudaStream_t stream, bool count, uint32_t img_w,
-                                uint32_t img_h, const uint32_t* sched_rd, uint32_t* sched_wr, uint32_t group)
+                                uint32_t img_h, const uint32_t* sched_rd, uint32_t* sched_wr, uint32_t group,
+                                bool bricks_only)
 {
   const size_t smem = trace_smem_bytes(stack_cap);
   // the ANALYTIC / NEWTON / IT node solvers live in their own instantiation,
@@ -1995,6 +2001,7 @@ cudaError_t launch_trace(const DevScene& S, const float4* rays, lrt_hit* hits, u
     if (count && solvers) go(k_trace<true, true, true>);
     else if (count) go(k_trace<true, false, true>);
     else if (solvers) go(k_trace<false, true, true>);
+    else if (bricks_only) go(k_trace<false, false, true, 6>);
     else go(k_trace<false, false, true>);
   } else {
     if (count && solvers) go(k_trace<true, true, false>);
@@ -2020,12 +2027,16 @@ cudaError_t set_trace_smem(uint32_t stack_cap)
   set(k_trace<true, true, true>);
   set(k_trace<false, true, true>);
   set(k_trace<false, false, true>);
+  set(k_trace<false, false, true, 6>);
   return e;
 }
 
-cudaError_t trace_occupancy(uint32_t stack_cap, int* blocks_per_sm)
+cudaError_t trace_occupancy(uint32_t stack_cap, int* blocks_per_sm, bool bricks_only)
 {
   const size_t smem = trace_smem_bytes(stack_cap);
+  if (bricks_only)
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_trace<false, false, true, 6>,
+                                                         kTraceThreads, smem);
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_trace<false, false, false>, kTraceThreads,
                                                        smem);
 }
