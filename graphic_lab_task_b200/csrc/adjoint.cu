@@ -436,8 +436,12 @@ lrt_status lrt_render_rgba8(lrt_scene* s, const lrt_camera* camera, const lrt_li
   M.triTc = d->triTc;
   if (mode == LRT_RENDER_MODE_OUTLINE_BORDER) return render_outline_border(s, S, slot, cam, L, M, RM, image_dev, grid, stream);
   if ((st = sched_prepare(s, stream, cam.width, cam.height, false, &rd, &wr)) != LRT_OK) return st;
+  // one LAMBERT_NO_TEX sample of a brick-only scene: the 80-register kernel and its grid
+  const bool bricks = d->bricksOnly && mode == LRT_RENDER_MODE_LAMBERT_NO_TEX && RM.samples == 1 && !RM.transparency;
+  const int rgrid = bricks ? int(std::min<uint64_t>(uint64_t(d->gridBricks), (tiles * 32 + kTraceThreads - 1) / kTraceThreads))
+                           : grid;
   const cudaError_t e = lrt_exact::launch_render_rgba8(S, cam, L, image_dev, &slot->work, &slot->err, d->stackCap,
-                                                       grid, stream, rd, wr, &M, &RM);
+                                                       rgrid, stream, rd, wr, &M, &RM, bricks);
   if (e != cudaSuccess) return cuda_fail(s, e, "render launch");
   sched_commit(s, stream, cam.width, cam.height, false);
   return LRT_OK;

@@ -25,7 +25,7 @@
                                   uint32_t stack_cap, int grid, cudaStream_t stream,                            \
                                   const uint32_t* sched_rd = nullptr, uint32_t* sched_wr = nullptr,             \
                                   const lrt::DevMaterials* materials = nullptr,                                 \
-                                  const lrt::DevRenderModes* modes = nullptr);                                  \
+                                  const lrt::DevRenderModes* modes = nullptr, bool bricks_only = false);        \
   cudaError_t launch_fill_gbuffer_transparency(const lrt::DevScene& S, const lrt::DevCamera& cam,               \
                                                const lrt::DevMaterials& M, float4* transparency, lrt_hit* gbuffer,\
                                                unsigned long long* work_counter, uint32_t* err_word,            \

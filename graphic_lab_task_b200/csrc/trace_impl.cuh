@@ -1505,8 +1505,10 @@ __device__ __forceinline__ float lambert(const lrt_hit& h, f3 dir, f3 L)
 // triangle and turned towards the viewer as in loadNormalTcFromGbuffer :27-75,
 // SDF normals decoded from the hit) and Tonemap (:536-542) into RGBA8.  A warp
 // takes 8x4-pixel tiles from a global counter.
-template <bool MODES>
-__global__ void __launch_bounds__(kTraceThreads, 7) k_render_rgba8(DevScene S, DevCamera cam, DevLights L,
+// MINB as for k_trace: 6 (80 registers) for one LAMBERT_NO_TEX sample of a
+// scene whose geometries are all sparse-brick sets, else 7 (72 registers).
+template <bool MODES, int MINB = 7>
+__global__ void __launch_bounds__(kTraceThreads, MINB) k_render_rgba8(DevScene S, DevCamera cam, DevLights L,
                                                                 uint32_t* __restrict__ image,
                                                                 unsigned long long* __restrict__ work_counter,
                                                                 uint32_t* __restrict__ err_word, uint32_t stack_cap,
@@ -1878,14 +1880,14 @@ __global__ void __launch_bounds__(kTraceThreads, 7) k_adjoint_lambert(DevScene S
 cudaError_t launch_render_rgba8(const DevScene& S, const DevCamera& cam, const DevLights& lights, uint32_t* image,
                                 unsigned long long* work_counter, uint32_t* err_word, uint32_t stack_cap, int grid,
                                 cudaStream_t stream, const uint32_t* sched_rd, uint32_t* sched_wr,
-                                const DevMaterials* materials, const DevRenderModes* rm)
+                                const DevMaterials* materials, const DevRenderModes* rm, bool bricks_only)
 {
   const size_t smem = trace_smem_bytes(stack_cap);
   // one sample of LAMBERT_NO_TEX keeps its own instantiation (the benchmarked
-  // render); the other modes, several samples and transparency share the
-  // general one
+  // render; bounded to 80 registers for brick-only scenes); the other modes,
+  // several samples and transparency share the general one
   const bool modes = rm && (rm->mode != LRT_RENDER_MODE_LAMBERT_NO_TEX || rm->samples != 1 || rm->transparency);
-  auto kernel = modes ? k_render_rgba8<true> : k_render_rgba8<false>;
+  auto kernel = modes ? k_render_rgba8<true> : bricks_only ? k_render_rgba8<false, 6> : k_render_rgba8<false>;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(trace_smem_bytes(kMaxStackDev + 1)));
   if (e != cudaSuccess) return e;
@@ -2034,6 +2036,7 @@ cudaError_t set_trace_smem(uint32_t stack_cap)
 cudaError_t trace_occupancy(uint32_t stack_cap, int* blocks_per_sm, bool bricks_only)
 {
   const size_t smem = trace_smem_bytes(stack_cap);
+  // (k_render_rgba8<false, 6> has the same bound and shared memory)
   if (bricks_only)
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_trace<false, false, true, 6>,
                                                          kTraceThreads, smem);
