@@ -157,7 +157,8 @@ lrt_status launch(lrt_scene* s, const float4* rays, lrt_hit* hits, uint64_t n, c
   // Row order: rays to a warp.  A launch of fewer rays than one wave of the
   // kernel's warps can hold takes as long as its slowest warp, and a warp's
   // time grows with the number of slow rays among its lanes, so such a launch
-  // gives each warp 16 or 8 rays while the warps still fit in one wave.
+  // gives each warp 16 or 8 rays while the warps still fit in one wave, taken
+  // with a stride across the launch's rays (k_trace).
   uint32_t group = 32;
   if (!img_w) {
     const uint64_t slots = uint64_t(d->grid) * (kTraceThreads / 32);

@@ -956,6 +956,15 @@ __global__ void __launch_bounds__(kTraceThreads, MINB) k_trace(DevScene S, const
     }
     uint64_t i = base + lane;
     bool valid = i < n && (IMG || lane < group);
+    if (!IMG && group < 32) {
+      // A launch smaller than one wave lasts as long as its slowest warp, and
+      // the slow rays of an image (grazing ones) lie next to each other: warp
+      // g takes rays g, g + G, g + 2G, ... of the G groups instead of `group`
+      // consecutive ones, so that they spread over many warps.
+      const uint64_t G = (n + group - 1) / group;
+      i = base / group + uint64_t(lane) * G;
+      valid = lane < group && i < n;
+    }
     if (IMG) {
       const uint64_t b = base >> 5;
       const uint32_t x = uint32_t(b % tilesX) * kImgTileW + (lane % kImgTileW);
