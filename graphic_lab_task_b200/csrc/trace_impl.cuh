@@ -913,7 +913,8 @@ __device__ __forceinline__ void l2_prefetch_scene(const DevScene& S)
 // MINB: blocks per SM the register allocation is bounded for (7: 72
 // registers; 6: 80 registers, used for the image-order launches of scenes
 // whose geometries are all sparse-brick sets, where the brick march and the
-// sphere trace spill at 72).
+// sphere trace spill at 72, and for row-order launches smaller than one wave,
+// which wait on their slowest warp's chain of dependent steps).
 template <bool COUNT, bool SOLVERS, bool IMG, int MINB = 7>
 __global__ void __launch_bounds__(kTraceThreads, MINB) k_trace(DevScene S, const float4* __restrict__ rays,
                                                          lrt_hit* __restrict__ hits, uint64_t n,
@@ -2018,6 +2019,7 @@ cudaError_t launch_trace(const DevScene& S, const float4* rays, lrt_hit* hits, u
     if (count && solvers) go(k_trace<true, true, false>);
     else if (count) go(k_trace<true, false, false>);
     else if (solvers) go(k_trace<false, true, false>);
+    else if (group < 32) go(k_trace<false, false, false, 6>); // latency-bound: fewer spills per step
     else go(k_trace<false, false, false>);
   }
   return cudaGetLastError();
@@ -2039,6 +2041,7 @@ cudaError_t set_trace_smem(uint32_t stack_cap)
   set(k_trace<false, true, true>);
   set(k_trace<false, false, true>);
   set(k_trace<false, false, true, 6>);
+  set(k_trace<false, false, false, 6>);
   return e;
 }
 
