@@ -259,8 +259,11 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize(dev)
     sc.sync(stream=sp)
     kernel_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    # the same rays traced in row order (lrt_trace_nearest, 32 consecutive rays per warp)
+    # the same rays traced in row order (lrt_trace_nearest, 32 consecutive rays per warp; the groups
+    # follow the stream's schedule from the second launch of this ray count on: three untimed first)
     row_ms = []
+    for _ in range(3):
+        sc.trace_device(rays.data_ptr(), hits.data_ptr(), n, stream=sp)
     for i in range(min(args.steps, 50)):
         flush.zero_()
         starts[i].record(stream)
@@ -354,7 +357,7 @@ def run_ours(args, rank, world, local_rank):
                 "gpu_launches": args.steps * len(pipeline_chunks(n)),
                 "call": "lrt_trace_nearest, pinned host buffers (chunked copy/trace/copy pipeline)"},
         "row_order": {"ms_per_step": sum(row_ms) / len(row_ms), "value": n / (sum(row_ms) / len(row_ms)) / 1e3,
-                      "unit": "Mrays/s", "call": "lrt_trace_nearest (same rays, 32 consecutive rays per warp)"},
+                      "unit": "Mrays/s", "call": "lrt_trace_nearest (same rays, 32 consecutive rays per warp, the 32-ray groups in the stream's schedule for this ray count)"},
         "moving_camera": {"ms_per_step": sum(mov_ms) / len(mov_ms), "value": n / (sum(mov_ms) / len(mov_ms)) / 1e3,
                           "unit": "Mrays/s",
                           "call": "lrt_trace_nearest_image, camera moved by up to 0.04 before every launch (the "

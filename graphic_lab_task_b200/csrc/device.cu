@@ -520,6 +520,20 @@ lrt_status lrt_trace_nearest(lrt_scene* s, const float* rays, lrt_hit* hits, uin
   if (flags & LRT_TRACE_DEVICE_POINTERS) {
     if ((reinterpret_cast<uintptr_t>(rays) | reinterpret_cast<uintptr_t>(hits)) & 15)
       return fail(s, LRT_ERR_INVALID_ARGUMENT, "device rays/hits must be 16-byte aligned");
+    // A trace of a wave or more of 32-ray groups that repeats the previous
+    // trace's ray count on this stream (a renderer's frames) goes through the
+    // image-order kernel as an image 8 rays wide, whose 8x4 tiles are the same
+    // 32 consecutive rays: the groups are then handed out in the stream's
+    // schedule for this ray count (slowest groups first, the slowest split
+    // over two warps when the previous launch was tail-bound).  Traces of
+    // changing counts keep plain row order and allocate no schedule.
+    uint64_t& last = d->lastRays[stream];
+    const bool repeat = last == n;
+    last = n;
+    const uint64_t slots = uint64_t(d->grid) * (kTraceThreads / 32);
+    if (repeat && !(flags & (LRT_TRACE_COUNT_WORK | LRT_TRACE_NATURAL_ORDER)) && (n + 15) / 16 > slots &&
+        (n + 7) / 8 <= 0xFFFFFFFFull)
+      return launch(s, reinterpret_cast<const float4*>(rays), hits, n, stream, flags, slot, 8, uint32_t((n + 7) / 8));
     return launch(s, reinterpret_cast<const float4*>(rays), hits, n, stream, flags, slot);
   }
   if (n > d->cap) {

@@ -91,6 +91,9 @@ struct DeviceScene {
   uint64_t texVersion = 0;
   std::map<SchedKey, ImageSchedule> sched; // per stream and image size of image-order launches
   uint64_t schedUses = 0;
+  // ray count of the last device-pointer lrt_trace_nearest on each stream: a
+  // trace of the same count again has its 32-ray groups scheduled
+  std::map<cudaStream_t, uint64_t> lastRays;
   // staging buffers for host-pointer calls
   float4* rays = nullptr;
   lrt_hit* hits = nullptr;

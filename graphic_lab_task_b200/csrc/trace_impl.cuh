@@ -972,6 +972,7 @@ __global__ void __launch_bounds__(kTraceThreads, MINB) k_trace(DevScene S, const
       const uint32_t y = uint32_t(b / tilesX) * kImgTileH + (lane / kImgTileW);
       valid = x < img_w && y < img_h && mine;
       i = uint64_t(y) * img_w + x;
+      valid = valid && i < n; // a row-order launch traced as an 8-wide image has a ragged last row
     }
     if (valid) {
       const float4 pn = __ldg(rays + 2 * i), df = __ldg(rays + 2 * i + 1);

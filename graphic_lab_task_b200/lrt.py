@@ -303,10 +303,11 @@ class SceneRT:
         flags = LRT_TRACE_FAST_MATH if fast_math else 0
         self._check(lib().lrt_trace_nearest(self.h, C.c_void_p(rays_ptr), C.c_void_p(hits_ptr), n, None, flags))
 
-    def trace_device(self, rays_ptr, hits_ptr, n, stream=0, fast_math=False, count_work=False):
-        """Asynchronous trace of device buffers (16-byte aligned) on `stream`."""
+    def trace_device(self, rays_ptr, hits_ptr, n, stream=0, fast_math=False, count_work=False, natural_order=False):
+        """Asynchronous trace of device buffers (16-byte aligned) on `stream`;
+        natural_order: no schedule for the 32-ray groups of a large trace."""
         flags = LRT_TRACE_DEVICE_POINTERS | (LRT_TRACE_FAST_MATH if fast_math else 0) | \
-            (LRT_TRACE_COUNT_WORK if count_work else 0)
+            (LRT_TRACE_COUNT_WORK if count_work else 0) | (LRT_TRACE_NATURAL_ORDER if natural_order else 0)
         self._check(lib().lrt_trace_nearest(self.h, C.c_void_p(rays_ptr), C.c_void_p(hits_ptr), n,
                                             C.c_void_p(stream) if stream else None, flags))
 

@@ -313,14 +313,21 @@ lrt_status lrt_scene_export(const lrt_scene* scene, lrt_scene_arrays* out);
 #define LRT_TRACE_FAST_MATH 0x2u       /* FMA-contracted kernels (tolerance
                                           parity); default is the exact build */
 #define LRT_TRACE_COUNT_WORK 0x4u      /* also accumulate work counters     */
-#define LRT_TRACE_NATURAL_ORDER 0x8u   /* image-order calls: tiles in row
-                                          order, no tile schedule          */
+#define LRT_TRACE_NATURAL_ORDER 0x8u   /* image-order calls and large device-
+                                          pointer traces: no tile schedule */
 
 /* Batched BVHRT::RayQuery_NearestHit.  rays: n x {float4 posAndNear,
  * float4 dirAndFar} (32 bytes per ray), hits: n x lrt_hit.  A ray whose
  * dirAndFar.w <= 0 is traced stop-on-first-hit with tfar = -w, exactly like
  * the reference (BVH2Common.cpp:3324-3326).  stream is a cudaStream_t (NULL =
- * legacy default stream).  With host pointers the call is synchronous. */
+ * legacy default stream).  With host pointers the call is synchronous.  A
+ * warp traces 32 consecutive rays; a device-pointer trace of fewer rays than
+ * the GPU holds warps gives each warp 16 or 8 rays strided across the call,
+ * and one of more rays that repeats the previous device-pointer trace's ray
+ * count on the stream hands its 32-ray groups out in a schedule kept per
+ * stream and ray count, as lrt_trace_nearest_image does with its tiles
+ * (slowest groups first; LRT_TRACE_NATURAL_ORDER turns it off).  The order
+ * never changes a hit. */
 lrt_status lrt_trace_nearest(lrt_scene* scene, const float* rays, lrt_hit* hits, uint64_t n, void* stream,
                              uint32_t flags);
 

@@ -380,3 +380,33 @@ def test_image_sizes_alternating_on_one_stream(cuda):
             sc.sync()
             got = out.cpu().numpy().view(HIT_DTYPE)
             assert bit_equal(got, want).all(), (k, w, h, hit_summary(got, want))
+
+
+def test_device_traces_in_their_schedule_keep_every_hit(cuda):
+    """A device-pointer trace of more rays than one wave of warps holds goes
+    through the image-order kernel as an image 8 rays wide: its 32-ray
+    groups are handed out in the stream's schedule for that ray count
+    (slowest first from the second launch on, the slowest split over two
+    warps once a launch was tail-bound).  Every launch returns the hits of
+    the same rays traced without a schedule, a ragged last group (a count
+    that is not a multiple of 8) included."""
+    torch = cuda
+    from graphic_lab_task_b200 import HIT_DTYPE
+    hdr, nodes, vals, vf = wl.sbs_from_spheres(wl.spheres(64, seed=1), grid_res=128)
+    sc = SceneRT()
+    sc.AddInstance(sc.AddGeom_SdfSBS(hdr, nodes, vals, vf), wl.IDENTITY)
+    sc.CommitScene()
+    rays = wl.eye_rays_host(wl.camera((0, 0, 3), width=523, height=401))  # 209,723 rays
+    n = len(rays)
+    R = torch.from_numpy(rays).cuda()
+    ref = torch.zeros(n * 8, dtype=torch.float32, device="cuda")
+    sc.trace_device(R.data_ptr(), ref.data_ptr(), n, natural_order=True)
+    sc.sync()
+    want = ref.cpu().numpy().view(HIT_DTYPE)
+    assert (want["primId"] != MISS).sum() > 0.05 * n
+    for k in range(5):
+        out = torch.zeros(n * 8, dtype=torch.float32, device="cuda")
+        sc.trace_device(R.data_ptr(), out.data_ptr(), n)
+        sc.sync()
+        got = out.cpu().numpy().view(HIT_DTYPE)
+        assert bit_equal(got, want).all(), (k, hit_summary(got, want))
