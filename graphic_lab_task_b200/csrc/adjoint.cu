@@ -214,9 +214,29 @@ lrt_status lambert_begin(lrt_scene* s, const char* who, const float* rays_dev, u
   return LRT_OK;
 }
 
+// A ray-order pass (width 0) of a wave or more of 32-ray groups that repeats
+// the previous device trace's ray count on its stream (an optimisation loop's
+// iterations) runs as an image 8 rays wide, whose 8x4 tiles are 32
+// consecutive rays: the groups then follow the stream's schedule for that
+// count, as lrt_trace_nearest's do.  Returns the image's width and height.
+void rows_as_image(lrt_scene* s, cudaStream_t stream, uint64_t n, uint32_t flags, uint32_t& width, uint32_t& height)
+{
+  if (width) return;
+  DeviceScene* d = s->dev;
+  uint64_t& last = d->lastRays[stream];
+  const bool repeat = last == n;
+  last = n;
+  const uint64_t slots = uint64_t(d->grid) * (kTraceThreads / 32);
+  if (repeat && !(flags & LRT_TRACE_NATURAL_ORDER) && (n + 31) / 32 > slots && (n + 7) / 8 <= 0xFFFFFFFFull) {
+    width = 8;
+    height = uint32_t((n + 7) / 8);
+  }
+}
+
 lrt_status render_lambert(lrt_scene* s, const float* rays_dev, uint64_t n, uint32_t width, uint32_t height,
                           const float light[3], float* image_dev, cudaStream_t stream, uint32_t flags)
 {
+  if (s && s->dev && n) rows_as_image(s, stream, n, flags, width, height);
   StreamSlot* slot = nullptr;
   DevScene S;
   int grid = 1;
@@ -241,6 +261,7 @@ lrt_status adjoint_lambert(lrt_scene* s, const float* rays_dev, uint64_t n, uint
                            const float light[3], const float* dimage_dev, float* grad_dev, cudaStream_t stream,
                            uint32_t flags)
 {
+  if (s && s->dev && n) rows_as_image(s, stream, n, flags, width, height);
   StreamSlot* slot = nullptr;
   DevScene S;
   int grid = 1;

@@ -1753,6 +1753,7 @@ __device__ __forceinline__ bool next_ray(uint64_t n, uint32_t img_w, uint32_t im
     const uint32_t y = (tile / tilesX) * kImgTileH + lane / kImgTileW;
     valid = x < img_w && y < img_h && item_has_lane(item, lane);
     i = uint64_t(y) * img_w + x;
+    valid = valid && i < n; // ray-order rays traced as an 8-wide image have a ragged last row
     return true;
   }
   unsigned long long base = 0;

@@ -476,7 +476,11 @@ lrt_status lrt_generate_bounce_rays_sorted(lrt_scene* scene, const float* rays_d
  * image[i] = max(0, n_i . light) for the nearest hit's decoded normal
  * (MultiRenderer_resolve.cpp:617-666 for LAMBERT_NO_TEX, one directional
  * light of unit colour, albedo 1), 0 for misses.  Asynchronous on `stream`;
- * lrt_trace_sync(stream) reports bounded-loop limits. */
+ * lrt_trace_sync(stream) reports bounded-loop limits.  A call of a wave or
+ * more of rays that repeats the previous device trace's ray count on the
+ * stream (an optimisation loop) hands its 32-ray groups out in the stream's
+ * schedule for that count, as lrt_trace_nearest does; the pixels are the
+ * same, the gradient's atomic additions come in another order. */
 lrt_status lrt_render_lambert(lrt_scene* scene, const float* rays_dev, uint64_t n, const float light[3],
                               float* image_dev, void* stream);
 
