@@ -126,6 +126,44 @@ def test_adjoint_image_order_matches_row_order(small):
         assert np.linalg.norm(g - g0) <= 1e-5 * np.linalg.norm(g0)
 
 
+def test_ray_order_repeats_follow_the_group_schedule(cuda):
+    """Ray-order passes of a wave or more that repeat the previous device
+    trace's ray count on their stream run as an image 8 rays wide in the
+    stream's schedule.  On a ray count that leaves that image's last row
+    ragged: the repeated adjoints add the same contributions as the first
+    (plain-order) call, and every pixel of the repeated forward passes, which
+    share the adjoints' schedule, equals the oracle's."""
+    torch = cuda
+    hdr, nodes, vals, vf, target, cams, rays = wl.adjoint_workload(grid_res=64, views=3, res=288)
+    n = len(rays) - 5
+    assert n % 8 and n // 32 > 148 * 8 * 4  # more 32-ray groups than the launch's warps
+    rays = np.ascontiguousarray(rays[:n])
+    sc = SceneRT()
+    sc.AddInstance(sc.AddGeom_SdfSBS(hdr, nodes, vals, vf), wl.IDENTITY)
+    sc.CommitScene()
+    R = torch.from_numpy(rays).cuda()
+    rng = np.random.default_rng(5)
+    dimage = torch.from_numpy((rng.standard_normal(n) * 1e-3).astype(np.float32)).cuda()
+    grads = []
+    for _ in range(4):
+        g = torch.zeros(len(vf), dtype=torch.float32, device="cuda")
+        sc.adjoint_lambert(R.data_ptr(), n, LIGHT, dimage.data_ptr(), g.data_ptr())
+        sc.sync()
+        grads.append(g.cpu().numpy().astype(np.float64))
+    g0 = grads[0]
+    assert np.count_nonzero(g0) > 1000
+    for g in grads[1:]:
+        assert np.array_equal(g != 0, g0 != 0)
+        assert np.linalg.norm(g - g0) <= 1e-5 * np.linalg.norm(g0)
+    want = po.port_render_lambert(sc.export_arrays(), rays, LIGHT).view(np.uint32)
+    for _ in range(3):
+        img = torch.full((n,), -1.0, dtype=torch.float32, device="cuda")
+        sc.render_lambert(R.data_ptr(), n, LIGHT, img.data_ptr())
+        sc.sync()
+        assert np.array_equal(img.cpu().numpy().view(np.uint32), want)
+    sc.close()
+
+
 def test_adjoint_matches_central_differences(small):
     """Central differences of the mean-L2 loss, h = 1e-3 and 1e-4, on seeded
     voxels whose adjoint gradient is nonzero.  The loss is piecewise smooth
