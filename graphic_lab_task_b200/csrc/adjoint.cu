@@ -219,6 +219,8 @@ lrt_status lambert_begin(lrt_scene* s, const char* who, const float* rays_dev, u
 // iterations) runs as an image 8 rays wide, whose 8x4 tiles are 32
 // consecutive rays: the groups then follow the stream's schedule for that
 // count, as lrt_trace_nearest's do.  Returns the image's width and height.
+// Called once the call's arguments have been checked and its stream has a
+// slot (the launch grid, a full wave, is the same in both shapes).
 void rows_as_image(lrt_scene* s, cudaStream_t stream, uint64_t n, uint32_t flags, uint32_t& width, uint32_t& height)
 {
   if (width) return;
@@ -236,7 +238,6 @@ void rows_as_image(lrt_scene* s, cudaStream_t stream, uint64_t n, uint32_t flags
 lrt_status render_lambert(lrt_scene* s, const float* rays_dev, uint64_t n, uint32_t width, uint32_t height,
                           const float light[3], float* image_dev, cudaStream_t stream, uint32_t flags)
 {
-  if (s && s->dev && n) rows_as_image(s, stream, n, flags, width, height);
   StreamSlot* slot = nullptr;
   DevScene S;
   int grid = 1;
@@ -245,6 +246,7 @@ lrt_status render_lambert(lrt_scene* s, const float* rays_dev, uint64_t n, uint3
   if (st != LRT_OK) return st;
   if ((st = check_rays(s, image_dev)) != LRT_OK) return st;
   if (n == 0) return LRT_OK;
+  rows_as_image(s, stream, n, flags, width, height);
   const bool natural = !width || (flags & LRT_TRACE_NATURAL_ORDER);
   const uint32_t* rd = nullptr;
   uint32_t* wr = nullptr;
@@ -261,7 +263,6 @@ lrt_status adjoint_lambert(lrt_scene* s, const float* rays_dev, uint64_t n, uint
                            const float light[3], const float* dimage_dev, float* grad_dev, cudaStream_t stream,
                            uint32_t flags)
 {
-  if (s && s->dev && n) rows_as_image(s, stream, n, flags, width, height);
   StreamSlot* slot = nullptr;
   DevScene S;
   int grid = 1;
@@ -270,6 +271,7 @@ lrt_status adjoint_lambert(lrt_scene* s, const float* rays_dev, uint64_t n, uint
   if (st != LRT_OK) return st;
   if (!dimage_dev || !grad_dev) return fail(s, LRT_ERR_INVALID_ARGUMENT, "lrt_adjoint_lambert_sbs: NULL argument");
   if (n == 0) return LRT_OK;
+  rows_as_image(s, stream, n, flags, width, height);
   const bool natural = !width || (flags & LRT_TRACE_NATURAL_ORDER);
   const uint32_t* rd = nullptr;
   uint32_t* wr = nullptr;
