@@ -64,7 +64,7 @@ INVALID = 0xFFFFFFFF
 LRT_TRACE_DEVICE_POINTERS = 0x1
 LRT_TRACE_FAST_MATH = 0x2
 LRT_TRACE_COUNT_WORK = 0x4
-LRT_TRACE_NATURAL_ORDER = 0x8  # image-order traces: tiles in row order, no schedule
+LRT_TRACE_NATURAL_ORDER = 0x8  # image-order and repeated device traces: no longest-first schedule
 
 STATUS_NAMES = {0: "LRT_OK", 1: "LRT_ERR_INVALID_ARGUMENT", 2: "LRT_ERR_BAD_SCENE", 3: "LRT_ERR_NOT_COMMITTED",
                 4: "LRT_ERR_CUDA", 5: "LRT_ERR_DEVICE_LIMIT", 6: "LRT_ERR_UNSUPPORTED", 7: "LRT_ERR_OUT_OF_MEMORY"}
